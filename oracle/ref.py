@@ -1,0 +1,259 @@
+"""CPU oracle: ctypes access to the reference's own ED library.
+
+TEST INFRASTRUCTURE ONLY -- imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference arm, never by the product package.
+
+The library (oracle/_ref/libqcm_ed_ref.so) is the reference's src_ed + src_util
+compiled from its sources by oracle/ref_build/Makefile, with the flat C layer
+oracle/ref_build/ref_capi.cpp on top of namespace ED (src_ed/qcm_ED.hpp:23-340).
+The reference keeps its models and instances in process-global maps
+(src_ed/qcm_ED.cpp:25-26), so one process holds one oracle state; tests that
+need a clean slate use fresh model names / instance labels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libqcm_ed_ref.so")
+
+_lib = None
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise OracleError(f"oracle library not built: {LIB_PATH} (run make -C oracle/ref_build)")
+        L = C.CDLL(LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        lp = C.POINTER(C.c_long)
+        sig = {
+            "ref_last_error": [C.c_char_p, C.c_int],
+            "ref_init": [],
+            "ref_set_int": [C.c_char_p, C.c_long],
+            "ref_set_double": [C.c_char_p, C.c_double],
+            "ref_set_char": [C.c_char_p, C.c_char],
+            "ref_set_bool": [C.c_char_p, C.c_int],
+            "ref_new_model": [C.c_char_p, C.c_int, C.c_int],
+            "ref_new_operator": [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, ip, ip, dp],
+            "ref_new_instance": [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, C.c_char_p, C.c_int],
+            "ref_erase_instance": [C.c_int],
+            "ref_ground_state": [C.c_int, dp, C.c_char_p, C.c_int],
+            "ref_green_solve": [C.c_int],
+            "ref_gf_dim": [C.c_int],
+            "ref_mixing": [C.c_int],
+            "ref_green_function": [C.c_int, C.c_int, C.c_int, dp, dp],
+            "ref_self_energy": [C.c_int, C.c_int, C.c_int, dp, dp],
+            "ref_hybridization_function": [C.c_int, C.c_int, C.c_int, dp, dp],
+            "ref_green_function_average": [C.c_int, C.c_int, dp],
+            "ref_potthoff": [C.c_int, dp],
+            "ref_qmatrix": [C.c_int, C.c_int, ip, ip, dp, dp],
+            "ref_cf_coeffs": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, ip, dp, dp],
+            "ref_gs_vector": [C.c_int, lp, dp, dp],
+            "ref_halfbasis": [C.c_int, C.c_int, C.POINTER(C.c_uint), lp],
+            "ref_destroy_table": [C.c_int, C.c_int, C.c_int, C.c_int, lp, ip],
+            "ref_hv_apply": [C.c_void_p, dp, dp],
+            "ref_hv_bench": [C.c_void_p, C.c_int, dp],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.ref_hv_create.argtypes = [C.c_int, C.c_char_p, lp]
+        L.ref_hv_create.restype = C.c_void_p
+        L.ref_hv_destroy.argtypes = [C.c_void_p]
+        L.ref_hv_destroy.restype = None
+        if L.ref_init() != 0:
+            raise OracleError("ref_init failed")
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        buf = C.create_string_buffer(4096)
+        lib().ref_last_error(buf, 4096)
+        raise OracleError(buf.value.decode())
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def set_param(name: str, value):
+    L = lib()
+    n = name.encode()
+    if isinstance(value, bool):
+        _check(L.ref_set_bool(n, int(value)))
+    elif isinstance(value, int):
+        _check(L.ref_set_int(n, value))
+    elif isinstance(value, float):
+        _check(L.ref_set_double(n, value))
+    elif isinstance(value, str) and len(value) == 1:
+        _check(L.ref_set_char(n, value.encode()))
+    else:
+        raise TypeError(value)
+
+
+def new_model(name, n_sites, n_bath):
+    _check(lib().ref_new_model(name.encode(), n_sites, n_bath))
+
+
+def new_operator(model, op, typ, elements):
+    n = len(elements)
+    r = (C.c_int * n)(*[int(e[0]) for e in elements])
+    c = (C.c_int * n)(*[int(e[1]) for e in elements])
+    v = (C.c_double * n)(*[float(e[2]) for e in elements])
+    _check(lib().ref_new_operator(model.encode(), op.encode(), typ.encode(), n, r, c, v))
+
+
+def new_instance(model, params: dict, sectors: str, label: int):
+    names = list(params)
+    arr = (C.c_char_p * len(names))(*[k.encode() for k in names])
+    vals = (C.c_double * len(names))(*[float(params[k]) for k in names])
+    _check(lib().ref_new_instance(model.encode(), len(names), arr, vals, sectors.encode(), label))
+
+
+def load_problem(prob, label: int, model_name: str | None = None):
+    """Defines model + operators (once per model name) and an instance."""
+    mname = model_name or prob.name
+    new_model(mname, prob.n_sites, prob.n_bath)
+    for op, (typ, el) in prob.operators.items():
+        new_operator(mname, op, typ, el)
+    new_instance(mname, prob.params, prob.sectors, label)
+
+
+def ground_state(label):
+    E = C.c_double()
+    buf = C.create_string_buffer(256)
+    _check(lib().ref_ground_state(label, C.byref(E), buf, 256))
+    return E.value, buf.value.decode()
+
+
+def green_solve(label):
+    _check(lib().ref_green_solve(label))
+
+
+def gf_dim(label):
+    return lib().ref_gf_dim(label)
+
+
+def mixing(label):
+    return lib().ref_mixing(label)
+
+
+def _zcall(fn, label, z, spin_down, n):
+    z = np.ascontiguousarray(np.atleast_1d(np.asarray(z, dtype=np.complex128)))
+    out = np.zeros((len(z), n, n), dtype=np.complex128)
+    _check(fn(label, int(spin_down), len(z), _dp(z.view(np.float64)), _dp(out.view(np.float64))))
+    # column-major n x n blocks -> [k, row, col]
+    return out.transpose(0, 2, 1).copy()
+
+
+def green_function(label, z, spin_down=False):
+    return _zcall(lib().ref_green_function, label, z, spin_down, gf_dim(label))
+
+
+def self_energy(label, z, spin_down=False):
+    return _zcall(lib().ref_self_energy, label, z, spin_down, gf_dim(label))
+
+
+def hybridization_function(label, z, spin_down=False):
+    return _zcall(lib().ref_hybridization_function, label, z, spin_down, gf_dim(label))
+
+
+def green_function_average(label, spin_down=False):
+    n = gf_dim(label)
+    out = np.zeros((n, n), dtype=np.complex128)
+    _check(lib().ref_green_function_average(label, int(spin_down), _dp(out.view(np.float64))))
+    return out.T.copy()
+
+
+def potthoff(label):
+    w = C.c_double()
+    _check(lib().ref_potthoff(label, C.byref(w)))
+    return w.value
+
+
+def qmatrix(label, spin_down=False, capacity=1 << 16):
+    M = C.c_int(capacity)
+    L = C.c_int(0)
+    e = np.zeros(capacity)
+    v = np.zeros((capacity * 64, 2))
+    _check(lib().ref_qmatrix(label, int(spin_down), C.byref(M), C.byref(L), _dp(e), _dp(v)))
+    m, l = M.value, L.value
+    vv = (v[: m * l, 0] + 1j * v[: m * l, 1]).reshape(m, l).T  # column-major L x M
+    return e[:m].copy(), vv.copy()
+
+
+def cf_coeffs(label, o1, o2, pm, spin_down=False, capacity=4096):
+    n = C.c_int(capacity)
+    a = np.zeros(capacity)
+    b = np.zeros(capacity)
+    _check(lib().ref_cf_coeffs(label, int(spin_down), o1, o2, pm, C.byref(n), _dp(a), _dp(b)))
+    return a[: n.value].copy(), b[: n.value].copy()
+
+
+def gs_vector(label):
+    d = C.c_long()
+    E = C.c_double()
+    _check(lib().ref_gs_vector(label, C.byref(d), C.byref(E), None))
+    psi = np.zeros(d.value)
+    _check(lib().ref_gs_vector(label, C.byref(d), C.byref(E), _dp(psi)))
+    return E.value, psi
+
+
+def halfbasis(L, N):
+    d = C.c_long()
+    _check(lib().ref_halfbasis(L, N, None, C.byref(d)))
+    out = np.zeros(d.value, dtype=np.uint32)
+    _check(lib().ref_halfbasis(L, N, out.ctypes.data_as(C.POINTER(C.c_uint)), C.byref(d)))
+    return out
+
+
+def destroy_table(L, n_up, n_dn, a):
+    dim = len(halfbasis(L, n_up)) * len(halfbasis(L, n_dn))
+    tgt = np.zeros(dim, dtype=np.int64)
+    ph = np.zeros(dim, dtype=np.int32)
+    _check(lib().ref_destroy_table(L, n_up, n_dn, a, tgt.ctypes.data_as(C.POINTER(C.c_long)),
+                                   ph.ctypes.data_as(C.POINTER(C.c_int))))
+    return tgt, ph
+
+
+class RefHamiltonian:
+    """y += H x through the reference's factorized Hamiltonian, for one sector."""
+
+    def __init__(self, label, sector: str):
+        d = C.c_long()
+        self.h = lib().ref_hv_create(label, sector.encode(), C.byref(d))
+        if not self.h:
+            _check(1)
+        self.dim = d.value
+
+    def mult_add(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        assert y.dtype == np.float64 and y.flags.c_contiguous
+        _check(lib().ref_hv_apply(self.h, _dp(x), _dp(y)))
+
+    def bench(self, reps):
+        s = C.c_double()
+        _check(lib().ref_hv_bench(self.h, reps, C.byref(s)))
+        return s.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ref_hv_destroy(self.h)
+            self.h = None

@@ -1,0 +1,292 @@
+// CPU oracle: a flat C entry layer over the reference's own ED library
+// (namespace ED, src_ed/qcm_ED.hpp:23-340), compiled from the reference sources.
+//
+// TEST INFRASTRUCTURE ONLY. Only tests/, __graft_entry__.smoke() and bench.py's
+// CPU-baseline / reference arm load the library this file is linked into. It is
+// never part of the product path.
+//
+// Conventions follow the reference's Python binding (src_python/qcm_ED_wrap.hpp):
+//  - the QCM global-parameter defaults are installed (src_util/global_parameter.cpp:10-92),
+//    which is what pyqcm uses (src_python/qcm_lib.cpp:63);
+//  - operator matrix elements are passed 0-based (the binding subtracts 1,
+//    src_python/qcm_ED_wrap.hpp:199-200);
+//  - complex outputs are interleaved (re, im) doubles, column-major like matrix<T>.
+// Every entry returns 0 on success; on a thrown qcm_error it returns 1 and the
+// message is available from ref_last_error().
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "qcm_ED.hpp"
+#include "model_instance.hpp"
+#include "global_parameter.hpp"
+
+namespace QCM { void global_parameter_init(); }
+
+// Globals defined by the reference at src_ed/qcm_ED.cpp:25-26.
+extern map<string, shared_ptr<model>> models;
+extern map<size_t, shared_ptr<model_instance_base>> model_instances;
+
+namespace {
+std::string g_err;
+
+template <class F> int guarded(F &&f) {
+  try {
+    f();
+    return 0;
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return 1;
+  } catch (const H5::Exception &e) {
+    g_err = e.getDetailMsg();
+    return 1;
+  }
+}
+
+void put_complex(const matrix<Complex> &g, double *out) {
+  for (size_t i = 0; i < g.v.size(); ++i) {
+    out[2 * i] = g.v[i].real();
+    out[2 * i + 1] = g.v[i].imag();
+  }
+}
+
+struct hv_handle {
+  std::unique_ptr<Hamiltonian<double>> H;
+};
+}  // namespace
+
+extern "C" {
+
+int ref_last_error(char *buf, int n) {
+  if (n > 0) {
+    std::strncpy(buf, g_err.c_str(), (size_t)n - 1);
+    buf[n - 1] = 0;
+  }
+  return (int)g_err.size();
+}
+
+int ref_init(void) {
+  return guarded([] { QCM::global_parameter_init(); });
+}
+
+int ref_set_int(const char *name, long v) {
+  return guarded([&] { set_global_int(name, (size_t)v); });
+}
+int ref_set_double(const char *name, double v) {
+  return guarded([&] { set_global_double(name, v); });
+}
+int ref_set_char(const char *name, char v) {
+  return guarded([&] { set_global_char(name, v); });
+}
+int ref_set_bool(const char *name, int v) {
+  return guarded([&] { set_global_bool(name, v != 0); });
+}
+
+int ref_new_model(const char *name, int n_sites, int n_bath) {
+  return guarded([&] { ED::new_model(name, n_sites, n_bath, {}, false); });
+}
+
+int ref_new_operator(const char *model_name, const char *op, const char *type, int n, const int *r,
+                     const int *c, const double *v) {
+  return guarded([&] {
+    std::vector<matrix_element<double>> el(n);
+    for (int i = 0; i < n; ++i) el[i] = matrix_element<double>(r[i], c[i], v[i]);
+    ED::new_operator(model_name, op, type, el);
+  });
+}
+
+int ref_new_instance(const char *model_name, int n, const char **names, const double *values,
+                     const char *sectors, int label) {
+  return guarded([&] {
+    map<string, double> p;
+    for (int i = 0; i < n; ++i) p[names[i]] = values[i];
+    ED::new_model_instance(model_name, p, sectors, (size_t)label);
+  });
+}
+
+int ref_erase_instance(int label) {
+  return guarded([&] { ED::erase_model_instance((size_t)label); });
+}
+
+int ref_ground_state(int label, double *E0, char *sec, int seclen) {
+  return guarded([&] {
+    auto r = ED::ground_state_solve((size_t)label);
+    *E0 = r.first;
+    std::strncpy(sec, r.second.c_str(), (size_t)seclen - 1);
+    sec[seclen - 1] = 0;
+  });
+}
+
+int ref_green_solve(int label) {
+  return guarded([&] { ED::Green_function_solve((size_t)label); });
+}
+
+int ref_gf_dim(int label) { return (int)ED::Green_function_dimension((size_t)label); }
+
+int ref_mixing(int label) { return ED::mixing((size_t)label); }
+
+// G(z) for nz frequencies; G_out holds nz blocks of n x n complex, column-major.
+int ref_green_function(int label, int spin_down, int nz, const double *z, double *G_out) {
+  return guarded([&] {
+    for (int k = 0; k < nz; ++k) {
+      Complex w(z[2 * k], z[2 * k + 1]);
+      auto g = ED::Green_function(w, spin_down != 0, (size_t)label, false);
+      put_complex(g, G_out + 2 * (size_t)k * g.v.size());
+    }
+  });
+}
+
+int ref_self_energy(int label, int spin_down, int nz, const double *z, double *S_out) {
+  return guarded([&] {
+    for (int k = 0; k < nz; ++k) {
+      Complex w(z[2 * k], z[2 * k + 1]);
+      auto g = ED::self_energy(w, spin_down != 0, (size_t)label);
+      put_complex(g, S_out + 2 * (size_t)k * g.v.size());
+    }
+  });
+}
+
+int ref_hybridization_function(int label, int spin_down, int nz, const double *z, double *out) {
+  return guarded([&] {
+    for (int k = 0; k < nz; ++k) {
+      Complex w(z[2 * k], z[2 * k + 1]);
+      auto g = ED::hybridization_function(w, spin_down != 0, (size_t)label);
+      put_complex(g, out + 2 * (size_t)k * g.v.size());
+    }
+  });
+}
+
+int ref_green_function_average(int label, int spin_down, double *out) {
+  return guarded([&] {
+    auto g = ED::Green_function_average(spin_down != 0, (size_t)label);
+    put_complex(g, out);
+  });
+}
+
+int ref_potthoff(int label, double *omega) {
+  return guarded([&] { *omega = ED::Potthoff_functional((size_t)label); });
+}
+
+// Lehmann representation: eigenvalues e[M], residues v (L x M complex, column-major).
+// On entry *M is the capacity; on exit the actual number of poles.
+int ref_qmatrix(int label, int spin_down, int *M, int *L, double *e, double *v) {
+  return guarded([&] {
+    auto q = ED::qmatrix(spin_down != 0, (size_t)label);
+    int m = (int)q.first.size();
+    int l = m ? (int)(q.second.size() / m) : 0;
+    if (m > *M) throw qcm_error("ref_qmatrix: capacity too small");
+    *M = m;
+    *L = l;
+    for (int i = 0; i < m; ++i) e[i] = q.first[i];
+    for (size_t i = 0; i < q.second.size(); ++i) {
+      v[2 * i] = q.second[i].real();
+      v[2 * i + 1] = q.second[i].imag();
+    }
+  });
+}
+
+// Continued-fraction coefficients of the first state, real Hilbert space,
+// trivial group: element (o1, o2), o2 <= o1, electron (pm=+1) or hole (pm=-1).
+// On entry *n is the capacity of a and b; on exit the number of levels.
+int ref_cf_coeffs(int label, int spin_down, int o1, int o2, int pm, int *n, double *a, double *b) {
+  return guarded([&] {
+    auto inst = dynamic_pointer_cast<model_instance<double>>(model_instances.at((size_t)label));
+    if (!inst) throw qcm_error("ref_cf_coeffs: complex instance");
+    if (!inst->gf_solved) inst->Green_function_solve();
+    auto &st = *inst->states.begin();
+    auto cf = dynamic_pointer_cast<continued_fraction_set>(spin_down ? st->gf_down : st->gf);
+    if (!cf) throw qcm_error("ref_cf_coeffs: not a continued-fraction instance");
+    continued_fraction &f = (pm > 0) ? cf->e[0](o1, o2) : cf->h[0](o1, o2);
+    int m = (int)f.a.size();
+    if (m > *n) throw qcm_error("ref_cf_coeffs: capacity too small");
+    *n = m;
+    for (int i = 0; i < m; ++i) a[i] = f.a[i];
+    for (int i = 0; i < m && i < (int)f.b.size(); ++i) b[i] = f.b[i];
+  });
+}
+
+// Ground-state vector of the first (lowest) state: dimension, energy, psi.
+int ref_gs_vector(int label, long *dim, double *energy, double *psi) {
+  return guarded([&] {
+    auto inst = dynamic_pointer_cast<model_instance<double>>(model_instances.at((size_t)label));
+    if (!inst) throw qcm_error("ref_gs_vector: complex instance");
+    if (!inst->gs_solved) inst->low_energy_states();
+    auto &st = *inst->states.begin();
+    *dim = (long)st->psi.size();
+    *energy = st->energy;
+    if (psi) std::memcpy(psi, st->psi.data(), st->psi.size() * sizeof(double));
+  });
+}
+
+// Sorted N-of-L bit strings of ED_halfbasis (src_ed/ED_basis.cpp:115-125).
+int ref_halfbasis(int L, int N, unsigned *out, long *dim) {
+  return guarded([&] {
+    ED_halfbasis B(L, N);
+    *dim = (long)B.dim;
+    if (out)
+      for (size_t i = 0; i < B.dim; ++i) out[i] = B.bin[i];
+  });
+}
+
+// Factorized-basis Destroy (src_ed/ED_basis.cpp:79-110) applied to every state
+// of sector (Nup, Ndn) of an L-orbital model for orbital a (a >= L: spin down).
+// Writes, per source state, the target index (or -1) and the phase bit.
+int ref_destroy_table(int L, int Nup, int Ndn, int a, long *target, int *phase) {
+  return guarded([&] {
+    sector sx(Nup + Ndn, Nup - Ndn, 0);
+    int up = (a >= L) ? 0 : 1;
+    sector sy(Nup + Ndn - 1, (Nup - up) - (Ndn - (1 - up)), 0);
+    ED_factorized_basis Bx(sx, L), By(sy, L);
+    for (uint32_t I = 0; I < Bx.dim; ++I) {
+      auto T = Destroy(a, I, Bx, By);
+      target[I] = std::get<3>(T) ? (long)std::get<0>(T) : -1;
+      phase[I] = std::get<1>(T);
+    }
+  });
+}
+
+// y += H x in a sector of a solved-or-not instance, through the reference's
+// factorized Hamiltonian (src_ed/Hamiltonian/Hamiltonian_Factorized.hpp:51-58).
+void *ref_hv_create(int label, const char *sec, long *dim) {
+  void *h = nullptr;
+  int rc = guarded([&] {
+    auto &I = *model_instances.at((size_t)label);
+    if (!I.the_model->is_factorized) throw qcm_error("ref_hv_create: model is not factorized");
+    auto *hh = new hv_handle;
+    hh->H.reset(new Hamiltonian_Factorized<double>(I.the_model, I.value, sector(sec)));
+    *dim = (long)hh->H->dim;
+    h = hh;
+  });
+  return rc ? nullptr : h;
+}
+
+int ref_hv_apply(void *h, const double *x, double *y) {
+  return guarded([&] {
+    auto *hh = (hv_handle *)h;
+    size_t d = hh->H->dim;
+    std::vector<double> xv(x, x + d), yv(y, y + d);
+    hh->H->mult_add(xv, yv);
+    std::memcpy(y, yv.data(), d * sizeof(double));
+  });
+}
+
+// Timing entry: applies y += H x `reps` times on internally held vectors, so the
+// measured time is the reference's mult_add alone (no copies across the FFI).
+int ref_hv_bench(void *h, int reps, double *checksum) {
+  return guarded([&] {
+    auto *hh = (hv_handle *)h;
+    size_t d = hh->H->dim;
+    std::vector<double> x(d), y(d, 0.0);
+    for (size_t i = 0; i < d; ++i) x[i] = 1.0 / (1.0 + (double)(i % 97));
+    for (int r = 0; r < reps; ++r) hh->H->mult_add(x, y);
+    double s = 0.0;
+    for (size_t i = 0; i < d; i += 4099) s += y[i];
+    *checksum = s;
+  });
+}
+
+void ref_hv_destroy(void *h) { delete (hv_handle *)h; }
+
+}  // extern "C"

@@ -1,0 +1,160 @@
+"""Cluster-model builders for the synthetic workloads this solver is measured on.
+
+Each builder returns a plain description (orbital counts, operator element
+lists, parameter values, sector string) that can be fed to either this
+package's ED API or the CPU oracle, so both solve the identical problem.
+
+Conventions follow the reference's cluster-model definitions:
+  * orbital index i < n_orb is spin up, i + n_orb is spin down
+    (src_ed/model.hpp:34-41, src_ed/binary_state.hpp:60-63);
+  * a one-body element (r, c, v) means v c^+_r c_c, given with r <= c; the
+    Hermitian partner is added by the solver (src_ed/Operators/one_body_operator.hpp:63-71);
+  * an interaction element (r, c, v) means v n_r n_c (src_ed/Operators/HS_interaction_operator.hpp:44-53);
+  * the chemical potential enters as -mu * N (diagonal elements -1), so mu = U/2
+    is half filling for a bipartite cluster.
+All indices here are 0-based.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class ClusterProblem:
+    name: str
+    n_sites: int
+    n_bath: int
+    operators: dict = field(default_factory=dict)   # name -> (type, [(r, c, v), ...])
+    params: dict = field(default_factory=dict)      # name -> value
+    sectors: str = "R0"
+
+    @property
+    def n_orb(self) -> int:
+        return self.n_sites + self.n_bath
+
+
+def _both_spins(n_orb, pairs):
+    out = []
+    for (r, c, v) in pairs:
+        out.append((r, c, v))
+        out.append((r + n_orb, c + n_orb, v))
+    return out
+
+
+def lattice_bonds(nx: int, ny: int, diagonal: bool = False):
+    """Open-boundary nx x ny cluster: site index x + nx*y. Returns (nn, nnn) bond lists."""
+    nn, nnn = [], []
+    for y in range(ny):
+        for x in range(nx):
+            i = x + nx * y
+            if x + 1 < nx:
+                nn.append((i, i + 1))
+            if y + 1 < ny:
+                nn.append((i, i + nx))
+            if diagonal and x + 1 < nx and y + 1 < ny:
+                nnn.append((i, i + nx + 1))
+            if diagonal and x > 0 and y + 1 < ny:
+                nnn.append((i, i + nx - 1))
+    return nn, nnn
+
+
+def hubbard_cluster(nx: int, ny: int, t: float = -1.0, tp: float | None = None, U: float = 4.0,
+                    mu: float | None = None, M: float | None = None, n_up: int | None = None,
+                    n_dn: int | None = None, name: str | None = None) -> ClusterProblem:
+    """Hubbard model on an open nx x ny cluster (chains: ny = 1).
+
+    Operators: 't' (nearest-neighbour hop), optional "t'" (next-nearest), 'U'
+    (on-site), 'mu' (-N), optional 'M' (staggered Neel field, +1 up / -1 down on
+    sublattice A and the opposite on B, which makes the two spins different).
+    """
+    L = nx * ny
+    nn, nnn = lattice_bonds(nx, ny, diagonal=tp is not None)
+    prob = ClusterProblem(name or f"hub{nx}x{ny}", L, 0)
+    prob.operators["t"] = ("one-body", _both_spins(L, [(a, b, 1.0) for a, b in nn]))
+    if tp is not None and nnn:
+        prob.operators["tp"] = ("one-body", _both_spins(L, [(a, b, 1.0) for a, b in nnn]))
+        prob.params["tp"] = tp
+    prob.operators["U"] = ("interaction", [(i, i + L, 1.0) for i in range(L)])
+    prob.operators["mu"] = ("one-body", _both_spins(L, [(i, i, -1.0) for i in range(L)]))
+    prob.params.update({"t": t, "U": U, "mu": U / 2 if mu is None else mu})
+    if M is not None:
+        el = []
+        for y in range(ny):
+            for x in range(nx):
+                i = x + nx * y
+                s = 1.0 if (x + y) % 2 == 0 else -1.0
+                el.append((i, i, s))
+                el.append((i + L, i + L, -s))
+        prob.operators["M"] = ("one-body", el)
+        prob.params["M"] = M
+    nu = L // 2 if n_up is None else n_up
+    nd = L // 2 if n_dn is None else n_dn
+    prob.sectors = f"R0:N{nu + nd}:S{nu - nd}"
+    return prob
+
+
+def plaquette_bath(eps, hyb, U: float = 8.0, t: float = -1.0, mu: float | None = None,
+                   name: str = "plaq8b") -> ClusterProblem:
+    """2x2 plaquette with 8 bath orbitals, two per cluster site.
+
+    eps[b] is the energy of bath orbital b, hyb[b] its hybridisation with
+    cluster site b // 2. Orbitals 0-3 are the plaquette, 4-11 the bath.
+    """
+    ns, nb = 4, 8
+    L = ns + nb
+    nn, _ = lattice_bonds(2, 2)
+    prob = ClusterProblem(name, ns, nb)
+    prob.operators["t"] = ("one-body", _both_spins(L, [(a, b, 1.0) for a, b in nn]))
+    prob.operators["U"] = ("interaction", [(i, i + L, 1.0) for i in range(ns)])
+    prob.operators["mu"] = ("one-body", _both_spins(L, [(i, i, -1.0) for i in range(ns)]))
+    prob.params.update({"t": t, "U": U, "mu": U / 2 if mu is None else mu})
+    for b in range(nb):
+        prob.operators[f"eb{b}"] = ("one-body", _both_spins(L, [(ns + b, ns + b, 1.0)]))
+        prob.operators[f"tb{b}"] = ("one-body", _both_spins(L, [(b // 2, ns + b, 1.0)]))
+        prob.params[f"eb{b}"] = float(eps[b])
+        prob.params[f"tb{b}"] = float(hyb[b])
+    prob.sectors = "R0:N12:S0"
+    return prob
+
+
+def matsubara(n: int = 256, beta: float = 50.0) -> np.ndarray:
+    """Fermionic Matsubara frequencies i(2k+1)pi/beta, k = 0..n-1."""
+    return 1j * (2 * np.arange(n) + 1) * math.pi / beta
+
+
+# Named workloads (the five synthetic configurations this solver is judged on).
+def chain8() -> ClusterProblem:
+    """1D chain L=8, open, t=-1, U=4, mu=2, sector N_up=N_dn=4 (dim 4900)."""
+    return hubbard_cluster(8, 1, t=-1.0, U=4.0, mu=2.0, name="chain8")
+
+
+def square4x4() -> ClusterProblem:
+    """4x4 open square, t=-1, t'=0.3, U=8, half filling (dim 12870^2)."""
+    return hubbard_cluster(4, 4, t=-1.0, tp=0.3, U=8.0, mu=4.0, name="sq4x4")
+
+
+def random_batch(n: int = 1024, seed: int = 12345):
+    """Seeded draw of independent clusters with every (N_up, N_dn) sector listed."""
+    rng = np.random.default_rng(seed)
+    geoms = [(2, 2), (2, 3), (2, 4), (8, 1), (10, 1)]
+    out = []
+    for k in range(n):
+        nx, ny = geoms[rng.integers(len(geoms))]
+        U = float(rng.uniform(0, 12))
+        mu = float(rng.uniform(0, U))
+        M = float(rng.uniform(0, 0.3))
+        p = hubbard_cluster(nx, ny, t=-1.0, U=U, mu=mu, M=M, name=f"b{nx}x{ny}")
+        L = nx * ny
+        secs = [f"R0:N{a + b}:S{a - b}" for a in range(L + 1) for b in range(L + 1)]
+        p.sectors = "/".join(secs)
+        out.append(p)
+    return out
+
+
+def random_baths(n: int = 256, seed: int = 4242):
+    """Seeded bath-parameter points for the 2x2 + 8-bath cluster."""
+    rng = np.random.default_rng(seed)
+    return [plaquette_bath(rng.uniform(-2, 2, 8), rng.uniform(0, 1, 8)) for _ in range(n)]

@@ -1,0 +1,164 @@
+/*
+ * qed_b200.h -- C ABI of the B200 exact-diagonalization (ED) impurity solver.
+ *
+ * This is the drop-in boundary for pyqcm's cluster ground-state and cluster
+ * Green-function path. Each entry point below names the reference interface
+ * it replaces (paths relative to the pyqcm source tree). The reference's ED
+ * layer is the C++ namespace ED (src_ed/qcm_ED.hpp:23-340); its inner plugin
+ * point is the Hamiltonian<HilbertField> interface
+ * (src_ed/Hamiltonian/Hamiltonian_base.hpp:43-82), chosen per sector by
+ * model_instance::create_hamiltonian (src_ed/model_instance.hpp:193-238).
+ *
+ * Conventions
+ *  - Every function returns a status code (QED_OK == 0). On failure the
+ *    message is available from qed_last_error() (per thread). The C++ adapter
+ *    rethrows a non-zero status as qcm_error, matching qcm_ED_throw
+ *    (src_util/parser.cpp:323-328).
+ *  - Orbital indices are 0-based: orbital i < n_orb is spin up, i + n_orb is
+ *    spin down (n_orb = n_sites + n_bath), as in the reference's operators
+ *    after its Python binding subtracts 1 (src_python/qcm_ED_wrap.hpp:199-200).
+ *  - Complex numbers are interleaved (re, im) doubles. Matrices are
+ *    column-major, like the reference's matrix<T> (src_util/matrix.cpp:11-16).
+ *  - All array arguments are host memory owned by the caller, except where a
+ *    function name ends in _device (device pointers on the current device).
+ *  - Device memory is owned by the instance / Hamiltonian handles and freed by
+ *    qed_erase_model_instance / qed_hamiltonian_destroy. No device pointer
+ *    owned by the library escapes it.
+ *  - Thread safety: calls on different instance labels may run concurrently;
+ *    calls on one label are serialised internally.
+ */
+#ifndef QED_B200_H
+#define QED_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define QED_OK 0
+#define QED_ERR_ARGUMENT 1      /* bad argument, unknown name/label, invalid sector       */
+#define QED_ERR_LANCZOS 2       /* Lanczos iteration cap (src_ed/Hamiltonian/Lanczos.hpp:92) */
+#define QED_ERR_QMATRIX 3       /* Q-matrix norm check (src_ed/Q_matrix.hpp:255-259)         */
+#define QED_ERR_CUDA 4          /* CUDA runtime error                                       */
+#define QED_ERR_MEMORY 5        /* device memory budget exceeded                            */
+#define QED_ERR_UNSUPPORTED 6   /* model outside this solver's scope (e.g. g > 1, anomalous) */
+#define QED_ERR_NO_DEVICE 7     /* no CUDA device / extension not usable                    */
+#define QED_ERR_INTERNAL 8
+
+/* Copies the last error message of the calling thread; returns its length. */
+int qed_last_error(char *buf, int len);
+
+/* Selects the CUDA device used by this process (default 0). */
+int qed_init(int device);
+
+/* Global options, same names and defaults as the reference's QCM initialisation
+ * (src_util/global_parameter.cpp:10-92; setters src_util/global_parameter.hpp:74-77).
+ * The get variants return QED_ERR_ARGUMENT for an unknown name. */
+int qed_set_global_int(const char *name, long value);
+int qed_set_global_double(const char *name, double value);
+int qed_set_global_char(const char *name, char value);
+int qed_set_global_bool(const char *name, int value);
+int qed_get_global_double(const char *name, double *value);
+
+/* ED::new_model (src_ed/qcm_ED.hpp:33). Only the trivial point group (no
+ * generators) is supported: the spin-factorized Hamiltonian requires g = 1
+ * (src_ed/model_instance_base.cpp:85-97). */
+int qed_new_model(const char *name, int n_sites, int n_bath);
+
+/* ED::new_operator (src_ed/qcm_ED.hpp:56), real elements. type is "one-body"
+ * or "interaction". Elements (r[k], c[k], v[k]) follow the reference: one-body
+ * elements with r > c are ignored and r < c ones get their Hermitian partner
+ * (src_ed/Operators/one_body_operator.hpp:63-71); interaction elements are
+ * ordered r <= c (src_ed/Operators/interaction_operator.hpp:45-50). */
+int qed_new_operator(const char *model, const char *name, const char *type, int n, const int *r,
+                     const int *c, const double *v);
+
+/* ED::new_model_instance (src_ed/qcm_ED.hpp:80). sectors: "R0:N8:S0[/...]". */
+int qed_new_model_instance(const char *model, int n, const char **names, const double *values,
+                           const char *sectors, int label);
+
+/* ED::erase_model_instance (src_ed/qcm_ED.cpp:65-68). Frees device memory. */
+int qed_erase_model_instance(int label);
+
+/* ED::mixing (src_ed/qcm_ED.hpp:92): 0 normal, 4 up-down. */
+int qed_mixing(int label, int *mixing);
+
+/* ED::ground_state_solve (src_ed/qcm_ED.hpp:104 -> model_instance::low_energy_states,
+ * src_ed/model_instance.hpp:245-347). Returns the GS energy and the sector
+ * string of the kept states ("R0:N8:S0:1" style, as GS_string()). */
+int qed_ground_state_solve(int label, double *energy, char *sectors, int len);
+
+/* ED::Green_function_solve (src_ed/qcm_ED.hpp:122 -> src_ed/model_instance.hpp:517-555):
+ * band-Lanczos Q-matrix (GF_method 'L') or continued fractions ('F'). */
+int qed_Green_function_solve(int label);
+
+/* ED::Green_function_dimension (src_ed/qcm_ED.hpp:241). */
+int qed_Green_function_dimension(int label, int *dim);
+
+/* ED::Green_function (src_ed/qcm_ED.hpp:134 -> src_ed/model_instance.hpp:566-635),
+ * batched over nz frequencies z (interleaved complex). G receives nz blocks of
+ * dim x dim complex, column-major, evaluated on the GPU. */
+int qed_Green_function(int label, int spin_down, int nz, const double *z, double *G);
+
+/* ED::self_energy (src_ed/qcm_ED.hpp:180 -> src_ed/model_instance.hpp:683-700), batched. */
+int qed_self_energy(int label, int spin_down, int nz, const double *z, double *S);
+
+/* ED::hybridization_function (src_ed/qcm_ED.hpp:210 -> src_ed/model_instance.hpp:1004-1018), batched. */
+int qed_hybridization_function(int label, int spin_down, int nz, const double *z, double *H);
+
+/* ED::Green_function_average (src_ed/qcm_ED.hpp:146): <c^+_b c_a>, dim x dim complex. */
+int qed_Green_function_average(int label, int spin_down, double *M);
+
+/* ED::Potthoff_functional (src_ed/qcm_ED.hpp:222; SEF_bath + E0, src_ed/qcm_ED.cpp:330-334). */
+int qed_Potthoff_functional(int label, double *omega);
+
+/* ED::qmatrix (src_ed/qcm_ED.hpp:286 -> src_ed/model_instance.hpp:1425-1451).
+ * On entry *M is the capacity of e (and of v, in columns); on exit the number
+ * of poles. v is L x M complex, column-major. */
+int qed_qmatrix(int label, int spin_down, int *M, int *L, double *e, double *v);
+
+/* Continued-fraction coefficients (GF_method 'F') of the first state for the
+ * pair (o1, o2), o2 <= o1, electron (pm = +1) or hole (pm = -1); the
+ * continued_fraction a/b arrays of src_ed/continued_fraction.cpp:33-39.
+ * On entry *n is the capacity; on exit the number of levels. */
+int qed_cf_coefficients(int label, int spin_down, int o1, int o2, int pm, int *n, double *a,
+                        double *b);
+
+/* Ground-state vector of the first kept state (factorized layout
+ * psi[up_rank + dim_up * dn_rank], src_ed/ED_basis.cpp:142-165).
+ * *dim receives the dimension; psi may be NULL to query it. */
+int qed_ground_state_vector(int label, long *dim, double *psi);
+
+/* ---- plugin point: the Hamiltonian of one sector --------------------------
+ * Hamiltonian<double> (src_ed/Hamiltonian/Hamiltonian_base.hpp:43-82) realised
+ * on the device in spin-factorized form (replaces Hamiltonian_Factorized,
+ * src_ed/Hamiltonian/Hamiltonian_Factorized.hpp:32-87). */
+typedef struct qed_hamiltonian qed_hamiltonian;
+
+int qed_hamiltonian_create(int label, const char *sector, qed_hamiltonian **h, long *dim);
+/* y += H x with host vectors (Hamiltonian::mult_add). */
+int qed_hamiltonian_mult_add(qed_hamiltonian *h, const double *x, double *y);
+/* y = H x with device vectors on the current device, enqueued on `stream`
+ * (a cudaStream_t, or NULL for the library's stream of this Hamiltonian). */
+int qed_hamiltonian_apply_device(qed_hamiltonian *h, const double *x, double *y, void *stream);
+/* Hamiltonian::diag (src_ed/Hamiltonian/Hamiltonian_base.hpp:57). */
+int qed_hamiltonian_diag(qed_hamiltonian *h, double *d);
+int qed_hamiltonian_destroy(qed_hamiltonian *h);
+
+/* ---- basis (ED_halfbasis, src_ed/ED_basis.cpp:115-135) ---------------------
+ * All L-bit strings with N set bits in ascending order, generated on the GPU by
+ * unranking in the combinatorial number system (bit-exact with the sorted list). */
+int qed_halfbasis(int L, int N, unsigned *strings, long *dim);
+/* Rank of each string (ED_halfbasis::index; returns dim for a string not in the
+ * basis), computed on the GPU. */
+int qed_halfbasis_rank(int L, int N, long n, const unsigned *strings, unsigned *ranks);
+
+/* c_a applied to every basis state of sector (N_up, N_dn) (Destroy,
+ * src_ed/ED_basis.cpp:79-110), computed on the GPU: target index (or -1) and
+ * fermion phase bit per source state. */
+int qed_destroy_table(int L, int n_up, int n_dn, int a, long *target, int *phase);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QED_B200_H */

@@ -36,7 +36,10 @@ def lib():
     if _lib is None:
         if not available():
             raise OracleError(f"oracle library not built: {LIB_PATH} (run make -C oracle/ref_build)")
-        L = C.CDLL(LIB_PATH)
+        # RTLD_DEEPBIND: resolve the oracle's LAPACK/BLAS calls in its own
+        # OpenBLAS, not in libraries already loaded into the process (torch's
+        # libtorch_cpu exports an incompatible zgetrf_, for instance).
+        L = C.CDLL(LIB_PATH, mode=os.RTLD_LOCAL | os.RTLD_DEEPBIND)
         dp = C.POINTER(C.c_double)
         ip = C.POINTER(C.c_int)
         lp = C.POINTER(C.c_long)
@@ -49,7 +52,7 @@ def lib():
             "ref_set_bool": [C.c_char_p, C.c_int],
             "ref_new_model": [C.c_char_p, C.c_int, C.c_int],
             "ref_new_operator": [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, ip, ip, dp],
-            "ref_new_instance": [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, C.c_char_p, C.c_int],
+            "ref_new_instance": [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, C.c_char_p, C.c_int, C.c_char],
             "ref_erase_instance": [C.c_int],
             "ref_ground_state": [C.c_int, dp, C.c_char_p, C.c_int],
             "ref_green_solve": [C.c_int],
@@ -120,20 +123,27 @@ def new_operator(model, op, typ, elements):
     _check(lib().ref_new_operator(model.encode(), op.encode(), typ.encode(), n, r, c, v))
 
 
-def new_instance(model, params: dict, sectors: str, label: int):
+def new_instance(model, params: dict, sectors: str, label: int, fmt: str = "F"):
+    """fmt: Hamiltonian_format of this instance ('F' factorized, 'S' CSR)."""
     names = list(params)
     arr = (C.c_char_p * len(names))(*[k.encode() for k in names])
     vals = (C.c_double * len(names))(*[float(params[k]) for k in names])
-    _check(lib().ref_new_instance(model.encode(), len(names), arr, vals, sectors.encode(), label))
+    _check(lib().ref_new_instance(model.encode(), len(names), arr, vals, sectors.encode(), label,
+                                  fmt.encode()))
 
 
-def load_problem(prob, label: int, model_name: str | None = None):
-    """Defines model + operators (once per model name) and an instance."""
+def load_problem(prob, label: int, model_name: str | None = None, fmt: str = "F"):
+    """Defines model + operators (once per model name) and an instance.
+
+    The reference's continued-fraction builder dereferences the Hamiltonian's
+    mixed basis, which its factorized format never sets
+    (src_ed/model_instance.cpp:52 with Hamiltonian_Factorized); use fmt='S'
+    for GF_method 'F'."""
     mname = model_name or prob.name
     new_model(mname, prob.n_sites, prob.n_bath)
     for op, (typ, el) in prob.operators.items():
         new_operator(mname, op, typ, el)
-    new_instance(mname, prob.params, prob.sectors, label)
+    new_instance(mname, prob.params, prob.sectors, label, fmt)
 
 
 def ground_state(label):

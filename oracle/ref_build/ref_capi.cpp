@@ -97,9 +97,22 @@ int ref_new_operator(const char *model_name, const char *op, const char *type, i
   });
 }
 
+// `format` is the Hamiltonian_format letter for this instance. The reference
+// reads that option only when its first instance is built
+// (src_ed/model_instance_base.cpp:38-48); the global it sets is assigned here
+// before every instance so that one process can hold instances of both the
+// factorized ('F') and CSR ('S') formats.
 int ref_new_instance(const char *model_name, int n, const char **names, const double *values,
-                     const char *sectors, int label) {
+                     const char *sectors, int label, char format) {
   return guarded([&] {
+    set_global_char("Hamiltonian_format", format);
+    switch (format) {
+      case 'F': Hamiltonian_format = H_FORMAT::H_format_factorized; break;
+      case 'S': Hamiltonian_format = H_FORMAT::H_format_csr; break;
+      case 'O': Hamiltonian_format = H_FORMAT::H_format_ops; break;
+      case 'N': Hamiltonian_format = H_FORMAT::H_format_onthefly; break;
+      default: throw qcm_error(std::string("ref_new_instance: unsupported format ") + format);
+    }
     map<string, double> p;
     for (int i = 0; i < n; ++i) p[names[i]] = values[i];
     ED::new_model_instance(model_name, p, sectors, (size_t)label);

@@ -3,9 +3,9 @@
 //
 // Test infrastructure only. The reference implements these members with Eigen
 // (src_util/matrix.cpp:24-230), which is not installed in this image. This file
-// gives the same contracts, written against the LAPACK exported by the image's
-// OpenBLAS: eigenvalues ascending with orthonormal eigenvector columns, inverse
-// by LU, determinant with the permutation sign, lower Cholesky factor. Eigenvector
+// gives the same contracts: eigenvalues ascending with orthonormal eigenvector
+// columns (LAPACK dsyev/zheev of the image's OpenBLAS), inverse by Gauss-Jordan,
+// determinant with the permutation sign, lower Cholesky factor (dpotrf). Eigenvector
 // signs/phases may differ from Eigen's; every quantity the ED path builds from
 // them (Q = P.U, Lehmann sums) is invariant under a per-column phase.
 #include <cmath>
@@ -41,17 +41,49 @@ int lapack_zheev(char jobz, int n, Complex *a, double *w) {
 
 }  // namespace
 
+// Gauss-Jordan elimination with partial pivoting, in place (column-major).
+// Kept free of LAPACK so that the oracle does not depend on which LU routine
+// the dynamic linker binds when other libraries (e.g. PyTorch's
+// libtorch_cpu, which exports zgetrf_) are already loaded.
+// Pivot magnitude |re| + |im| (LAPACK's dcabs1), computed inline so no libm
+// complex routine is involved.
+static double mag1(double x) { return fabs(x); }
+static double mag1(const Complex &z) { return fabs(z.real()) + fabs(z.imag()); }
+
+template <class T> static bool gauss_jordan_inverse(size_t n, T *a) {
+  auto at = [&](size_t i, size_t j) -> T & { return a[i + n * j]; };
+  vector<size_t> piv(n);
+  for (size_t k = 0; k < n; ++k) {
+    size_t p = k;
+    double best = mag1(at(k, k));
+    for (size_t i = k + 1; i < n; ++i)
+      if (mag1(at(i, k)) > best) { best = mag1(at(i, k)); p = i; }
+    if (best == 0.0) return false;
+    piv[k] = p;
+    if (p != k)
+      for (size_t j = 0; j < n; ++j) std::swap(at(k, j), at(p, j));
+    T inv = T(1.0) / at(k, k);
+    at(k, k) = T(1.0);
+    for (size_t j = 0; j < n; ++j) at(k, j) *= inv;
+    for (size_t i = 0; i < n; ++i) {
+      if (i == k) continue;
+      T f = at(i, k);
+      if (f == T(0.0)) continue;
+      at(i, k) = T(0.0);
+      for (size_t j = 0; j < n; ++j) at(i, j) -= f * at(k, j);
+    }
+  }
+  for (size_t k = n; k-- > 0;)
+    if (piv[k] != k)
+      for (size_t i = 0; i < n; ++i) std::swap(at(i, k), at(i, piv[k]));
+  return true;
+}
+
 template <> void matrix<double>::inverse() {
   QCM_ASSERT(r == c);
   if (r == 0) return;
   if (r == 1) { v[0] = 1 / v[0]; return; }
-  integer n = r, lda = r, info = 0, lwork = (integer)(64 * r);
-  vector<integer> piv(r);
-  dgetrf_(&n, &n, v.data(), &lda, piv.data(), &info);
-  QCM_ASSERT(info == 0);
-  vector<double> work(lwork);
-  dgetri_(&n, v.data(), &lda, piv.data(), work.data(), &lwork, &info);
-  QCM_ASSERT(info == 0);
+  QCM_ASSERT(gauss_jordan_inverse<double>(r, v.data()));
 }
 
 template <> bool matrix<Complex>::is_real(double accuracy) {
@@ -81,26 +113,29 @@ template <> void matrix<double>::eigenvalues(vector<double> &d) {
 template <> void matrix<Complex>::inverse() {
   QCM_ASSERT(r == c);
   if (r == 0) return;
-  integer n = r, lda = r, info = 0, lwork = (integer)(64 * r);
-  vector<integer> piv(r);
-  zgetrf_(&n, &n, (doublecomplex *)v.data(), &lda, piv.data(), &info);
-  QCM_ASSERT(info == 0);
-  vector<doublecomplex> work(lwork);
-  zgetri_(&n, (doublecomplex *)v.data(), &lda, piv.data(), work.data(), &lwork, &info);
-  QCM_ASSERT(info == 0);
+  QCM_ASSERT(gauss_jordan_inverse<Complex>(r, v.data()));
 }
 
+// Determinant by Gaussian elimination with partial pivoting (sign included).
 template <> Complex matrix<Complex>::determinant() {
   if (r == 0) return Complex(0);
   vector<Complex> a(v);
-  integer n = r, lda = r, info = 0;
-  vector<integer> piv(r);
-  zgetrf_(&n, &n, (doublecomplex *)a.data(), &lda, piv.data(), &info);
-  if (info > 0) return Complex(0);
+  auto at = [&](size_t i, size_t j) -> Complex & { return a[i + r * j]; };
   Complex det(1.0);
-  for (size_t i = 0; i < r; ++i) {
-    det *= a[i + r * i];
-    if (piv[i] != (integer)(i + 1)) det = -det;
+  for (size_t k = 0; k < r; ++k) {
+    size_t p = k;
+    for (size_t i = k + 1; i < r; ++i)
+      if (mag1(at(i, k)) > mag1(at(p, k))) p = i;
+    if (at(p, k) == Complex(0.0)) return Complex(0.0);
+    if (p != k) {
+      for (size_t j = 0; j < r; ++j) std::swap(at(k, j), at(p, j));
+      det = -det;
+    }
+    det *= at(k, k);
+    for (size_t i = k + 1; i < r; ++i) {
+      Complex f = at(i, k) / at(k, k);
+      for (size_t j = k; j < r; ++j) at(i, j) -= f * at(k, j);
+    }
   }
   return det;
 }

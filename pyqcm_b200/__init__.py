@@ -1,0 +1,329 @@
+"""pyqcm_b200 -- B200 (sm_100a) exact-diagonalization solver for pyqcm's cluster path.
+
+This module mirrors the reference's ED API (namespace ED, src_ed/qcm_ED.hpp:23-340,
+as exposed to Python by src_python/qcm_ED_wrap.hpp) on top of the C ABI in
+include/qed_b200.h. Every call goes through the CUDA library
+pyqcm_b200/libqed_b200.so; there is no CPU fallback: if the library or a GPU is
+missing, the calls raise QEDError.
+
+Differences from the reference's Python binding, all deliberate:
+  * operator matrix elements are 0-based (the C++ ED API convention);
+  * Green_function / self_energy / hybridization_function accept an array of
+    frequencies and evaluate all of them in one GPU launch.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = [
+    "QEDError", "lib", "set_global_parameter", "new_model", "new_operator", "new_model_instance",
+    "erase_model_instance", "mixing", "ground_state_solve", "Green_function_solve",
+    "Green_function_dimension", "Green_function", "self_energy", "hybridization_function",
+    "Green_function_average", "Potthoff_functional", "qmatrix", "cf_coefficients",
+    "ground_state_vector", "Hamiltonian", "halfbasis", "halfbasis_rank", "destroy_table",
+    "load_problem",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqed_b200.so")
+
+QED_OK = 0
+_CODES = {1: "argument", 2: "lanczos", 3: "qmatrix", 4: "cuda", 5: "memory", 6: "unsupported",
+          7: "no-device", 8: "internal"}
+
+
+class QEDError(RuntimeError):
+    """Error raised by the solver; .code is the C-ABI status (include/qed_b200.h)."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"[{_CODES.get(code, code)}] {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Loads the CUDA library (built by python -m pyqcm_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise QEDError(7, f"CUDA extension not built: {LIB_PATH} (run python -m pyqcm_b200.build)")
+    L = C.CDLL(LIB_PATH)
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    lp = C.POINTER(C.c_long)
+    up = C.POINTER(C.c_uint)
+    sig = {
+        "qed_last_error": [C.c_char_p, C.c_int],
+        "qed_init": [C.c_int],
+        "qed_set_global_int": [C.c_char_p, C.c_long],
+        "qed_set_global_double": [C.c_char_p, C.c_double],
+        "qed_set_global_char": [C.c_char_p, C.c_char],
+        "qed_set_global_bool": [C.c_char_p, C.c_int],
+        "qed_get_global_double": [C.c_char_p, dp],
+        "qed_new_model": [C.c_char_p, C.c_int, C.c_int],
+        "qed_new_operator": [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, ip, ip, dp],
+        "qed_new_model_instance": [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, C.c_char_p, C.c_int],
+        "qed_erase_model_instance": [C.c_int],
+        "qed_mixing": [C.c_int, ip],
+        "qed_ground_state_solve": [C.c_int, dp, C.c_char_p, C.c_int],
+        "qed_Green_function_solve": [C.c_int],
+        "qed_Green_function_dimension": [C.c_int, ip],
+        "qed_Green_function": [C.c_int, C.c_int, C.c_int, dp, dp],
+        "qed_self_energy": [C.c_int, C.c_int, C.c_int, dp, dp],
+        "qed_hybridization_function": [C.c_int, C.c_int, C.c_int, dp, dp],
+        "qed_Green_function_average": [C.c_int, C.c_int, dp],
+        "qed_Potthoff_functional": [C.c_int, dp],
+        "qed_qmatrix": [C.c_int, C.c_int, ip, ip, dp, dp],
+        "qed_cf_coefficients": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, ip, dp, dp],
+        "qed_ground_state_vector": [C.c_int, lp, dp],
+        "qed_hamiltonian_create": [C.c_int, C.c_char_p, C.POINTER(C.c_void_p), lp],
+        "qed_hamiltonian_mult_add": [C.c_void_p, dp, dp],
+        "qed_hamiltonian_apply_device": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+        "qed_hamiltonian_diag": [C.c_void_p, dp],
+        "qed_hamiltonian_destroy": [C.c_void_p],
+        "qed_halfbasis": [C.c_int, C.c_int, up, lp],
+        "qed_halfbasis_rank": [C.c_int, C.c_int, C.c_long, up, up],
+        "qed_destroy_table": [C.c_int, C.c_int, C.c_int, C.c_int, lp, ip],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != QED_OK:
+        buf = C.create_string_buffer(8192)
+        lib().qed_last_error(buf, 8192)
+        raise QEDError(rc, buf.value.decode(errors="replace"))
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def init(device: int = 0):
+    _check(lib().qed_init(device))
+
+
+# ---- options ----------------------------------------------------------------
+
+def set_global_parameter(name: str, value=None):
+    """set_global_parameter (src_python/qcm_ED_wrap.hpp:296-315): None sets a bool to True."""
+    L, n = lib(), name.encode()
+    if value is None or isinstance(value, bool):
+        _check(L.qed_set_global_bool(n, 1 if value is None else int(value)))
+    elif isinstance(value, (int, np.integer)):
+        _check(L.qed_set_global_int(n, int(value)))
+    elif isinstance(value, float):
+        _check(L.qed_set_global_double(n, value))
+    elif isinstance(value, str) and len(value) == 1:
+        _check(L.qed_set_global_char(n, value.encode()))
+    else:
+        raise TypeError(f"unknown type of global_parameter: {value!r}")
+
+
+def get_global_double(name: str) -> float:
+    v = C.c_double()
+    _check(lib().qed_get_global_double(name.encode(), C.byref(v)))
+    return v.value
+
+
+# ---- models and instances ---------------------------------------------------
+
+def new_model(name: str, n_sites: int, n_bath: int = 0):
+    _check(lib().qed_new_model(name.encode(), n_sites, n_bath))
+
+
+def new_operator(model: str, op: str, typ: str, elements):
+    """elements: iterable of 0-based (r, c, v)."""
+    el = list(elements)
+    n = len(el)
+    r = (C.c_int * max(n, 1))(*[int(e[0]) for e in el])
+    c = (C.c_int * max(n, 1))(*[int(e[1]) for e in el])
+    v = (C.c_double * max(n, 1))(*[float(e[2]) for e in el])
+    _check(lib().qed_new_operator(model.encode(), op.encode(), typ.encode(), n, r, c, v))
+
+
+def new_model_instance(model: str, values: dict, sectors: str, label: int = 0):
+    names = list(values)
+    arr = (C.c_char_p * max(len(names), 1))(*[k.encode() for k in names])
+    vals = (C.c_double * max(len(names), 1))(*[float(values[k]) for k in names])
+    _check(lib().qed_new_model_instance(model.encode(), len(names), arr, vals, sectors.encode(), label))
+
+
+def load_problem(prob, label: int = 0, model_name: str | None = None):
+    """Defines the model (with its operators) of a workloads.ClusterProblem and an instance."""
+    mname = model_name or prob.name
+    new_model(mname, prob.n_sites, prob.n_bath)
+    for op, (typ, el) in prob.operators.items():
+        new_operator(mname, op, typ, el)
+    new_model_instance(mname, prob.params, prob.sectors, label)
+
+
+def erase_model_instance(label: int):
+    _check(lib().qed_erase_model_instance(label))
+
+
+def mixing(label: int = 0) -> int:
+    m = C.c_int()
+    _check(lib().qed_mixing(label, C.byref(m)))
+    return m.value
+
+
+def ground_state_solve(label: int = 0):
+    """Returns (ground-state energy, sector string), like ED::ground_state_solve."""
+    E = C.c_double()
+    buf = C.create_string_buffer(1024)
+    _check(lib().qed_ground_state_solve(label, C.byref(E), buf, 1024))
+    return E.value, buf.value.decode()
+
+
+def Green_function_solve(label: int = 0):
+    _check(lib().qed_Green_function_solve(label))
+
+
+def Green_function_dimension(label: int = 0) -> int:
+    d = C.c_int()
+    _check(lib().qed_Green_function_dimension(label, C.byref(d)))
+    return d.value
+
+
+def _zbatch(fn, z, spin_down, label):
+    scalar = np.ndim(z) == 0
+    zz = np.ascontiguousarray(np.atleast_1d(np.asarray(z, dtype=np.complex128)))
+    n = Green_function_dimension(label)
+    out = np.zeros((len(zz), n, n), dtype=np.complex128)
+    _check(fn(label, int(spin_down), len(zz), _dp(zz.view(np.float64)), _dp(out.view(np.float64))))
+    out = out.transpose(0, 2, 1)  # column-major blocks -> [k, row, col]
+    return out[0].copy() if scalar else out.copy()
+
+
+def Green_function(z, spin_down: bool = False, label: int = 0):
+    """G(z) (n x n) for a scalar z, or (nz, n, n) for an array of frequencies."""
+    return _zbatch(lib().qed_Green_function, z, spin_down, label)
+
+
+def self_energy(z, spin_down: bool = False, label: int = 0):
+    return _zbatch(lib().qed_self_energy, z, spin_down, label)
+
+
+def hybridization_function(z, spin_down: bool = False, label: int = 0):
+    return _zbatch(lib().qed_hybridization_function, z, spin_down, label)
+
+
+def Green_function_average(spin_down: bool = False, label: int = 0):
+    n = Green_function_dimension(label)
+    out = np.zeros((n, n), dtype=np.complex128)
+    _check(lib().qed_Green_function_average(label, int(spin_down), _dp(out.view(np.float64))))
+    return out.T.copy()
+
+
+def Potthoff_functional(label: int = 0) -> float:
+    w = C.c_double()
+    _check(lib().qed_Potthoff_functional(label, C.byref(w)))
+    return w.value
+
+
+def qmatrix(spin_down: bool = False, label: int = 0, capacity: int = 1 << 16):
+    """Lehmann representation: (poles e[M], residues V as an L x M complex matrix)."""
+    M = C.c_int(capacity)
+    L = C.c_int(0)
+    n = Green_function_dimension(label)
+    e = np.zeros(capacity)
+    v = np.zeros((capacity * n, 2))
+    _check(lib().qed_qmatrix(label, int(spin_down), C.byref(M), C.byref(L), _dp(e), _dp(v)))
+    m, l = M.value, L.value
+    vv = (v[: m * l, 0] + 1j * v[: m * l, 1]).reshape(m, l).T
+    return e[:m].copy(), vv.copy()
+
+
+def cf_coefficients(o1: int, o2: int, pm: int, spin_down: bool = False, label: int = 0, capacity=4096):
+    n = C.c_int(capacity)
+    a = np.zeros(capacity)
+    b = np.zeros(capacity)
+    _check(lib().qed_cf_coefficients(label, int(spin_down), o1, o2, pm, C.byref(n), _dp(a), _dp(b)))
+    return a[: n.value].copy(), b[: n.value].copy()
+
+
+def ground_state_vector(label: int = 0):
+    d = C.c_long()
+    _check(lib().qed_ground_state_vector(label, C.byref(d), None))
+    psi = np.zeros(d.value)
+    _check(lib().qed_ground_state_vector(label, C.byref(d), _dp(psi)))
+    return psi
+
+
+# ---- plugin point and basis -------------------------------------------------
+
+class Hamiltonian:
+    """Device Hamiltonian of one sector (Hamiltonian<double> plugin point)."""
+
+    def __init__(self, label: int, sector: str):
+        h = C.c_void_p()
+        d = C.c_long()
+        _check(lib().qed_hamiltonian_create(label, sector.encode(), C.byref(h), C.byref(d)))
+        self._h = h
+        self.dim = d.value
+
+    def mult_add(self, x, y):
+        """y += H x on host arrays (Hamiltonian::mult_add)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if not (y.dtype == np.float64 and y.flags.c_contiguous and y.size == self.dim):
+            raise ValueError("y must be a contiguous float64 array of the sector dimension")
+        _check(lib().qed_hamiltonian_mult_add(self._h, _dp(x), _dp(y)))
+
+    def apply_device(self, x_ptr: int, y_ptr: int, stream: int = 0):
+        """y = H x on device pointers (e.g. torch tensors' data_ptr())."""
+        _check(lib().qed_hamiltonian_apply_device(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr),
+                                                  C.c_void_p(stream) if stream else None))
+
+    def diag(self):
+        d = np.zeros(self.dim)
+        _check(lib().qed_hamiltonian_diag(self._h, _dp(d)))
+        return d
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().qed_hamiltonian_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def halfbasis(L: int, N: int):
+    d = C.c_long()
+    _check(lib().qed_halfbasis(L, N, None, C.byref(d)))
+    out = np.zeros(d.value, dtype=np.uint32)
+    _check(lib().qed_halfbasis(L, N, out.ctypes.data_as(C.POINTER(C.c_uint)), C.byref(d)))
+    return out
+
+
+def halfbasis_rank(L: int, N: int, strings):
+    s = np.ascontiguousarray(strings, dtype=np.uint32)
+    r = np.zeros(len(s), dtype=np.uint32)
+    _check(lib().qed_halfbasis_rank(L, N, len(s), s.ctypes.data_as(C.POINTER(C.c_uint)),
+                                    r.ctypes.data_as(C.POINTER(C.c_uint))))
+    return r
+
+
+def destroy_table(L: int, n_up: int, n_dn: int, a: int):
+    from math import comb
+    dim = comb(L, n_up) * comb(L, n_dn)
+    tgt = np.zeros(dim, dtype=np.int64)
+    ph = np.zeros(dim, dtype=np.int32)
+    _check(lib().qed_destroy_table(L, n_up, n_dn, a, tgt.ctypes.data_as(C.POINTER(C.c_long)),
+                                   ph.ctypes.data_as(C.POINTER(C.c_int))))
+    return tgt, ph

@@ -1,0 +1,481 @@
+// The C ABI of include/qed_b200.h: registries of models / instances / sector
+// Hamiltonians, and the error convention (status code + per-thread message).
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "common.hpp"
+#include "instance.hpp"
+#include "options.hpp"
+#include "qed_b200.h"
+
+using namespace qed;
+
+struct qed_hamiltonian {
+  std::unique_ptr<SectorOp> H;
+  DevBuf<double> x, y;
+};
+
+namespace {
+
+thread_local std::string t_err;
+
+// Models and instances live in process-global maps, as the reference's
+// (src_ed/qcm_ED.cpp:25-26). One Workspace (stream + reduction buffers) per
+// device context; GPU work from different host threads is serialised on it.
+std::mutex g_reg;
+std::map<std::string, std::shared_ptr<Model>> g_models;
+std::map<int, std::shared_ptr<Instance>> g_instances;
+std::recursive_mutex g_gpu;
+std::unique_ptr<Workspace> g_ws;
+int g_device = 0;
+
+Workspace &ws() {
+  if (!g_ws) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+      fail(QED_ERR_NO_DEVICE, std::string("no CUDA device available: ") + cudaGetErrorString(e));
+    QED_CUDA(cudaSetDevice(g_device));
+    g_ws.reset(new Workspace());
+  }
+  return *g_ws;
+}
+
+template <class F> int guarded(F &&f) {
+  try {
+    f();
+    return QED_OK;
+  } catch (const Error &e) {
+    t_err = e.what();
+    return e.code;
+  } catch (const std::out_of_range &e) {
+    t_err = std::string("unknown name or label: ") + e.what();
+    return QED_ERR_ARGUMENT;
+  } catch (const std::exception &e) {
+    t_err = e.what();
+    return QED_ERR_INTERNAL;
+  }
+}
+
+std::shared_ptr<Instance> instance(int label) {
+  std::lock_guard<std::mutex> l(g_reg);
+  auto it = g_instances.find(label);
+  if (it == g_instances.end())
+    fail(QED_ERR_ARGUMENT, "The cluster instance label " + std::to_string(label) + " is out of range.");
+  return it->second;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qed_last_error(char *buf, int len) {
+  if (buf && len > 0) {
+    std::strncpy(buf, t_err.c_str(), (size_t)len - 1);
+    buf[len - 1] = 0;
+  }
+  return (int)t_err.size();
+}
+
+int qed_init(int device) {
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    if (g_ws && device != g_device) fail(QED_ERR_ARGUMENT, "qed_init: device already selected");
+    g_device = device;
+    ws();
+  });
+}
+
+int qed_set_global_int(const char *name, long v) { return guarded([&] { set_opt_int(name, v); }); }
+int qed_set_global_double(const char *name, double v) { return guarded([&] { set_opt_double(name, v); }); }
+int qed_set_global_char(const char *name, char v) { return guarded([&] { set_opt_char(name, v); }); }
+int qed_set_global_bool(const char *name, int v) { return guarded([&] { set_opt_bool(name, v != 0); }); }
+int qed_get_global_double(const char *name, double *v) { return guarded([&] { *v = opt_double(name); }); }
+
+int qed_new_model(const char *name, int n_sites, int n_bath) {
+  return guarded([&] {
+    // ED::new_model (src_ed/qcm_ED.cpp:46-60)
+    if (n_bath > 32 || n_bath < 0) fail(QED_ERR_ARGUMENT, "number of bath orbitals exceeds limits or negative!");
+    if (n_sites > 1024 || n_sites < 1) fail(QED_ERR_ARGUMENT, "number of cluster sites  exceeds limits or negative!");
+    std::lock_guard<std::mutex> l(g_reg);
+    if (g_models.count(name)) return;  // reused, as the reference does (with a warning)
+    auto m = std::make_shared<Model>();
+    m->name = name;
+    m->n_sites = n_sites;
+    m->n_bath = n_bath;
+    m->n_orb = n_sites + n_bath;
+    if (m->n_orb > 32) fail(QED_ERR_UNSUPPORTED, "more than 32 orbitals per spin");
+    m->in_bath.assign(2 * m->n_orb, false);
+    for (int i = n_sites; i < m->n_orb; ++i) m->in_bath[i] = m->in_bath[i + m->n_orb] = true;
+    g_models[name] = m;
+  });
+}
+
+int qed_new_operator(const char *model, const char *name, const char *type, int n, const int *r,
+                     const int *c, const double *v) {
+  return guarded([&] {
+    if (n <= 0) return;  // ED::new_operator ignores empty element lists
+    std::shared_ptr<Model> m;
+    {
+      std::lock_guard<std::mutex> l(g_reg);
+      auto it = g_models.find(model);
+      if (it == g_models.end())
+        fail(QED_ERR_ARGUMENT, std::string("The model ") + model + " is not defined. Check spelling.");
+      m = it->second;
+    }
+    std::vector<Element> el(n);
+    for (int k = 0; k < n; ++k) el[k] = {r[k], c[k], v[k]};
+    auto op = make_operator(*m, name, type, el);
+    std::lock_guard<std::mutex> l(m->mtx);
+    if (m->is_closed) return;  // closed for modifications (warning in the reference)
+    m->term[name] = op;
+  });
+}
+
+int qed_new_model_instance(const char *model, int n, const char **names, const double *values,
+                           const char *sectors, int label) {
+  return guarded([&] {
+    std::shared_ptr<Model> m;
+    {
+      std::lock_guard<std::mutex> l(g_reg);
+      auto it = g_models.find(model);
+      if (it == g_models.end())
+        fail(QED_ERR_ARGUMENT, std::string("The model ") + model +
+                                   " is not defined and so no model instance based on it is allowed.");
+      m = it->second;
+      g_instances.erase(label);
+    }
+    std::map<std::string, double> param;
+    {
+      std::lock_guard<std::mutex> l(m->mtx);
+      m->is_closed = true;
+      for (int k = 0; k < n; ++k)  // values of undefined operators are dropped (src_ed/qcm_ED.cpp:137-145)
+        if (m->term.count(names[k])) param[names[k]] = values[k];
+    }
+    auto inst = std::make_shared<Instance>(label, m, param, sectors);
+    std::lock_guard<std::mutex> l(g_reg);
+    g_instances[label] = inst;
+  });
+}
+
+int qed_erase_model_instance(int label) {
+  return guarded([&] {
+    std::shared_ptr<Instance> keep;
+    {
+      std::lock_guard<std::mutex> l(g_reg);
+      auto it = g_instances.find(label);
+      if (it == g_instances.end()) return;
+      keep = it->second;
+      g_instances.erase(it);
+    }
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    keep.reset();
+  });
+}
+
+int qed_mixing(int label, int *mixing) {
+  return guarded([&] { *mixing = instance(label)->mix; });
+}
+
+int qed_ground_state_solve(int label, double *energy, char *sectors, int len) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    auto r = I->low_energy_states(ws());
+    *energy = r.first;
+    if (sectors && len > 0) {
+      std::strncpy(sectors, r.second.c_str(), (size_t)len - 1);
+      sectors[len - 1] = 0;
+    }
+  });
+}
+
+int qed_Green_function_solve(int label) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    I->green_solve(ws());
+  });
+}
+
+int qed_Green_function_dimension(int label, int *dim) {
+  return guarded([&] { *dim = instance(label)->dim_GF; });
+}
+
+int qed_Green_function(int label, int spin_down, int nz, const double *z, double *G) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    I->green_function(reinterpret_cast<const cplx *>(z), nz, spin_down != 0, reinterpret_cast<cplx *>(G), ws());
+  });
+}
+
+int qed_self_energy(int label, int spin_down, int nz, const double *z, double *S) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    I->self_energy(reinterpret_cast<const cplx *>(z), nz, spin_down != 0, reinterpret_cast<cplx *>(S), ws());
+  });
+}
+
+int qed_hybridization_function(int label, int spin_down, int nz, const double *z, double *H) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    I->hybridization(reinterpret_cast<const cplx *>(z), nz, spin_down != 0, reinterpret_cast<cplx *>(H));
+  });
+}
+
+int qed_Green_function_average(int label, int spin_down, double *M) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    I->green_solve(ws());
+    const auto &src = I->Mave[(spin_down && (I->mix & mixing::up_down)) ? 1 : 0];
+    std::memcpy(M, src.data(), src.size() * sizeof(cplx));
+  });
+}
+
+int qed_Potthoff_functional(int label, double *omega) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    *omega = I->potthoff(ws());
+  });
+}
+
+int qed_qmatrix(int label, int spin_down, int *M, int *L, double *e, double *v) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    if (I->use_cf) fail(QED_ERR_ARGUMENT, "Green function format is not Lehmann! Cannot output the Q matrix.");
+    {
+      std::lock_guard<std::recursive_mutex> g(g_gpu);
+      I->green_solve(ws());
+    }
+    // model_instance::qmatrix (src_ed/model_instance.hpp:1425-1451): one state
+    // as is; several states appended, each scaled by sqrt(weight) once more.
+    const int sd = spin_down ? 1 : 0;
+    std::vector<double> ee, vv;
+    int l = I->dim_GF;
+    for (auto &st : I->states) {
+      const QMat &q = st->q[sd];
+      double sc = I->states.size() > 1 ? std::sqrt(st->weight) : 1.0;
+      ee.insert(ee.end(), q.e.begin(), q.e.end());
+      for (double x : q.V) vv.push_back(x * sc);
+    }
+    int m = (int)ee.size();
+    if (m > *M) fail(QED_ERR_ARGUMENT, "qed_qmatrix: capacity too small (" + std::to_string(m) + " poles)");
+    *M = m;
+    *L = l;
+    for (int i = 0; i < m; ++i) e[i] = ee[i];
+    for (size_t i = 0; i < vv.size(); ++i) {
+      v[2 * i] = vv[i];
+      v[2 * i + 1] = 0.0;
+    }
+  });
+}
+
+int qed_cf_coefficients(int label, int spin_down, int o1, int o2, int pm, int *n, double *a, double *b) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    if (!I->use_cf) fail(QED_ERR_ARGUMENT, "not a continued-fraction instance");
+    {
+      std::lock_guard<std::recursive_mutex> g(g_gpu);
+      I->green_solve(ws());
+    }
+    const CFSet &cf = I->states.front()->cf[spin_down ? 1 : 0];
+    if (o1 < 0 || o2 < 0 || o2 > o1 || o1 >= cf.n) fail(QED_ERR_ARGUMENT, "bad orbital pair");
+    size_t idx = (size_t)o1 * cf.n + o2;
+    const auto &A = pm > 0 ? cf.ea[idx] : cf.ha[idx];
+    const auto &B = pm > 0 ? cf.eb[idx] : cf.hb[idx];
+    if ((int)A.size() > *n) fail(QED_ERR_ARGUMENT, "capacity too small");
+    *n = (int)A.size();
+    for (size_t i = 0; i < A.size(); ++i) a[i] = A[i];
+    for (size_t i = 0; i < A.size() && i < B.size(); ++i) b[i] = B[i];
+  });
+}
+
+int qed_ground_state_vector(int label, long *dim, double *psi) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    I->low_energy_states(ws());
+    const State &st = *I->states.front();
+    *dim = (long)st.psi.n;
+    if (psi) {
+      st.psi.download(psi, st.psi.n, ws().stream);
+      ws().sync();
+    }
+  });
+}
+
+int qed_hamiltonian_create(int label, const char *sector, qed_hamiltonian **h, long *dim) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    auto *hh = new qed_hamiltonian;
+    try {
+      hh->H.reset(new SectorOp(I->terms, Sector(sector), ws()));
+    } catch (...) {
+      delete hh;
+      throw;
+    }
+    *dim = (long)hh->H->D;
+    *h = hh;
+  });
+}
+
+int qed_hamiltonian_mult_add(qed_hamiltonian *h, const double *x, double *y) {
+  return guarded([&] {
+    if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    const size_t D = h->H->D;
+    if (!D) return;
+    if (h->x.n < D) { h->x.alloc(D); h->y.alloc(D); }
+    Workspace &w = ws();
+    h->x.upload(x, D, w.stream);
+    h->y.upload(y, D, w.stream);
+    // y += H x : row pass writes H_rows x + y, column pass adds the rest
+    SubList sub;
+    sub.n = 1;
+    sub.c[0] = -1.0;
+    sub.z[0] = h->y.p;
+    launch_hv_rows(h->H->op, h->x.p, 1.0, h->y.p, sub, w.stream);
+    launch_hv_cols(h->H->op, h->x.p, 1.0, h->y.p, 0, w.red, w.stream);
+    h->y.download(y, D, w.stream);
+    w.sync();
+  });
+}
+
+int qed_hamiltonian_apply_device(qed_hamiltonian *h, const double *x, double *y, void *stream) {
+  return guarded([&] {
+    if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    Workspace &w = ws();
+    cudaStream_t s = stream ? (cudaStream_t)stream : w.stream;
+    if (!h->H->D) return;
+    SubList none;
+    launch_hv_rows(h->H->op, x, 1.0, y, none, s);
+    launch_hv_cols(h->H->op, x, 1.0, y, 0, w.red, s);
+  });
+}
+
+int qed_hamiltonian_diag(qed_hamiltonian *h, double *d) {
+  return guarded([&] {
+    if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    // diagonal = H applied to unit vectors is wasteful; rebuild it from the tables on the host
+    const SectorOp &H = *h->H;
+    std::vector<double> du(H.up.dim), dd(H.dn.dim);
+    Workspace &w = ws();
+    H.up.diag.download(du.data(), du.size(), w.stream);
+    H.dn.diag.download(dd.data(), dd.size(), w.stream);
+    std::vector<double> vin;
+    if (H.op.inter.mode >= 2) {
+      vin.resize(H.vinter.n);
+      H.vinter.download(vin.data(), vin.size(), w.stream);
+    }
+    w.sync();
+    const int n = H.L;
+    for (uint32_t b = 0; b < H.dn.dim; ++b)
+      for (uint32_t a = 0; a < H.up.dim; ++a) {
+        uint32_t up = H.up.hbits[a], dn = H.dn.hbits[b];
+        double s = du[a] + dd[b];
+        const auto &it = H.op.inter;
+        if (it.mode == 1) s += it.u * __builtin_popcount(up & dn);
+        else if (it.mode == 2) { for (int r = 0; r < n; ++r) if ((up & dn) >> r & 1u) s += vin[r]; }
+        else if (it.mode == 3) {
+          for (int r = 0; r < n; ++r)
+            if (dn >> r & 1u)
+              for (int c = 0; c < n; ++c)
+                if (up >> c & 1u) s += vin[(size_t)r * n + c];
+        }
+        d[a + (size_t)H.up.dim * b] = s;
+      }
+  });
+}
+
+int qed_hamiltonian_destroy(qed_hamiltonian *h) {
+  return guarded([&] {
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    delete h;
+  });
+}
+
+int qed_halfbasis(int L, int N, unsigned *strings, long *dim) {
+  return guarded([&] {
+    if (L < 1 || L > 32 || N < 0 || N > L) fail(QED_ERR_ARGUMENT, "bad (L, N)");
+    uint64_t d = binom(L, N);
+    *dim = (long)d;
+    if (!strings || !d) return;
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    Workspace &w = ws();
+    DevBuf<uint32_t> b(d);
+    launch_unrank(L, N, (uint32_t)d, b.p, w.stream);
+    b.download(strings, d, w.stream);
+    w.sync();
+  });
+}
+
+int qed_halfbasis_rank(int L, int N, long n, const unsigned *strings, unsigned *ranks) {
+  return guarded([&] {
+    if (L < 1 || L > 32 || N < 0 || N > L) fail(QED_ERR_ARGUMENT, "bad (L, N)");
+    if (n <= 0) return;
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    Workspace &w = ws();
+    DevBuf<uint32_t> s(n), r(n);
+    s.upload(strings, n, w.stream);
+    launch_rank(L, N, n, s.p, r.p, w.stream);
+    r.download(ranks, n, w.stream);
+    w.sync();
+  });
+}
+
+int qed_destroy_table(int L, int n_up, int n_dn, int a, long *target, int *phase) {
+  return guarded([&] {
+    if (L < 1 || L > 32 || a < 0 || a >= 2 * L) fail(QED_ERR_ARGUMENT, "bad orbital");
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    Workspace &w = ws();
+    // Evaluate c_a on every source state with the device gather: the source
+    // state index is encoded as its value, so the gathered value identifies it.
+    const int spin = a >= L ? 1 : 0, orb = a % L;
+    const int tnu = n_up - (spin ? 0 : 1), tnd = n_dn - (spin ? 1 : 0);
+    const uint64_t sdu = binom(L, n_up), sdd = binom(L, n_dn);
+    const uint64_t tdu = (tnu < 0) ? 0 : binom(L, tnu), tdd = (tnd < 0) ? 0 : binom(L, tnd);
+    const size_t Ds = sdu * sdd, Dt = tdu * tdd;
+    for (size_t i = 0; i < Ds; ++i) { target[i] = -1; phase[i] = 0; }
+    if (!Dt) return;
+    DevBuf<uint32_t> tub(tdu), tdb(tdd);
+    launch_unrank(L, tnu, (uint32_t)tdu, tub.p, w.stream);
+    launch_unrank(L, tnd, (uint32_t)tdd, tdb.p, w.stream);
+    std::vector<double> code(Ds);
+    for (size_t i = 0; i < Ds; ++i) code[i] = (double)(i + 1);
+    DevBuf<double> src(Ds), y(Dt);
+    src.upload(code, w.stream);
+    launch_cdag_gather(L, spin, orb, -1, tub.p, (uint32_t)tdu, tdb.p, (uint32_t)tdd, n_up, n_dn,
+                       (uint32_t)sdu, src.p, y.p, 1.0, 0, w.stream);
+    std::vector<double> hy(Dt);
+    y.download(hy.data(), Dt, w.stream);
+    w.sync();
+    for (size_t I = 0; I < Dt; ++I) {
+      if (hy[I] == 0.0) continue;
+      long s = (long)std::llround(std::fabs(hy[I])) - 1;
+      target[s] = (long)I;
+      phase[s] = hy[I] < 0 ? 1 : 0;
+    }
+  });
+}
+
+}  // extern "C"

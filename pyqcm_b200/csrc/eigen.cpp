@@ -1,0 +1,233 @@
+// Host-side dense eigensolvers (see eigen.hpp for the published algorithms).
+#include "eigen.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+namespace qed {
+
+namespace {
+
+constexpr double kEps = 2.220446049250313e-16;
+
+// Implicit-shift QL on (d, e); e[i] couples i and i+1, e has n entries (last unused).
+// rot(i, c, s) is called for every plane rotation acting on columns (i, i+1) of
+// the eigenvector matrix, so a caller can accumulate all of it or one row.
+template <class Rot>
+bool ql_implicit(int n, double *d, double *e, Rot &&rot) {
+  if (n <= 1) return true;
+  e[n - 1] = 0.0;
+  for (int l = 0; l < n; ++l) {
+    int iter = 0;
+    while (true) {
+      int m = l;
+      for (; m < n - 1; ++m) {
+        double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+        if (std::fabs(e[m]) <= kEps * dd) break;
+      }
+      if (m == l) break;
+      if (++iter > 100) return false;
+      // Wilkinson-type shift from the leading 2x2 block.
+      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      double r = std::hypot(g, 1.0);
+      g = d[m] - d[l] + e[l] / (g + std::copysign(r, g));
+      double s = 1.0, c = 1.0, p = 0.0;
+      int i = m - 1;
+      bool underflow = false;
+      for (; i >= l; --i) {
+        double f = s * e[i];
+        double b = c * e[i];
+        r = std::hypot(f, g);
+        e[i + 1] = r;
+        if (r == 0.0) {  // split: recover and restart the sweep
+          d[i + 1] -= p;
+          e[m] = 0.0;
+          underflow = true;
+          break;
+        }
+        s = f / r;
+        c = g / r;
+        g = d[i + 1] - p;
+        r = (d[i] - g) * s + 2.0 * c * b;
+        p = s * r;
+        d[i + 1] = g + p;
+        g = c * r - b;
+        rot(i, c, s);
+      }
+      if (underflow) continue;
+      d[l] -= p;
+      e[l] = g;
+      e[m] = 0.0;
+    }
+  }
+  return true;
+}
+
+}  // namespace
+
+bool tridiag_eig(int n, std::vector<double> &d, std::vector<double> e, std::vector<double> *z) {
+  e.resize(std::max(n, 1));
+  if (z) {
+    z->assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) (*z)[i + (size_t)n * i] = 1.0;
+  }
+  double *Z = z ? z->data() : nullptr;
+  bool ok = ql_implicit(n, d.data(), e.data(), [&](int i, double c, double s) {
+    if (!Z) return;
+    double *ci = Z + (size_t)n * i, *cj = Z + (size_t)n * (i + 1);
+    for (int k = 0; k < n; ++k) {
+      double f = cj[k];
+      cj[k] = s * ci[k] + c * f;
+      ci[k] = c * ci[k] - s * f;
+    }
+  });
+  if (!ok) return false;
+  // sort ascending (stable on ties), permuting eigenvector columns
+  std::vector<int> idx(n);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return d[a] < d[b]; });
+  std::vector<double> d2(n);
+  for (int k = 0; k < n; ++k) d2[k] = d[idx[k]];
+  d = d2;
+  if (Z) {
+    std::vector<double> z2((size_t)n * n);
+    for (int k = 0; k < n; ++k)
+      std::copy(Z + (size_t)n * idx[k], Z + (size_t)n * (idx[k] + 1), z2.data() + (size_t)n * k);
+    *z = std::move(z2);
+  }
+  return true;
+}
+
+bool tridiag_lowest_last(int n, const double *alpha, const double *beta, double *lambda0,
+                         double *last) {
+  if (n == 1) {
+    *lambda0 = alpha[0];
+    *last = 1.0;
+    return true;
+  }
+  std::vector<double> d(alpha, alpha + n), e(n, 0.0);
+  for (int i = 0; i < n - 1; ++i) e[i] = beta[i];
+  std::vector<double> row(n, 0.0);  // last row of the eigenvector matrix
+  row[n - 1] = 1.0;
+  bool ok = ql_implicit(n, d.data(), e.data(), [&](int i, double c, double s) {
+    double f = row[i + 1];
+    row[i + 1] = s * row[i] + c * f;
+    row[i] = c * row[i] - s * f;
+  });
+  if (!ok) return false;
+  int k = 0;
+  for (int i = 1; i < n; ++i)
+    if (d[i] < d[k]) k = i;
+  *lambda0 = d[k];
+  *last = row[k];
+  return true;
+}
+
+bool sym_eig(int n, const std::vector<double> &A, std::vector<double> &w, std::vector<double> *V) {
+  w.assign(n, 0.0);
+  if (n == 0) return true;
+  // Householder reduction A = Q T Q^T, working on a full copy; column-major a(i,j) = a[i + n*j].
+  std::vector<double> a(A);
+  auto at = [&](int i, int j) -> double & { return a[i + (size_t)n * j]; };
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < j; ++i) at(i, j) = at(j, i);  // symmetrise from the lower triangle
+  std::vector<double> d(n), e(n, 0.0);
+  std::vector<double> Q;
+  if (V) {
+    Q.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) Q[i + (size_t)n * i] = 1.0;
+  }
+  std::vector<double> v(n), p(n), q(n);
+  for (int k = 0; k < n - 2; ++k) {
+    // Householder vector annihilating a(k+2:n, k)
+    double alpha = 0.0;
+    for (int i = k + 1; i < n; ++i) alpha += at(i, k) * at(i, k);
+    alpha = std::sqrt(alpha);
+    if (alpha == 0.0) { e[k] = 0.0; continue; }
+    double x0 = at(k + 1, k);
+    if (x0 > 0) alpha = -alpha;
+    // v = x - alpha e1, normalised so that H = I - 2 v v^T / (v^T v)
+    for (int i = 0; i < n; ++i) v[i] = 0.0;
+    v[k + 1] = x0 - alpha;
+    for (int i = k + 2; i < n; ++i) v[i] = at(i, k);
+    double vv = 0.0;
+    for (int i = k + 1; i < n; ++i) vv += v[i] * v[i];
+    if (vv == 0.0) { e[k] = at(k + 1, k); continue; }
+    double beta2 = 2.0 / vv;
+    // p = beta2 * A v (trailing block), K = beta2/2 * v^T p, q = p - K v
+    for (int i = k; i < n; ++i) {  // A symmetric: row i of A == column i
+      double s = 0.0;
+      const double *ci = a.data() + (size_t)n * i;
+      for (int j = k + 1; j < n; ++j) s += ci[j] * v[j];
+      p[i] = beta2 * s;
+    }
+    double K = 0.0;
+    for (int i = k + 1; i < n; ++i) K += v[i] * p[i];
+    K *= 0.5 * beta2;
+    for (int i = k; i < n; ++i) q[i] = p[i] - K * v[i];
+    // A <- A - v q^T - q v^T on rows/cols k..n-1 (v[k] = 0)
+    for (int j = k; j < n; ++j)
+      for (int i = k; i < n; ++i) at(i, j) -= v[i] * q[j] + q[i] * v[j];
+    if (V) {  // Q <- Q H = Q - beta2 (Q v) v^T
+      std::fill(q.begin(), q.end(), 0.0);
+      for (int j = k + 1; j < n; ++j) {
+        const double *cj = Q.data() + (size_t)n * j;
+        for (int i = 0; i < n; ++i) q[i] += cj[i] * v[j];
+      }
+      for (int j = k + 1; j < n; ++j) {
+        double *cj = Q.data() + (size_t)n * j;
+        double f = beta2 * v[j];
+        for (int i = 0; i < n; ++i) cj[i] -= q[i] * f;
+      }
+    }
+  }
+  for (int i = 0; i < n; ++i) d[i] = at(i, i);
+  for (int i = 0; i < n - 1; ++i) e[i] = at(i + 1, i);
+  std::vector<double> Z;
+  if (!tridiag_eig(n, d, e, V ? &Z : nullptr)) return false;
+  w = d;
+  if (V) {  // V = Q Z
+    V->assign((size_t)n * n, 0.0);
+    for (int j = 0; j < n; ++j)
+      for (int k = 0; k < n; ++k) {
+        double zkj = Z[k + (size_t)n * j];
+        if (zkj == 0.0) continue;
+        const double *qk = Q.data() + (size_t)n * k;
+        double *vj = V->data() + (size_t)n * j;
+        for (int i = 0; i < n; ++i) vj[i] += qk[i] * zkj;
+      }
+  }
+  return true;
+}
+
+bool complex_inverse(int n, std::complex<double> *a) {
+  auto at = [&](int i, int j) -> std::complex<double> & { return a[i + (size_t)n * j]; };
+  std::vector<int> piv(n);
+  for (int k = 0; k < n; ++k) {
+    int pr = k;
+    double best = std::abs(at(k, k));
+    for (int i = k + 1; i < n; ++i)
+      if (std::abs(at(i, k)) > best) { best = std::abs(at(i, k)); pr = i; }
+    if (best == 0.0) return false;
+    piv[k] = pr;
+    if (pr != k)
+      for (int j = 0; j < n; ++j) std::swap(at(k, j), at(pr, j));
+    std::complex<double> inv = 1.0 / at(k, k);
+    at(k, k) = 1.0;
+    for (int j = 0; j < n; ++j) at(k, j) *= inv;
+    for (int i = 0; i < n; ++i) {
+      if (i == k) continue;
+      std::complex<double> f = at(i, k);
+      if (f == 0.0) continue;
+      at(i, k) = 0.0;
+      for (int j = 0; j < n; ++j) at(i, j) -= f * at(k, j);
+    }
+  }
+  for (int k = n - 1; k >= 0; --k)
+    if (piv[k] != k)
+      for (int i = 0; i < n; ++i) std::swap(at(i, k), at(i, piv[k]));
+  return true;
+}
+
+}  // namespace qed

@@ -1,0 +1,39 @@
+// Host-side dense eigensolvers for the small projected problems of the ED
+// solver: the Lanczos tridiagonal (Ritz test, src_ed/Hamiltonian/Lanczos.cpp:25-52),
+// the band-Lanczos projected matrix (src_ed/Hamiltonian/Lanczos.hpp:340-384)
+// and the Q-matrix streamlining (src_ed/Q_matrix.hpp:286-318).
+//
+// Algorithms: Householder reduction to tridiagonal form followed by the
+// implicit-shift QL iteration (Wilkinson shift), as published by Bowdler,
+// Martin, Reinsch and Wilkinson (Handbook for Automatic Computation II,
+// procedures tred2/tql2). Eigenvalues are returned in ascending order with
+// orthonormal eigenvector columns, the contract of LAPACK dstev/dsyev that the
+// reference relies on.
+#pragma once
+#include <complex>
+#include <vector>
+
+namespace qed {
+
+// Symmetric tridiagonal eigenproblem: diagonal d[n], off-diagonal e[n-1].
+// On return d holds the eigenvalues ascending. If z != nullptr it receives the
+// n x n eigenvector matrix (column-major, column k <-> d[k]).
+// Returns false if the QL iteration did not converge.
+bool tridiag_eig(int n, std::vector<double> &d, std::vector<double> e, std::vector<double> *z);
+
+// Lowest eigenvalue of the tridiagonal (alpha[n], beta[n-1]) and the last
+// component of its normalised eigenvector, in O(n^2): QL rotations applied to
+// the last row of the eigenvector matrix only. This is exactly what the
+// reference's Ritz-residual test consumes (evector.back(), Lanczos.hpp:82-83).
+bool tridiag_lowest_last(int n, const double *alpha, const double *beta, double *lambda0,
+                         double *last);
+
+// Dense symmetric eigenproblem, A column-major n x n (lower triangle used).
+// w receives eigenvalues ascending; V (if non-null) the eigenvectors.
+bool sym_eig(int n, const std::vector<double> &A, std::vector<double> &w, std::vector<double> *V);
+
+// In-place inverse of a complex n x n column-major matrix (Gauss-Jordan with
+// partial pivoting). Returns false if singular.
+bool complex_inverse(int n, std::complex<double> *a);
+
+}  // namespace qed

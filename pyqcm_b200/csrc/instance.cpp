@@ -1,0 +1,561 @@
+// Model instance (see instance.hpp).
+#include "instance.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <iomanip>
+#include <sstream>
+
+#include "eigen.hpp"
+#include "options.hpp"
+
+namespace qed {
+
+namespace {
+constexpr double kSmall = 1.0e-12;   // SMALL_VALUE (src_util/vector_num.hpp:23)
+constexpr double kMiddle = 1.0e-8;   // MIDDLE_VALUE (src_util/vector_num.hpp:24)
+constexpr double kMinGap = 1.0e-6;   // MIN_GAP (src_ed/model.hpp:20)
+
+double max_gap() {
+  double g = -std::log(opt_double("minimum_weight")) * opt_double("temperature");
+  return g < kMinGap ? kMinGap : g;
+}
+}  // namespace
+
+// symmetry_group::sector_is_valid for the trivial group (src_ed/symmetry_group.cpp:515-532)
+bool sector_is_valid(const Sector &s, int n_orb) {
+  if (s.N < Sector::odd) {
+    if (s.N < 0 || s.N > 2 * n_orb) return false;
+    if (s.S < Sector::odd) {
+      if (s.S > s.N || s.S < -s.N) return false;
+      if ((s.N + s.S) % 2) return false;
+    }
+  }
+  if (s.S < Sector::odd && (s.S > n_orb || s.S < -n_orb)) return false;
+  return s.irrep == 0;
+}
+
+// symmetry_group::shift_sector (src_ed/symmetry_group.cpp:540-558)
+Sector shift_sector(const Sector &s, int pm, int spin) {
+  Sector t = s;
+  t.N += pm;
+  t.S += spin ? -pm : pm;
+  return t;
+}
+
+Instance::Instance(int lab, std::shared_ptr<Model> m, std::map<std::string, double> val,
+                   const std::string &sectors)
+    : label(lab), model(std::move(m)), value(std::move(val)) {
+  // model_instance_base ctor (src_ed/model_instance_base.cpp:14-130)
+  if (value.empty())
+    fail(QED_ERR_ARGUMENT, "ED model instance (label = " + std::to_string(label) + ") for model " +
+                               model->name + " has no parameters!");
+  char gf = opt_char("GF_method");
+  if (gf == 'L' && opt_bool("continued_fraction")) gf = 'F';
+  if (gf == 'M' || (gf == 'L' && opt_bool("combine_mcf")))
+    fail(QED_ERR_UNSUPPORTED, "matrix continued fractions (GF_method 'M') are not in this solver");
+  use_cf = (gf == 'F');
+  if (opt_char("Ground_state_method") != 'L')
+    fail(QED_ERR_UNSUPPORTED, "only the Lanczos ground-state method ('L') is in this solver");
+  if (opt_int("n_states") > 1)
+    fail(QED_ERR_UNSUPPORTED, "n_states > 1 needs the Davidson solver, not in this solver");
+  for (auto &v : value) {
+    const Operator &op = *model->term.at(v.first);
+    mix |= op.mix;
+    if (op.is_interaction) is_correlated = true;
+  }
+  if (mix > 5) mix &= mixing::full;
+  if (mix == 5) mix &= mixing::anomalous;
+  if (model->mix == -1) model->mix = mix;
+  else if ((mix | model->mix) != model->mix)
+    fail(QED_ERR_ARGUMENT, "The new instance mixing state of model " + model->name + " (" +
+                               std::to_string(mix) + ") is not compatible with the first instance mixing (" +
+                               std::to_string(model->mix) + ")");
+  else mix = model->mix;
+  if (mix != mixing::normal && mix != mixing::up_down)
+    fail(QED_ERR_UNSUPPORTED, "mixing " + std::to_string(mix) +
+                                  " (anomalous / spin-flip) is outside the spin-factorized solver");
+  dim_GF = model->n_sites;
+  // sectors: slash-separated list
+  std::stringstream ss(sectors);
+  std::string item;
+  while (std::getline(ss, item, '/')) {
+    if (item.empty()) continue;
+    Sector S(item);
+    if (!sector_is_valid(S, model->n_orb)) fail(QED_ERR_ARGUMENT, "sector " + item + " is not valid");
+    if (S.S && mix == mixing::normal) mix = mixing::up_down;
+    if (S.S >= Sector::odd)
+      fail(QED_ERR_ARGUMENT, "sector string " + S.name() +
+                                 " defines a non conserved spin, but spin is conserved in the model (instance " +
+                                 std::to_string(label) + ")");
+    if (S.N >= Sector::odd)
+      fail(QED_ERR_ARGUMENT, "sector string " + S.name() +
+                                 " defines a non conserved particle number, but particle number is conserved in the model (instance " +
+                                 std::to_string(label) + ")");
+    target_sectors.insert(S);
+  }
+  if (target_sectors.empty()) fail(QED_ERR_ARGUMENT, "no target sectors were specified for model " + model->name);
+  terms = collect_terms(*model, value);
+  set_hopping_matrix();
+}
+
+// set_hopping_matrix (src_ed/model_instance.hpp:424-474), real case.
+void Instance::set_hopping_matrix() {
+  if (hopping_solved) return;
+  const int no = model->n_orb, ns = model->n_sites, nb = model->n_bath;
+  SEF_bath = 0.0;
+  for (int sp = 0; sp < 2; ++sp) {
+    const std::vector<double> &t = sp ? terms.t_dn : terms.t_up;
+    tc[sp].assign((size_t)ns * ns, 0.0);
+    tb[sp].assign((size_t)nb * nb, 0.0);
+    tcb[sp].assign((size_t)ns * nb, 0.0);
+    for (int a = 0; a < ns; ++a)
+      for (int b = 0; b < ns; ++b) tc[sp][a + (size_t)ns * b] = t[(size_t)a * no + b];
+    for (int a = 0; a < nb; ++a)
+      for (int b = 0; b < nb; ++b) tb[sp][a + (size_t)nb * b] = t[(size_t)(ns + a) * no + ns + b];
+    for (int a = 0; a < ns; ++a)
+      for (int b = 0; b < nb; ++b) tcb[sp][a + (size_t)ns * b] = t[(size_t)a * no + ns + b];
+    if (nb) {
+      bool diag = true;
+      for (int a = 0; a < nb; ++a)
+        for (int b = 0; b < nb; ++b)
+          if (a != b && std::fabs(tb[sp][a + (size_t)nb * b]) > 1e-8) diag = false;
+      if (!diag) {
+        std::vector<double> d, Sb;
+        if (!sym_eig(nb, tb[sp], d, &Sb)) fail(QED_ERR_INTERNAL, "bath diagonalisation failed");
+        std::fill(tb[sp].begin(), tb[sp].end(), 0.0);
+        for (int a = 0; a < nb; ++a) tb[sp][a + (size_t)nb * a] = d[a];
+        std::vector<double> t2((size_t)ns * nb, 0.0);
+        for (int a = 0; a < ns; ++a)
+          for (int b = 0; b < nb; ++b) {
+            double s = 0.0;
+            for (int k = 0; k < nb; ++k) s += tcb[sp][a + (size_t)ns * k] * Sb[k + (size_t)nb * b];
+            t2[a + (size_t)ns * b] = s;
+          }
+        tcb[sp] = t2;
+      }
+      // bath contribution to the Potthoff functional
+      if (sp == 0 || (mix & mixing::up_down))
+        for (int i = 0; i < nb; ++i)
+          if (tb[sp][i + (size_t)nb * i] < 0) SEF_bath -= tb[sp][i + (size_t)nb * i];
+    }
+  }
+  if (mix == mixing::normal) SEF_bath *= 2.0;
+  hopping_solved = true;
+}
+
+std::string Instance::gs_string() const {
+  if (!is_correlated) return "uncorrelated";
+  std::map<Sector, double, SectorLess> ws;
+  for (auto &s : states) ws[s->sec] += s->weight;
+  std::ostringstream out;
+  bool first = true;
+  for (auto &x : ws) {
+    if (!first) out << '/';
+    first = false;
+    out << x.first.name() << ':' << std::setprecision(3) << x.second;
+  }
+  return out.str();
+}
+
+// low_energy_states (src_ed/model_instance.hpp:245-347)
+std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
+  if (gs_solved) return {GS_energy, gs_string()};
+  if (!is_correlated)
+    fail(QED_ERR_UNSUPPORTED, "uncorrelated instances (no interaction term) are solved by the one-body "
+                              "path, which is not in this solver");
+  GS_energy = 1.0e12;
+  const double gap = max_gap();
+  const uint64_t seed = (uint64_t)opt_int("seed");
+  for (auto &s : target_sectors) {
+    SectorOp H(terms, s, ws);
+    if (H.D == 0) continue;
+    auto st = std::make_shared<State>();
+    st->sec = s;
+    LanczosResult r;
+    try {
+      r = lanczos_ground_state(H, ws, st->psi, seed);
+    } catch (const Error &e) {
+      fail(e.code, std::string(e.what()) + "\n  in cluster model '" + model->name + "', instance '" +
+                       model->name + "_" + std::to_string(label) + "', sector '" + s.name() + "'");
+    }
+    st->energy = r.energy;
+    // Hamiltonian::states (src_ed/Hamiltonian/Hamiltonian_base.hpp:197-206)
+    if (r.energy < GS_energy) GS_energy = r.energy;
+    if (r.energy - GS_energy > gap) continue;
+    states.push_back(st);
+  }
+  compute_weights();
+  const double wmin = opt_double("minimum_weight");
+  std::vector<std::shared_ptr<State>> kept;
+  double tot = 0.0;
+  for (auto &x : states)
+    if (x->weight >= wmin) { kept.push_back(x); tot += x->weight; }
+  states = kept;
+  for (auto &x : states) x->weight /= tot;
+  bool updown = false;
+  for (auto &x : states)
+    if (x->sec.S) updown = true;
+  if (mix == mixing::normal && updown) mix = mixing::up_down;
+  GS_energy = 1.0e18;
+  E0 = 0.0;
+  for (auto &x : states) {
+    E0 += x->weight * x->energy;
+    if (x->energy < GS_energy) GS_energy = x->energy;
+  }
+  gs_solved = true;
+  return {GS_energy, gs_string()};
+}
+
+// compute_weights (src_ed/model_instance.hpp:356-417)
+void Instance::compute_weights() {
+  const double T = opt_double("temperature");
+  if (T < kMiddle) {
+    double e0 = 1e12;
+    for (auto &x : states) e0 = std::min(e0, x->energy);
+    std::vector<std::shared_ptr<State>> keep;
+    for (auto &x : states)
+      if (x->energy - e0 <= kSmall) keep.push_back(x);
+    states = keep;
+    if (states.empty()) fail(QED_ERR_INTERNAL, "instance has no low-energy state!");
+    for (auto &x : states) x->weight = 1.0 / states.size();
+    E0 = states.front()->energy;
+    return;
+  }
+  const double gap = max_gap();
+  std::vector<std::shared_ptr<State>> keep;
+  for (auto &x : states)
+    if (x->energy - GS_energy <= gap) keep.push_back(x);
+  states = keep;
+  double Z = 0.0;
+  for (auto &x : states) {
+    x->weight = std::exp(-(x->energy - GS_energy) / T);
+    Z += x->weight;
+  }
+  E0 = GS_energy - T * std::log(Z);
+  for (auto &x : states) x->weight /= Z;
+}
+
+void Instance::apply_cdag(const State &st, int pm, int spin, int orb, const SectorOp &H, double *y,
+                          double coef, bool accumulate, Workspace &ws) {
+  const int L = model->n_orb;
+  const int src_nup = st.sec.Nup(), src_ndn = st.sec.Ndw();
+  const uint32_t du_s = (uint32_t)((src_nup < 0 || src_nup > L) ? 0 : binom(L, src_nup));
+  launch_cdag_gather(L, spin, orb, pm, H.up.bits.p, H.up.dim, H.dn.bits.p, H.dn.dim, src_nup, src_ndn,
+                     du_s, st.psi.p, y, coef, accumulate ? 1 : 0, ws.stream);
+}
+
+// Q-matrix streamlining (Q_matrix::streamline / streamlineQ, src_ed/Q_matrix.hpp:181-318)
+static void streamline(std::vector<double> &e, std::vector<double> &V, int L) {
+  const double wtol = opt_double("Qmatrix_wtol"), vtol = opt_double("Qmatrix_vtol");
+  if (vtol < 1e-12) return;
+  const int M = (int)e.size();
+  std::vector<double> e2, V2;
+  e2.reserve(M);
+  V2.reserve(V.size());
+  for (int i = 0; i < M; ++i) {
+    int j = i + 1;
+    for (; j < M; ++j)
+      if (std::fabs(e[j] - e[i]) > wtol) break;
+    const int n = j - i;
+    if (n == 1) {
+      double nn = 0.0;
+      for (int a = 0; a < L; ++a) nn += V[(size_t)i * L + a] * V[(size_t)i * L + a];
+      if (nn >= vtol) {
+        e2.push_back(e[i]);
+        V2.insert(V2.end(), V.begin() + (size_t)i * L, V.begin() + (size_t)(i + 1) * L);
+      }
+    } else {
+      std::vector<double> QQ((size_t)L * L, 0.0), d, U;
+      for (int a = 0; a < L; ++a)
+        for (int b = 0; b < L; ++b) {
+          double s = 0.0;
+          for (int k = i; k < j; ++k) s += V[(size_t)k * L + a] * V[(size_t)k * L + b];
+          QQ[a + (size_t)L * b] = s;
+        }
+      if (!sym_eig(L, QQ, d, &U)) fail(QED_ERR_INTERNAL, "streamline eigensolver failed");
+      for (int k = 0; k < L; ++k)
+        if (d[k] > vtol) {
+          e2.push_back(e[i]);
+          double sq = std::sqrt(d[k]);
+          for (int a = 0; a < L; ++a) V2.push_back(U[a + (size_t)L * k] * sq);
+        }
+    }
+    i += n - 1;
+  }
+  e = e2;
+  V = V2;
+}
+
+// build_qmatrix (src_ed/model_instance.hpp:711-817), sequential branch.
+void Instance::build_qmatrix(State &st, bool spin_down, Workspace &ws) {
+  const int p = model->n_sites;
+  std::vector<double> eall[2], Vall[2];  // [0] hole (pm=-1), [1] electron
+  for (int s = 0; s < 2; ++s) {
+    const int pm = 2 * s - 1;
+    const int spin = spin_down ? 1 : 0;
+    Sector tsec = shift_sector(st.sec, pm, spin);
+    if (!sector_is_valid(tsec, model->n_orb)) continue;
+    SectorOp H(terms, tsec, ws);
+    if (H.D == 0) continue;
+    std::vector<DevBuf<double>> phi;
+    phi.reserve(p);
+    for (int i = 0; i < p; ++i) {
+      phi.emplace_back(H.D);
+      apply_cdag(st, pm, spin, i, H, phi.back().p, 1.0, false, ws);
+    }
+    std::vector<double> ev, Q;
+    int M = 0;
+    bool ok = band_lanczos_qmatrix(H, ws, phi, ev, Q, M);
+    std::vector<double> e, V;
+    if (ok && M > 0) {
+      e = ev;
+      V = Q;
+      for (auto &x : e) x -= st.energy;
+      if (pm == -1)
+        for (auto &x : e) x = -x;
+      streamline(e, V, p);
+    }
+    eall[s] = e;
+    Vall[s] = V;
+  }
+  QMat &q = st.q[spin_down ? 1 : 0];
+  q.L = p;
+  q.e = eall[0];
+  q.e.insert(q.e.end(), eall[1].begin(), eall[1].end());
+  q.V = Vall[0];
+  q.V.insert(q.V.end(), Vall[1].begin(), Vall[1].end());
+  q.M = (int)q.e.size();
+  // check_norm (src_ed/Q_matrix.hpp:236-260), before the weight factor
+  double ztot = 0.0;
+  for (int i = 0; i < p; ++i) {
+    double z = 0.0;
+    for (int k = 0; k < q.M; ++k) z += q.V[(size_t)k * p + i] * q.V[(size_t)k * p + i];
+    ztot += (z - 1.0) * (z - 1.0);
+    for (int j = 0; j < i; ++j) {
+      double zz = 0.0;
+      for (int k = 0; k < q.M; ++k) zz += q.V[(size_t)k * p + i] * q.V[(size_t)k * p + j];
+      ztot += 2.0 * zz * zz;
+    }
+  }
+  if (ztot > opt_double("accur_Q_matrix"))
+    fail(QED_ERR_QMATRIX, "Q-matrix does not satisfy unitary condition by " + std::to_string(ztot));
+  const double sw = std::sqrt(st.weight);
+  for (auto &x : q.V) x *= sw;
+  q.de.upload(q.e, ws.stream);
+  q.dV.upload(q.V, ws.stream);
+  ws.sync();
+}
+
+// build_cf (src_ed/model_instance.cpp:34-99), real Hilbert space.
+void Instance::build_cf(State &st, bool spin_down, Workspace &ws) {
+  const int n = model->n_sites;
+  CFSet &cf = st.cf[spin_down ? 1 : 0];
+  cf.n = n;
+  cf.ea.assign((size_t)n * n, {});
+  cf.eb.assign((size_t)n * n, {});
+  cf.ha.assign((size_t)n * n, {});
+  cf.hb.assign((size_t)n * n, {});
+  for (int pm = -1; pm < 2; pm += 2) {
+    Sector tsec = shift_sector(st.sec, pm, spin_down ? 1 : 0);
+    if (!sector_is_valid(tsec, model->n_orb)) continue;
+    SectorOp H(terms, tsec, ws);
+    if (H.D == 0) continue;
+    DevBuf<double> psi(H.D), q(H.D);
+    for (int o1 = 0; o1 < n; ++o1)
+      for (int o2 = 0; o2 <= o1; ++o2) {
+        apply_cdag(st, pm, spin_down ? 1 : 0, o1, H, psi.p, 1.0, false, ws);
+        if (o1 != o2) apply_cdag(st, pm, spin_down ? 1 : 0, o2, H, psi.p, 1.0, true, ws);
+        VecList one;
+        one.n = 1;
+        one.v[0] = psi.p;
+        int nb = launch_dots(H.D, psi.p, 1.0, 0, one, ws.red, ws.stream);
+        const double norm = ws.sums(nb, 1)[0];
+        if (norm <= 1e-14) continue;
+        launch_scale(H.D, psi.p, 1.0 / std::sqrt(norm), ws.stream);
+        std::vector<double> a, b;
+        lanczos_green(H, ws, psi.p, q.p, a, b);
+        // continued_fraction ctor (src_ed/continued_fraction.cpp:33-39)
+        for (auto &x : b) x *= x;
+        b[0] = norm * st.weight;
+        if (pm == 1)
+          for (auto &x : a) x -= st.energy;
+        else
+          for (auto &x : a) x = -x + st.energy;
+        const size_t idx = (size_t)o1 * n + o2;
+        if (pm == 1) { cf.ea[idx] = a; cf.eb[idx] = b; }
+        else { cf.ha[idx] = a; cf.hb[idx] = b; }
+      }
+  }
+}
+
+// Green_function_solve (src_ed/model_instance.hpp:517-555)
+void Instance::green_solve(Workspace &ws) {
+  if (gf_solved) return;
+  if (!gs_solved) low_energy_states(ws);
+  if (opt_bool("merge_states") && states.size() > 1 && !use_cf)
+    fail(QED_ERR_UNSUPPORTED, "merge_states is not in this solver");
+  for (auto &x : states) {
+    if (use_cf) build_cf(*x, false, ws);
+    else build_qmatrix(*x, false, ws);
+    if (mix & mixing::up_down) {
+      if (use_cf) build_cf(*x, true, ws);
+      else build_qmatrix(*x, true, ws);
+    }
+  }
+  gf_solved = true;
+  green_average();
+  // Green_function_density (src_ed/model_instance.hpp:657-675)
+  const int ns = model->n_sites;
+  double nG = 0.0;
+  for (int i = 0; i < ns; ++i) nG += Mave[0][i + (size_t)ns * i].real();
+  if (mix & mixing::up_down)
+    for (int i = 0; i < ns; ++i) nG += Mave[1][i + (size_t)ns * i].real();
+  GF_density = nG / ns;
+  if (mix == mixing::normal) GF_density *= 2;
+}
+
+// Green_function_average (src_ed/model_instance.hpp:643-652): Q-matrix
+// integrated_Green_function (src_ed/Q_matrix.hpp:160-172) or the CF version
+// (src_ed/continued_fraction_set.cpp:103-125), accumulated over states.
+void Instance::green_average() {
+  const int n = model->n_sites;
+  for (int sd = 0; sd < 2; ++sd) {
+    Mave[sd].assign((size_t)n * n, 0.0);
+    if (sd == 1 && !(mix & mixing::up_down)) continue;
+    for (auto &st : states) {
+      if (!use_cf) {
+        const QMat &q = st->q[sd];
+        for (int i = 0; i < q.M; ++i) {
+          if (q.e[i] >= 0.0) continue;
+          for (int a = 0; a < n; ++a)
+            for (int b = 0; b < n; ++b) Mave[sd][b + (size_t)n * a] += q.V[(size_t)i * n + a] * q.V[(size_t)i * n + b];
+        }
+      } else {
+        const CFSet &cf = st->cf[sd];
+        auto b0 = [&](size_t idx) { return cf.hb[idx].empty() ? 0.0 : cf.hb[idx][0]; };
+        for (int o1 = 0; o1 < n; ++o1) Mave[sd][o1 + (size_t)n * o1] += b0((size_t)o1 * n + o1);
+        for (int o1 = 0; o1 < n; ++o1)
+          for (int o2 = 0; o2 < o1; ++o2) {
+            cplx tmp = 0.5 * (b0((size_t)o1 * n + o2) - Mave[sd][o1 + (size_t)n * o1] - Mave[sd][o2 + (size_t)n * o2]);
+            Mave[sd][o1 + (size_t)n * o2] += tmp;
+            Mave[sd][o2 + (size_t)n * o1] += tmp;
+          }
+      }
+    }
+  }
+}
+
+// Green_function (src_ed/model_instance.hpp:566-635), batched over frequencies.
+void Instance::green_function(const cplx *z, int nz, bool spin_down, cplx *out, Workspace &ws) {
+  if (spin_down && !(mix & mixing::up_down || mix == 0))
+    fail(QED_ERR_ARGUMENT, "spin_down=True impossible with Hilbert space mixing " + std::to_string(mix));
+  if (!gf_solved) green_solve(ws);
+  const int n = model->n_sites;
+  const int sd = (spin_down && (mix & mixing::up_down)) ? 1 : 0;
+  const size_t nn = (size_t)n * n;
+  std::fill(out, out + nn * nz, cplx(0.0));
+  if (nz <= 0) return;
+  DevBuf<double> dz(2 * (size_t)nz);
+  dz.upload(reinterpret_cast<const double *>(z), 2 * (size_t)nz, ws.stream);
+  if (!use_cf) {
+    DevBuf<double> dG(2 * nn * nz);
+    QED_CUDA(cudaMemsetAsync(dG.p, 0, dG.bytes(), ws.stream));
+    for (auto &st : states) {
+      const QMat &q = st->q[sd];
+      launch_qmatrix_gf(n, q.M, q.de.p, q.dV.p, nz, dz.p, dG.p, ws.stream);
+    }
+    dG.download(reinterpret_cast<double *>(out), 2 * nn * nz, ws.stream);
+    ws.sync();
+    return;
+  }
+  // continued fractions: evaluate every fraction of every state on the GPU,
+  // then combine per continued_fraction_set::Green_function (src_ed/continued_fraction_set.cpp:63-98)
+  for (auto &st : states) {
+    const CFSet &cf = st->cf[sd];
+    std::vector<int> off, len;
+    std::vector<double> A, B;
+    auto push = [&](const std::vector<double> &a, const std::vector<double> &b) {
+      off.push_back((int)A.size());
+      len.push_back((int)a.size());
+      A.insert(A.end(), a.begin(), a.end());
+      B.insert(B.end(), b.begin(), b.begin() + std::min(a.size(), b.size()));
+      if (b.size() < a.size()) B.resize(A.size(), 0.0);
+    };
+    for (size_t idx = 0; idx < nn; ++idx) {
+      push(cf.ea[idx], cf.eb[idx]);
+      push(cf.ha[idx], cf.hb[idx]);
+    }
+    const int nf = (int)off.size();
+    DevBuf<int> doff(nf), dlen(nf);
+    DevBuf<double> dA(std::max<size_t>(A.size(), 1)), dB(std::max<size_t>(B.size(), 1)), dF(2 * (size_t)nf * nz);
+    doff.upload(off, ws.stream);
+    dlen.upload(len, ws.stream);
+    if (!A.empty()) { dA.upload(A, ws.stream); dB.upload(B, ws.stream); }
+    launch_cf_eval(nf, doff.p, dlen.p, dA.p, dB.p, nz, dz.p, dF.p, ws.stream);
+    std::vector<cplx> F((size_t)nf * nz);
+    dF.download(reinterpret_cast<double *>(F.data()), 2 * (size_t)nf * nz, ws.stream);
+    ws.sync();
+    for (int k = 0; k < nz; ++k) {
+      const cplx *f = F.data() + (size_t)k * nf;
+      cplx *G = out + nn * k;
+      auto ev = [&](int o1, int o2) { size_t idx = (size_t)o1 * n + o2; return f[2 * idx] + f[2 * idx + 1]; };
+      std::vector<cplx> Gt(n);
+      for (int o1 = 0; o1 < n; ++o1) {
+        Gt[o1] = ev(o1, o1);
+        G[o1 + (size_t)n * o1] += Gt[o1];
+      }
+      for (int o1 = 0; o1 < n; ++o1)
+        for (int o2 = 0; o2 < o1; ++o2) {
+          cplx tmp = 0.5 * (ev(o1, o2) - Gt[o1] - Gt[o2]);
+          G[o1 + (size_t)n * o2] += tmp;
+          G[o2 + (size_t)n * o1] += tmp;
+        }
+    }
+  }
+}
+
+// hybridization_function (src_ed/model_instance.hpp:1004-1018)
+void Instance::hybridization(const cplx *z, int nz, bool spin_down, cplx *out) {
+  const int n = model->n_sites, nb = model->n_bath;
+  const int sd = (spin_down && (mix & mixing::up_down)) ? 1 : 0;
+  const size_t nn = (size_t)n * n;
+  for (int k = 0; k < nz; ++k) {
+    cplx *G = out + nn * k;
+    std::fill(G, G + nn, cplx(0.0));
+    for (int i = 0; i < nb; ++i) {
+      cplx w = 1.0 / (z[k] - tb[sd][i + (size_t)nb * i]);
+      for (int a = 0; a < n; ++a)
+        for (int b = 0; b < n; ++b)
+          G[a + (size_t)n * b] += tcb[sd][a + (size_t)n * i] * tcb[sd][b + (size_t)n * i] * w;
+    }
+  }
+}
+
+// self_energy (src_ed/model_instance.hpp:683-700): z - t_c - Gamma(z) - G(z)^-1
+void Instance::self_energy(const cplx *z, int nz, bool spin_down, cplx *out, Workspace &ws) {
+  const int n = model->n_sites;
+  const size_t nn = (size_t)n * n;
+  const int sd = (spin_down && (mix & mixing::up_down)) ? 1 : 0;
+  green_function(z, nz, spin_down, out, ws);
+  std::vector<cplx> Gam(nn * std::max(nz, 1));
+  if (model->n_bath) hybridization(z, nz, spin_down, Gam.data());
+  for (int k = 0; k < nz; ++k) {
+    cplx *S = out + nn * k;
+    if (!complex_inverse(n, S)) fail(QED_ERR_INTERNAL, "singular Green function in self_energy");
+    for (size_t i = 0; i < nn; ++i) {
+      S[i] += tc[sd][i];
+      if (model->n_bath) S[i] += Gam[nn * k + i];
+      S[i] = -S[i];
+    }
+    for (int a = 0; a < n; ++a) S[a + (size_t)n * a] += z[k];
+  }
+}
+
+// Potthoff_functional (src_ed/qcm_ED.cpp:330-334)
+double Instance::potthoff(Workspace &ws) {
+  if (!gf_solved) green_solve(ws);
+  return SEF_bath + E0;
+}
+
+}  // namespace qed

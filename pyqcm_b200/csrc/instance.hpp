@@ -1,0 +1,86 @@
+// Model instance: ground-state search over sectors, Green-function
+// representations and their evaluation. Follows model_instance<double>
+// (src_ed/model_instance.hpp) and model_instance_base (src_ed/model_instance_base.cpp)
+// for the spin-conserving, trivial-group case.
+#pragma once
+#include <complex>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "model.hpp"
+#include "solver.hpp"
+
+namespace qed {
+
+using cplx = std::complex<double>;
+
+// Lehmann representation of one state (Q_matrix, src_ed/Q_matrix.hpp:20-40):
+// poles e[M], residues V (L x M, column-major), plus a device copy for G(z).
+struct QMat {
+  int L = 0, M = 0;
+  std::vector<double> e, V;
+  DevBuf<double> de, dV;
+};
+
+// Continued fractions of one state (continued_fraction_set, src_ed/continued_fraction_set.cpp):
+// electron (e) and hole (h) fractions for pairs o2 <= o1 of the n cluster sites.
+struct CFSet {
+  int n = 0;
+  std::vector<std::vector<double>> ea, eb, ha, hb;  // index o1*n + o2
+};
+
+struct State {
+  Sector sec;
+  double energy = 0.0, weight = 0.0;
+  DevBuf<double> psi;
+  QMat q[2];   // [spin_down]
+  CFSet cf[2];
+};
+
+struct Instance {
+  int label = 0;
+  std::shared_ptr<Model> model;
+  std::map<std::string, double> value;
+  SectorSet target_sectors;
+  int mix = 0;
+  bool is_correlated = false;
+  bool use_cf = false;
+  int dim_GF = 0;
+  bool gs_solved = false, gf_solved = false, hopping_solved = false;
+  double GS_energy = 0.0, E0 = 0.0, SEF_bath = 0.0, GF_density = 0.0;
+  std::vector<std::shared_ptr<State>> states;
+  SpinData terms;
+  std::vector<double> tc[2], tb[2], tcb[2];  // cluster, bath (diagonalised), cluster-bath
+  std::vector<cplx> Mave[2];
+  std::mutex mtx;
+
+  Instance(int label, std::shared_ptr<Model> m, std::map<std::string, double> value,
+           const std::string &sectors);
+
+  std::pair<double, std::string> low_energy_states(Workspace &ws);
+  void green_solve(Workspace &ws);
+  // G(z) for nz frequencies: out[k*n*n + b + a*n] (column-major blocks)
+  void green_function(const cplx *z, int nz, bool spin_down, cplx *out, Workspace &ws);
+  void self_energy(const cplx *z, int nz, bool spin_down, cplx *out, Workspace &ws);
+  void hybridization(const cplx *z, int nz, bool spin_down, cplx *out);
+  double potthoff(Workspace &ws);
+  std::string gs_string() const;
+  void set_hopping_matrix();
+
+ private:
+  void build_qmatrix(State &st, bool spin_down, Workspace &ws);
+  void build_cf(State &st, bool spin_down, Workspace &ws);
+  void compute_weights();
+  void green_average();
+  // fills phi = c^{pm}_{orb, spin} |psi> on the target sector of H
+  void apply_cdag(const State &st, int pm, int spin, int orb, const SectorOp &H, double *y,
+                  double coef, bool accumulate, Workspace &ws);
+};
+
+bool sector_is_valid(const Sector &s, int n_orb);
+Sector shift_sector(const Sector &s, int pm, int spin);
+
+}  // namespace qed

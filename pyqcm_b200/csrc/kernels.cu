@@ -1,0 +1,649 @@
+// sm_100a kernels of the ED solver (see kernels.cuh for the contracts).
+//
+// Layout in HBM: a sector vector is the dim_dn x dim_up matrix x[dn][up],
+// row-major (index up + dim_up * dn), the factorized basis order of the
+// reference (src_ed/ED_basis.cpp:142-165). Up-spin hops act along rows,
+// down-spin hops along columns. All arithmetic is FP64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "common.hpp"
+#include "kernels.cuh"
+
+namespace qed {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// C(n, k) for n, k <= 32 (C(32,16) < 2^32).
+__constant__ uint32_t c_binom[33][33];
+bool g_binom_ready = false;
+
+void ensure_binom() {
+  if (g_binom_ready) return;
+  uint32_t h[33][33] = {};
+  for (int n = 0; n <= 32; ++n)
+    for (int k = 0; k <= 32; ++k) h[n][k] = (uint32_t)binom(n, k);
+  QED_CUDA(cudaMemcpyToSymbol(c_binom, h, sizeof(h)));
+  g_binom_ready = true;
+}
+
+// Colex rank of an N-of-L string: sum_k C(p_k, k+1) over set bits p_0 < p_1 < ...
+// Equals the position in the ascending list of N-of-L strings, i.e.
+// ED_halfbasis::index (src_ed/ED_basis.cpp:130-135).
+__device__ __forceinline__ uint32_t colex_rank(uint32_t b) {
+  uint32_t r = 0;
+  int k = 1;
+  while (b) {
+    int p = __ffs(b) - 1;
+    r += c_binom[p][k++];
+    b &= b - 1;
+  }
+  return r;
+}
+
+__device__ __forceinline__ uint32_t colex_unrank(uint32_t I, int L, int N) {
+  uint32_t b = 0;
+  int p = L - 1;
+  for (int k = N; k >= 1; --k) {
+    while (c_binom[p][k] > I) --p;
+    b |= 1u << p;
+    I -= c_binom[p][k];
+    --p;
+  }
+  return b;
+}
+
+template <int NRED>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NRED], double *partials, int nred) {
+  __shared__ double sm[NRED > 0 ? NRED : 1][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NRED; ++i) {
+    double x = v[i];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sm[i][warp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < nred) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += sm[threadIdx.x][w];
+    partials[(size_t)blockIdx.x * Reducer::kMaxRed + threadIdx.x] = s;
+  }
+}
+
+__global__ void k_finalize(const double *partials, int nblocks, double *out) {
+  // one block per slot, fixed-order tree sum
+  __shared__ double sm[kThreads];
+  const int slot = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[(size_t)b * Reducer::kMaxRed + slot];
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[slot] = sm[0];
+}
+
+int grid_for(size_t n, int num_sms, int per_sm = 4) {
+  size_t g = (n + kThreads - 1) / kThreads;
+  size_t cap = (size_t)num_sms * per_sm;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+int device_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+// ---------------------------------------------------------------- basis ----
+
+__global__ void k_unrank(int L, int N, uint32_t dim, uint32_t *out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < dim; i += gridDim.x * blockDim.x)
+    out[i] = colex_unrank(i, L, N);
+}
+
+__global__ void k_rank(int L, int N, size_t n, const uint32_t *s, uint32_t *r) {
+  const uint32_t dim = c_binom[L][N];
+  const uint32_t lim = (L >= 32) ? 0xffffffffu : ((1u << L) - 1u);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t b = s[i];
+    r[i] = ((b & ~lim) == 0 && __popc(b) == N) ? colex_rank(b) : dim;
+  }
+}
+
+__device__ __forceinline__ uint32_t between_mask(int a, int b) {
+  int lo = a < b ? a : b, hi = a < b ? b : a;
+  uint64_t m = ((1ull << hi) - 1ull) & ~((2ull << lo) - 1ull);
+  return (uint32_t)m;
+}
+
+// One-body hops c^+_r c_c on every string (HS_half_operator ctor,
+// src_ed/Operators/HS_half_operator.hpp:17-45): allowed when bit c is set and
+// bit r empty; phase (-1)^(number of set bits strictly between r and c)
+// (binary_state::one_body / interphase, src_ed/binary_state.cpp:23-28,
+// src_ed/binary_state.hpp:42-47).
+__global__ void k_build_hops(int L, int N, uint32_t dim, const uint32_t *bits, int npairs,
+                             const int *pd, const int *ps, const int *pslot, uint8_t *cnt,
+                             uint32_t *ell, int width) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < dim; i += gridDim.x * blockDim.x) {
+    uint32_t b = bits[i];
+    int k = 0;
+    for (int q = 0; q < npairs; ++q) {
+      int r = pd[q], c = ps[q];
+      if (!((b >> c) & 1u) || ((b >> r) & 1u)) continue;
+      uint32_t nb = b ^ (1u << c) ^ (1u << r);
+      int sgn = __popc(nb & between_mask(r, c)) & 1;
+      uint32_t J = colex_rank(nb);
+      if (k < width) ell[(size_t)k * dim + i] = (J << 8) | (uint32_t)(pslot[q] + sgn);
+      ++k;
+    }
+    cnt[i] = (uint8_t)(k < width ? k : width);
+  }
+}
+
+__global__ void k_diag_half(int L, uint32_t dim, const uint32_t *bits, const double *tdiag,
+                            const double *vsame, double *diag) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < dim; i += gridDim.x * blockDim.x) {
+    uint32_t b = bits[i];
+    double s = 0.0;
+    for (int r = 0; r < L; ++r)
+      if ((b >> r) & 1u) {
+        s += tdiag[r];
+        for (int c = r; c < L; ++c)
+          if ((b >> c) & 1u) s += vsame[r * L + c];
+      }
+    diag[i] = s;
+  }
+}
+
+__global__ void k_cdag_gather(int L, int spin, int a, int pm, const uint32_t *tub, uint32_t du_t,
+                              const uint32_t *tdb, uint32_t dd_t, int src_nup, int src_ndn,
+                              uint32_t du_s, const double *psi, double *y, double coef, int acc) {
+  const size_t D = (size_t)du_t * dd_t;
+  const uint32_t bit = 1u << a, below = bit - 1u;
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
+    uint32_t u = (uint32_t)(I % du_t), d = (uint32_t)(I / du_t);
+    uint32_t tu = tub[u];
+    double val = 0.0;
+    if (spin == 0) {
+      bool occ = (tu & bit) != 0;
+      if (pm < 0 ? !occ : occ) {
+        uint32_t s = tu ^ bit;  // source up string
+        int ph = __popc((pm < 0 ? s : tu) & below) & 1;
+        size_t src = (size_t)colex_rank(s) + (size_t)du_s * d;
+        val = ph ? -psi[src] : psi[src];
+      }
+    } else {
+      uint32_t td = tdb[d];
+      bool occ = (td & bit) != 0;
+      if (pm < 0 ? !occ : occ) {
+        uint32_t s = td ^ bit;  // source dn string
+        int ph = (__popc((pm < 0 ? s : td) & below) + __popc(tu)) & 1;
+        size_t src = (size_t)u + (size_t)du_s * colex_rank(s);
+        val = ph ? -psi[src] : psi[src];
+      }
+    }
+    y[I] = (acc ? y[I] : 0.0) + coef * val;
+  }
+}
+
+// ------------------------------------------------------------------ H.v ----
+
+__device__ __forceinline__ double inter_term(const InterSpin &it, uint32_t up, uint32_t dn) {
+  if (it.mode == 1) return it.u * (double)__popc(up & dn);
+  double s = 0.0;
+  if (it.mode == 2) {
+    uint32_t w = up & dn;
+    while (w) {
+      int r = __ffs(w) - 1;
+      s += __ldg(it.v + r);
+      w &= w - 1;
+    }
+  } else if (it.mode == 3) {
+    uint32_t wd = dn;
+    while (wd) {
+      int r = __ffs(wd) - 1;
+      uint32_t wu = up;
+      while (wu) {
+        int c = __ffs(wu) - 1;
+        s += __ldg(it.v + r * it.n + c);
+        wu &= wu - 1;
+      }
+      wd &= wd - 1;
+    }
+  }
+  return s;
+}
+
+// Row pass: one CTA per dn row (grid-stride). The row of x is staged in shared
+// memory when it fits, so the up-spin gathers hit on-chip memory.
+template <bool SMEM>
+__global__ void __launch_bounds__(512) k_hv_rows(HvOperator op, const double *__restrict__ x,
+                                                  double xs, double *y, SubList sub) {
+  extern __shared__ double xsm[];
+  __shared__ double vals[256];
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  for (int i = threadIdx.x; i < op.up.nvals; i += blockDim.x) vals[i] = op.up.vals[i];
+  for (uint32_t d = blockIdx.x; d < dd; d += gridDim.x) {
+    const double *xr = x + (size_t)d * du;
+    if (SMEM) {
+      __syncthreads();
+      for (uint32_t u = threadIdx.x; u < du; u += blockDim.x) xsm[u] = xr[u];
+    }
+    __syncthreads();
+    const uint32_t dnb = op.dn.bits[d];
+    const double ddn = op.dn.diag[d];
+    for (uint32_t u = threadIdx.x; u < du; u += blockDim.x) {
+      const double diag = op.up.diag[u] + ddn + inter_term(op.inter, op.up.bits[u], dnb);
+      double acc = diag * (SMEM ? xsm[u] : xr[u]);
+      const int c = op.up.cnt[u];
+      for (int k = 0; k < c; ++k) {
+        const uint32_t e = __ldg(op.up.ell + (size_t)k * du + u);
+        acc += vals[e & 255u] * (SMEM ? xsm[e >> 8] : __ldg(xr + (e >> 8)));
+      }
+      const size_t I = (size_t)d * du + u;
+      acc *= xs;
+      for (int s = 0; s < sub.n; ++s) acc -= sub.c[s] * sub.z[s][I];
+      y[I] = acc;
+    }
+  }
+}
+
+// Column pass: work item = (column chunk, group of R rows), chunk-major so the
+// CTAs in flight share one chunk of columns and the down-spin gathers of x
+// rows hit L2. Each thread owns VEC adjacent columns.
+template <int VEC, int R>
+__global__ void __launch_bounds__(kThreads) k_hv_cols(HvOperator op, const double *__restrict__ x,
+                                                       double xs, double *y, int red_mask,
+                                                       double *partials) {
+  __shared__ double vals[256];
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  for (int i = threadIdx.x; i < op.dn.nvals; i += blockDim.x) vals[i] = op.dn.vals[i];
+  __syncthreads();
+  const uint32_t W = VEC * blockDim.x;
+  const uint32_t nchunk = (du + W - 1) / W, nrg = (dd + R - 1) / R;
+  const size_t nitems = (size_t)nchunk * nrg;
+  double red[3] = {0.0, 0.0, 0.0};
+  for (size_t t = blockIdx.x; t < nitems; t += gridDim.x) {
+    const uint32_t chunk = (uint32_t)(t / nrg), rg = (uint32_t)(t % nrg);
+    const uint32_t u0 = chunk * W + VEC * threadIdx.x;
+    if (u0 >= du) continue;
+    for (int rr = 0; rr < R; ++rr) {
+      const uint32_t d = rg * R + rr;
+      if (d >= dd) break;
+      const int c = op.dn.cnt[d];
+      const size_t base = (size_t)d * du + u0;
+      if (VEC == 2) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int k = 0; k < c; ++k) {
+          const uint32_t e = __ldg(op.dn.ell + (size_t)k * dd + d);
+          const double v = vals[e & 255u];
+          const double2 xv = __ldg(reinterpret_cast<const double2 *>(x + (size_t)(e >> 8) * du + u0));
+          acc.x += v * xv.x;
+          acc.y += v * xv.y;
+        }
+        double2 yv = *reinterpret_cast<double2 *>(y + base);
+        yv.x += xs * acc.x;
+        yv.y += xs * acc.y;
+        *reinterpret_cast<double2 *>(y + base) = yv;
+        if (red_mask) {
+          const double2 xv = __ldg(reinterpret_cast<const double2 *>(x + base));
+          red[0] += xs * (xv.x * yv.x + xv.y * yv.y);
+          red[1] += yv.x * yv.x + yv.y * yv.y;
+          red[2] += xs * xs * (xv.x * xv.x + xv.y * xv.y);
+        }
+      } else {
+        double acc = 0.0;
+        for (int k = 0; k < c; ++k) {
+          const uint32_t e = __ldg(op.dn.ell + (size_t)k * dd + d);
+          acc += vals[e & 255u] * __ldg(x + (size_t)(e >> 8) * du + u0);
+        }
+        const double yv = y[base] + xs * acc;
+        y[base] = yv;
+        if (red_mask) {
+          const double xv = x[base];
+          red[0] += xs * xv * yv;
+          red[1] += yv * yv;
+          red[2] += xs * xs * xv * xv;
+        }
+      }
+    }
+  }
+  if (red_mask) block_reduce_store<3>(red, partials, 3);
+}
+
+// --------------------------------------------------------- vector kernels ----
+
+template <int G>
+__global__ void k_dots(size_t D, double *x, double xs, int write_x, VecList ys, int first,
+                       double *partials) {
+  double acc[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) acc[g] = 0.0;
+  const int n = min(G, ys.n - first);
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
+    double xv = x[I] * xs;
+    if (write_x) x[I] = xv;
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+      if (g < n) acc[g] += xv * ys.v[first + g][I];
+  }
+  // store into slots first..first+n
+  __shared__ double sm[G][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
+    double v = acc[g];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sm[g][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < n) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += sm[threadIdx.x][w];
+    partials[(size_t)blockIdx.x * Reducer::kMaxRed + first + threadIdx.x] = s;
+  }
+}
+
+__global__ void k_multi_axpy(size_t D, const double *x, double xs, VecList ys, int norm_first,
+                             double *partials) {
+  double nrm[1] = {0.0};
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
+    const double xv = x[I] * xs;
+    for (int i = 0; i < ys.n; ++i) {
+      double v = ys.v[i][I] - ys.c[i] * xv;
+      ys.v[i][I] = v;
+      if (i == 0 && norm_first) nrm[0] += v * v;
+    }
+  }
+  if (norm_first) block_reduce_store<1>(nrm, partials, 1);
+}
+
+__global__ void k_axpby(size_t D, double a, double *y, double b, const double *x, int norm,
+                        double *partials) {
+  double nrm[1] = {0.0};
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
+    double v = (a != 0.0 ? a * y[I] : 0.0) + (x ? b * x[I] : 0.0);
+    y[I] = v;
+    nrm[0] += v * v;
+  }
+  if (norm) block_reduce_store<1>(nrm, partials, 1);
+}
+
+__global__ void k_swap_scale(size_t D, double *q, double *p, double beta) {
+  const double z = 1.0 / beta;
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
+    const double t = p[I];
+    p[I] = q[I] * z;
+    q[I] = -beta * t;
+  }
+}
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+__global__ void k_random(size_t D, uint64_t seed, double *y, double *partials) {
+  double nrm[1] = {0.0};
+  const uint64_t key = splitmix64(seed ^ 0x5eedull);
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
+    // Box-Muller on two 53-bit uniforms from a counter-based hash
+    uint64_t h1 = splitmix64(key + 2 * I), h2 = splitmix64(key + 2 * I + 1);
+    double u1 = ((h1 >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    double u2 = (h2 >> 11) * (1.0 / 9007199254740992.0);
+    double v = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+    y[I] = v;
+    nrm[0] += v * v;
+  }
+  block_reduce_store<1>(nrm, partials, 1);
+}
+
+__global__ void k_scale(size_t D, double *y, double a) {
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x)
+    y[I] *= a;
+}
+
+// -------------------------------------------------------- Green functions ----
+
+// G(z) of a Lehmann representation for a batch of frequencies: one CTA per
+// frequency; poles are streamed through shared memory in chunks.
+// (Q_matrix::Green_function + VDVH kernel, src_ed/Q_matrix.hpp:133-151,
+//  src_util/VDVH_kernel.cpp:28-36)
+__global__ void k_qmatrix_gf(int L, int M, const double *e, const double *V, int nz,
+                             const double *z, double *G) {
+  constexpr int CH = 64;
+  __shared__ double vs[64 * CH];
+  __shared__ double ur[CH], ui[CH];
+  const int k = blockIdx.x;
+  const double zr = z[2 * k], zi = z[2 * k + 1];
+  const int LL = L * L;
+  for (int pbase = 0; pbase < LL; pbase += blockDim.x) {
+    const int pidx = pbase + threadIdx.x;
+    const int a = pidx / L, b = pidx % L;
+    double gr = 0.0, gi = 0.0;
+    for (int i0 = 0; i0 < M; i0 += CH) {
+      const int nc = min(CH, M - i0);
+      __syncthreads();
+      for (int t = threadIdx.x; t < nc * L; t += blockDim.x) vs[t] = V[(size_t)i0 * L + t];
+      for (int t = threadIdx.x; t < nc; t += blockDim.x) {
+        double dr = zr - e[i0 + t], di = zi;
+        double den = dr * dr + di * di;
+        ur[t] = dr / den;
+        ui[t] = -di / den;
+      }
+      __syncthreads();
+      if (pidx < LL) {
+        for (int i = 0; i < nc; ++i) {
+          double w = vs[i * L + a] * vs[i * L + b];
+          gr += w * ur[i];
+          gi += w * ui[i];
+        }
+      }
+    }
+    if (pidx < LL) {
+      double *g = G + 2 * ((size_t)k * LL + b + (size_t)a * L);
+      g[0] += gr;
+      g[1] += gi;
+    }
+  }
+}
+
+// Jacobi continued fractions, backward recursion (continued_fraction::evaluate,
+// src_ed/continued_fraction.cpp:52-57); one thread per (fraction, frequency).
+__global__ void k_cf_eval(int nf, const int *off, const int *len, const double *a, const double *b,
+                          int nz, const double *z, double *F) {
+  const size_t n = (size_t)nf * nz;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const int f = (int)(t % nf), k = (int)(t / nf);
+    const double zr = z[2 * k], zi = z[2 * k + 1];
+    const int o = off[f];
+    double gr = 0.0, gi = 0.0;
+    for (int i = len[f] - 1; i >= 0; --i) {
+      // G = b_i / (z - a_i - G)
+      double dr = zr - a[o + i] - gr, di = zi - gi;
+      double den = dr * dr + di * di;
+      double bi = b[o + i];
+      gr = bi * dr / den;
+      gi = -bi * di / den;
+    }
+    F[2 * t] = gr;
+    F[2 * t + 1] = gi;
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ launchers ----
+
+void launch_unrank(int L, int N, uint32_t dim, uint32_t *out, cudaStream_t s) {
+  ensure_binom();
+  k_unrank<<<grid_for(dim, device_sms()), kThreads, 0, s>>>(L, N, dim, out);
+  QED_LAUNCH();
+}
+
+void launch_rank(int L, int N, size_t n, const uint32_t *strings, uint32_t *ranks, cudaStream_t s) {
+  ensure_binom();
+  k_rank<<<grid_for(n, device_sms()), kThreads, 0, s>>>(L, N, n, strings, ranks);
+  QED_LAUNCH();
+}
+
+void launch_build_hops(int L, int N, uint32_t dim, const uint32_t *bits, int npairs,
+                       const int *pd, const int *ps, const int *pslot, uint8_t *cnt, uint32_t *ell,
+                       int width, cudaStream_t s) {
+  ensure_binom();
+  k_build_hops<<<grid_for(dim, device_sms()), kThreads, 0, s>>>(L, N, dim, bits, npairs, pd, ps,
+                                                                 pslot, cnt, ell, width);
+  QED_LAUNCH();
+}
+
+void launch_diag_half(int L, uint32_t dim, const uint32_t *bits, const double *tdiag,
+                      const double *vsame, double *diag, cudaStream_t s) {
+  k_diag_half<<<grid_for(dim, device_sms()), kThreads, 0, s>>>(L, dim, bits, tdiag, vsame, diag);
+  QED_LAUNCH();
+}
+
+void launch_cdag_gather(int L, int spin, int a, int pm, const uint32_t *tub, uint32_t du_t,
+                        const uint32_t *tdb, uint32_t dd_t, int src_nup, int src_ndn, uint32_t du_s,
+                        const double *psi, double *y, double coef, int accumulate, cudaStream_t s) {
+  ensure_binom();
+  size_t D = (size_t)du_t * dd_t;
+  k_cdag_gather<<<grid_for(D, device_sms(), 8), kThreads, 0, s>>>(
+      L, spin, a, pm, tub, du_t, tdb, dd_t, src_nup, src_ndn, du_s, psi, y, coef, accumulate);
+  QED_LAUNCH();
+}
+
+namespace {
+constexpr size_t kRowSmemMax = 112 * 1024;
+}
+
+void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,
+                    const SubList &sub, cudaStream_t s) {
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const size_t smem = (size_t)du * sizeof(double);
+  int threads = du >= 512 ? 512 : (du >= 256 ? 256 : 128);
+  if (smem <= kRowSmemMax) {
+    static bool attr = false;
+    if (!attr) {
+      QED_CUDA(cudaFuncSetAttribute(k_hv_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kRowSmemMax));
+      attr = true;
+    }
+    int per_sm = smem > 100 * 1024 ? 2 : 4;
+    int grid = (int)std::min<size_t>(dd, (size_t)device_sms() * per_sm);
+    k_hv_rows<true><<<grid, threads, smem, s>>>(op, x, xs, y, sub);
+  } else {
+    int grid = (int)std::min<size_t>(dd, (size_t)device_sms() * 4);
+    k_hv_rows<false><<<grid, threads, 0, s>>>(op, x, xs, y, sub);
+  }
+  QED_LAUNCH();
+}
+
+int launch_hv_cols(const HvOperator &op, const double *x, double xs, double *y, int red_mask,
+                   Reducer &r, cudaStream_t s) {
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const int R = 4;
+  const bool vec2 = (du % 2 == 0);
+  const uint32_t W = (vec2 ? 2 : 1) * kThreads;
+  size_t nitems = (size_t)((du + W - 1) / W) * ((dd + R - 1) / R);
+  int grid = (int)std::min<size_t>(nitems, (size_t)device_sms() * 8);
+  if (red_mask && grid > r.max_blocks) grid = r.max_blocks;
+  if (vec2)
+    k_hv_cols<2, R><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
+  else
+    k_hv_cols<1, R><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
+  QED_LAUNCH();
+  return grid;
+}
+
+int launch_dots(size_t D, double *x, double xs, int write_x, const VecList &ys, Reducer &r,
+                cudaStream_t s) {
+  int grid = std::min(grid_for(D, device_sms(), 4), r.max_blocks);
+  constexpr int G = 8;
+  if (ys.n == 0 && write_x) {
+    k_scale<<<grid, kThreads, 0, s>>>(D, x, xs);
+    QED_LAUNCH();
+    return grid;
+  }
+  for (int first = 0; first < ys.n; first += G) {
+    // x is scaled in place only on the first sweep; later sweeps read the scaled x.
+    const bool wx = write_x && first == 0;
+    const double sc = (write_x && first > 0) ? 1.0 : xs;
+    k_dots<G><<<grid, kThreads, 0, s>>>(D, x, sc, wx, ys, first, r.partials);
+    QED_LAUNCH();
+  }
+  return grid;
+}
+
+int launch_multi_axpy(size_t D, const double *x, double xs, const VecList &ys, int norm_first,
+                      Reducer &r, cudaStream_t s) {
+  int grid = std::min(grid_for(D, device_sms(), 4), r.max_blocks);
+  k_multi_axpy<<<grid, kThreads, 0, s>>>(D, x, xs, ys, norm_first, r.partials);
+  QED_LAUNCH();
+  return grid;
+}
+
+int launch_axpby(size_t D, double a, double *y, double b, const double *x, int norm, Reducer &r,
+                 cudaStream_t s) {
+  int grid = std::min(grid_for(D, device_sms(), 4), r.max_blocks);
+  k_axpby<<<grid, kThreads, 0, s>>>(D, a, y, b, x, norm, r.partials);
+  QED_LAUNCH();
+  return grid;
+}
+
+void launch_swap_scale(size_t D, double *q, double *p, double beta, cudaStream_t s) {
+  k_swap_scale<<<grid_for(D, device_sms(), 4), kThreads, 0, s>>>(D, q, p, beta);
+  QED_LAUNCH();
+}
+
+int launch_random(size_t D, uint64_t seed, double *y, Reducer &r, cudaStream_t s) {
+  int grid = std::min(grid_for(D, device_sms(), 4), r.max_blocks);
+  k_random<<<grid, kThreads, 0, s>>>(D, seed, y, r.partials);
+  QED_LAUNCH();
+  return grid;
+}
+
+void launch_scale(size_t D, double *y, double a, cudaStream_t s) {
+  k_scale<<<grid_for(D, device_sms(), 4), kThreads, 0, s>>>(D, y, a);
+  QED_LAUNCH();
+}
+
+void finalize_sums(Reducer &r, int nblocks, int nred, cudaStream_t s) {
+  k_finalize<<<nred, kThreads, 0, s>>>(r.partials, nblocks, r.out);
+  QED_LAUNCH();
+  QED_CUDA(cudaMemcpyAsync(r.host, r.out, nred * sizeof(double), cudaMemcpyDeviceToHost, s));
+}
+
+void launch_qmatrix_gf(int L, int M, const double *e, const double *V, int nz, const double *z,
+                       double *G, cudaStream_t s) {
+  if (nz <= 0 || M <= 0) return;
+  if (L > 64) fail(QED_ERR_UNSUPPORTED, "Green function dimension above 64");
+  k_qmatrix_gf<<<nz, kThreads, 0, s>>>(L, M, e, V, nz, z, G);
+  QED_LAUNCH();
+}
+
+void launch_cf_eval(int nf, const int *off, const int *len, const double *a, const double *b,
+                    int nz, const double *z, double *F, cudaStream_t s) {
+  if (nf <= 0 || nz <= 0) return;
+  size_t n = (size_t)nf * nz;
+  k_cf_eval<<<grid_for(n, device_sms(), 8), kThreads, 0, s>>>(nf, off, len, a, b, nz, z, F);
+  QED_LAUNCH();
+}
+
+}  // namespace qed

@@ -1,0 +1,122 @@
+// Launch wrappers of the sm_100a kernels of the ED solver. Host C++ code calls
+// these; every wrapper enqueues on the given stream and checks the launch.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace qed {
+
+constexpr int kMaxVec = 64;  // vectors per multi-vector kernel call
+
+// Device view of one spin species' basis and hopping table (ELL layout):
+//   bits[i]            i-th N-of-L string in ascending order (ED_halfbasis::bin)
+//   cnt[i]             number of hops out of string i
+//   ell[k*dim + i]     (target index << 8) | value slot   for k < cnt[i]
+//   vals[slot]         signed hopping amplitude (sign of the fermion phase folded in)
+//   diag[i]            one-body diagonal + same-spin density-density terms of string i
+struct SpinTable {
+  const uint32_t *bits = nullptr;
+  const uint8_t *cnt = nullptr;
+  const uint32_t *ell = nullptr;
+  const double *vals = nullptr;
+  const double *diag = nullptr;
+  uint32_t dim = 0;
+  int nvals = 0;
+};
+
+// Inter-spin density-density terms sum_{r,s} v[r][s] dn_r up_s.
+//   mode 0: none; 1: diagonal and uniform (u * popc(up & dn));
+//   mode 2: diagonal per site (vdiag[r]); 3: general n x n (vfull, row r = dn bit).
+struct InterSpin {
+  int mode = 0;
+  int n = 0;
+  double u = 0.0;
+  const double *v = nullptr;  // device: n (mode 2) or n*n (mode 3)
+};
+
+struct HvOperator {
+  SpinTable up, dn;
+  InterSpin inter;
+  int num_sms = 148;
+};
+
+// List of (coefficient, vector) pairs subtracted in the row pass epilogue:
+// y -= sum_k c[k] * z[k].
+struct SubList {
+  int n = 0;
+  double c[32];
+  const double *z[32];
+};
+
+// Deterministic two-stage reductions: kernels write per-block partial sums,
+// finalize_sums adds them in a fixed order into out[0..nred).
+struct Reducer {
+  double *partials = nullptr;  // [max_blocks * kMaxRed]
+  double *out = nullptr;       // [kMaxRed] device
+  double *host = nullptr;      // [kMaxRed] pinned
+  int max_blocks = 0;
+  static constexpr int kMaxRed = 72;
+};
+
+// ---- basis -----------------------------------------------------------------
+void launch_unrank(int L, int N, uint32_t dim, uint32_t *out, cudaStream_t s);
+void launch_rank(int L, int N, size_t n, const uint32_t *strings, uint32_t *ranks, cudaStream_t s);
+// Builds the ELL hop table of one spin species on the device. pairs: directed
+// (dst, src) orbital pairs with the value slot of the + sign (slot ^ 1 holds -t).
+void launch_build_hops(int L, int N, uint32_t dim, const uint32_t *bits, int npairs,
+                       const int *pair_dst, const int *pair_src, const int *pair_slot,
+                       uint8_t *cnt, uint32_t *ell, int width, cudaStream_t s);
+void launch_diag_half(int L, uint32_t dim, const uint32_t *bits, const double *tdiag,
+                      const double *vsame, double *diag, cudaStream_t s);
+// c_a / c^+_a gathered onto the target sector (Destroy, src_ed/ED_basis.cpp:79-110)
+void launch_cdag_gather(int L, int spin, int a, int pm, const uint32_t *tgt_up_bits,
+                        uint32_t du_t, const uint32_t *tgt_dn_bits, uint32_t dd_t, int src_nup,
+                        int src_ndn, uint32_t du_s, const double *psi, double *y, double coef,
+                        int accumulate, cudaStream_t s);
+
+// ---- H.v ------------------------------------------------------------------
+// Row pass: y = (diag + up hops) x - sum_k sub.c[k] sub.z[k]   (x scaled by xs)
+void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,
+                    const SubList &sub, cudaStream_t s);
+// Column pass: y += xs * (dn hops) x ; optional reductions into red slots:
+//   red_mask bit0: sum x*y, bit1: sum y*y, bit2: sum x*x   (post-update y)
+int launch_hv_cols(const HvOperator &op, const double *x, double xs, double *y, int red_mask,
+                    Reducer &r, cudaStream_t s);
+
+// ---- vector kernels -------------------------------------------------------
+struct VecList {
+  int n = 0;
+  double *v[kMaxVec];
+  double c[kMaxVec];
+};
+// out[i] = sum (xs*x) . y_i  (y_i = list.v[i]); if write_x, x *= xs in place.
+int launch_dots(size_t D, double *x, double xs, int write_x, const VecList &ys, Reducer &r,
+                 cudaStream_t s);
+// y_i -= c_i * (xs*x); if norm_first, out[0] = |y_0|^2 after the update.
+int launch_multi_axpy(size_t D, const double *x, double xs, const VecList &ys, int norm_first,
+                       Reducer &r, cudaStream_t s);
+// y = a*y + b*x ; optional out[0] = |y|^2 (post)
+int launch_axpby(size_t D, double a, double *y, double b, const double *x, int norm, Reducer &r,
+                  cudaStream_t s);
+// LanczosGreen swap: p <- q/beta ; q <- -beta p_old   (src_util/vector_num.hpp:274-282)
+void launch_swap_scale(size_t D, double *q, double *p, double beta, cudaStream_t s);
+// y = seeded normal random entries (counter-based), out[0] = |y|^2
+int launch_random(size_t D, uint64_t seed, double *y, Reducer &r, cudaStream_t s);
+void launch_scale(size_t D, double *y, double a, cudaStream_t s);
+// Reduction kernels return their block count; finalize_sums adds the per-block
+// partials of `nred` slots in a fixed order into r.out and copies them to
+// r.host (the caller synchronises the stream before reading r.host).
+void finalize_sums(Reducer &r, int nblocks, int nred, cudaStream_t s);
+
+// ---- Green functions on a frequency grid ----------------------------------
+// G[k][b + a*L] += sum_i V[a + i*L] V[b + i*L] / (z_k - e_i)   (real V, L <= 64)
+void launch_qmatrix_gf(int L, int M, const double *e, const double *V, int nz, const double *z,
+                       double *G, cudaStream_t s);
+// Continued fractions: F[k][f] = b_f[0] / (z_k - a_f[0] - b_f[1] / (z_k - ...)), for nf
+// fractions with offsets off[f] into a/b and lengths len[f].
+void launch_cf_eval(int nf, const int *off, const int *len, const double *a, const double *b,
+                    int nz, const double *z, double *F, cudaStream_t s);
+
+}  // namespace qed

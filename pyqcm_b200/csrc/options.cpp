@@ -1,0 +1,103 @@
+// Global options (see options.hpp). Defaults follow src_util/global_parameter.cpp:10-92.
+#include "options.hpp"
+
+#include <map>
+#include <mutex>
+
+#include "common.hpp"
+
+namespace qed {
+
+namespace {
+
+struct Table {
+  std::map<std::string, bool> b;
+  std::map<std::string, long> i;
+  std::map<std::string, double> d;
+  std::map<std::string, char> c;
+  std::mutex m;
+  Table() {
+    // ED options that drive this solver
+    b["check_lanczos_residual"] = false;
+    b["no_degenerate_BL"] = false;
+    b["continued_fraction"] = false;
+    b["verb_ED"] = false;
+    b["verb_Hilbert"] = false;
+    b["verb_warning"] = false;
+    b["parallel_sectors"] = false;
+    b["merge_states"] = false;
+    b["combine_mcf"] = false;
+    b["block_Lanczos_QR"] = false;
+    b["nosym"] = false;
+    b["print_Hamiltonian"] = false;
+    b["strip_anomalous_self"] = false;
+    b["print_variances"] = false;
+    d["accur_band_lanczos"] = 1e-12;
+    d["accur_continued_fraction"] = 0.01;
+    d["accur_Davidson"] = 1.0e-5;
+    d["accur_deflation"] = 1e-7;
+    d["accur_lanczos"] = 1e-12;
+    d["accur_Q_matrix"] = 1.0e-5;
+    d["band_lanczos_minimum_gap"] = 1e-5;
+    d["minimum_weight"] = 0.01;
+    d["Qmatrix_wtol"] = 1.0e-5;
+    d["Qmatrix_vtol"] = 1.0e-10;
+    d["temperature"] = 0.0;
+    i["n_states"] = 1;
+    i["max_dim_print"] = 64;
+    i["max_dim_full"] = 256;
+    i["max_iter_BL"] = 600;
+    i["max_iter_CF"] = 400;
+    i["max_iter_lanczos"] = 1000;
+    i["seed"] = 0;
+    i["GF_lookup_depth"] = 64;
+    c["Hamiltonian_format"] = 'E';
+    c["Ground_state_method"] = 'L';
+    c["GF_method"] = 'L';
+    // lattice-layer options: accepted, unused here
+    for (auto s : {"dual_basis", "periodic", "periodized_averages", "zero_dim", "print_all",
+                   "compact_tiling_per_site", "use_pcubature", "verb_integrals"})
+      b[s] = false;
+    d["eta"] = 0.0001;
+    d["small_scale"] = 0.5;
+    d["cutoff_scale"] = 1.0e12;
+    d["accur_OP"] = 1e-4;
+    d["large_scale"] = 20;
+    d["accur_SEF"] = 5e-8;
+    d["cdmft_jacobian_delta"] = 1.0e-5;
+    i["kgrid_side"] = 32;
+    i["max_iter_QN"] = 60;
+    i["print_precision"] = 9;
+    c["periodization"] = 'G';
+  }
+};
+
+Table &T() {
+  static Table t;
+  return t;
+}
+
+template <class M> typename M::mapped_type get(M &m, const std::string &name) {
+  auto it = m.find(name);
+  if (it == m.end()) fail(QED_ERR_ARGUMENT, "global parameter " + name + " does not exist.");
+  return it->second;
+}
+template <class M, class V> void put(M &m, const std::string &name, V v) {
+  auto it = m.find(name);
+  if (it == m.end()) fail(QED_ERR_ARGUMENT, "global parameter " + name + " does not exist.");
+  it->second = v;
+}
+
+}  // namespace
+
+bool opt_bool(const std::string &n) { std::lock_guard<std::mutex> l(T().m); return get(T().b, n); }
+long opt_int(const std::string &n) { std::lock_guard<std::mutex> l(T().m); return get(T().i, n); }
+double opt_double(const std::string &n) { std::lock_guard<std::mutex> l(T().m); return get(T().d, n); }
+char opt_char(const std::string &n) { std::lock_guard<std::mutex> l(T().m); return get(T().c, n); }
+
+void set_opt_bool(const std::string &n, bool v) { std::lock_guard<std::mutex> l(T().m); put(T().b, n, v); }
+void set_opt_int(const std::string &n, long v) { std::lock_guard<std::mutex> l(T().m); put(T().i, n, v); }
+void set_opt_double(const std::string &n, double v) { std::lock_guard<std::mutex> l(T().m); put(T().d, n, v); }
+void set_opt_char(const std::string &n, char v) { std::lock_guard<std::mutex> l(T().m); put(T().c, n, v); }
+
+}  // namespace qed

@@ -1,0 +1,478 @@
+// Device sector Hamiltonian and Krylov drivers (see solver.hpp).
+#include "solver.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+
+#include "eigen.hpp"
+#include "options.hpp"
+
+namespace qed {
+
+// ---------------------------------------------------------------- Workspace --
+
+Workspace::Workspace() {
+  QED_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  red.max_blocks = 4096;
+  partials.alloc((size_t)red.max_blocks * Reducer::kMaxRed);
+  out.alloc(Reducer::kMaxRed);
+  QED_CUDA(cudaMallocHost(&host, Reducer::kMaxRed * sizeof(double)));
+  red.partials = partials.p;
+  red.out = out.p;
+  red.host = host;
+}
+
+Workspace::~Workspace() {
+  if (host) cudaFreeHost(host);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+const double *Workspace::sums(int nblocks, int nred) {
+  finalize_sums(red, nblocks, nred, stream);
+  sync();
+  return host;
+}
+
+void Workspace::sync() { QED_CUDA(cudaStreamSynchronize(stream)); }
+
+// ------------------------------------------------------------- SectorOp ------
+
+namespace {
+
+constexpr double kSmall = 1.0e-12;  // SMALL_VALUE (src_util/vector_num.hpp:23)
+
+void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
+                const std::vector<double> &vsame, Workspace &ws) {
+  h.L = L;
+  h.N = N;
+  uint64_t dim = (N < 0 || N > L) ? 0 : binom(L, N);
+  if (dim >= (1ull << 24)) fail(QED_ERR_UNSUPPORTED, "half basis dimension above 2^24");
+  h.dim = (uint32_t)dim;
+  if (!dim) return;
+  h.bits.alloc(dim);
+  launch_unrank(L, N, h.dim, h.bits.p, ws.stream);
+  // directed hop pairs (dst r, src c) with value slots; value table dedupes |t|
+  std::vector<int> pd, ps, pslot;
+  std::vector<double> vals;
+  std::map<double, int> slot_of;
+  for (int r = 0; r < L; ++r)
+    for (int c = 0; c < L; ++c) {
+      if (r == c) continue;
+      double v = t[(size_t)r * L + c];
+      if (std::fabs(v) < kSmall) continue;
+      auto it = slot_of.find(v);
+      int slot;
+      if (it == slot_of.end()) {
+        slot = (int)vals.size();
+        vals.push_back(v);
+        vals.push_back(-v);
+        slot_of[v] = slot;
+      } else {
+        slot = it->second;
+      }
+      pd.push_back(r);
+      ps.push_back(c);
+      pslot.push_back(slot);
+    }
+  if (vals.size() > 256) fail(QED_ERR_UNSUPPORTED, "more than 128 distinct hopping amplitudes per spin");
+  int width = std::min<int>((int)pd.size(), N * (L - N));
+  if (width > 255) fail(QED_ERR_UNSUPPORTED, "more than 255 hops per basis string");
+  h.width = width;
+  h.nvals = (int)vals.size();
+  h.cnt.alloc(dim);
+  h.vals.alloc(std::max<size_t>(vals.size(), 1));
+  if (!vals.empty()) h.vals.upload(vals, ws.stream);
+  if (width > 0) {
+    h.ell.alloc((size_t)width * dim);
+    DevBuf<int> dpd(pd.size()), dps(ps.size()), dsl(pslot.size());
+    dpd.upload(pd, ws.stream);
+    dps.upload(ps, ws.stream);
+    dsl.upload(pslot, ws.stream);
+    launch_build_hops(L, N, h.dim, h.bits.p, (int)pd.size(), dpd.p, dps.p, dsl.p, h.cnt.p, h.ell.p,
+                      width, ws.stream);
+    ws.sync();  // the pair arrays are freed on scope exit
+  } else {
+    QED_CUDA(cudaMemsetAsync(h.cnt.p, 0, dim, ws.stream));
+  }
+  std::vector<double> tdiag(L);
+  for (int r = 0; r < L; ++r) tdiag[r] = t[(size_t)r * L + r];
+  DevBuf<double> dt(L), dv(vsame.size());
+  dt.upload(tdiag, ws.stream);
+  dv.upload(vsame, ws.stream);
+  h.diag.alloc(dim);
+  launch_diag_half(L, h.dim, h.bits.p, dt.p, dv.p, h.diag.p, ws.stream);
+  h.hbits.resize(dim);
+  h.bits.download(h.hbits.data(), dim, ws.stream);
+  ws.sync();
+}
+
+SpinTable view(const HalfTables &h) {
+  SpinTable s;
+  s.bits = h.bits.p;
+  s.cnt = h.cnt.p;
+  s.ell = h.ell.p;
+  s.vals = h.vals.p;
+  s.diag = h.diag.p;
+  s.dim = h.dim;
+  s.nvals = h.nvals;
+  return s;
+}
+
+}  // namespace
+
+SectorOp::SectorOp(const SpinData &t, const Sector &s, Workspace &ws) : sec(s), L(t.n) {
+  if (s.N >= Sector::odd || s.S >= Sector::odd)
+    fail(QED_ERR_UNSUPPORTED, "sector " + s.name() + " does not conserve N and S");
+  if ((s.N + s.S) % 2) fail(QED_ERR_ARGUMENT, "sector " + s.name() + " is not valid");
+  if (L > 32) fail(QED_ERR_UNSUPPORTED, "more than 32 orbitals per spin");
+  build_half(up, L, s.Nup(), t.t_up, t.v_uu, ws);
+  build_half(dn, L, s.Ndw(), t.t_dn, t.v_dd, ws);
+  D = (size_t)up.dim * dn.dim;
+  // inter-spin density-density terms
+  const int n = L;
+  bool any = false, offdiag = false;
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < n; ++c)
+      if (t.v_du[(size_t)r * n + c] != 0.0) {
+        any = true;
+        if (r != c) offdiag = true;
+      }
+  op.inter.n = n;
+  if (!any) {
+    op.inter.mode = 0;
+  } else if (!offdiag) {
+    double u0 = t.v_du[0];
+    bool uniform = true;
+    for (int r = 0; r < n; ++r)
+      if (t.v_du[(size_t)r * n + r] != u0) uniform = false;
+    if (uniform) {
+      op.inter.mode = 1;
+      op.inter.u = u0;
+    } else {
+      std::vector<double> dg(n);
+      for (int r = 0; r < n; ++r) dg[r] = t.v_du[(size_t)r * n + r];
+      vinter.upload(dg, ws.stream);
+      op.inter.mode = 2;
+      op.inter.v = vinter.p;
+    }
+  } else {
+    vinter.upload(t.v_du, ws.stream);
+    op.inter.mode = 3;
+    op.inter.v = vinter.p;
+  }
+  op.up = view(up);
+  op.dn = view(dn);
+  int dev = 0;
+  QED_CUDA(cudaGetDevice(&dev));
+  QED_CUDA(cudaDeviceGetAttribute(&op.num_sms, cudaDevAttrMultiProcessorCount, dev));
+  ws.sync();
+}
+
+void SectorOp::apply(const double *x, double *y, Workspace &ws) const {
+  if (!D) return;
+  SubList none;
+  launch_hv_rows(op, x, 1.0, y, none, ws.stream);
+  launch_hv_cols(op, x, 1.0, y, 0, ws.red, ws.stream);
+}
+
+// ------------------------------------------------------ Lanczos (ground state) --
+
+LanczosResult lanczos_ground_state(const SectorOp &H, Workspace &ws, DevBuf<double> &psi,
+                                   uint64_t seed) {
+  LanczosResult res;
+  const size_t D = H.D;
+  const double accur = opt_double("accur_lanczos");
+  const long max_iter = opt_int("max_iter_lanczos");
+  cudaStream_t s = ws.stream;
+  DevBuf<double> A(D), B(D), C(D), S(D);
+  // random start vector, normalised (Hamiltonian::states -> random(), src_util/vector_num.cpp:114-119)
+  int nb = launch_random(D, seed, B.p, ws.red, s);
+  double n2 = ws.sums(nb, 1)[0];
+  launch_scale(D, B.p, 1.0 / std::sqrt(n2), s);
+  QED_CUDA(cudaMemcpyAsync(S.p, B.p, D * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  double *pa = A.p, *pb = B.p, *pc = C.p;
+  std::vector<double> &alpha = res.alpha, &beta = res.beta;
+  double ritz = 2.0 * accur;
+  double lambda0 = 0.0;
+  while (ritz > accur) {
+    // w = H v_j - beta_{j-1} v_{j-1}
+    SubList sub;
+    if (!beta.empty()) {
+      sub.n = 1;
+      sub.c[0] = beta.back();
+      sub.z[0] = pa;
+    }
+    launch_hv_rows(H.op, pb, 1.0, pc, sub, s);
+    nb = launch_hv_cols(H.op, pb, 1.0, pc, 1, ws.red, s);
+    const double a = ws.sums(nb, 1)[0];  // alpha_j = <v_j, w>
+    nb = launch_axpby(D, 1.0, pc, -a, pb, 1, ws.red, s);
+    const double b = std::sqrt(ws.sums(nb, 1)[0]);  // beta_j = |w - alpha_j v_j|
+    alpha.push_back(a);
+    beta.push_back(b);
+    double last = 1.0;
+    if (!tridiag_lowest_last((int)alpha.size(), alpha.data(), beta.data(), &lambda0, &last))
+      fail(QED_ERR_LANCZOS, "tridiagonal eigensolver did not converge");
+    ritz = std::fabs(last * b);
+    if ((long)alpha.size() > max_iter)
+      fail(QED_ERR_LANCZOS, "Lanczos procedure exceeded " + std::to_string(max_iter) + " iterations");
+    if (ritz > accur) {
+      launch_scale(D, pc, 1.0 / b, s);  // v_{j+1}
+      std::swap(pa, pb);                // v_{j-1} <- v_j
+      std::swap(pb, pc);                // v_j <- v_{j+1}
+    }
+  }
+  res.energy = lambda0;
+  res.iterations = (int)alpha.size();
+  // eigenvector pass (LanczosEigenvector, src_ed/Hamiltonian/Lanczos.hpp:109-143)
+  const int M = (int)alpha.size();
+  std::vector<double> d(alpha), e(beta), Z;
+  if (!tridiag_eig(M, d, e, &Z)) fail(QED_ERR_LANCZOS, "tridiagonal eigensolver did not converge");
+  psi.alloc(D);
+  QED_CUDA(cudaMemcpyAsync(B.p, S.p, D * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  launch_axpby(D, 0.0, psi.p, Z[0], B.p, 0, ws.red, s);
+  pa = A.p;
+  pb = B.p;
+  pc = C.p;
+  for (int j = 1; j < M; ++j) {
+    SubList sub;
+    sub.n = 1;
+    sub.c[0] = alpha[j - 1];
+    sub.z[0] = pb;
+    if (j >= 2) {
+      sub.n = 2;
+      sub.c[1] = beta[j - 2];
+      sub.z[1] = pa;
+    }
+    launch_hv_rows(H.op, pb, 1.0, pc, sub, s);
+    launch_hv_cols(H.op, pb, 1.0, pc, 0, ws.red, s);
+    launch_scale(D, pc, 1.0 / beta[j - 1], s);
+    launch_axpby(D, 1.0, psi.p, Z[j], pc, 0, ws.red, s);
+    std::swap(pa, pb);
+    std::swap(pb, pc);
+  }
+  ws.sync();
+  return res;
+}
+
+// ------------------------------------------------------------ LanczosGreen --
+
+void lanczos_green(const SectorOp &H, Workspace &ws, double *psi, double *q,
+                   std::vector<double> &a, std::vector<double> &b) {
+  const size_t D = H.D;
+  const double accur = opt_double("accur_continued_fraction");
+  const size_t max_iter = (size_t)opt_int("max_iter_CF");
+  cudaStream_t s = ws.stream;
+  a.clear();
+  b.assign(1, 1.0);
+  QED_CUDA(cudaMemsetAsync(q, 0, D * sizeof(double), s));
+  double prod = 1.0;
+  while (prod > accur && std::fabs(b.back()) > accur && a.size() < max_iter) {
+    if (!a.empty()) launch_swap_scale(D, q, psi, b.back(), s);
+    SubList sub;  // q <- H psi + q  (row pass subtracts -1 * q in place)
+    sub.n = 1;
+    sub.c[0] = -1.0;
+    sub.z[0] = q;
+    launch_hv_rows(H.op, psi, 1.0, q, sub, s);
+    int nb = launch_hv_cols(H.op, psi, 1.0, q, 1, ws.red, s);
+    const double z = ws.sums(nb, 1)[0];
+    a.push_back(z);
+    nb = launch_axpby(D, 1.0, q, -z, psi, 1, ws.red, s);
+    const double zz = std::sqrt(ws.sums(nb, 1)[0]);
+    b.push_back(zz);
+    prod *= std::fabs(zz);
+  }
+}
+
+// ------------------------------------------------------------ band Lanczos --
+
+namespace {
+
+// Pool of device vectors of one length, recycled by slot index.
+struct VecPool {
+  size_t D;
+  std::vector<DevBuf<double>> bufs;
+  std::vector<int> free_list;
+  explicit VecPool(size_t d) : D(d) {}
+  int get() {
+    if (!free_list.empty()) {
+      int k = free_list.back();
+      free_list.pop_back();
+      return k;
+    }
+    bufs.emplace_back(D);
+    return (int)bufs.size() - 1;
+  }
+  void put(int k) {
+    if (k >= 0) free_list.push_back(k);
+  }
+  double *p(int k) { return bufs[k].p; }
+};
+
+}  // namespace
+
+bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
+                          std::vector<double> &evals, std::vector<double> &Q, int &Mout) {
+  const size_t D = H.D;
+  const int p = (int)phi.size();
+  cudaStream_t s = ws.stream;
+  if (D == 0 || p == 0) {
+    Mout = 0;
+    return false;
+  }
+  // number of iterations (Hamiltonian::build_Q_matrix, Hamiltonian_base.hpp:236-239)
+  int M0 = (int)(14 * p * std::log(1.0 * D));
+  if (!(M0 > 1)) fail(QED_ERR_INTERNAL, "Assertion failed: M>1 in build_Q_matrix");
+  const double accur_deflation = opt_double("accur_deflation");
+  double accur_bl = opt_double("accur_band_lanczos");
+  if (accur_bl < 0.0) accur_bl = 0.0;
+  const long max_iter_BL = opt_int("max_iter_BL");
+  const double min_gap = opt_double("band_lanczos_minimum_gap");
+  const bool no_degenerate = opt_bool("no_degenerate_BL");
+  // bandLanczos (src_ed/Hamiltonian/Lanczos.hpp:214-395)
+  int pc = p;
+  if (M0 > max_iter_BL) M0 = (int)max_iter_BL;
+  int M0p = (M0 / p + 1) * p;
+  M0 = M0p - pc;
+  VecPool pool(D);
+  std::vector<int> v(M0p + 1, -1);  // slot of Lanczos vector j
+  std::vector<double> t((size_t)M0 * M0, 0.0);
+  auto T = [&](int r, int c) -> double & { return t[(size_t)r + (size_t)M0 * c]; };
+  std::vector<double> P((size_t)p * std::max(M0, 1), 0.0);
+  std::vector<int> def(M0 + 1, 0), I;
+  for (int i = 0; i < p; ++i) {
+    v[i] = pool.get();
+    QED_CUDA(cudaMemcpyAsync(pool.p(v[i]), phi[i].p, D * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  }
+  bool phi_alive = true;
+  double ev_old = 1e12;
+  int j = 0;
+  int nd = 0;
+  VecList ys;
+  for (j = 0; j < M0; ++j) {
+    if (phi_alive && j >= p) {  // P(k, j) is only used for j < p (Q = P U over k < p)
+      for (auto &f : phi) f.release();
+      phi_alive = false;
+    }
+    // step (3): z = |v_j|
+    ys.n = 1;
+    ys.v[0] = pool.p(v[j]);
+    int nb = launch_dots(D, pool.p(v[j]), 1.0, 0, ys, ws.red, s);
+    const double z = std::sqrt(ws.sums(nb, 1)[0]);
+    if (z < accur_deflation) {  // step (4): deflation
+      if (j >= pc) {
+        I.push_back(j - pc);
+        def[j - pc] = 1;
+        nd++;
+      }
+      pc--;
+      if (pc == 0) break;
+      pool.put(v[j]);
+      for (int k = j; k < j + pc; ++k) v[k] = v[k + 1];
+      v[j + pc] = -1;
+      j--;
+      continue;
+    }
+    if (j >= pc) T(j, j - pc) = z;
+    // normalise v_j; dots with phi (j < p) and with the window v_{j+1..j+pc-1}
+    ys.n = 0;
+    const bool need_P = (j < p) && phi_alive;
+    if (need_P)
+      for (int k = 0; k < p; ++k) { ys.v[ys.n] = phi[k].p; ys.c[ys.n++] = 0.0; }
+    const int nP = ys.n;
+    for (int k = j + 1; k < j + pc; ++k) { ys.v[ys.n] = pool.p(v[k]); ys.c[ys.n++] = 0.0; }
+    nb = launch_dots(D, pool.p(v[j]), 1.0 / z, 1, ys, ws.red, s);
+    std::vector<double> dots;
+    if (ys.n) {
+      const double *h = ws.sums(nb, ys.n);
+      dots.assign(h, h + ys.n);
+    }
+    for (int k = 0; k < nP; ++k) P[(size_t)k + (size_t)p * j] = dots[k];
+    // step (6): v_k -= <v_j, v_k> v_j
+    VecList ax;
+    for (int k = j + 1; k < j + pc; ++k) {
+      double zz = dots[nP + (k - j - 1)];
+      ax.v[ax.n] = pool.p(v[k]);
+      ax.c[ax.n++] = zz;
+      if (k >= pc) T(j, k - pc) = zz;
+    }
+    if (ax.n) launch_multi_axpy(D, pool.p(v[j]), 1.0, ax, 0, ws.red, s);
+    // step (7): v_{j+pc} = H v_j, fused with step (8): - sum_{k0<=k<j} t(k,j) v_k
+    int k0 = 0;
+    if (j > pc) {
+      k0 = j - pc;
+      if (def[k0 - 1] == 0) {
+        pool.put(v[k0 - 1]);
+        v[k0 - 1] = -1;
+      }
+    }
+    v[j + pc] = pool.get();
+    double *w = pool.p(v[j + pc]);
+    SubList sub;
+    for (int k = k0; k < j; ++k) {
+      T(k, j) = T(j, k);
+      if (sub.n == 32) fail(QED_ERR_UNSUPPORTED, "band width above 32");
+      sub.c[sub.n] = T(k, j);
+      sub.z[sub.n++] = pool.p(v[k]);
+    }
+    launch_hv_rows(H.op, pool.p(v[j]), 1.0, w, sub, s);
+    nb = launch_hv_cols(H.op, pool.p(v[j]), 1.0, w, nd == 0 ? 1 : 0, ws.red, s);
+    double wjj;
+    if (nd == 0) {
+      wjj = ws.sums(nb, 1)[0];
+    } else {
+      // step (9): orthogonalise against the deflated vectors, one at a time
+      for (int k = 0; k < nd; ++k) {
+        VecList one;
+        one.n = 1;
+        one.v[0] = w;
+        int nb2 = launch_dots(D, pool.p(v[I[k]]), 1.0, 0, one, ws.red, s);
+        double ww = ws.sums(nb2, 1)[0];
+        launch_axpby(D, 1.0, w, -ww, pool.p(v[I[k]]), 0, ws.red, s);
+        T(I[k], j) = ww;
+      }
+      VecList one;
+      one.n = 1;
+      one.v[0] = w;
+      int nb2 = launch_dots(D, pool.p(v[j]), 1.0, 0, one, ws.red, s);
+      wjj = ws.sums(nb2, 1)[0];
+    }
+    launch_axpby(D, 1.0, w, -wjj, pool.p(v[j]), 0, ws.red, s);
+    T(j, j) = wjj;
+    for (int k = 0; k < nd; ++k) T(j, I[k]) = T(I[k], j);
+    // step (12): convergence test on the lowest eigenvalue of the projected matrix
+    if (j >= 4 * p && j % p == 0) {
+      std::vector<double> Hpr((size_t)j * j), ev;
+      for (int c = 0; c < j; ++c)
+        for (int r = 0; r < j; ++r) Hpr[(size_t)r + (size_t)j * c] = T(r, c);
+      if (!sym_eig(j, Hpr, ev, nullptr)) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
+      double test = std::fabs(ev[0] - ev_old);
+      ev_old = ev[0];
+      bool converged = test < accur_bl;
+      if (j > 1 && ev[1] - ev[0] < min_gap && no_degenerate)
+        fail(QED_ERR_LANCZOS, "band Lanczos: the gap between the first two eigenvalues is smaller than " +
+                                  std::to_string(min_gap));
+      if (converged) break;
+    }
+  }
+  ws.sync();
+  Mout = j;
+  if (j == 0) return false;
+  // projected eigensystem and Q = P U, summed over the first p Lanczos vectors
+  std::vector<double> Hpr((size_t)j * j), U;
+  for (int c = 0; c < j; ++c)
+    for (int r = 0; r < j; ++r) Hpr[(size_t)r + (size_t)j * c] = T(r, c);
+  if (!sym_eig(j, Hpr, evals, &U)) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
+  const int kmax = std::min(p, j);
+  Q.assign((size_t)p * j, 0.0);
+  for (int m = 0; m < j; ++m)
+    for (int i = 0; i < p; ++i) {
+      double acc = 0.0;
+      for (int k = 0; k < kmax; ++k) acc += P[(size_t)i + (size_t)p * k] * U[(size_t)k + (size_t)j * m];
+      Q[(size_t)i + (size_t)p * m] = acc;
+    }
+  return true;
+}
+
+}  // namespace qed

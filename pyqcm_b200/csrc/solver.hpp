@@ -1,0 +1,81 @@
+// Device-resident sector Hamiltonian and the Krylov solvers built on it.
+//
+// SectorOp is this solver's realisation of the reference's Hamiltonian
+// plugin (Hamiltonian<double>, src_ed/Hamiltonian/Hamiltonian_base.hpp:43-82)
+// in spin-factorized form (Hamiltonian_Factorized, .../Hamiltonian_Factorized.hpp).
+// The Krylov drivers follow src_ed/Hamiltonian/Lanczos.hpp step for step; their
+// vector work runs in the kernels of kernels.cu, only the small tridiagonal /
+// banded projected problems are solved on the host.
+#pragma once
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "common.hpp"
+#include "kernels.cuh"
+#include "model.hpp"
+
+namespace qed {
+
+// Per-process device context: stream, reduction buffers.
+struct Workspace {
+  cudaStream_t stream = nullptr;
+  Reducer red;
+  DevBuf<double> partials, out;
+  double *host = nullptr;
+  Workspace();
+  ~Workspace();
+  // finalize + wait: returns host pointer with nred sums
+  const double *sums(int nblocks, int nred);
+  void sync();
+};
+
+// One spin species: basis strings and hop table on the device.
+struct HalfTables {
+  int L = 0, N = 0;
+  uint32_t dim = 0;
+  DevBuf<uint32_t> bits;
+  std::vector<uint32_t> hbits;
+  DevBuf<uint8_t> cnt;
+  DevBuf<uint32_t> ell;
+  DevBuf<double> vals, diag;
+  int nvals = 0, width = 0;
+};
+
+struct SectorOp {
+  Sector sec;
+  int L = 0;
+  HalfTables up, dn;
+  DevBuf<double> vinter;
+  HvOperator op;
+  size_t D = 0;
+  // Builds all tables for `sec` from the collected terms, on `ws.stream`.
+  SectorOp(const SpinData &terms, const Sector &sec, Workspace &ws);
+  // y = H x (device vectors)
+  void apply(const double *x, double *y, Workspace &ws) const;
+};
+
+// Ground state by Lanczos (LanczosEigenvalue + LanczosEigenvector,
+// src_ed/Hamiltonian/Lanczos.hpp:41-143). psi receives the normalised vector.
+struct LanczosResult {
+  double energy = 0.0;
+  int iterations = 0;
+  std::vector<double> alpha, beta;
+};
+LanczosResult lanczos_ground_state(const SectorOp &H, Workspace &ws, DevBuf<double> &psi,
+                                   uint64_t seed);
+
+// LanczosGreen (src_ed/Hamiltonian/Lanczos.hpp:156-183) from a normalised start
+// vector psi (overwritten). Returns the (a, b) coefficients.
+void lanczos_green(const SectorOp &H, Workspace &ws, double *psi, double *q,
+                   std::vector<double> &a, std::vector<double> &b);
+
+// Band Lanczos (src_ed/Hamiltonian/Lanczos.hpp:214-395) followed by the
+// projected eigensystem; returns false when no iteration was possible.
+// phi: p device start vectors of length H.D (consumed). Outputs the eigenvalues
+// and the Q-matrix residues Q = P U (p x M, column-major), as
+// Hamiltonian::build_Q_matrix does (src_ed/Hamiltonian/Hamiltonian_base.hpp:229-254).
+bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
+                          std::vector<double> &evals, std::vector<double> &Q, int &M);
+
+}  // namespace qed

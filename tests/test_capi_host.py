@@ -1,0 +1,73 @@
+"""CPU tests of the C ABI boundary: the library loads, exports every symbol the
+header declares, and its host-side model logic mirrors the reference's error
+behaviour. No kernel is launched here."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from pyqcm_b200 import workloads as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "qed_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(qed_[a-zA-Z_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(qed):
+    L = ctypes.CDLL(qed.LIB_PATH)
+    syms = declared_symbols()
+    assert len(syms) >= 30
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_model_and_instance_host_logic(qed, fresh):
+    suffix, label = fresh()
+    prob = W.chain8()
+    qed.load_problem(prob, label, model_name="cpu" + suffix)
+    assert qed.Green_function_dimension(label) == 8
+    assert qed.mixing(label) == 0
+    # staggered field makes the two spins different (mixing up_down = 4)
+    suffix, label = fresh()
+    qed.load_problem(W.hubbard_cluster(4, 2, U=4.0, M=0.1), label, model_name="cpu" + suffix)
+    assert qed.mixing(label) == 4
+
+
+def test_errors_follow_reference_conventions(qed, fresh):
+    suffix, label = fresh()
+    with pytest.raises(qed.QEDError) as e:
+        qed.new_model_instance("no_such_model" + suffix, {"t": 1.0}, "R0:N2:S0", label)
+    assert e.value.code == 1 and "not defined" in str(e.value)
+    qed.new_model("m" + suffix, 4, 0)
+    qed.new_operator("m" + suffix, "t", "one-body", [(0, 1, 1.0), (4, 5, 1.0)])
+    qed.new_operator("m" + suffix, "U", "interaction", [(i, i + 4, 1.0) for i in range(4)])
+    with pytest.raises(qed.QEDError) as e:
+        qed.new_model_instance("m" + suffix, {"t": -1.0, "U": 2.0}, "R0:N3:S0", label)
+    assert "not valid" in str(e.value)
+    # a spin-flip one-body term leaves the spin-factorized solver's scope
+    qed.new_model("sf" + suffix, 4, 0)
+    qed.new_operator("sf" + suffix, "t", "one-body", [(0, 1, 1.0), (4, 5, 1.0)])
+    qed.new_operator("sf" + suffix, "sf", "one-body", [(0, 5, 1.0)])
+    with pytest.raises(qed.QEDError) as e:
+        qed.new_model_instance("sf" + suffix, {"t": -1.0, "sf": 0.5}, "R0:N4:S0", label + 1)
+    assert e.value.code == 6
+    with pytest.raises(qed.QEDError) as e:
+        qed.new_operator("m" + suffix, "an", "anomalous", [(0, 5, 1.0)])
+    assert e.value.code == 6
+    with pytest.raises(qed.QEDError):
+        qed.set_global_parameter("no_such_option", 1.0)
+    with pytest.raises(qed.QEDError) as e:
+        qed.ground_state_solve(987654)
+    assert e.value.code == 1
+
+
+def test_unknown_label_and_options(qed):
+    qed.set_global_parameter("accur_lanczos", 1e-12)
+    assert qed.get_global_double("accur_lanczos") == 1e-12
+    qed.set_global_parameter("kgrid_side", 32)  # lattice-layer option is accepted

@@ -1,0 +1,145 @@
+"""GPU parity of the hot path against the reference's own ED (the CPU oracle).
+
+Tolerances: basis indices, ranks and signs bit-exact; H.v within 1e-13
+relative (FP64 round-off of a different summation order); ground-state
+energies within 1e-10 relative; G(i w_n) within 1e-8 (absolute, on the
+Matsubara grid of beta = 50, where |G| <= 1/w_0 ~ 16).
+"""
+import numpy as np
+import pytest
+
+from pyqcm_b200 import workloads as W
+from tests.helpers import load_both, rel_err, set_both
+
+pytestmark = pytest.mark.gpu
+
+GS_TOL = 1e-10
+GF_TOL = 1e-8
+
+
+@pytest.mark.parametrize("L,N", [(4, 2), (8, 4), (8, 3), (10, 5), (12, 6), (16, 8), (16, 9), (7, 0), (7, 7)])
+def test_halfbasis_bit_exact(qed, oracle, L, N):
+    a = qed.halfbasis(L, N)
+    b = oracle.halfbasis(L, N)
+    assert a.dtype == np.uint32 and np.array_equal(a, b)
+    r = qed.halfbasis_rank(L, N, b)
+    assert np.array_equal(r, np.arange(len(b), dtype=np.uint32))
+    # strings outside the basis rank to dim (ED_halfbasis::index)
+    bad = np.array([0xFFFFFFFF, (1 << L) | 1], dtype=np.uint32)
+    assert np.all(qed.halfbasis_rank(L, N, bad) == len(b))
+
+
+@pytest.mark.parametrize("L,nu,nd,a", [(6, 3, 3, 0), (6, 3, 3, 5), (6, 3, 2, 7), (6, 3, 3, 11), (8, 4, 4, 3),
+                                       (8, 4, 4, 12), (5, 1, 4, 9)])
+def test_destroy_table_bit_exact(qed, oracle, L, nu, nd, a):
+    t1, p1 = qed.destroy_table(L, nu, nd, a)
+    t2, p2 = oracle.destroy_table(L, nu, nd, a)
+    assert np.array_equal(t1, t2)
+    assert np.array_equal(p1[t1 >= 0], p2[t2 >= 0] % 2)
+
+
+def _hv_problems():
+    return [
+        ("chain8", W.chain8(), "R0:N8:S0"),
+        ("chain8_N7", W.hubbard_cluster(8, 1, U=3.0, n_up=4, n_dn=3), "R0:N7:S1"),
+        ("sq2x3_tp", W.hubbard_cluster(3, 2, tp=0.3, U=6.0), "R0:N6:S0"),
+        ("neel2x4", W.hubbard_cluster(4, 2, U=5.0, mu=1.7, M=0.25), "R0:N8:S0"),
+        ("plaq8b", W.plaquette_bath(np.linspace(-1.5, 1.5, 8), np.linspace(0.2, 0.9, 8)), "R0:N12:S0"),
+        ("plaq8b_p", W.plaquette_bath(np.linspace(-1.5, 1.5, 8), np.linspace(0.2, 0.9, 8)), "R0:N13:S1"),
+    ]
+
+
+@pytest.mark.parametrize("case", range(6))
+def test_hv_matches_reference(qed, oracle, fresh, case):
+    name, prob, sec = _hv_problems()[case]
+    suffix, label = fresh()
+    load_both(qed, oracle, prob, suffix, label, fmt="F")
+    Hq = qed.Hamiltonian(label, sec)
+    Hr = oracle.RefHamiltonian(label, sec)
+    assert Hq.dim == Hr.dim
+    rng = np.random.default_rng(7 + case)
+    x = rng.standard_normal(Hq.dim)
+    y0 = rng.standard_normal(Hq.dim)
+    y1, y2 = y0.copy(), y0.copy()
+    Hq.mult_add(x, y1)
+    Hr.mult_add(x, y2)
+    assert rel_err(y1, y2) < 1e-13, name
+    # diagonal via unit vectors on a few entries
+    d = Hq.diag()
+    for i in rng.integers(0, Hq.dim, 5):
+        e = np.zeros(Hq.dim)
+        e[i] = 1.0
+        y = np.zeros(Hq.dim)
+        Hr.mult_add(e, y)
+        assert abs(d[i] - y[i]) < 1e-12
+
+
+GS_CASES = [
+    ("chain8", lambda: W.chain8()),
+    ("sq2x3_tp", lambda: W.hubbard_cluster(3, 2, tp=0.3, U=6.0)),
+    ("neel2x4", lambda: W.hubbard_cluster(4, 2, U=5.0, mu=1.7, M=0.25)),
+    ("plaq8b", lambda: W.plaquette_bath(np.linspace(-1.5, 1.5, 8), np.linspace(0.2, 0.9, 8))),
+    ("chain10", lambda: W.hubbard_cluster(10, 1, U=7.0)),
+]
+
+
+@pytest.mark.parametrize("case", range(len(GS_CASES)))
+def test_ground_state_energy(qed, oracle, fresh, case):
+    name, mk = GS_CASES[case]
+    suffix, label = fresh()
+    set_both(qed, oracle, GF_method="L")
+    load_both(qed, oracle, mk(), suffix, label, fmt="F")
+    e1, s1 = qed.ground_state_solve(label)
+    e2, s2 = oracle.ground_state(label)
+    assert abs(e1 - e2) <= GS_TOL * abs(e2), (name, e1, e2)
+    assert s1 == s2
+
+
+@pytest.mark.parametrize("case", range(len(GS_CASES)))
+def test_green_function_band_lanczos(qed, oracle, fresh, case):
+    name, mk = GS_CASES[case]
+    suffix, label = fresh()
+    set_both(qed, oracle, GF_method="L")
+    load_both(qed, oracle, mk(), suffix, label, fmt="F")
+    z = W.matsubara(256)
+    G1 = qed.Green_function(z, label=label)
+    G2 = oracle.green_function(label, z)
+    assert np.max(np.abs(G1 - G2)) < GF_TOL, name
+    if qed.mixing(label) & 4:
+        G1d = qed.Green_function(z, spin_down=True, label=label)
+        G2d = oracle.green_function(label, z, spin_down=True)
+        assert np.max(np.abs(G1d - G2d)) < GF_TOL, name
+    assert abs(qed.Potthoff_functional(label) - oracle.potthoff(label)) < 1e-9
+    M1 = qed.Green_function_average(label=label)
+    M2 = oracle.green_function_average(label)
+    assert np.max(np.abs(M1 - M2)) < 1e-8
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_green_function_continued_fraction(qed, oracle, fresh, case):
+    name, mk = GS_CASES[case]
+    suffix, label = fresh()
+    set_both(qed, oracle, GF_method="F")
+    try:
+        load_both(qed, oracle, mk(), suffix, label, fmt="S")
+        z = W.matsubara(256)
+        G1 = qed.Green_function(z, label=label)
+        G2 = oracle.green_function(label, z)
+    finally:
+        set_both(qed, oracle, GF_method="L")
+    assert np.max(np.abs(G1 - G2)) < GF_TOL, name
+
+
+def test_self_energy_and_hybridization(qed, oracle, fresh):
+    suffix, label = fresh()
+    set_both(qed, oracle, GF_method="L")
+    prob = W.plaquette_bath(np.linspace(-1.5, 1.5, 8), np.linspace(0.2, 0.9, 8))
+    load_both(qed, oracle, prob, suffix, label, fmt="F")
+    z = W.matsubara(32)
+    S1 = qed.self_energy(z, label=label)
+    oracle.green_solve(label)  # the reference's self_energy needs a solved GF (src_ed/model_instance.hpp:683-700)
+    S2 = oracle.self_energy(label, z)
+    assert np.max(np.abs(S1 - S2)) < 1e-6
+    H1 = qed.hybridization_function(z, label=label)
+    H2 = oracle.hybridization_function(label, z)
+    assert np.max(np.abs(H1 - H2)) < 1e-12

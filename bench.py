@@ -1,0 +1,296 @@
+"""Benchmark: spin-factorized H.v throughput on the 4x4 Hubbard cluster.
+
+Workload: 4x4 open square cluster, t=-1, t'=0.3, U=8, half filling
+(sector R0:N16:S0, dimension 12870^2 = 165,636,900; one FP64 vector = 1.33 GB).
+One step = one application y = H x of the solver's device Hamiltonian to an
+HBM-resident vector (the operation the Lanczos and band-Lanczos recurrences
+repeat). Metric: H.v algorithmic HBM throughput, 16 bytes per basis state per
+application (read x once, write y once); inputs are 1.33 GB, larger than L2,
+so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--solve]
+
+N > 1 runs one replica per GPU (launched by torch.distributed.run); the line
+reports the aggregate of all replicas, timed as the max over ranks.
+--impl reference times the reference's own CPU H.v (Hamiltonian_Factorized::mult_add,
+compiled from its sources in oracle/_ref) on the same sector.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "H.v HBM GB/s"
+UNIT = "GB/s"
+WORKLOAD = "4x4 Hubbard cluster (open, t=-1, t'=0.3, U=8, half filling, sector R0:N16:S0, dim 165636900)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--solve", action="store_true", help="also time a full ground state of the 4x4 cluster")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run: warm-up and timed H.v only (no e2e, clocks or CPU baseline)")
+    ap.add_argument("--sector", default=None, help="sector of the 4x4 cluster to use (default R0:N16:S0)")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if (args.impl == "ours" and torch.cuda.is_available()) else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per H.v from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "hv_sq4x4_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_hv"):
+                return float(line.split("=")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "100"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline_sample():
+    """The reference's mult_add on the same sector, one application, one core."""
+    from oracle import ref
+    from pyqcm_b200 import workloads as W
+    p = W.square4x4()
+    ref.load_problem(p, 9001, model_name="bench_ref_sq4x4", fmt="F")
+    H = ref.RefHamiltonian(9001, p.sectors)
+    return H
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    H = cpu_baseline_sample()
+    D = H.dim
+    steps, warm = max(1, min(args.steps, 3)), min(args.warmup, 1)
+    for _ in range(warm):
+        H.bench(1)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        H.bench(1)
+    dt = (time.perf_counter() - t0) / steps
+    v = 16.0 * D / dt / 1e9
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+            "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "inputs": "larger than L2 (1.33 GB vectors)",
+                       "reference": "Hamiltonian_Factorized::mult_add compiled from the reference sources (oracle/_ref)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": f"{steps} full H.v application(s) of the 4x4 sector; the reference's H.v has no threading"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import pyqcm_b200 as qed
+    from pyqcm_b200 import workloads as W
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    qed.init(local)
+    prob = W.square4x4()
+    if args.sector:
+        prob.sectors = args.sector
+    label = 7000 + rank
+    qed.load_problem(prob, label, model_name="bench_sq4x4")
+    H = qed.Hamiltonian(label, prob.sectors)
+    D = H.dim
+    g = torch.Generator(device=f"cuda:{local}").manual_seed(1234 + rank)
+    x = torch.randn(D, dtype=torch.float64, device=f"cuda:{local}", generator=g)
+    y = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        H.apply_device(x.data_ptr(), y.data_ptr(), sh)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        H.apply_device(x.data_ptr(), y.data_ptr(), sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile": True, "dim": D, "ms_per_hv": ms,
+                              "GBps_16D": 16.0 * D / (ms * 1e-3) / 1e9}), flush=True)
+        return
+    # end to end through the C ABI with host buffers (y += H x, copies inside)
+    xh = torch.empty(D, dtype=torch.float64, pin_memory=True).numpy()
+    yh = torch.empty(D, dtype=torch.float64, pin_memory=True).numpy()
+    xh[:] = x.cpu().numpy()
+    yh[:] = 0.0
+    H.mult_add(xh, yh)  # warm-up
+    e2e_steps = 3
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        H.mult_add(xh, yh)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    ms_t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms, e2e_s = float(ms_t[0]), float(ms_t[1])
+    solve = None
+    if args.solve:
+        qed.set_global_parameter("GF_method", "L")
+        qed.load_problem(prob, label + 100, model_name="bench_sq4x4")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e, sec = qed.ground_state_solve(label + 100)
+        solve = {"ground_state_seconds": time.perf_counter() - t0, "E0": e, "sector": sec}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            Hr = cpu_baseline_sample()
+            t0 = time.perf_counter()
+            Hr.bench(1)
+            dt = time.perf_counter() - t0
+            cpu = {"value": 16.0 * D / dt / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": "one full H.v application of the 4x4 sector by the reference's "
+                             "Hamiltonian_Factorized::mult_add (no threading in the reference's H.v)"}
+    if rank != 0:
+        return
+    alg = 16.0 * D
+    peak, src = peaks()
+    achieved = alg / (ms * 1e-3) / 1e9
+    traffic = ncu_traffic()
+    line = {
+        "metric": METRIC, "value": world * alg / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "inputs": "larger than L2 (1.33 GB vectors), no flush",
+                   "parallelism": f"replicas x{world}", "bytes_per_step": alg},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": src,
+                     "unit_of_work": "one H.v (row pass + column pass kernels), 16 B per basis state"},
+        "e2e": {"value": world * alg / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 16 * D,
+                "d2h_bytes_per_step": 8 * D, "path": "qed_hamiltonian_mult_add (y += H x) with pinned host buffers"},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    if solve:
+        line["solve"] = solve
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -139,7 +139,8 @@ int qed_hamiltonian_create(int label, const char *sector, qed_hamiltonian **h, l
 /* y += H x with host vectors (Hamiltonian::mult_add). */
 int qed_hamiltonian_mult_add(qed_hamiltonian *h, const double *x, double *y);
 /* y = H x with device vectors on the current device, enqueued on `stream`
- * (a cudaStream_t, or NULL for the library's stream of this Hamiltonian). */
+ * (a cudaStream_t; NULL is the legacy default stream, as in the CUDA runtime).
+ * Asynchronous: returns after the launches are enqueued. */
 int qed_hamiltonian_apply_device(qed_hamiltonian *h, const double *x, double *y, void *stream);
 /* Hamiltonian::diag (src_ed/Hamiltonian/Hamiltonian_base.hpp:57). */
 int qed_hamiltonian_diag(qed_hamiltonian *h, double *d);

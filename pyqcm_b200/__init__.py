@@ -282,9 +282,10 @@ class Hamiltonian:
         _check(lib().qed_hamiltonian_mult_add(self._h, _dp(x), _dp(y)))
 
     def apply_device(self, x_ptr: int, y_ptr: int, stream: int = 0):
-        """y = H x on device pointers (e.g. torch tensors' data_ptr())."""
+        """y = H x on device pointers (e.g. torch tensors' data_ptr()), enqueued on the
+        cudaStream_t handle `stream` (0 = legacy default stream, torch's default)."""
         _check(lib().qed_hamiltonian_apply_device(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr),
-                                                  C.c_void_p(stream) if stream else None))
+                                                  C.c_void_p(stream)))
 
     def diag(self):
         d = np.zeros(self.dim)

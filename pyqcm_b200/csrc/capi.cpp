@@ -364,7 +364,7 @@ int qed_hamiltonian_apply_device(qed_hamiltonian *h, const double *x, double *y,
     if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
     std::lock_guard<std::recursive_mutex> g(g_gpu);
     Workspace &w = ws();
-    cudaStream_t s = stream ? (cudaStream_t)stream : w.stream;
+    cudaStream_t s = (cudaStream_t)stream;
     if (!h->H->D) return;
     SubList none;
     launch_hv_rows(h->H->op, x, 1.0, y, none, s);

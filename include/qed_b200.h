@@ -142,6 +142,14 @@ int qed_hamiltonian_mult_add(qed_hamiltonian *h, const double *x, double *y);
  * (a cudaStream_t; NULL is the legacy default stream, as in the CUDA runtime).
  * Asynchronous: returns after the launches are enqueued. */
 int qed_hamiltonian_apply_device(qed_hamiltonian *h, const double *x, double *y, void *stream);
+/* y = H x fused with the reductions a Lanczos step needs (LanczosEigenvalue,
+ * src_ed/Hamiltonian/Lanczos.hpp:68-77, takes <v, Hv> and norms right after
+ * mult_add): dots[0] = <x, y>, dots[1] = <y, y>, dots[2] = <x, x>, written to
+ * the device array `dots` (3 doubles). Enqueued on `stream` (NULL = legacy
+ * default stream); the per-block partial sums live in a buffer the handle
+ * allocates with cudaMalloc on its first call. */
+int qed_hamiltonian_apply_dots_device(qed_hamiltonian *h, const double *x, double *y, double *dots,
+                                      void *stream);
 /* Hamiltonian::diag (src_ed/Hamiltonian/Hamiltonian_base.hpp:57). */
 int qed_hamiltonian_diag(qed_hamiltonian *h, double *d);
 int qed_hamiltonian_destroy(qed_hamiltonian *h);

@@ -85,6 +85,7 @@ def lib():
         "qed_hamiltonian_create": [C.c_int, C.c_char_p, C.POINTER(C.c_void_p), lp],
         "qed_hamiltonian_mult_add": [C.c_void_p, dp, dp],
         "qed_hamiltonian_apply_device": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+        "qed_hamiltonian_apply_dots_device": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
         "qed_hamiltonian_diag": [C.c_void_p, dp],
         "qed_hamiltonian_destroy": [C.c_void_p],
         "qed_halfbasis": [C.c_int, C.c_int, up, lp],
@@ -286,6 +287,11 @@ class Hamiltonian:
         cudaStream_t handle `stream` (0 = legacy default stream, torch's default)."""
         _check(lib().qed_hamiltonian_apply_device(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr),
                                                   C.c_void_p(stream)))
+
+    def apply_dots_device(self, x_ptr: int, y_ptr: int, dots_ptr: int, stream: int = 0):
+        """y = H x and dots = (<x,y>, <y,y>, <x,x>) on device pointers, in one pass."""
+        _check(lib().qed_hamiltonian_apply_dots_device(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr),
+                                                       C.c_void_p(dots_ptr), C.c_void_p(stream)))
 
     def diag(self):
         d = np.zeros(self.dim)

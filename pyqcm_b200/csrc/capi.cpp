@@ -16,6 +16,7 @@ using namespace qed;
 struct qed_hamiltonian {
   std::unique_ptr<SectorOp> H;
   DevBuf<double> x, y;
+  DevBuf<double> partials;  // per-block partial sums of apply_dots_device
 };
 
 namespace {
@@ -369,6 +370,29 @@ int qed_hamiltonian_apply_device(qed_hamiltonian *h, const double *x, double *y,
     SubList none;
     launch_hv_rows(h->H->op, x, 1.0, y, none, s);
     launch_hv_cols(h->H->op, x, 1.0, y, 0, w.red, s);
+  });
+}
+
+int qed_hamiltonian_apply_dots_device(qed_hamiltonian *h, const double *x, double *y, double *dots,
+                                      void *stream) {
+  return guarded([&] {
+    if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
+    if (!dots) fail(QED_ERR_ARGUMENT, "null output array");
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    ws();
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!h->H->D) {
+      QED_CUDA(cudaMemsetAsync(dots, 0, 3 * sizeof(double), s));
+      return;
+    }
+    if (!h->partials.n) h->partials.alloc((size_t)kHvColsMaxBlocks * Reducer::kMaxRed);
+    Reducer r;
+    r.partials = h->partials.p;
+    r.max_blocks = kHvColsMaxBlocks;
+    SubList none;
+    launch_hv_rows(h->H->op, x, 1.0, y, none, s);
+    int nb = launch_hv_cols(h->H->op, x, 1.0, y, 7, r, s);
+    launch_finalize(r.partials, nb, 3, dots, s);
   });
 }
 

@@ -630,6 +630,12 @@ void finalize_sums(Reducer &r, int nblocks, int nred, cudaStream_t s) {
   QED_CUDA(cudaMemcpyAsync(r.host, r.out, nred * sizeof(double), cudaMemcpyDeviceToHost, s));
 }
 
+void launch_finalize(const double *partials, int nblocks, int nred, double *out, cudaStream_t s) {
+  k_finalize<<<nred, kThreads, 0, s>>>(partials, nblocks, out);
+  QED_LAUNCH();
+}
+
+
 void launch_qmatrix_gf(int L, int M, const double *e, const double *V, int nz, const double *z,
                        double *G, cudaStream_t s) {
   if (nz <= 0 || M <= 0) return;

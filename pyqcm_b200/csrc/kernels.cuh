@@ -109,6 +109,12 @@ void launch_scale(size_t D, double *y, double a, cudaStream_t s);
 // partials of `nred` slots in a fixed order into r.out and copies them to
 // r.host (the caller synchronises the stream before reading r.host).
 void finalize_sums(Reducer &r, int nblocks, int nred, cudaStream_t s);
+// Adds per-block partials (stride Reducer::kMaxRed) of `nred` slots into the
+// device array out[0..nred), on stream s; nothing is copied to the host.
+void launch_finalize(const double *partials, int nblocks, int nred, double *out, cudaStream_t s);
+// Number of per-block partial-sum rows a reducing H.v column pass can use.
+constexpr int kHvColsMaxBlocks = 8 * 148;
+
 
 // ---- Green functions on a frequency grid ----------------------------------
 // G[k][b + a*L] += sum_i V[a + i*L] V[b + i*L] / (z_k - e_i)   (real V, L <= 64)

@@ -1,0 +1,54 @@
+"""The GPU solver against the committed golden fixtures (made by the reference's
+own ED, tests/golden/make_golden.py). Runs without the oracle library."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from pyqcm_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+BUILDERS = {
+    "chain8": W.chain8,
+    "sq2x3_tp": lambda: W.hubbard_cluster(3, 2, tp=0.3, U=6.0),
+    "neel2x4": lambda: W.hubbard_cluster(4, 2, U=5.0, mu=1.7, M=0.25),
+    "plaq8b": lambda: W.plaquette_bath(np.linspace(-1.5, 1.5, 8), np.linspace(0.2, 0.9, 8)),
+    "chain10": lambda: W.hubbard_cluster(10, 1, U=7.0),
+}
+
+
+def test_small_cases_against_fixtures(qed, fresh):
+    g = np.load(os.path.join(GOLDEN, "small_cases.npz"), allow_pickle=False)
+    z = g["z"]
+    for i, name in enumerate(str(n) for n in g["names"]):
+        base, method = name.rsplit("_", 1)
+        qed.set_global_parameter("GF_method", method)
+        try:
+            suffix, label = fresh()
+            qed.load_problem(BUILDERS[base](), label, model_name="gold_" + name + suffix)
+            e, _ = qed.ground_state_solve(label)
+            G = qed.Green_function(z, label=label)
+            n = int(g["dims"][i])
+            assert abs(e - g["E0"][i]) <= 1e-10 * abs(g["E0"][i]), name
+            assert np.max(np.abs(G - g["G"][i][:, :n, :n])) < 1e-8, name
+            if qed.mixing(label) & 4:
+                Gd = qed.Green_function(z, spin_down=True, label=label)
+                assert np.max(np.abs(Gd - g["G_down"][i][:, :n, :n])) < 1e-8, name
+            assert abs(qed.Potthoff_functional(label) - g["omega"][i]) < 1e-9, name
+        finally:
+            qed.set_global_parameter("GF_method", "L")
+
+
+def test_sq4x4_ground_state_against_fixture(qed, fresh):
+    path = os.path.join(GOLDEN, "sq4x4_gs.json")
+    if not os.path.exists(path):
+        pytest.skip("4x4 fixture not generated yet")
+    ref = json.load(open(path))
+    suffix, label = fresh()
+    qed.load_problem(W.square4x4(), label, model_name="gold_sq4x4" + suffix)
+    e, sec = qed.ground_state_solve(label)
+    assert abs(e - ref["E0"]) <= 1e-10 * abs(ref["E0"])
+    assert sec == ref["sector"]

@@ -143,3 +143,27 @@ def test_self_energy_and_hybridization(qed, oracle, fresh):
     H1 = qed.hybridization_function(z, label=label)
     H2 = oracle.hybridization_function(label, z)
     assert np.max(np.abs(H1 - H2)) < 1e-12
+
+
+def test_apply_dots_device_matches_host_path(qed, oracle, fresh):
+    """Fused H.v + Lanczos reductions on device pointers (torch-owned memory)."""
+    import torch
+    suffix, label = fresh()
+    prob = W.hubbard_cluster(4, 2, U=5.0, mu=1.7, M=0.25)
+    load_both(qed, oracle, prob, suffix, label, fmt="F")
+    H = qed.Hamiltonian(label, prob.sectors)
+    Hr = oracle.RefHamiltonian(label, prob.sectors)
+    x = np.random.default_rng(3).standard_normal(H.dim)
+    xd = torch.tensor(x, device="cuda")
+    yd = torch.empty_like(xd)
+    dots = torch.zeros(3, dtype=torch.float64, device="cuda")
+    H.apply_dots_device(xd.data_ptr(), yd.data_ptr(), dots.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    y_ref = np.zeros(H.dim)
+    Hr.mult_add(x, y_ref)
+    y = yd.cpu().numpy()
+    assert rel_err(y, y_ref) < 1e-13
+    d = dots.cpu().numpy()
+    assert abs(d[0] - x @ y_ref) < 1e-10 * abs(x @ y_ref)
+    assert abs(d[1] - y_ref @ y_ref) < 1e-10 * (y_ref @ y_ref)
+    assert abs(d[2] - x @ x) < 1e-12 * (x @ x)

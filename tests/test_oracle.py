@@ -142,5 +142,6 @@ def test_golden_fixtures_reproduce(oracle, fresh):
             G = oracle.green_function(label, W.matsubara(256))
         finally:
             oracle.set_param("GF_method", "L")
+        n = int(g["dims"][i])
         assert abs(e - g["E0"][i]) <= 1e-10 * abs(e)
-        assert np.max(np.abs(G - g["G"][i])) < 1e-8
+        assert np.max(np.abs(G - g["G"][i][:, :n, :n])) < 1e-8

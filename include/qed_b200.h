@@ -150,6 +150,22 @@ int qed_hamiltonian_apply_device(qed_hamiltonian *h, const double *x, double *y,
  * allocates with cudaMalloc on its first call. */
 int qed_hamiltonian_apply_dots_device(qed_hamiltonian *h, const double *x, double *y, double *dots,
                                       void *stream);
+/* Same result as qed_hamiltonian_apply_dots_device, but the call allocates no
+ * memory at all: no cudaMalloc, cudaFree or allocating library routine. It has
+ * no counterpart in the reference; it exists for callers that cannot allocate
+ * device memory when they call in, e.g. a process whose device memory belongs
+ * to another runtime's pool, or a loop that cannot afford cudaMalloc's implicit
+ * device synchronisation. The caller passes x, y and dots (3 doubles) in device
+ * memory; the per-block partial sums live in a fixed 682 KB array compiled into
+ * the library (1184 rows), which every GPU that loads the library holds until
+ * the process exits. A Hamiltonian whose column pass would need more rows than
+ * that is rejected with QED_ERR_MEMORY (never on a 148-SM B200). The first call
+ * on a device looks up the array's device address; make that first call before
+ * any stream capture. All calls share the array: calls that overlap on the GPU
+ * (different streams, no ordering between them) race and give wrong sums; a
+ * call leaves nothing that a later call depends on. */
+int qed_hamiltonian_apply_dots_device_noalloc(qed_hamiltonian *h, const double *x, double *y,
+                                              double *dots, void *stream);
 /* Hamiltonian::diag (src_ed/Hamiltonian/Hamiltonian_base.hpp:57). */
 int qed_hamiltonian_diag(qed_hamiltonian *h, double *d);
 int qed_hamiltonian_destroy(qed_hamiltonian *h);

@@ -396,6 +396,23 @@ int qed_hamiltonian_apply_dots_device(qed_hamiltonian *h, const double *x, doubl
   });
 }
 
+// No-allocation variant of qed_hamiltonian_apply_dots_device (see the header):
+// no workspace lookup, no buffer growth; the scratch is the fixed device array
+// behind launch_hv_dots_noalloc.
+int qed_hamiltonian_apply_dots_device_noalloc(qed_hamiltonian *h, const double *x, double *y,
+                                              double *dots, void *stream) {
+  return guarded([&] {
+    if (!h || !x || !y || !dots) fail(QED_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!h->H->D) {
+      QED_CUDA(cudaMemsetAsync(dots, 0, 3 * sizeof(double), s));
+      return;
+    }
+    launch_hv_dots_noalloc(h->H->op, x, y, dots, s);
+  });
+}
+
 int qed_hamiltonian_diag(qed_hamiltonian *h, double *d) {
   return guarded([&] {
     if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");

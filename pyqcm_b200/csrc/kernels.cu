@@ -8,6 +8,8 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
+#include <string>
 
 #include "common.hpp"
 #include "kernels.cuh"
@@ -635,6 +637,64 @@ void launch_finalize(const double *partials, int nblocks, int nred, double *out,
   QED_LAUNCH();
 }
 
+// ---- H.v + dots without any device allocation -------------------------------
+//
+// For callers that cannot allocate device memory at call time: a process whose
+// device memory is owned by another runtime's pool, a real-time loop that cannot
+// take cudaMalloc's implicit synchronisation, or code that must not grow the
+// footprint after set-up. The scratch below is part of the library image: every
+// GPU that loads the library holds it (682 KB) until the process exits.
+
+namespace {
+
+// Per-block partial sums of the reducing column pass: kHvColsMaxBlocks rows of
+// Reducer::kMaxRed doubles (1184 x 72 x 8 B = 682 KB).
+static __device__ __align__(256) double g_noalloc_partials[kHvColsMaxBlocks * Reducer::kMaxRed];
+
+// Device address of g_noalloc_partials, looked up once per device with that
+// device current. In host code the array's name is only a host-side stand-in,
+// so kernels must be given this address, never the symbol itself.
+double *noalloc_partials_address() {
+  static std::mutex mtx;
+  static double *addr[64] = {};
+  int dev = 0;
+  QED_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) fail(QED_ERR_ARGUMENT, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(mtx);
+  if (!addr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess || !p)
+      fail(QED_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    addr[dev] = static_cast<double *>(p);
+  }
+  return addr[dev];
+}
+
+}  // namespace
+
+void launch_hv_dots_noalloc(const HvOperator &op, const double *x, double *y, double *dots,
+                            cudaStream_t s) {
+  // Work items of the column pass and the grid it launches (grid-stride):
+  // at most 8 CTAs per SM, and never more rows than the scratch holds.
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const uint32_t W = ((du % 2 == 0) ? 2 : 1) * kThreads;
+  const size_t nitems = (size_t)((du + W - 1) / W) * ((dd + 3) / 4);
+  const size_t want = std::min<size_t>(nitems, (size_t)device_sms() * 8);
+  if (want > (size_t)kHvColsMaxBlocks)
+    fail(QED_ERR_MEMORY, "H.v without allocation: the column pass needs " + std::to_string(want) +
+                             " partial-sum rows, the fixed scratch holds " +
+                             std::to_string(kHvColsMaxBlocks));
+  Reducer r;
+  r.partials = noalloc_partials_address();
+  r.max_blocks = kHvColsMaxBlocks;
+  SubList none;
+  launch_hv_rows(op, x, 1.0, y, none, s);
+  int nb = launch_hv_cols(op, x, 1.0, y, 7, r, s);
+  // Every block of this launch overwrites its own row, and the sum reads only
+  // those rows, so nothing has to be cleared between calls.
+  launch_finalize(r.partials, nb, 3, dots, s);
+}
 
 void launch_qmatrix_gf(int L, int M, const double *e, const double *V, int nz, const double *z,
                        double *G, cudaStream_t s) {

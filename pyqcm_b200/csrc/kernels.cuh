@@ -115,6 +115,13 @@ void launch_finalize(const double *partials, int nblocks, int nred, double *out,
 // Number of per-block partial-sum rows a reducing H.v column pass can use.
 constexpr int kHvColsMaxBlocks = 8 * 148;
 
+// y = H x with dots = (<x,y>, <y,y>, <x,x>) written to device memory, using
+// no memory allocated by anyone: the per-block partial sums go to a fixed
+// file-scope device array of kHvColsMaxBlocks rows (see kernels.cu). The first
+// call on a device looks up that array's device address (cudaGetSymbolAddress).
+// Throws Error(QED_ERR_MEMORY) when the column pass would need more rows.
+void launch_hv_dots_noalloc(const HvOperator &op, const double *x, double *y, double *dots,
+                            cudaStream_t s);
 
 // ---- Green functions on a frequency grid ----------------------------------
 // G[k][b + a*L] += sum_i V[a + i*L] V[b + i*L] / (z_k - e_i)   (real V, L <= 64)

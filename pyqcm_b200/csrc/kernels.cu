@@ -328,6 +328,155 @@ __global__ void __launch_bounds__(kThreads) k_hv_cols(HvOperator op, const doubl
   if (red_mask) block_reduce_store<3>(red, partials, 3);
 }
 
+// Row pass, two dn rows per CTA step: the rows are staged interleaved in shared
+// memory (one double2 per up string), so every hop-table entry and every
+// shared-memory gather serves both rows, and the gathers are 16 bytes wide.
+__global__ void __launch_bounds__(1024) k_hv_rows2(HvOperator op, const double *__restrict__ x,
+                                                   double xs, double *y, SubList sub) {
+  extern __shared__ double2 xs2[];
+  __shared__ double vals[256];
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  for (int i = threadIdx.x; i < op.up.nvals; i += blockDim.x) vals[i] = op.up.vals[i];
+  for (uint32_t d0 = 2 * blockIdx.x; d0 < dd; d0 += 2 * gridDim.x) {
+    const bool two = d0 + 1 < dd;
+    const double *x0 = x + (size_t)d0 * du;
+    __syncthreads();
+    for (uint32_t u = threadIdx.x; u < du; u += blockDim.x)
+      xs2[u] = make_double2(x0[u], two ? x0[u + du] : 0.0);
+    __syncthreads();
+    const uint32_t b0 = op.dn.bits[d0], b1 = two ? op.dn.bits[d0 + 1] : 0u;
+    const double e0 = op.dn.diag[d0], e1 = two ? op.dn.diag[d0 + 1] : 0.0;
+    for (uint32_t u = threadIdx.x; u < du; u += blockDim.x) {
+      const uint32_t ub = op.up.bits[u];
+      const double dup = op.up.diag[u];
+      const double2 xu = xs2[u];
+      double a0 = (dup + e0 + inter_term(op.inter, ub, b0)) * xu.x;
+      double a1 = (dup + e1 + inter_term(op.inter, ub, b1)) * xu.y;
+      const int c = op.up.cnt[u];
+      const uint32_t *ep = op.up.ell + u;
+      int k = 0;
+      for (; k + 2 <= c; k += 2) {  // two independent gathers in flight
+        const uint32_t f0 = __ldg(ep + (size_t)k * du), f1 = __ldg(ep + (size_t)(k + 1) * du);
+        const double2 t0 = xs2[f0 >> 8], t1 = xs2[f1 >> 8];
+        const double v0 = vals[f0 & 255u], v1 = vals[f1 & 255u];
+        a0 += v0 * t0.x;
+        a1 += v0 * t0.y;
+        a0 += v1 * t1.x;
+        a1 += v1 * t1.y;
+      }
+      if (k < c) {
+        const uint32_t f0 = __ldg(ep + (size_t)k * du);
+        const double2 t0 = xs2[f0 >> 8];
+        const double v0 = vals[f0 & 255u];
+        a0 += v0 * t0.x;
+        a1 += v0 * t0.y;
+      }
+      const size_t I0 = (size_t)d0 * du + u;
+      a0 *= xs;
+      a1 *= xs;
+      for (int s = 0; s < sub.n; ++s) {
+        a0 -= sub.c[s] * sub.z[s][I0];
+        if (two) a1 -= sub.c[s] * sub.z[s][I0 + du];
+      }
+      y[I0] = a0;
+      if (two) y[I0 + du] = a1;
+    }
+  }
+}
+
+// Column pass with staged hop entries: the CTA decodes the hop entries of its
+// R rows into shared memory once per work item, then every thread issues
+// UNROLL independent 16-byte gathers of x row segments (from L2) at a time.
+constexpr int kColsR = 4;
+constexpr int kMaxHops = 256;
+
+template <int VEC>
+__global__ void __launch_bounds__(kThreads) k_hv_cols2(HvOperator op, const double *__restrict__ x,
+                                                        double xs, double *y, int red_mask,
+                                                        double *partials) {
+  __shared__ double cval[kColsR][kMaxHops];
+  __shared__ uint32_t cidx[kColsR][kMaxHops];
+  __shared__ int ccnt[kColsR];
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const uint32_t W = VEC * blockDim.x;
+  const uint32_t nchunk = (du + W - 1) / W, nrg = (dd + kColsR - 1) / kColsR;
+  const size_t nitems = (size_t)nchunk * nrg;
+  double red[3] = {0.0, 0.0, 0.0};
+  for (size_t t = blockIdx.x; t < nitems; t += gridDim.x) {
+    const uint32_t chunk = (uint32_t)(t / nrg), rg = (uint32_t)(t % nrg);
+    __syncthreads();  // the previous item is done with the staged entries
+    if (threadIdx.x < kColsR) {
+      const uint32_t d = rg * kColsR + threadIdx.x;
+      ccnt[threadIdx.x] = d < dd ? (int)op.dn.cnt[d] : 0;
+    }
+    for (int j = threadIdx.x; j < kColsR * kMaxHops; j += blockDim.x) {
+      const int rr = j / kMaxHops, k = j % kMaxHops;
+      const uint32_t d = rg * kColsR + rr;
+      if (d < dd && k < (int)op.dn.cnt[d]) {
+        const uint32_t e = __ldg(op.dn.ell + (size_t)k * dd + d);
+        cval[rr][k] = op.dn.vals[e & 255u];
+        cidx[rr][k] = e >> 8;
+      }
+    }
+    __syncthreads();
+    const uint32_t u0 = chunk * W + VEC * threadIdx.x;
+    if (u0 >= du) continue;
+    for (int rr = 0; rr < kColsR; ++rr) {
+      const uint32_t d = rg * kColsR + rr;
+      if (d >= dd) break;
+      const int c = ccnt[rr];
+      const size_t base = (size_t)d * du + u0;
+      if (VEC == 2) {
+        const double *xb = x + u0;
+        double ax = 0.0, ay = 0.0;
+        int k = 0;
+        for (; k + 4 <= c; k += 4) {
+          const double2 t0 = __ldg(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k] * du));
+          const double2 t1 = __ldg(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k + 1] * du));
+          const double2 t2 = __ldg(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k + 2] * du));
+          const double2 t3 = __ldg(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k + 3] * du));
+          ax += cval[rr][k] * t0.x + cval[rr][k + 1] * t1.x + cval[rr][k + 2] * t2.x + cval[rr][k + 3] * t3.x;
+          ay += cval[rr][k] * t0.y + cval[rr][k + 1] * t1.y + cval[rr][k + 2] * t2.y + cval[rr][k + 3] * t3.y;
+        }
+        for (; k < c; ++k) {
+          const double2 t0 = __ldg(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k] * du));
+          ax += cval[rr][k] * t0.x;
+          ay += cval[rr][k] * t0.y;
+        }
+        double2 yv = *reinterpret_cast<double2 *>(y + base);
+        yv.x += xs * ax;
+        yv.y += xs * ay;
+        *reinterpret_cast<double2 *>(y + base) = yv;
+        if (red_mask) {
+          const double2 xv = __ldg(reinterpret_cast<const double2 *>(x + base));
+          red[0] += xs * (xv.x * yv.x + xv.y * yv.y);
+          red[1] += yv.x * yv.x + yv.y * yv.y;
+          red[2] += xs * xs * (xv.x * xv.x + xv.y * xv.y);
+        }
+      } else {
+        const double *xb = x + u0;
+        double a = 0.0;
+        int k = 0;
+        for (; k + 4 <= c; k += 4) {
+          const double t0 = __ldg(xb + (size_t)cidx[rr][k] * du), t1 = __ldg(xb + (size_t)cidx[rr][k + 1] * du);
+          const double t2 = __ldg(xb + (size_t)cidx[rr][k + 2] * du), t3 = __ldg(xb + (size_t)cidx[rr][k + 3] * du);
+          a += cval[rr][k] * t0 + cval[rr][k + 1] * t1 + cval[rr][k + 2] * t2 + cval[rr][k + 3] * t3;
+        }
+        for (; k < c; ++k) a += cval[rr][k] * __ldg(xb + (size_t)cidx[rr][k] * du);
+        const double yv = y[base] + xs * a;
+        y[base] = yv;
+        if (red_mask) {
+          const double xv = x[base];
+          red[0] += xs * xv * yv;
+          red[1] += yv * yv;
+          red[2] += xs * xs * xv * xv;
+        }
+      }
+    }
+  }
+  if (red_mask) block_reduce_store<3>(red, partials, 3);
+}
+
 // --------------------------------------------------------- vector kernels ----
 
 template <int G>
@@ -533,6 +682,14 @@ void launch_cdag_gather(int L, int spin, int a, int pm, const uint32_t *tub, uin
 
 namespace {
 constexpr size_t kRowSmemMax = 112 * 1024;
+constexpr size_t kRowSmem2Max = 220 * 1024;  // below the 227 KB per-CTA limit
+}
+
+int hv_cols_grid(const HvOperator &op) {
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const uint32_t W = ((du % 2 == 0) ? 2 : 1) * kThreads;
+  const size_t nitems = (size_t)((du + W - 1) / W) * ((dd + kColsR - 1) / kColsR);
+  return (int)std::max<size_t>(1, std::min<size_t>(nitems, (size_t)device_sms() * 8));
 }
 
 void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,
@@ -540,7 +697,19 @@ void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,
   const uint32_t du = op.up.dim, dd = op.dn.dim;
   const size_t smem = (size_t)du * sizeof(double);
   int threads = du >= 512 ? 512 : (du >= 256 ? 256 : 128);
-  if (smem <= kRowSmemMax) {
+  const size_t smem2 = 2 * smem;  // two rows interleaved
+  if (smem2 <= kRowSmem2Max && dd >= 2) {
+    static bool attr2 = false;
+    if (!attr2) {
+      QED_CUDA(cudaFuncSetAttribute(k_hv_rows2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kRowSmem2Max));
+      attr2 = true;
+    }
+    const int t2 = du >= 1024 ? 1024 : threads;
+    const int per_sm = smem2 > 110 * 1024 ? 1 : (smem2 > 72 * 1024 ? 2 : 3);
+    int grid = (int)std::min<size_t>((dd + 1) / 2, (size_t)device_sms() * per_sm);
+    k_hv_rows2<<<grid, t2, smem2, s>>>(op, x, xs, y, sub);
+  } else if (smem <= kRowSmemMax) {
     static bool attr = false;
     if (!attr) {
       QED_CUDA(cudaFuncSetAttribute(k_hv_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -559,17 +728,13 @@ void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,
 
 int launch_hv_cols(const HvOperator &op, const double *x, double xs, double *y, int red_mask,
                    Reducer &r, cudaStream_t s) {
-  const uint32_t du = op.up.dim, dd = op.dn.dim;
-  const int R = 4;
-  const bool vec2 = (du % 2 == 0);
-  const uint32_t W = (vec2 ? 2 : 1) * kThreads;
-  size_t nitems = (size_t)((du + W - 1) / W) * ((dd + R - 1) / R);
-  int grid = (int)std::min<size_t>(nitems, (size_t)device_sms() * 8);
+  const bool vec2 = (op.up.dim % 2 == 0);
+  int grid = hv_cols_grid(op);
   if (red_mask && grid > r.max_blocks) grid = r.max_blocks;
   if (vec2)
-    k_hv_cols<2, R><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
+    k_hv_cols2<2><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
   else
-    k_hv_cols<1, R><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
+    k_hv_cols2<1><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
   QED_LAUNCH();
   return grid;
 }
@@ -675,12 +840,9 @@ double *noalloc_partials_address() {
 
 void launch_hv_dots_noalloc(const HvOperator &op, const double *x, double *y, double *dots,
                             cudaStream_t s) {
-  // Work items of the column pass and the grid it launches (grid-stride):
-  // at most 8 CTAs per SM, and never more rows than the scratch holds.
-  const uint32_t du = op.up.dim, dd = op.dn.dim;
-  const uint32_t W = ((du % 2 == 0) ? 2 : 1) * kThreads;
-  const size_t nitems = (size_t)((du + W - 1) / W) * ((dd + 3) / 4);
-  const size_t want = std::min<size_t>(nitems, (size_t)device_sms() * 8);
+  // The grid the column pass launches (grid-stride, at most 8 CTAs per SM);
+  // each CTA needs one row of the scratch.
+  const size_t want = (size_t)hv_cols_grid(op);
   if (want > (size_t)kHvColsMaxBlocks)
     fail(QED_ERR_MEMORY, "H.v without allocation: the column pass needs " + std::to_string(want) +
                              " partial-sum rows, the fixed scratch holds " +

@@ -331,6 +331,7 @@ __global__ void __launch_bounds__(kThreads) k_hv_cols(HvOperator op, const doubl
 // Row pass, two dn rows per CTA step: the rows are staged interleaved in shared
 // memory (one double2 per up string), so every hop-table entry and every
 // shared-memory gather serves both rows, and the gathers are 16 bytes wide.
+template <int UNROLL>
 __global__ void __launch_bounds__(1024) k_hv_rows2(HvOperator op, const double *__restrict__ x,
                                                    double xs, double *y, SubList sub) {
   extern __shared__ double2 xs2[];
@@ -355,16 +356,19 @@ __global__ void __launch_bounds__(1024) k_hv_rows2(HvOperator op, const double *
       const int c = op.up.cnt[u];
       const uint32_t *ep = op.up.ell + u;
       int k = 0;
-      for (; k + 2 <= c; k += 2) {  // two independent gathers in flight
-        const uint32_t f0 = __ldg(ep + (size_t)k * du), f1 = __ldg(ep + (size_t)(k + 1) * du);
-        const double2 t0 = xs2[f0 >> 8], t1 = xs2[f1 >> 8];
-        const double v0 = vals[f0 & 255u], v1 = vals[f1 & 255u];
-        a0 += v0 * t0.x;
-        a1 += v0 * t0.y;
-        a0 += v1 * t1.x;
-        a1 += v1 * t1.y;
+      for (; k + UNROLL <= c; k += UNROLL) {  // UNROLL independent gathers in flight
+        uint32_t f[UNROLL];
+#pragma unroll
+        for (int q = 0; q < UNROLL; ++q) f[q] = __ldg(ep + (size_t)(k + q) * du);
+#pragma unroll
+        for (int q = 0; q < UNROLL; ++q) {
+          const double2 t = xs2[f[q] >> 8];
+          const double v = vals[f[q] & 255u];
+          a0 += v * t.x;
+          a1 += v * t.y;
+        }
       }
-      if (k < c) {
+      for (; k < c; ++k) {
         const uint32_t f0 = __ldg(ep + (size_t)k * du);
         const double2 t0 = xs2[f0 >> 8];
         const double v0 = vals[f0 & 255u];
@@ -390,7 +394,11 @@ __global__ void __launch_bounds__(1024) k_hv_rows2(HvOperator op, const double *
 constexpr int kColsR = 4;
 constexpr int kMaxHops = 256;
 
-template <int VEC>
+template <class T> __device__ __forceinline__ T gather_ld(const T *p, bool l2only) {
+  return l2only ? __ldcg(p) : __ldg(p);
+}
+
+template <int VEC, bool CG>
 __global__ void __launch_bounds__(kThreads) k_hv_cols2(HvOperator op, const double *__restrict__ x,
                                                         double xs, double *y, int red_mask,
                                                         double *partials) {
@@ -431,15 +439,15 @@ __global__ void __launch_bounds__(kThreads) k_hv_cols2(HvOperator op, const doub
         double ax = 0.0, ay = 0.0;
         int k = 0;
         for (; k + 4 <= c; k += 4) {
-          const double2 t0 = __ldg(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k] * du));
-          const double2 t1 = __ldg(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k + 1] * du));
-          const double2 t2 = __ldg(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k + 2] * du));
-          const double2 t3 = __ldg(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k + 3] * du));
+          const double2 t0 = gather_ld(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k] * du), CG);
+          const double2 t1 = gather_ld(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k + 1] * du), CG);
+          const double2 t2 = gather_ld(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k + 2] * du), CG);
+          const double2 t3 = gather_ld(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k + 3] * du), CG);
           ax += cval[rr][k] * t0.x + cval[rr][k + 1] * t1.x + cval[rr][k + 2] * t2.x + cval[rr][k + 3] * t3.x;
           ay += cval[rr][k] * t0.y + cval[rr][k + 1] * t1.y + cval[rr][k + 2] * t2.y + cval[rr][k + 3] * t3.y;
         }
         for (; k < c; ++k) {
-          const double2 t0 = __ldg(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k] * du));
+          const double2 t0 = gather_ld(reinterpret_cast<const double2 *>(xb + (size_t)cidx[rr][k] * du), CG);
           ax += cval[rr][k] * t0.x;
           ay += cval[rr][k] * t0.y;
         }
@@ -685,6 +693,17 @@ constexpr size_t kRowSmemMax = 112 * 1024;
 constexpr size_t kRowSmem2Max = 220 * 1024;  // below the 227 KB per-CTA limit
 }
 
+// Launch variant of the H.v passes (bit 0: column-pass gathers cached in L2
+// only; bit 1: row pass with four gathers in flight). QED_HV_VARIANT overrides.
+int hv_variant() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("QED_HV_VARIANT");
+    v = e ? atoi(e) : 0;
+  }
+  return v;
+}
+
 int hv_cols_grid(const HvOperator &op) {
   const uint32_t du = op.up.dim, dd = op.dn.dim;
   const uint32_t W = ((du % 2 == 0) ? 2 : 1) * kThreads;
@@ -701,14 +720,19 @@ void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,
   if (smem2 <= kRowSmem2Max && dd >= 2) {
     static bool attr2 = false;
     if (!attr2) {
-      QED_CUDA(cudaFuncSetAttribute(k_hv_rows2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      QED_CUDA(cudaFuncSetAttribute(k_hv_rows2<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kRowSmem2Max));
+      QED_CUDA(cudaFuncSetAttribute(k_hv_rows2<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kRowSmem2Max));
       attr2 = true;
     }
     const int t2 = du >= 1024 ? 1024 : threads;
     const int per_sm = smem2 > 110 * 1024 ? 1 : (smem2 > 72 * 1024 ? 2 : 3);
     int grid = (int)std::min<size_t>((dd + 1) / 2, (size_t)device_sms() * per_sm);
-    k_hv_rows2<<<grid, t2, smem2, s>>>(op, x, xs, y, sub);
+    if (hv_variant() & 2)
+      k_hv_rows2<4><<<grid, t2, smem2, s>>>(op, x, xs, y, sub);
+    else
+      k_hv_rows2<2><<<grid, t2, smem2, s>>>(op, x, xs, y, sub);
   } else if (smem <= kRowSmemMax) {
     static bool attr = false;
     if (!attr) {
@@ -731,10 +755,13 @@ int launch_hv_cols(const HvOperator &op, const double *x, double xs, double *y, 
   const bool vec2 = (op.up.dim % 2 == 0);
   int grid = hv_cols_grid(op);
   if (red_mask && grid > r.max_blocks) grid = r.max_blocks;
-  if (vec2)
-    k_hv_cols2<2><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
+  const bool cg = hv_variant() & 1;
+  if (vec2 && cg)
+    k_hv_cols2<2, true><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
+  else if (vec2)
+    k_hv_cols2<2, false><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
   else
-    k_hv_cols2<1><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
+    k_hv_cols2<1, false><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
   QED_LAUNCH();
   return grid;
 }

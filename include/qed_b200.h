@@ -88,6 +88,18 @@ int qed_mixing(int label, int *mixing);
  * string of the kept states ("R0:N8:S0:1" style, as GS_string()). */
 int qed_ground_state_solve(int label, double *energy, char *sectors, int len);
 
+/* Batched ground states (the per-instance loop of the lattice layer,
+ * src_qcm/lattice_model_instance.cpp:107-113, run by OpenMP threads there):
+ * solves the instances labels[0..n) concurrently on `threads` host threads
+ * (0 = hardware concurrency, capped at 64), each driving its own CUDA stream.
+ * energies[i] receives the ground-state energy of labels[i]. Every instance is
+ * attempted; the status of the first failure is returned (message via
+ * qed_last_error). */
+int qed_ground_state_solve_batch(const int *labels, int n, int threads, double *energies);
+
+/* Batched Green_function_solve over labels[0..n), same threading rules. */
+int qed_Green_function_solve_batch(const int *labels, int n, int threads);
+
 /* ED::Green_function_solve (src_ed/qcm_ED.hpp:122 -> src_ed/model_instance.hpp:517-555):
  * band-Lanczos Q-matrix (GF_method 'L') or continued fractions ('F'). */
 int qed_Green_function_solve(int label);

@@ -192,6 +192,27 @@ def Green_function_solve(label: int = 0):
     _check(lib().qed_Green_function_solve(label))
 
 
+def ground_state_solve_batch(labels, threads: int = 0):
+    """Ground states of many instances at once, on `threads` host threads with one
+    CUDA stream each (0 = all hardware threads). Returns the energies."""
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    e = np.zeros(len(lab))
+    L = lib()
+    L.qed_ground_state_solve_batch.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(C.c_double)]
+    L.qed_ground_state_solve_batch.restype = C.c_int
+    _check(L.qed_ground_state_solve_batch(lab.ctypes.data_as(C.POINTER(C.c_int)), len(lab), threads, _dp(e)))
+    return e
+
+
+def Green_function_solve_batch(labels, threads: int = 0):
+    """Green_function_solve for many instances at once (see ground_state_solve_batch)."""
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    L = lib()
+    L.qed_Green_function_solve_batch.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_int]
+    L.qed_Green_function_solve_batch.restype = C.c_int
+    _check(L.qed_Green_function_solve_batch(lab.ctypes.data_as(C.POINTER(C.c_int)), len(lab), threads))
+
+
 def Green_function_dimension(label: int = 0) -> int:
     d = C.c_int()
     _check(lib().qed_Green_function_dimension(label, C.byref(d)))

@@ -1,6 +1,9 @@
 // The C ABI of include/qed_b200.h: registries of models / instances / sector
 // Hamiltonians, and the error convention (status code + per-thread message).
+#include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <thread>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -17,6 +20,7 @@ struct qed_hamiltonian {
   std::unique_ptr<SectorOp> H;
   DevBuf<double> x, y;
   DevBuf<double> partials;  // per-block partial sums of apply_dots_device
+  std::mutex m;             // calls on one handle are serialised
 };
 
 namespace {
@@ -24,25 +28,37 @@ namespace {
 thread_local std::string t_err;
 
 // Models and instances live in process-global maps, as the reference's
-// (src_ed/qcm_ED.cpp:25-26). One Workspace (stream + reduction buffers) per
-// device context; GPU work from different host threads is serialised on it.
+// (src_ed/qcm_ED.cpp:25-26). GPU work runs on a Workspace (stream + reduction
+// buffers) owned by the calling host thread, so threads driving different
+// instances overlap on the GPU; calls on one instance are serialised by its mutex.
 std::mutex g_reg;
 std::map<std::string, std::shared_ptr<Model>> g_models;
 std::map<int, std::shared_ptr<Instance>> g_instances;
-std::recursive_mutex g_gpu;
-std::unique_ptr<Workspace> g_ws;
-int g_device = 0;
+std::atomic<int> g_device{0};
+std::atomic<bool> g_device_fixed{false};
 
 Workspace &ws() {
-  if (!g_ws) {
+  thread_local std::unique_ptr<Workspace> tws;
+  if (!tws) {
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);
     if (e != cudaSuccess || n == 0)
       fail(QED_ERR_NO_DEVICE, std::string("no CUDA device available: ") + cudaGetErrorString(e));
-    QED_CUDA(cudaSetDevice(g_device));
-    g_ws.reset(new Workspace());
+    const int dev = g_device.load();
+    QED_CUDA(cudaSetDevice(dev));
+    static std::once_flag pool_once;
+    std::call_once(pool_once, [dev] {
+      // keep freed blocks in the device's pool: repeated solves reuse them
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+      }
+    });
+    g_device_fixed = true;
+    tws.reset(new Workspace());
   }
-  return *g_ws;
+  return *tws;
 }
 
 template <class F> int guarded(F &&f) {
@@ -69,6 +85,36 @@ std::shared_ptr<Instance> instance(int label) {
   return it->second;
 }
 
+// Runs fn(i) for i in [0, n) on `threads` host threads (each with its own
+// Workspace / CUDA stream). Returns the status of the first failure.
+template <class F> int run_batch(int n, int threads, F &&fn) {
+  if (n <= 0) return QED_OK;
+  int hw = (int)std::thread::hardware_concurrency();
+  if (threads <= 0) threads = hw > 0 ? hw : 8;
+  threads = std::max(1, std::min({threads, n, 64}));
+  std::atomic<int> next{0};
+  std::atomic<int> first_code{QED_OK};
+  std::mutex emtx;
+  std::string first_msg;
+  auto work = [&] {
+    for (int i = next++; i < n; i = next++) {
+      int rc = guarded([&] { fn(i); });
+      if (rc != QED_OK) {
+        int expected = QED_OK;
+        if (first_code.compare_exchange_strong(expected, rc)) {
+          std::lock_guard<std::mutex> l(emtx);
+          first_msg = t_err;
+        }
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < threads; ++t) pool.emplace_back(work);
+  work();
+  for (auto &th : pool) th.join();
+  if (first_code != QED_OK) t_err = first_msg;
+  return first_code;
+}
 }  // namespace
 
 extern "C" {
@@ -83,8 +129,7 @@ int qed_last_error(char *buf, int len) {
 
 int qed_init(int device) {
   return guarded([&] {
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
-    if (g_ws && device != g_device) fail(QED_ERR_ARGUMENT, "qed_init: device already selected");
+    if (g_device_fixed && device != g_device) fail(QED_ERR_ARGUMENT, "qed_init: device already selected");
     g_device = device;
     ws();
   });
@@ -172,7 +217,7 @@ int qed_erase_model_instance(int label) {
       keep = it->second;
       g_instances.erase(it);
     }
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    ws();
     keep.reset();
   });
 }
@@ -185,7 +230,6 @@ int qed_ground_state_solve(int label, double *energy, char *sectors, int len) {
   return guarded([&] {
     auto I = instance(label);
     std::lock_guard<std::mutex> li(I->mtx);
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     auto r = I->low_energy_states(ws());
     *energy = r.first;
     if (sectors && len > 0) {
@@ -195,11 +239,35 @@ int qed_ground_state_solve(int label, double *energy, char *sectors, int len) {
   });
 }
 
+
+int qed_ground_state_solve_batch(const int *labels, int n, int threads, double *energies) {
+  if (n > 0 && (!labels || !energies)) {
+    t_err = "null argument";
+    return QED_ERR_ARGUMENT;
+  }
+  return run_batch(n, threads, [&](int i) {
+    auto I = instance(labels[i]);
+    std::lock_guard<std::mutex> li(I->mtx);
+    energies[i] = I->low_energy_states(ws()).first;
+  });
+}
+
+int qed_Green_function_solve_batch(const int *labels, int n, int threads) {
+  if (n > 0 && !labels) {
+    t_err = "null argument";
+    return QED_ERR_ARGUMENT;
+  }
+  return run_batch(n, threads, [&](int i) {
+    auto I = instance(labels[i]);
+    std::lock_guard<std::mutex> li(I->mtx);
+    I->green_solve(ws());
+  });
+}
+
 int qed_Green_function_solve(int label) {
   return guarded([&] {
     auto I = instance(label);
     std::lock_guard<std::mutex> li(I->mtx);
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     I->green_solve(ws());
   });
 }
@@ -212,7 +280,6 @@ int qed_Green_function(int label, int spin_down, int nz, const double *z, double
   return guarded([&] {
     auto I = instance(label);
     std::lock_guard<std::mutex> li(I->mtx);
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     I->green_function(reinterpret_cast<const cplx *>(z), nz, spin_down != 0, reinterpret_cast<cplx *>(G), ws());
   });
 }
@@ -221,7 +288,6 @@ int qed_self_energy(int label, int spin_down, int nz, const double *z, double *S
   return guarded([&] {
     auto I = instance(label);
     std::lock_guard<std::mutex> li(I->mtx);
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     I->self_energy(reinterpret_cast<const cplx *>(z), nz, spin_down != 0, reinterpret_cast<cplx *>(S), ws());
   });
 }
@@ -238,7 +304,6 @@ int qed_Green_function_average(int label, int spin_down, double *M) {
   return guarded([&] {
     auto I = instance(label);
     std::lock_guard<std::mutex> li(I->mtx);
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     I->green_solve(ws());
     const auto &src = I->Mave[(spin_down && (I->mix & mixing::up_down)) ? 1 : 0];
     std::memcpy(M, src.data(), src.size() * sizeof(cplx));
@@ -249,7 +314,6 @@ int qed_Potthoff_functional(int label, double *omega) {
   return guarded([&] {
     auto I = instance(label);
     std::lock_guard<std::mutex> li(I->mtx);
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     *omega = I->potthoff(ws());
   });
 }
@@ -260,7 +324,6 @@ int qed_qmatrix(int label, int spin_down, int *M, int *L, double *e, double *v) 
     std::lock_guard<std::mutex> li(I->mtx);
     if (I->use_cf) fail(QED_ERR_ARGUMENT, "Green function format is not Lehmann! Cannot output the Q matrix.");
     {
-      std::lock_guard<std::recursive_mutex> g(g_gpu);
       I->green_solve(ws());
     }
     // model_instance::qmatrix (src_ed/model_instance.hpp:1425-1451): one state
@@ -292,7 +355,6 @@ int qed_cf_coefficients(int label, int spin_down, int o1, int o2, int pm, int *n
     std::lock_guard<std::mutex> li(I->mtx);
     if (!I->use_cf) fail(QED_ERR_ARGUMENT, "not a continued-fraction instance");
     {
-      std::lock_guard<std::recursive_mutex> g(g_gpu);
       I->green_solve(ws());
     }
     const CFSet &cf = I->states.front()->cf[spin_down ? 1 : 0];
@@ -311,7 +373,6 @@ int qed_ground_state_vector(int label, long *dim, double *psi) {
   return guarded([&] {
     auto I = instance(label);
     std::lock_guard<std::mutex> li(I->mtx);
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     I->low_energy_states(ws());
     const State &st = *I->states.front();
     *dim = (long)st.psi.n;
@@ -325,7 +386,6 @@ int qed_ground_state_vector(int label, long *dim, double *psi) {
 int qed_hamiltonian_create(int label, const char *sector, qed_hamiltonian **h, long *dim) {
   return guarded([&] {
     auto I = instance(label);
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     auto *hh = new qed_hamiltonian;
     try {
       hh->H.reset(new SectorOp(I->terms, Sector(sector), ws()));
@@ -341,7 +401,7 @@ int qed_hamiltonian_create(int label, const char *sector, qed_hamiltonian **h, l
 int qed_hamiltonian_mult_add(qed_hamiltonian *h, const double *x, double *y) {
   return guarded([&] {
     if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    std::lock_guard<std::mutex> hl(h->m);
     const size_t D = h->H->D;
     if (!D) return;
     if (h->x.n < D) { h->x.alloc(D); h->y.alloc(D); }
@@ -363,7 +423,7 @@ int qed_hamiltonian_mult_add(qed_hamiltonian *h, const double *x, double *y) {
 int qed_hamiltonian_apply_device(qed_hamiltonian *h, const double *x, double *y, void *stream) {
   return guarded([&] {
     if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    std::lock_guard<std::mutex> hl(h->m);
     Workspace &w = ws();
     cudaStream_t s = (cudaStream_t)stream;
     if (!h->H->D) return;
@@ -378,14 +438,17 @@ int qed_hamiltonian_apply_dots_device(qed_hamiltonian *h, const double *x, doubl
   return guarded([&] {
     if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
     if (!dots) fail(QED_ERR_ARGUMENT, "null output array");
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    std::lock_guard<std::mutex> hl(h->m);
     ws();
     cudaStream_t s = (cudaStream_t)stream;
     if (!h->H->D) {
       QED_CUDA(cudaMemsetAsync(dots, 0, 3 * sizeof(double), s));
       return;
     }
-    if (!h->partials.n) h->partials.alloc((size_t)kHvColsMaxBlocks * Reducer::kMaxRed);
+    if (!h->partials.n) {
+      h->partials.alloc((size_t)kHvColsMaxBlocks * Reducer::kMaxRed);
+      ws().sync();  // allocated in this thread's stream order, used on `stream`
+    }
     Reducer r;
     r.partials = h->partials.p;
     r.max_blocks = kHvColsMaxBlocks;
@@ -403,7 +466,6 @@ int qed_hamiltonian_apply_dots_device_noalloc(qed_hamiltonian *h, const double *
                                               double *dots, void *stream) {
   return guarded([&] {
     if (!h || !x || !y || !dots) fail(QED_ERR_ARGUMENT, "null argument");
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     cudaStream_t s = (cudaStream_t)stream;
     if (!h->H->D) {
       QED_CUDA(cudaMemsetAsync(dots, 0, 3 * sizeof(double), s));
@@ -416,7 +478,7 @@ int qed_hamiltonian_apply_dots_device_noalloc(qed_hamiltonian *h, const double *
 int qed_hamiltonian_diag(qed_hamiltonian *h, double *d) {
   return guarded([&] {
     if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
+    std::lock_guard<std::mutex> hl(h->m);
     // diagonal = H applied to unit vectors is wasteful; rebuild it from the tables on the host
     const SectorOp &H = *h->H;
     std::vector<double> du(H.up.dim), dd(H.dn.dim);
@@ -450,7 +512,6 @@ int qed_hamiltonian_diag(qed_hamiltonian *h, double *d) {
 
 int qed_hamiltonian_destroy(qed_hamiltonian *h) {
   return guarded([&] {
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     delete h;
   });
 }
@@ -461,7 +522,6 @@ int qed_halfbasis(int L, int N, unsigned *strings, long *dim) {
     uint64_t d = binom(L, N);
     *dim = (long)d;
     if (!strings || !d) return;
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     Workspace &w = ws();
     DevBuf<uint32_t> b(d);
     launch_unrank(L, N, (uint32_t)d, b.p, w.stream);
@@ -474,7 +534,6 @@ int qed_halfbasis_rank(int L, int N, long n, const unsigned *strings, unsigned *
   return guarded([&] {
     if (L < 1 || L > 32 || N < 0 || N > L) fail(QED_ERR_ARGUMENT, "bad (L, N)");
     if (n <= 0) return;
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     Workspace &w = ws();
     DevBuf<uint32_t> s(n), r(n);
     s.upload(strings, n, w.stream);
@@ -487,7 +546,6 @@ int qed_halfbasis_rank(int L, int N, long n, const unsigned *strings, unsigned *
 int qed_destroy_table(int L, int n_up, int n_dn, int a, long *target, int *phase) {
   return guarded([&] {
     if (L < 1 || L > 32 || a < 0 || a >= 2 * L) fail(QED_ERR_ARGUMENT, "bad orbital");
-    std::lock_guard<std::recursive_mutex> g(g_gpu);
     Workspace &w = ws();
     // Evaluate c_a on every source state with the device gather: the source
     // state index is encoded as its value, so the gathered value identifies it.

@@ -33,7 +33,16 @@ inline void cuda_check(cudaError_t e, const char *what, const char *file, int li
 #define QED_CUDA(x) ::qed::cuda_check((x), #x, __FILE__, __LINE__)
 #define QED_LAUNCH() ::qed::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
 
-// Owning device allocation (cudaMalloc / cudaFree).
+// Stream used for stream-ordered allocation by the calling host thread: the
+// stream of that thread's Workspace (legacy default stream before one exists).
+cudaStream_t alloc_stream();
+
+// Owning device allocation, stream-ordered (cudaMallocAsync / cudaFreeAsync on
+// the calling thread's stream, served from the device's memory pool), so that
+// allocating and freeing never synchronises the whole device and host threads
+// driving different instances do not serialise each other. Library calls
+// synchronise their stream before returning, so a buffer may be freed from any
+// thread once the call that used it has returned.
 template <class T> struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
@@ -49,11 +58,11 @@ template <class T> struct DevBuf {
   ~DevBuf() { release(); }
   void alloc(size_t count) {
     release();
-    if (count) QED_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    if (count) QED_CUDA(cudaMallocAsync((void **)&p, count * sizeof(T), alloc_stream()));
     n = count;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, alloc_stream());
     p = nullptr;
     n = 0;
   }

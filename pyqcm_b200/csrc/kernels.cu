@@ -22,15 +22,15 @@ constexpr int kThreads = 256;
 
 // C(n, k) for n, k <= 32 (C(32,16) < 2^32).
 __constant__ uint32_t c_binom[33][33];
-bool g_binom_ready = false;
+std::once_flag g_binom_once;
 
 void ensure_binom() {
-  if (g_binom_ready) return;
-  uint32_t h[33][33] = {};
-  for (int n = 0; n <= 32; ++n)
-    for (int k = 0; k <= 32; ++k) h[n][k] = (uint32_t)binom(n, k);
-  QED_CUDA(cudaMemcpyToSymbol(c_binom, h, sizeof(h)));
-  g_binom_ready = true;
+  std::call_once(g_binom_once, [] {
+    uint32_t h[33][33] = {};
+    for (int n = 0; n <= 32; ++n)
+      for (int k = 0; k <= 32; ++k) h[n][k] = (uint32_t)binom(n, k);
+    QED_CUDA(cudaMemcpyToSymbol(c_binom, h, sizeof(h)));
+  });
 }
 
 // Colex rank of an N-of-L string: sum_k C(p_k, k+1) over set bits p_0 < p_1 < ...
@@ -101,13 +101,12 @@ int grid_for(size_t n, int num_sms, int per_sm = 4) {
 }
 
 int device_sms() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
+  static const int n = [] {
+    int dev = 0, c = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
+    cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+    return c > 0 ? c : 148;
+  }();
   return n;
 }
 
@@ -696,11 +695,10 @@ constexpr size_t kRowSmem2Max = 220 * 1024;  // below the 227 KB per-CTA limit
 // Launch variant of the H.v passes (bit 0: column-pass gathers cached in L2
 // only; bit 1: row pass with four gathers in flight). QED_HV_VARIANT overrides.
 int hv_variant() {
-  static int v = -1;
-  if (v < 0) {
+  static const int v = [] {
     const char *e = getenv("QED_HV_VARIANT");
-    v = e ? atoi(e) : 0;
-  }
+    return e ? atoi(e) : 0;
+  }();
   return v;
 }
 
@@ -718,14 +716,14 @@ void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,
   int threads = du >= 512 ? 512 : (du >= 256 ? 256 : 128);
   const size_t smem2 = 2 * smem;  // two rows interleaved
   if (smem2 <= kRowSmem2Max && dd >= 2) {
-    static bool attr2 = false;
-    if (!attr2) {
+    static const bool attr2 = [] {
       QED_CUDA(cudaFuncSetAttribute(k_hv_rows2<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kRowSmem2Max));
       QED_CUDA(cudaFuncSetAttribute(k_hv_rows2<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kRowSmem2Max));
-      attr2 = true;
-    }
+      return true;
+    }();
+    (void)attr2;
     const int t2 = du >= 1024 ? 1024 : threads;
     const int per_sm = smem2 > 110 * 1024 ? 1 : (smem2 > 72 * 1024 ? 2 : 3);
     int grid = (int)std::min<size_t>((dd + 1) / 2, (size_t)device_sms() * per_sm);
@@ -734,12 +732,12 @@ void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,
     else
       k_hv_rows2<2><<<grid, t2, smem2, s>>>(op, x, xs, y, sub);
   } else if (smem <= kRowSmemMax) {
-    static bool attr = false;
-    if (!attr) {
+    static const bool attr = [] {
       QED_CUDA(cudaFuncSetAttribute(k_hv_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kRowSmemMax));
-      attr = true;
-    }
+      return true;
+    }();
+    (void)attr;
     int per_sm = smem > 100 * 1024 ? 2 : 4;
     int grid = (int)std::min<size_t>(dd, (size_t)device_sms() * per_sm);
     k_hv_rows<true><<<grid, threads, smem, s>>>(op, x, xs, y, sub);

@@ -13,8 +13,15 @@ namespace qed {
 
 // ---------------------------------------------------------------- Workspace --
 
+namespace {
+thread_local cudaStream_t tls_stream = nullptr;  // stream of this thread's Workspace
+}
+
+cudaStream_t alloc_stream() { return tls_stream; }
+
 Workspace::Workspace() {
   QED_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  tls_stream = stream;
   red.max_blocks = 4096;
   partials.alloc((size_t)red.max_blocks * Reducer::kMaxRed);
   out.alloc(Reducer::kMaxRed);
@@ -22,10 +29,16 @@ Workspace::Workspace() {
   red.partials = partials.p;
   red.out = out.p;
   red.host = host;
+  sync();
 }
 
 Workspace::~Workspace() {
+  // free the stream-ordered buffers while the stream still exists
+  partials.release();
+  out.release();
+  if (stream) cudaStreamSynchronize(stream);
   if (host) cudaFreeHost(host);
+  if (tls_stream == stream) tls_stream = nullptr;
   if (stream) cudaStreamDestroy(stream);
 }
 

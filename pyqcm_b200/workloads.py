@@ -136,10 +136,13 @@ def square4x4() -> ClusterProblem:
     return hubbard_cluster(4, 4, t=-1.0, tp=0.3, U=8.0, mu=4.0, name="sq4x4")
 
 
-def random_batch(n: int = 1024, seed: int = 12345):
-    """Seeded draw of independent clusters with every (N_up, N_dn) sector listed."""
+def random_batch(n: int = 1024, seed: int = 12345, geoms=None):
+    """Seeded draw of independent clusters with every (N_up, N_dn) sector listed.
+
+    Geometry uniform over 2x2, 2x3, 2x4, chain 8, chain 10 (or `geoms`), t=-1,
+    U ~ U[0,12], mu ~ U[0,U], staggered Neel field M ~ U[0,0.3]."""
     rng = np.random.default_rng(seed)
-    geoms = [(2, 2), (2, 3), (2, 4), (8, 1), (10, 1)]
+    geoms = geoms or [(2, 2), (2, 3), (2, 4), (8, 1), (10, 1)]
     out = []
     for k in range(n):
         nx, ny = geoms[rng.integers(len(geoms))]

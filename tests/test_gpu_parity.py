@@ -167,3 +167,28 @@ def test_apply_dots_device_matches_host_path(qed, oracle, fresh):
     assert abs(d[0] - x @ y_ref) < 1e-10 * abs(x @ y_ref)
     assert abs(d[1] - y_ref @ y_ref) < 1e-10 * (y_ref @ y_ref)
     assert abs(d[2] - x @ x) < 1e-12 * (x @ x)
+
+
+def test_batched_solves_match_reference(qed, oracle, fresh):
+    """Many random clusters (every sector listed, staggered field) solved concurrently."""
+    probs = W.random_batch(12, seed=77, geoms=[(2, 2), (2, 3), (2, 4), (8, 1)])
+    labels = []
+    for p in probs:
+        suffix, label = fresh()
+        load_both(qed, oracle, p, suffix, label, fmt="F")
+        labels.append(label)
+    set_both(qed, oracle, GF_method="L")
+    e = qed.ground_state_solve_batch(labels, threads=6)
+    qed.Green_function_solve_batch(labels, threads=6)
+    z = W.matsubara(64)
+    for p, lab, ei in zip(probs, labels, e):
+        e_ref, sec_ref = oracle.ground_state(lab)
+        assert abs(ei - e_ref) <= 1e-10 * max(1.0, abs(e_ref)), (p.name, ei, e_ref)
+        assert qed.ground_state_solve(lab)[1] == sec_ref
+        G1 = qed.Green_function(z, label=lab)
+        G2 = oracle.green_function(lab, z)
+        assert np.max(np.abs(G1 - G2)) < 1e-8, p.name
+        if qed.mixing(lab) & 4:
+            G1d = qed.Green_function(z, spin_down=True, label=lab)
+            G2d = oracle.green_function(lab, z, spin_down=True)
+            assert np.max(np.abs(G1d - G2d)) < 1e-8, p.name

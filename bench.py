@@ -47,6 +47,11 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: warm-up and timed H.v only (no e2e, clocks or CPU baseline)")
     ap.add_argument("--sector", default=None, help="sector of the 4x4 cluster to use (default R0:N16:S0)")
+    ap.add_argument("--workload", default="hv", choices=["hv", "batch", "baths"],
+                    help="hv: H.v on the 4x4 cluster (default); batch: independent random clusters, "
+                         "every sector, ground state + Green function; baths: 2x2 + 8-bath points")
+    ap.add_argument("--batch", type=int, default=64, help="instances per step for --workload batch/baths")
+    ap.add_argument("--threads", type=int, default=0, help="host threads for batched solves (0 = all)")
     return ap.parse_args()
 
 
@@ -290,11 +295,104 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def batch_problems(args, rank=0, world=1):
+    """The instances of one step, sharded round-robin over ranks (replicas)."""
+    from pyqcm_b200 import workloads as W
+    if args.workload == "batch":
+        probs = W.random_batch(args.batch, seed=12345)
+    else:
+        probs = W.random_baths(args.batch, seed=4242)
+    return probs[rank::world]
+
+
+def _ref_solve_one(payload):
+    """One instance through the reference (a worker process of the CPU pool)."""
+    prob, label, method = payload
+    from oracle import ref
+    ref.set_param("GF_method", method)
+    ref.load_problem(prob, label, model_name=f"refpool_{label}", fmt="F")
+    e, _ = ref.ground_state(label)
+    ref.green_solve(label)
+    return e
+
+
+def run_batch_workload(args, world, rank, local):
+    """ED solves/s: each instance = ground state over its listed sectors + Green function."""
+    metric = "ED solves/s"
+    wl = ("independent Hubbard clusters (2x2, 2x3, 2x4, chain 8, chain 10; U~U[0,12], mu~U[0,U], "
+          "Neel field M~U[0,0.3]; every (N_up,N_dn) sector), ground state + band-Lanczos Green function"
+          if args.workload == "batch" else
+          "2x2 plaquette + 8 bath orbitals, U=8, R0:N12:S0 (dim 853776), random baths; ground state + "
+          "4x4 band-Lanczos Green function")
+    probs = batch_problems(args, rank, world)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        import multiprocessing as mp
+        cores = os.cpu_count() or 8
+        n = min(len(probs), max(cores, 8 if args.workload == "batch" else 2))
+        sample = probs[:n]
+        ctx = mp.get_context("spawn")
+        t0 = time.perf_counter()
+        with ctx.Pool(cores) as pool:
+            pool.map(_ref_solve_one, [(p, 9100 + i, "L") for i, p in enumerate(sample)], chunksize=1)
+        dt = time.perf_counter() - t0
+        v = n / dt
+        line = {"metric": metric, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+                "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": wl, "instances_per_step": n},
+                "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "reference",
+                                 "sample": f"{n} instances, one process per core (the reference's ED is single-threaded per instance)"},
+                "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    import torch
+    import pyqcm_b200 as qed
+    torch.cuda.set_device(local)
+    qed.init(local)
+    qed.set_global_parameter("GF_method", "L")
+
+    def one_step(base):
+        labels = []
+        for i, p in enumerate(probs):
+            qed.load_problem(p, base + i, model_name=f"bw_{p.name}_{base + i}")
+            labels.append(base + i)
+        t0 = time.perf_counter()
+        qed.ground_state_solve_batch(labels, threads=args.threads)
+        qed.Green_function_solve_batch(labels, threads=args.threads)
+        G = [qed.Green_function(1j * np.pi / 50, label=l) for l in labels]  # results back on the host
+        dt = time.perf_counter() - t0
+        for l in labels:
+            qed.erase_model_instance(l)
+        return dt, G
+
+    for w in range(max(0, min(args.warmup, 1))):
+        one_step(200000 + 10000 * w)
+    steps = max(1, min(args.steps, 3))
+    times = [one_step(300000 + 10000 * k)[0] for k in range(steps)]
+    dt = sum(times) / steps
+    dt = max_over_ranks([dt], world, device=f"cuda:{local}")[0]
+    if rank == 0:
+        total = args.batch
+        line = {"metric": metric, "value": total / dt, "unit": "solves/s", "n_gpus": world, "steps": steps,
+                "warmup": min(args.warmup, 1), "ms_per_step": dt * 1e3, "higher_is_better": True,
+                "scaling": "weak" if world > 1 else "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": wl, "instances_per_step": total,
+                                                "host_threads": args.threads or os.cpu_count()},
+                "e2e": {"value": total / dt, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 16 * args.batch,
+                        "path": "qed_ground_state_solve_batch + qed_Green_function_solve_batch + G(z) read back"}}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     try:
-        if args.impl == "reference":
+        if args.workload != "hv":
+            run_batch_workload(args, world, rank, local)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_ours(args, world, rank, local)

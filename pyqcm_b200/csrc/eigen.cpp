@@ -11,6 +11,14 @@ namespace {
 
 constexpr double kEps = 2.220446049250313e-16;
 
+// sqrt(f^2 + g^2) without the cost of std::hypot; falls back to it only when
+// the squares under- or overflow.
+inline double pythag(double f, double g) {
+  const double r = std::sqrt(f * f + g * g);
+  if ((r == 0.0 && (f != 0.0 || g != 0.0)) || !std::isfinite(r)) return std::hypot(f, g);
+  return r;
+}
+
 // Implicit-shift QL on (d, e); e[i] couples i and i+1, e has n entries (last unused).
 // rot(i, c, s) is called for every plane rotation acting on columns (i, i+1) of
 // the eigenvector matrix, so a caller can accumulate all of it or one row.
@@ -30,7 +38,7 @@ bool ql_implicit(int n, double *d, double *e, Rot &&rot) {
       if (++iter > 100) return false;
       // Wilkinson-type shift from the leading 2x2 block.
       double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-      double r = std::hypot(g, 1.0);
+      double r = pythag(g, 1.0);
       g = d[m] - d[l] + e[l] / (g + std::copysign(r, g));
       double s = 1.0, c = 1.0, p = 0.0;
       int i = m - 1;
@@ -38,7 +46,7 @@ bool ql_implicit(int n, double *d, double *e, Rot &&rot) {
       for (; i >= l; --i) {
         double f = s * e[i];
         double b = c * e[i];
-        r = std::hypot(f, g);
+        r = pythag(f, g);
         e[i + 1] = r;
         if (r == 0.0) {  // split: recover and restart the sweep
           d[i + 1] -= p;
@@ -124,6 +132,68 @@ bool tridiag_lowest_last(int n, const double *alpha, const double *beta, double 
   return true;
 }
 
+void tridiag_lowest_fast(int n, const double *alpha, const double *beta, double upper,
+                         double *lambda0, double *last, std::vector<double> *vec) {
+  if (n == 1) {
+    *lambda0 = alpha[0];
+    *last = 1.0;
+    if (vec) vec->assign(1, 1.0);
+    return;
+  }
+  // Gershgorin interval
+  double lo = 1e300, hi = -1e300;
+  for (int i = 0; i < n; ++i) {
+    const double r = (i > 0 ? std::fabs(beta[i - 1]) : 0.0) + (i + 1 < n ? std::fabs(beta[i]) : 0.0);
+    lo = std::min(lo, alpha[i] - r);
+    hi = std::max(hi, alpha[i] + r);
+  }
+  if (std::isfinite(upper) && upper < hi) hi = upper + 1e-12 * (std::fabs(upper) + 1.0);
+  // number of eigenvalues < x (Sturm count via the LDL^T pivots)
+  auto count_below = [&](double x) {
+    int c = 0;
+    double q = alpha[0] - x;
+    if (q < 0) ++c;
+    for (int i = 1; i < n; ++i) {
+      const double b2 = beta[i - 1] * beta[i - 1];
+      q = alpha[i] - x - b2 / (q != 0.0 ? q : 1e-300);
+      if (q < 0) ++c;
+    }
+    return c;
+  };
+  if (count_below(hi) < 1) hi = hi + 2.0 * (hi - lo) + 1.0;  // guard a too-tight warm start
+  for (int it = 0; it < 200; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (mid <= lo || mid >= hi) break;
+    if (count_below(mid) >= 1) hi = mid;
+    else lo = mid;
+    if (hi - lo <= 2.0 * kEps * std::max(std::fabs(lo), std::fabs(hi))) break;
+  }
+  const double lam = 0.5 * (lo + hi);
+  // backward recurrence: u[n-1] = 1, (T - lam) u = 0 row by row from the bottom
+  std::vector<double> u(n);
+  u[n - 1] = 1.0;
+  u[n - 2] = (beta[n - 2] != 0.0) ? (lam - alpha[n - 1]) / beta[n - 2] : 0.0;
+  double scale = 1.0;  // u is stored divided by `scale` (rescaled to stay finite)
+  for (int k = n - 2; k >= 1; --k) {
+    double v = (beta[k - 1] != 0.0) ? ((lam - alpha[k]) * u[k] - beta[k] * u[k + 1]) / beta[k - 1] : 0.0;
+    u[k - 1] = v;
+    if (std::fabs(v) > 1e150) {  // rescale everything computed so far
+      for (int i = k - 1; i < n; ++i) u[i] *= 1e-150;
+      scale *= 1e-150;
+    }
+  }
+  double nrm = 0.0;
+  for (int i = 0; i < n; ++i) nrm += u[i] * u[i];
+  nrm = std::sqrt(nrm);
+  *lambda0 = lam;
+  *last = u[n - 1] / nrm;
+  if (vec) {
+    vec->resize(n);
+    for (int i = 0; i < n; ++i) (*vec)[i] = u[i] / nrm;
+  }
+  (void)scale;
+}
+
 bool sym_eig(int n, const std::vector<double> &A, std::vector<double> &w, std::vector<double> *V) {
   w.assign(n, 0.0);
   if (n == 0) return true;
@@ -198,6 +268,61 @@ bool sym_eig(int n, const std::vector<double> &A, std::vector<double> &w, std::v
         for (int i = 0; i < n; ++i) vj[i] += qk[i] * zkj;
       }
   }
+  return true;
+}
+
+bool band_eigenvalues(int n, int b, std::vector<double> A, std::vector<double> &w) {
+  w.assign(n, 0.0);
+  if (n == 0) return true;
+  if (b < 1) b = 1;
+  auto a = [&](int i, int j) -> double & { return A[(size_t)i + (size_t)n * j]; };
+  // symmetrise from the lower triangle and clear everything outside the band
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      if (std::abs(i - j) > b) a(i, j) = 0.0;
+      else if (i < j) a(i, j) = a(j, i);
+    }
+  // rotation in the (p, p+1) plane: A <- G A G^T, G = [[c, s], [-s, c]];
+  // rows/columns p, p+1 have nonzeros only within [p-b-1, p+b+2]
+  auto rotate = [&](int p, double c, double s) {
+    const int q = p + 1;
+    const int lo = std::max(0, p - b - 1), hi = std::min(n - 1, q + b + 1);
+    for (int j = lo; j <= hi; ++j) {
+      const double x = a(p, j), y = a(q, j);
+      a(p, j) = c * x + s * y;
+      a(q, j) = -s * x + c * y;
+    }
+    for (int i = lo; i <= hi; ++i) {
+      const double x = a(i, p), y = a(i, q);
+      a(i, p) = c * x + s * y;
+      a(i, q) = -s * x + c * y;
+    }
+  };
+  auto zero_with = [&](int p, int col) {  // zero a(p+1, col) using rows p, p+1
+    const double f = a(p, col), g = a(p + 1, col);
+    if (g == 0.0) return false;
+    const double r = pythag(f, g);
+    rotate(p, f / r, g / r);
+    a(p + 1, col) = 0.0;
+    a(col, p + 1) = 0.0;
+    return true;
+  };
+  for (int k = 0; k < n - 2; ++k) {
+    for (int i = std::min(k + b, n - 1); i >= k + 2; --i) {
+      if (!zero_with(i - 1, k)) continue;
+      // the rotation of rows i-1, i creates a bulge at (i+b, i-1); chase it down
+      for (int r = i; r + b < n; r += b) {
+        const int row = r + b, col = r - 1;
+        if (a(row, col) == 0.0) break;
+        zero_with(row - 1, col);
+      }
+    }
+  }
+  std::vector<double> d(n), e(n, 0.0);
+  for (int i = 0; i < n; ++i) d[i] = a(i, i);
+  for (int i = 0; i + 1 < n; ++i) e[i] = a(i + 1, i);
+  if (!tridiag_eig(n, d, e, nullptr)) return false;
+  w = d;
   return true;
 }
 

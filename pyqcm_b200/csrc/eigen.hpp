@@ -28,9 +28,25 @@ bool tridiag_eig(int n, std::vector<double> &d, std::vector<double> e, std::vect
 bool tridiag_lowest_last(int n, const double *alpha, const double *beta, double *lambda0,
                          double *last);
 
+// Same quantities in O(n) per call: the lowest eigenvalue by Sturm-sequence
+// bisection (Givens' method), started from `upper` (an upper bound, e.g. the
+// previous Lanczos step's value by Cauchy interlacing; pass +inf if unknown),
+// and the eigenvector by the three-term recurrence run backwards from the last
+// component, which is stable for an eigenvector whose weight sits at the start.
+// vec (optional) receives the whole normalised eigenvector.
+void tridiag_lowest_fast(int n, const double *alpha, const double *beta, double upper,
+                         double *lambda0, double *last, std::vector<double> *vec);
+
 // Dense symmetric eigenproblem, A column-major n x n (lower triangle used).
 // w receives eigenvalues ascending; V (if non-null) the eigenvectors.
 bool sym_eig(int n, const std::vector<double> &A, std::vector<double> &w, std::vector<double> *V);
+
+// Eigenvalues (ascending) of a symmetric band matrix of half-bandwidth b,
+// given as a full column-major n x n array (entries outside the band ignored).
+// Reduces to tridiagonal form by Givens rotations with bulge chasing
+// (H. R. Schwarz, "Tridiagonalization of a symmetric band matrix", Numer. Math.
+// 12, 1968), O(n^2 b), then QL. Used for the band-Lanczos convergence test.
+bool band_eigenvalues(int n, int b, std::vector<double> A, std::vector<double> &w);
 
 // In-place inverse of a complex n x n column-major matrix (Gauss-Jordan with
 // partial pivoting). Returns false if singular.

@@ -167,22 +167,25 @@ std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
   GS_energy = 1.0e12;
   const double gap = max_gap();
   const uint64_t seed = (uint64_t)opt_int("seed");
+  auto where = [&](const Sector &s) {
+    return "\n  in cluster model '" + model->name + "', instance '" + model->name + "_" +
+           std::to_string(label) + "', sector '" + s.name() + "'";
+  };
+  // eigenvalue pass over every target sector
   for (auto &s : target_sectors) {
     SectorOp H(terms, s, ws);
     if (H.D == 0) continue;
     auto st = std::make_shared<State>();
     st->sec = s;
-    LanczosResult r;
     try {
-      r = lanczos_ground_state(H, ws, st->psi, seed);
+      st->lanczos = lanczos_energy(H, ws, seed);
     } catch (const Error &e) {
-      fail(e.code, std::string(e.what()) + "\n  in cluster model '" + model->name + "', instance '" +
-                       model->name + "_" + std::to_string(label) + "', sector '" + s.name() + "'");
+      fail(e.code, std::string(e.what()) + where(s));
     }
-    st->energy = r.energy;
+    st->energy = st->lanczos.energy;
     // Hamiltonian::states (src_ed/Hamiltonian/Hamiltonian_base.hpp:197-206)
-    if (r.energy < GS_energy) GS_energy = r.energy;
-    if (r.energy - GS_energy > gap) continue;
+    if (st->energy < GS_energy) GS_energy = st->energy;
+    if (st->energy - GS_energy > gap) continue;
     states.push_back(st);
   }
   compute_weights();
@@ -191,6 +194,17 @@ std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
   double tot = 0.0;
   for (auto &x : states)
     if (x->weight >= wmin) { kept.push_back(x); tot += x->weight; }
+  // eigenvector pass, only for the states that are kept: the vector is the
+  // same one a single pass would give (same start vector, same tridiagonal)
+  for (auto &x : kept) {
+    try {
+      SectorOp H(terms, x->sec, ws);
+      lanczos_eigenvector(H, ws, x->lanczos, seed, x->psi);
+    } catch (const Error &e) {
+      fail(e.code, std::string(e.what()) + where(x->sec));
+    }
+    x->lanczos = LanczosResult();
+  }
   states = kept;
   for (auto &x : states) x->weight /= tot;
   bool updown = false;

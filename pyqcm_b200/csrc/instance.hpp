@@ -36,6 +36,7 @@ struct State {
   Sector sec;
   double energy = 0.0, weight = 0.0;
   DevBuf<double> psi;
+  LanczosResult lanczos;  // tridiagonal of the eigenvalue pass (replayed for psi)
   QMat q[2];   // [spin_down]
   CFSet cf[2];
 };

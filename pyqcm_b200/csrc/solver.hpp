@@ -56,12 +56,20 @@ struct SectorOp {
 };
 
 // Ground state by Lanczos (LanczosEigenvalue + LanczosEigenvector,
-// src_ed/Hamiltonian/Lanczos.hpp:41-143). psi receives the normalised vector.
+// src_ed/Hamiltonian/Lanczos.hpp:41-143), as two passes like the reference:
+// lanczos_energy runs the recurrence with the Ritz-residual stop and keeps the
+// tridiagonal; lanczos_eigenvector replays it from the same seeded start vector
+// and accumulates psi. The instance calls the second pass only for the sectors
+// whose state survives the Boltzmann-weight selection.
 struct LanczosResult {
   double energy = 0.0;
   int iterations = 0;
   std::vector<double> alpha, beta;
 };
+LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed);
+void lanczos_eigenvector(const SectorOp &H, Workspace &ws, const LanczosResult &res,
+                         uint64_t seed, DevBuf<double> &psi);
+// Both passes.
 LanczosResult lanczos_ground_state(const SectorOp &H, Workspace &ws, DevBuf<double> &psi,
                                    uint64_t seed);
 

@@ -97,16 +97,16 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per H.v from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "hv_sq4x4_traffic.txt")
-    try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_hv"):
-                return float(line.split("=")[1])
-    except OSError:
-        pass
-    return None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one H.v, i.e. one
+# k_hv_rows2 + one k_hv_cols2 launch, per basis state: ncu --set full on the
+# 4x4 N_up = N_dn = 6 sector (64,128,064 states, vectors larger than L2) read
+# 0.982 + 1.569 GB. Both passes stream the vectors once, so the traffic scales
+# with the number of states.
+TRAFFIC_BYTES_PER_STATE = (0.514027e9 + 0.467779e9 + 1.080543e9 + 0.487590e9) / 64128064
+
+
+def ncu_traffic(D):
+    return TRAFFIC_BYTES_PER_STATE * D
 
 
 class ClockSampler:
@@ -274,7 +274,7 @@ def run_ours(args, world, rank, local):
     alg = 16.0 * D
     peak, src = peaks()
     achieved = alg / (ms * 1e-3) / 1e9
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(D)
     line = {
         "metric": METRIC, "value": aggregate_value(alg, ms, world), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,

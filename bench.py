@@ -202,7 +202,7 @@ def run_ours(args, world, rank, local):
     if args.sector:
         prob.sectors = args.sector
     label = 7000 + rank
-    qed.load_problem(prob, label, model_name="bench_sq4x4")
+    qed.load_problem(prob, label, model_name="bench_sq4x4", fmt="F")
     H = qed.Hamiltonian(label, prob.sectors)
     D = H.dim
     g = torch.Generator(device=f"cuda:{local}").manual_seed(1234 + rank)
@@ -253,7 +253,7 @@ def run_ours(args, world, rank, local):
     solve = None
     if args.solve:
         qed.set_global_parameter("GF_method", "L")
-        qed.load_problem(prob, label + 100, model_name="bench_sq4x4")
+        qed.load_problem(prob, label + 100, model_name="bench_sq4x4", fmt="F")
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e, sec = qed.ground_state_solve(label + 100)
@@ -356,7 +356,7 @@ def run_batch_workload(args, world, rank, local):
     def one_step(base):
         labels = []
         for i, p in enumerate(probs):
-            qed.load_problem(p, base + i, model_name=f"bw_{p.name}_{base + i}")
+            qed.load_problem(p, base + i, model_name=f"bw_{p.name}_{base + i}", fmt="F")
             labels.append(base + i)
         t0 = time.perf_counter()
         qed.ground_state_solve_batch(labels, threads=args.threads)

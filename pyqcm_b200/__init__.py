@@ -161,8 +161,15 @@ def new_model_instance(model: str, values: dict, sectors: str, label: int = 0):
     _check(lib().qed_new_model_instance(model.encode(), len(names), arr, vals, sectors.encode(), label))
 
 
-def load_problem(prob, label: int = 0, model_name: str | None = None):
-    """Defines the model (with its operators) of a workloads.ClusterProblem and an instance."""
+def load_problem(prob, label: int = 0, model_name: str | None = None, fmt: str | None = None):
+    """Defines the model (with its operators) of a workloads.ClusterProblem and an instance.
+
+    fmt, if given, is set as the Hamiltonian_format option first ('F' factorized:
+    Lanczos in every sector; 'S', 'E', 'O', 'N': sectors below max_dim_full are
+    diagonalised densely, as in the reference). The format is latched by the
+    model's first instance."""
+    if fmt is not None:
+        set_global_parameter("Hamiltonian_format", fmt)
     mname = model_name or prob.name
     new_model(mname, prob.n_sites, prob.n_bath)
     for op, (typ, el) in prob.operators.items():

@@ -75,6 +75,18 @@ Instance::Instance(int lab, std::shared_ptr<Model> m, std::map<std::string, doub
   if (mix != mixing::normal && mix != mixing::up_down)
     fail(QED_ERR_UNSUPPORTED, "mixing " + std::to_string(mix) +
                                   " (anomalous / spin-flip) is outside the spin-factorized solver");
+  {
+    std::lock_guard<std::mutex> l(model->mtx);
+    if (!model->format) {
+      const char f = opt_char("Hamiltonian_format");
+      if (f != 'O' && f != 'S' && f != 'N' && f != 'F' && f != 'E')
+        fail(QED_ERR_ARGUMENT, "Hamiltonian_format is not one of : N, S, O, F, E");
+      model->format = f;
+      // every operator this solver accepts is factorizable, and the mixing is
+      // normal or up_down here, so the format alone decides
+      model->factorized = (f == 'F');
+    }
+  }
   dim_GF = model->n_sites;
   // sectors: slash-separated list
   std::stringstream ss(sectors);
@@ -171,10 +183,35 @@ std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
     return "\n  in cluster model '" + model->name + "', instance '" + model->name + "_" +
            std::to_string(label) + "', sector '" + s.name() + "'";
   };
+  const long max_full = opt_int("max_dim_full");
   // eigenvalue pass over every target sector
   for (auto &s : target_sectors) {
     SectorOp H(terms, s, ws);
     if (H.D == 0) continue;
+    if (!model->factorized && (long)H.D < max_full) {
+      // Hamiltonian_Dense::states (src_ed/Hamiltonian/Hamiltonian_Dense.hpp:110-125):
+      // every eigenstate of the sector within max_gap of the running minimum
+      std::vector<double> w, U;
+      try {
+        dense_eigensystem(H, ws, w, U);
+      } catch (const Error &e) {
+        fail(e.code, std::string(e.what()) + where(s));
+      }
+      if (w[0] < GS_energy) GS_energy = w[0];
+      for (size_t i = 0; i < w.size(); ++i) {
+        if (w[i] - GS_energy > gap) break;
+        auto st = std::make_shared<State>();
+        st->sec = s;
+        st->energy = w[i];
+        st->dense = true;
+        st->psi.alloc(H.D);
+        QED_CUDA(cudaMemcpyAsync(st->psi.p, U.data() + i * H.D, H.D * sizeof(double),
+                                 cudaMemcpyHostToDevice, ws.stream));
+        ws.sync();
+        states.push_back(st);
+      }
+      continue;
+    }
     auto st = std::make_shared<State>();
     st->sec = s;
     try {
@@ -197,6 +234,7 @@ std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
   // eigenvector pass, only for the states that are kept: the vector is the
   // same one a single pass would give (same start vector, same tridiagonal)
   for (auto &x : kept) {
+    if (x->dense) continue;
     try {
       SectorOp H(terms, x->sec, ws);
       lanczos_eigenvector(H, ws, x->lanczos, seed, x->psi);
@@ -320,7 +358,28 @@ void Instance::build_qmatrix(State &st, bool spin_down, Workspace &ws) {
     }
     std::vector<double> ev, Q;
     int M = 0;
-    bool ok = band_lanczos_qmatrix(H, ws, phi, ev, Q, M);
+    bool ok;
+    if (!model->factorized && (long)H.D < opt_int("max_dim_full")) {
+      // Hamiltonian_Dense::build_Q_matrix (src_ed/Hamiltonian/Hamiltonian_Dense.hpp:157-180):
+      // all D poles, Q(k, i) = sum_j phi_i[j] U[j, k]
+      std::vector<double> U, ph(H.D);
+      dense_eigensystem(H, ws, ev, U);
+      M = (int)H.D;
+      Q.assign((size_t)M * p, 0.0);
+      for (int i = 0; i < p; ++i) {
+        phi[i].download(ph.data(), H.D, ws.stream);
+        ws.sync();
+        for (int k = 0; k < M; ++k) {
+          const double *uk = U.data() + (size_t)k * H.D;
+          double acc = 0.0;
+          for (size_t j = 0; j < H.D; ++j) acc += ph[j] * uk[j];
+          Q[(size_t)k * p + i] = acc;
+        }
+      }
+      ok = true;
+    } else {
+      ok = band_lanczos_qmatrix(H, ws, phi, ev, Q, M);
+    }
     std::vector<double> e, V;
     if (ok && M > 0) {
       e = ev;

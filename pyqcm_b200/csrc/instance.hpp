@@ -37,6 +37,7 @@ struct State {
   double energy = 0.0, weight = 0.0;
   DevBuf<double> psi;
   LanczosResult lanczos;  // tridiagonal of the eigenvalue pass (replayed for psi)
+  bool dense = false;     // psi from full diagonalisation (small sector, non-factorized model)
   QMat q[2];   // [spin_down]
   CFSet cf[2];
 };

@@ -230,6 +230,26 @@ __device__ __forceinline__ double inter_term(const InterSpin &it, uint32_t up, u
   return s;
 }
 
+// Dense Hamiltonian: thread I writes row I (diagonal, up hops along the row,
+// dn hops across rows), the same matrix elements the H.v passes apply.
+__global__ void k_dense_hamiltonian(HvOperator op, double *__restrict__ h) {
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const size_t D = (size_t)du * dd;
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t u = (uint32_t)(I % du), d = (uint32_t)(I / du);
+    double *row = h + I * D;  // zeroed by the launcher
+    row[I] = op.up.diag[u] + op.dn.diag[d] + inter_term(op.inter, op.up.bits[u], op.dn.bits[d]);
+    for (int k = 0; k < op.up.cnt[u]; ++k) {
+      const uint32_t e = op.up.ell[(size_t)k * du + u];
+      row[(size_t)d * du + (e >> 8)] += op.up.vals[e & 255u];
+    }
+    for (int k = 0; k < op.dn.cnt[d]; ++k) {
+      const uint32_t e = op.dn.ell[(size_t)k * dd + d];
+      row[(size_t)(e >> 8) * du + u] += op.dn.vals[e & 255u];
+    }
+  }
+}
+
 // Row pass: one CTA per dn row (grid-stride). The row of x is staged in shared
 // memory when it fits, so the up-spin gathers hit on-chip memory.
 template <bool SMEM>
@@ -684,6 +704,14 @@ void launch_cdag_gather(int L, int spin, int a, int pm, const uint32_t *tub, uin
   size_t D = (size_t)du_t * dd_t;
   k_cdag_gather<<<grid_for(D, device_sms(), 8), kThreads, 0, s>>>(
       L, spin, a, pm, tub, du_t, tdb, dd_t, src_nup, src_ndn, du_s, psi, y, coef, accumulate);
+  QED_LAUNCH();
+}
+
+void launch_dense_hamiltonian(const HvOperator &op, double *h, cudaStream_t s) {
+  const size_t D = (size_t)op.up.dim * op.dn.dim;
+  if (!D) return;
+  QED_CUDA(cudaMemsetAsync(h, 0, D * D * sizeof(double), s));
+  k_dense_hamiltonian<<<grid_for(D, device_sms()), kThreads, 0, s>>>(op, h);
   QED_LAUNCH();
 }
 

@@ -76,6 +76,12 @@ void launch_cdag_gather(int L, int spin, int a, int pm, const uint32_t *tgt_up_b
                         int src_ndn, uint32_t du_s, const double *psi, double *y, double coef,
                         int accumulate, cudaStream_t s);
 
+// Dense D x D matrix of the sector Hamiltonian (row I = up + du*dn, the H.v
+// vector layout), for the full-diagonalisation path of small sectors
+// (Hamiltonian_Dense, src_ed/Hamiltonian/Hamiltonian_Dense.hpp:60-88). h must
+// hold D*D doubles; it is overwritten.
+void launch_dense_hamiltonian(const HvOperator &op, double *h, cudaStream_t s);
+
 // ---- H.v ------------------------------------------------------------------
 // Row pass: y = (diag + up hops) x - sum_k sub.c[k] sub.z[k]   (x scaled by xs)
 void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,

@@ -63,6 +63,12 @@ struct Model {
   int n_sites = 0, n_bath = 0, n_orb = 0;
   bool is_closed = false;
   int mix = -1;  // mixing fixed by the first instance (src_ed/model_instance_base.cpp:71-78)
+  // Hamiltonian_format latched at the model's first instance
+  // (src_ed/model_instance_base.cpp:45-54) and the factorized flag derived from
+  // it (:86-97). Non-factorized models diagonalise sectors smaller than
+  // max_dim_full densely (src_ed/model_instance.hpp:200-205).
+  char format = 0;
+  bool factorized = false;
   std::map<std::string, std::shared_ptr<Operator>> term;
   std::vector<bool> in_bath;  // 2*n_orb entries
   mutable std::mutex mtx;

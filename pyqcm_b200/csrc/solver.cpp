@@ -305,6 +305,19 @@ LanczosResult lanczos_ground_state(const SectorOp &H, Workspace &ws, DevBuf<doub
   return res;
 }
 
+// ------------------------------------------------------ full diagonalisation --
+
+void dense_eigensystem(const SectorOp &H, Workspace &ws, std::vector<double> &w,
+                       std::vector<double> &U) {
+  const size_t D = H.D;
+  DevBuf<double> h(D * D);
+  launch_dense_hamiltonian(H.op, h.p, ws.stream);
+  std::vector<double> A(D * D);
+  h.download(A.data(), D * D, ws.stream);
+  ws.sync();
+  if (!sym_eig((int)D, A, w, &U)) fail(QED_ERR_INTERNAL, "dense eigensolver did not converge");
+}
+
 // ------------------------------------------------------------ LanczosGreen --
 
 void lanczos_green(const SectorOp &H, Workspace &ws, double *psi, double *q,

@@ -73,6 +73,14 @@ void lanczos_eigenvector(const SectorOp &H, Workspace &ws, const LanczosResult &
 LanczosResult lanczos_ground_state(const SectorOp &H, Workspace &ws, DevBuf<double> &psi,
                                    uint64_t seed);
 
+// Full diagonalisation of a small sector (Hamiltonian_Dense::states and
+// ::build_Q_matrix, src_ed/Hamiltonian/Hamiltonian_Dense.hpp:110-180): the dense
+// matrix is assembled on the device from the sector tables, the D x D symmetric
+// eigenproblem is solved on the host. w: eigenvalues ascending; U: column-major
+// eigenvectors (column k <-> w[k]) in the H.v vector layout.
+void dense_eigensystem(const SectorOp &H, Workspace &ws, std::vector<double> &w,
+                       std::vector<double> &U);
+
 // LanczosGreen (src_ed/Hamiltonian/Lanczos.hpp:156-183) from a normalised start
 // vector psi (overwritten). Returns the (a, b) coefficients.
 void lanczos_green(const SectorOp &H, Workspace &ws, double *psi, double *q,

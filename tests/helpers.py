@@ -13,9 +13,10 @@ def set_both(qed, oracle, **opts):
 
 def load_both(qed, oracle, prob, suffix, label, fmt="F"):
     """Loads `prob` into both libraries under a unique model name and label.
-    fmt is the oracle's Hamiltonian_format ('F' factorized, 'S' CSR)."""
+    fmt is the Hamiltonian_format of both ('F' factorized, 'S' CSR: sectors below
+    max_dim_full are diagonalised densely)."""
     name = prob.name + suffix
-    qed.load_problem(prob, label, model_name=name)
+    qed.load_problem(prob, label, model_name=name, fmt=fmt)
     oracle.load_problem(prob, label, model_name=name, fmt=fmt)
     return name
 

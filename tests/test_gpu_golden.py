@@ -28,7 +28,8 @@ def test_small_cases_against_fixtures(qed, fresh):
         qed.set_global_parameter("GF_method", method)
         try:
             suffix, label = fresh()
-            qed.load_problem(BUILDERS[base](), label, model_name="gold_" + name + suffix)
+            qed.load_problem(BUILDERS[base](), label, model_name="gold_" + name + suffix,
+                             fmt="S" if method == "F" else "F")
             e, _ = qed.ground_state_solve(label)
             G = qed.Green_function(z, label=label)
             n = int(g["dims"][i])
@@ -48,7 +49,7 @@ def test_sq4x4_ground_state_against_fixture(qed, fresh):
         pytest.skip("4x4 fixture not generated yet")
     ref = json.load(open(path))
     suffix, label = fresh()
-    qed.load_problem(W.square4x4(), label, model_name="gold_sq4x4" + suffix)
+    qed.load_problem(W.square4x4(), label, model_name="gold_sq4x4" + suffix, fmt="F")
     e, sec = qed.ground_state_solve(label)
     assert abs(e - ref["E0"]) <= 1e-10 * abs(ref["E0"])
     assert sec == ref["sector"]

@@ -192,3 +192,58 @@ def test_batched_solves_match_reference(qed, oracle, fresh):
             G1d = qed.Green_function(z, spin_down=True, label=lab)
             G2d = oracle.green_function(lab, z, spin_down=True)
             assert np.max(np.abs(G1d - G2d)) < 1e-8, p.name
+
+
+# Non-factorized formats ('S' here): sectors below max_dim_full (256) are
+# diagonalised densely on both sides (Hamiltonian_Dense), which keeps every
+# degenerate ground state of a sector; larger sectors run Lanczos.
+DENSE_CASES = [
+    # 2x2, N=3, S=1: two-fold degenerate ground state inside the sector
+    ("plaq_N3_degenerate", lambda: W.hubbard_cluster(2, 2, U=4.0, mu=1.0, n_up=2, n_dn=1), None),
+    ("plaq_multi", lambda: W.hubbard_cluster(2, 2, U=6.0, mu=3.0),
+     "R0:N4:S0/R0:N3:S1/R0:N5:S1/R0:N3:S-1/R0:N5:S-1"),
+    # ground-state sector above the threshold (Lanczos), N-1 targets below it (dense)
+    ("chain8_low", lambda: W.hubbard_cluster(8, 1, U=4.0, mu=0.5, n_up=2, n_dn=2), None),
+    ("neel2x3", lambda: W.hubbard_cluster(3, 2, U=5.0, mu=2.0, M=0.2, n_up=2, n_dn=2), None),
+]
+
+
+@pytest.mark.parametrize("case", range(len(DENSE_CASES)))
+def test_dense_path_small_sectors(qed, oracle, fresh, case):
+    name, mk, sectors = DENSE_CASES[case]
+    prob = mk()
+    if sectors:
+        prob.sectors = sectors
+    suffix, label = fresh()
+    set_both(qed, oracle, GF_method="L")
+    load_both(qed, oracle, prob, suffix, label, fmt="S")
+    e1, s1 = qed.ground_state_solve(label)
+    e2, s2 = oracle.ground_state(label)
+    assert abs(e1 - e2) <= GS_TOL * abs(e2), (name, e1, e2)
+    assert s1 == s2
+    z = W.matsubara(256)
+    G1 = qed.Green_function(z, label=label)
+    G2 = oracle.green_function(label, z)
+    assert np.max(np.abs(G1 - G2)) < GF_TOL, name
+    if qed.mixing(label) & 4:
+        G1d = qed.Green_function(z, spin_down=True, label=label)
+        G2d = oracle.green_function(label, z, spin_down=True)
+        assert np.max(np.abs(G1d - G2d)) < GF_TOL, name
+    assert abs(qed.Potthoff_functional(label) - oracle.potthoff(label)) < 1e-9
+
+
+def test_dense_path_keeps_degenerate_states(qed, oracle, fresh):
+    """The same degenerate sector through the factorized format (one Lanczos
+    state, a start-vector-dependent vector of the degenerate pair) and through
+    'S' (both dense eigenstates at equal weight) gives different Green
+    functions; the 'S' one matches the reference in the same format."""
+    z = W.matsubara(64)
+    G = {}
+    for fmt in ("F", "S"):
+        suffix, label = fresh()
+        set_both(qed, oracle, GF_method="L")
+        load_both(qed, oracle, W.hubbard_cluster(2, 2, U=4.0, mu=1.0, n_up=2, n_dn=1), suffix, label, fmt=fmt)
+        G[fmt] = qed.Green_function(z, label=label)
+        if fmt == "S":
+            assert np.max(np.abs(G[fmt] - oracle.green_function(label, z))) < GF_TOL
+    assert np.max(np.abs(G["F"] - G["S"])) > 1e-6

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <functional>
 #include <thread>
 #include <map>
 #include <memory>
@@ -115,6 +116,119 @@ template <class F> int run_batch(int n, int threads, F &&fn) {
   if (first_code != QED_OK) t_err = first_msg;
   return first_code;
 }
+// Weighted tasks run longest-first (LPT) on the batch thread pool.
+struct Task {
+  double cost;
+  std::function<void()> fn;
+};
+
+int run_tasks(std::vector<Task> &tasks, int threads) {
+  std::stable_sort(tasks.begin(), tasks.end(), [](const Task &a, const Task &b) { return a.cost > b.cost; });
+  return run_batch((int)tasks.size(), threads, [&](int i) { tasks[i].fn(); });
+}
+
+// The instances of a batch call, each once, locked in label order for the
+// whole call (single-instance entries lock one instance at a time, so the
+// order cannot deadlock).
+struct BatchSet {
+  std::vector<std::shared_ptr<Instance>> inst;  // unique, by label
+  std::vector<std::unique_lock<std::mutex>> locks;
+  explicit BatchSet(const int *labels, int n) {
+    std::map<int, std::shared_ptr<Instance>> u;
+    for (int i = 0; i < n; ++i) u[labels[i]] = instance(labels[i]);
+    for (auto &x : u) inst.push_back(x.second);
+    for (auto &I : inst) locks.emplace_back(I->mtx);
+  }
+};
+
+// Ground states of a batch: every target sector of every unsolved instance as
+// one task (eigenvalue pass), the selection per instance, then the eigenvector
+// of every kept state as one task.
+int batch_ground_states(BatchSet &b, int threads) {
+  std::vector<Instance *> todo;
+  int rc = guarded([&] {
+    for (auto &I : b.inst)
+      if (!I->gs_solved) {
+        I->check_solvable();
+        todo.push_back(I.get());
+      }
+  });
+  if (rc != QED_OK || todo.empty()) return rc;
+  std::vector<std::vector<SectorSolve>> res(todo.size());
+  std::vector<Task> tasks;
+  for (size_t k = 0; k < todo.size(); ++k) {
+    Instance *I = todo[k];
+    res[k].resize(I->target_sectors.size());
+    size_t i = 0;
+    for (auto &sec : I->target_sectors) {
+      SectorSolve *out = &res[k][i++];
+      Sector s = sec;
+      tasks.push_back({(double)I->sector_dim(s), [I, s, out] { I->solve_sector(s, *out, ws()); }});
+    }
+  }
+  if ((rc = run_tasks(tasks, threads)) != QED_OK) return rc;
+  rc = guarded([&] {
+    for (size_t k = 0; k < todo.size(); ++k) todo[k]->select_states(res[k]);
+  });
+  if (rc != QED_OK) return rc;
+  res.clear();
+  tasks.clear();
+  for (Instance *I : todo)
+    for (auto &st : I->states) {
+      State *sp = st.get();
+      tasks.push_back({(double)I->sector_dim(sp->sec), [I, sp] { I->state_vector(*sp, ws()); }});
+    }
+  if ((rc = run_tasks(tasks, threads)) != QED_OK) return rc;
+  for (Instance *I : todo) I->finish_gs();
+  return QED_OK;
+}
+
+// Green functions of a batch: each Q-matrix half (state, spin, hole/electron)
+// or continued-fraction set (state, spin) as one task, then the per-state
+// combination and the per-instance averages.
+int batch_green_functions(BatchSet &b, int threads) {
+  int rc = batch_ground_states(b, threads);
+  if (rc != QED_OK) return rc;
+  struct Job {
+    Instance *I;
+    State *st;
+    bool sd;
+    QPart parts[2];
+  };
+  std::vector<Instance *> todo;
+  rc = guarded([&] {
+    for (auto &I : b.inst)
+      if (!I->gf_solved) {
+        I->check_gf_solvable();
+        todo.push_back(I.get());
+      }
+  });
+  if (rc != QED_OK || todo.empty()) return rc;
+  std::vector<std::unique_ptr<Job>> jobs;
+  std::vector<Task> tasks;
+  for (Instance *I : todo) {
+    const int p = I->model->n_sites;
+    for (auto &st : I->states)
+      for (int sd = 0; sd < ((I->mix & mixing::up_down) ? 2 : 1); ++sd) {
+        State *sp = st.get();
+        const double cost = (double)I->sector_dim(sp->sec) * p;
+        if (I->use_cf) {
+          tasks.push_back({cost * p, [I, sp, sd] { I->build_cf(*sp, sd != 0, ws()); }});
+          continue;
+        }
+        jobs.emplace_back(new Job{I, sp, sd != 0, {}});
+        Job *j = jobs.back().get();
+        for (int s = 0; s < 2; ++s)
+          tasks.push_back({cost, [j, s] { j->I->qmatrix_part(*j->st, j->sd, s, j->parts[s], ws()); }});
+      }
+  }
+  if ((rc = run_tasks(tasks, threads)) != QED_OK) return rc;
+  return guarded([&] {
+    for (auto &j : jobs) j->I->qmatrix_combine(*j->st, j->sd, j->parts, ws());
+    for (Instance *I : todo) I->finish_gf();
+  });
+}
+
 }  // namespace
 
 extern "C" {
@@ -245,10 +359,12 @@ int qed_ground_state_solve_batch(const int *labels, int n, int threads, double *
     t_err = "null argument";
     return QED_ERR_ARGUMENT;
   }
-  return run_batch(n, threads, [&](int i) {
-    auto I = instance(labels[i]);
-    std::lock_guard<std::mutex> li(I->mtx);
-    energies[i] = I->low_energy_states(ws()).first;
+  std::unique_ptr<BatchSet> b;
+  int rc = guarded([&] { b.reset(new BatchSet(labels, n)); });
+  if (rc != QED_OK) return rc;
+  if ((rc = batch_ground_states(*b, threads)) != QED_OK) return rc;
+  return guarded([&] {
+    for (int i = 0; i < n; ++i) energies[i] = instance(labels[i])->GS_energy;
   });
 }
 
@@ -257,11 +373,10 @@ int qed_Green_function_solve_batch(const int *labels, int n, int threads) {
     t_err = "null argument";
     return QED_ERR_ARGUMENT;
   }
-  return run_batch(n, threads, [&](int i) {
-    auto I = instance(labels[i]);
-    std::lock_guard<std::mutex> li(I->mtx);
-    I->green_solve(ws());
-  });
+  std::unique_ptr<BatchSet> b;
+  int rc = guarded([&] { b.reset(new BatchSet(labels, n)); });
+  if (rc != QED_OK) return rc;
+  return batch_green_functions(*b, threads);
 }
 
 int qed_Green_function_solve(int label) {

@@ -8,6 +8,7 @@
 
 #include "eigen.hpp"
 #include "options.hpp"
+#include "profile.hpp"
 
 namespace qed {
 
@@ -170,59 +171,72 @@ std::string Instance::gs_string() const {
   return out.str();
 }
 
-// low_energy_states (src_ed/model_instance.hpp:245-347)
-std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
-  if (gs_solved) return {GS_energy, gs_string()};
+std::string Instance::where(const Sector &s) const {
+  return "\n  in cluster model '" + model->name + "', instance '" + model->name + "_" + std::to_string(label) +
+         "', sector '" + s.name() + "'";
+}
+
+void Instance::check_solvable() const {
   if (!is_correlated)
     fail(QED_ERR_UNSUPPORTED, "uncorrelated instances (no interaction term) are solved by the one-body "
                               "path, which is not in this solver");
-  GS_energy = 1.0e12;
-  const double gap = max_gap();
-  const uint64_t seed = (uint64_t)opt_int("seed");
-  auto where = [&](const Sector &s) {
-    return "\n  in cluster model '" + model->name + "', instance '" + model->name + "_" +
-           std::to_string(label) + "', sector '" + s.name() + "'";
-  };
-  const long max_full = opt_int("max_dim_full");
-  // eigenvalue pass over every target sector
-  for (auto &s : target_sectors) {
+}
+
+size_t Instance::sector_dim(const Sector &s) const {
+  const int L = model->n_orb, nu = s.Nup(), nd = s.Ndw();
+  if (nu < 0 || nu > L || nd < 0 || nd > L) return 0;
+  return (size_t)binom(L, nu) * (size_t)binom(L, nd);
+}
+
+// Eigenvalue pass of one sector: Hamiltonian_Dense::states
+// (src_ed/Hamiltonian/Hamiltonian_Dense.hpp:110-125) below max_dim_full in the
+// non-factorized formats, the Lanczos eigenvalue pass otherwise.
+void Instance::solve_sector(const Sector &s, SectorSolve &out, Workspace &ws) {
+  out.sec = s;
+  try {
     SectorOp H(terms, s, ws);
-    if (H.D == 0) continue;
-    if (!model->factorized && (long)H.D < max_full) {
-      // Hamiltonian_Dense::states (src_ed/Hamiltonian/Hamiltonian_Dense.hpp:110-125):
-      // every eigenstate of the sector within max_gap of the running minimum
-      std::vector<double> w, U;
-      try {
-        dense_eigensystem(H, ws, w, U);
-      } catch (const Error &e) {
-        fail(e.code, std::string(e.what()) + where(s));
-      }
-      if (w[0] < GS_energy) GS_energy = w[0];
-      for (size_t i = 0; i < w.size(); ++i) {
-        if (w[i] - GS_energy > gap) break;
+    out.dim = H.D;
+    if (H.D == 0) return;
+    if (!model->factorized && (long)H.D < opt_int("max_dim_full")) {
+      out.dense = true;
+      dense_eigensystem(H, ws, out.w, out.U);
+    } else {
+      out.lanczos = lanczos_energy(H, ws, (uint64_t)opt_int("seed"));
+    }
+  } catch (const Error &e) {
+    fail(e.code, std::string(e.what()) + where(s));
+  }
+}
+
+// The selection part of low_energy_states (src_ed/model_instance.hpp:268-347),
+// in target-sector order: the running minimum of Hamiltonian::states
+// (src_ed/Hamiltonian/Hamiltonian_base.hpp:197-206), compute_weights, the
+// minimum_weight cut and the renormalisation.
+void Instance::select_states(std::vector<SectorSolve> &r) {
+  GS_energy = 1.0e12;
+  states.clear();
+  const double gap = max_gap();
+  for (auto &x : r) {
+    if (x.dim == 0) continue;
+    if (x.dense) {
+      if (x.w[0] < GS_energy) GS_energy = x.w[0];
+      for (size_t i = 0; i < x.w.size(); ++i) {
+        if (x.w[i] - GS_energy > gap) break;
         auto st = std::make_shared<State>();
-        st->sec = s;
-        st->energy = w[i];
+        st->sec = x.sec;
+        st->energy = x.w[i];
         st->dense = true;
-        st->psi.alloc(H.D);
-        QED_CUDA(cudaMemcpyAsync(st->psi.p, U.data() + i * H.D, H.D * sizeof(double),
-                                 cudaMemcpyHostToDevice, ws.stream));
-        ws.sync();
+        st->hpsi.assign(x.U.begin() + i * x.dim, x.U.begin() + (i + 1) * x.dim);
         states.push_back(st);
       }
       continue;
     }
     auto st = std::make_shared<State>();
-    st->sec = s;
-    try {
-      st->lanczos = lanczos_energy(H, ws, seed);
-    } catch (const Error &e) {
-      fail(e.code, std::string(e.what()) + where(s));
-    }
-    st->energy = st->lanczos.energy;
-    // Hamiltonian::states (src_ed/Hamiltonian/Hamiltonian_base.hpp:197-206)
+    st->sec = x.sec;
+    st->energy = x.lanczos.energy;
     if (st->energy < GS_energy) GS_energy = st->energy;
     if (st->energy - GS_energy > gap) continue;
+    st->lanczos = std::move(x.lanczos);
     states.push_back(st);
   }
   compute_weights();
@@ -230,19 +244,10 @@ std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
   std::vector<std::shared_ptr<State>> kept;
   double tot = 0.0;
   for (auto &x : states)
-    if (x->weight >= wmin) { kept.push_back(x); tot += x->weight; }
-  // eigenvector pass, only for the states that are kept: the vector is the
-  // same one a single pass would give (same start vector, same tridiagonal)
-  for (auto &x : kept) {
-    if (x->dense) continue;
-    try {
-      SectorOp H(terms, x->sec, ws);
-      lanczos_eigenvector(H, ws, x->lanczos, seed, x->psi);
-    } catch (const Error &e) {
-      fail(e.code, std::string(e.what()) + where(x->sec));
+    if (x->weight >= wmin) {
+      kept.push_back(x);
+      tot += x->weight;
     }
-    x->lanczos = LanczosResult();
-  }
   states = kept;
   for (auto &x : states) x->weight /= tot;
   bool updown = false;
@@ -255,7 +260,37 @@ std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
     E0 += x->weight * x->energy;
     if (x->energy < GS_energy) GS_energy = x->energy;
   }
-  gs_solved = true;
+}
+
+// Ground-state vector of a selected state: the eigenvector pass replays the
+// Lanczos recurrence (same start vector, same tridiagonal); dense states
+// upload their eigenvector.
+void Instance::state_vector(State &st, Workspace &ws) {
+  try {
+    if (st.dense) {
+      st.psi.upload(st.hpsi, ws.stream);
+      ws.sync();
+      st.hpsi = std::vector<double>();
+      return;
+    }
+    SectorOp H(terms, st.sec, ws);
+    lanczos_eigenvector(H, ws, st.lanczos, (uint64_t)opt_int("seed"), st.psi);
+  } catch (const Error &e) {
+    fail(e.code, std::string(e.what()) + where(st.sec));
+  }
+  st.lanczos = LanczosResult();
+}
+
+// low_energy_states (src_ed/model_instance.hpp:245-347)
+std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
+  if (gs_solved) return {GS_energy, gs_string()};
+  check_solvable();
+  std::vector<SectorSolve> r(target_sectors.size());
+  size_t i = 0;
+  for (auto &s : target_sectors) solve_sector(s, r[i++], ws);
+  select_states(r);
+  for (auto &x : states) state_vector(*x, ws);
+  finish_gs();
   return {GS_energy, gs_string()};
 }
 
@@ -340,64 +375,74 @@ static void streamline(std::vector<double> &e, std::vector<double> &V, int L) {
 }
 
 // build_qmatrix (src_ed/model_instance.hpp:711-817), sequential branch.
-void Instance::build_qmatrix(State &st, bool spin_down, Workspace &ws) {
+// One half of build_qmatrix: the hole (s = 0, pm = -1) or electron (s = 1,
+// pm = +1) excitations of state st, spin_down or up: start vectors c / c^+ |psi>,
+// band Lanczos (or the full eigensystem of a small non-factorized sector),
+// energy shift and sign, streamline.
+void Instance::qmatrix_part(State &st, bool spin_down, int s, QPart &out, Workspace &ws) {
   const int p = model->n_sites;
-  std::vector<double> eall[2], Vall[2];  // [0] hole (pm=-1), [1] electron
-  for (int s = 0; s < 2; ++s) {
-    const int pm = 2 * s - 1;
-    const int spin = spin_down ? 1 : 0;
-    Sector tsec = shift_sector(st.sec, pm, spin);
-    if (!sector_is_valid(tsec, model->n_orb)) continue;
-    SectorOp H(terms, tsec, ws);
-    if (H.D == 0) continue;
-    std::vector<DevBuf<double>> phi;
-    phi.reserve(p);
+  const int pm = 2 * s - 1;
+  const int spin = spin_down ? 1 : 0;
+  out.e.clear();
+  out.V.clear();
+  Sector tsec = shift_sector(st.sec, pm, spin);
+  if (!sector_is_valid(tsec, model->n_orb)) return;
+  SectorOp H(terms, tsec, ws);
+  if (H.D == 0) return;
+  std::vector<DevBuf<double>> phi;
+  phi.reserve(p);
+  {
+    PhaseScope ps_cdag(kPhCdag);
     for (int i = 0; i < p; ++i) {
       phi.emplace_back(H.D);
       apply_cdag(st, pm, spin, i, H, phi.back().p, 1.0, false, ws);
     }
-    std::vector<double> ev, Q;
-    int M = 0;
-    bool ok;
-    if (!model->factorized && (long)H.D < opt_int("max_dim_full")) {
-      // Hamiltonian_Dense::build_Q_matrix (src_ed/Hamiltonian/Hamiltonian_Dense.hpp:157-180):
-      // all D poles, Q(k, i) = sum_j phi_i[j] U[j, k]
-      std::vector<double> U, ph(H.D);
-      dense_eigensystem(H, ws, ev, U);
-      M = (int)H.D;
-      Q.assign((size_t)M * p, 0.0);
-      for (int i = 0; i < p; ++i) {
-        phi[i].download(ph.data(), H.D, ws.stream);
-        ws.sync();
-        for (int k = 0; k < M; ++k) {
-          const double *uk = U.data() + (size_t)k * H.D;
-          double acc = 0.0;
-          for (size_t j = 0; j < H.D; ++j) acc += ph[j] * uk[j];
-          Q[(size_t)k * p + i] = acc;
-        }
-      }
-      ok = true;
-    } else {
-      ok = band_lanczos_qmatrix(H, ws, phi, ev, Q, M);
-    }
-    std::vector<double> e, V;
-    if (ok && M > 0) {
-      e = ev;
-      V = Q;
-      for (auto &x : e) x -= st.energy;
-      if (pm == -1)
-        for (auto &x : e) x = -x;
-      streamline(e, V, p);
-    }
-    eall[s] = e;
-    Vall[s] = V;
+    ws.sync();
   }
+  std::vector<double> ev, Q;
+  int M = 0;
+  bool ok;
+  if (!model->factorized && (long)H.D < opt_int("max_dim_full")) {
+    // Hamiltonian_Dense::build_Q_matrix (src_ed/Hamiltonian/Hamiltonian_Dense.hpp:157-180):
+    // all D poles, Q(k, i) = sum_j phi_i[j] U[j, k]
+    std::vector<double> U, ph(H.D);
+    dense_eigensystem(H, ws, ev, U);
+    M = (int)H.D;
+    Q.assign((size_t)M * p, 0.0);
+    for (int i = 0; i < p; ++i) {
+      phi[i].download(ph.data(), H.D, ws.stream);
+      ws.sync();
+      for (int k = 0; k < M; ++k) {
+        const double *uk = U.data() + (size_t)k * H.D;
+        double acc = 0.0;
+        for (size_t j = 0; j < H.D; ++j) acc += ph[j] * uk[j];
+        Q[(size_t)k * p + i] = acc;
+      }
+    }
+    ok = true;
+  } else {
+    ok = band_lanczos_qmatrix(H, ws, phi, ev, Q, M);
+  }
+  if (ok && M > 0) {
+    out.e = std::move(ev);
+    out.V = std::move(Q);
+    for (auto &x : out.e) x -= st.energy;
+    if (pm == -1)
+      for (auto &x : out.e) x = -x;
+    streamline(out.e, out.V, p);
+  }
+}
+
+// The rest of build_qmatrix (src_ed/model_instance.hpp:711-817): append the two
+// halves, check_norm, times sqrt(weight), upload for G(z).
+void Instance::qmatrix_combine(State &st, bool spin_down, QPart (&parts)[2], Workspace &ws) {
+  const int p = model->n_sites;
   QMat &q = st.q[spin_down ? 1 : 0];
   q.L = p;
-  q.e = eall[0];
-  q.e.insert(q.e.end(), eall[1].begin(), eall[1].end());
-  q.V = Vall[0];
-  q.V.insert(q.V.end(), Vall[1].begin(), Vall[1].end());
+  q.e = parts[0].e;
+  q.e.insert(q.e.end(), parts[1].e.begin(), parts[1].e.end());
+  q.V = parts[0].V;
+  q.V.insert(q.V.end(), parts[1].V.begin(), parts[1].V.end());
   q.M = (int)q.e.size();
   // check_norm (src_ed/Q_matrix.hpp:236-260), before the weight factor
   double ztot = 0.0;
@@ -420,8 +465,15 @@ void Instance::build_qmatrix(State &st, bool spin_down, Workspace &ws) {
   ws.sync();
 }
 
+void Instance::build_qmatrix(State &st, bool spin_down, Workspace &ws) {
+  QPart parts[2];
+  for (int s = 0; s < 2; ++s) qmatrix_part(st, spin_down, s, parts[s], ws);
+  qmatrix_combine(st, spin_down, parts, ws);
+}
+
 // build_cf (src_ed/model_instance.cpp:34-99), real Hilbert space.
 void Instance::build_cf(State &st, bool spin_down, Workspace &ws) {
+  PhaseScope ps(kPhCf);
   const int n = model->n_sites;
   CFSet &cf = st.cf[spin_down ? 1 : 0];
   cf.n = n;
@@ -463,11 +515,15 @@ void Instance::build_cf(State &st, bool spin_down, Workspace &ws) {
 }
 
 // Green_function_solve (src_ed/model_instance.hpp:517-555)
+void Instance::check_gf_solvable() const {
+  if (opt_bool("merge_states") && states.size() > 1 && !use_cf)
+    fail(QED_ERR_UNSUPPORTED, "merge_states is not in this solver");
+}
+
 void Instance::green_solve(Workspace &ws) {
   if (gf_solved) return;
   if (!gs_solved) low_energy_states(ws);
-  if (opt_bool("merge_states") && states.size() > 1 && !use_cf)
-    fail(QED_ERR_UNSUPPORTED, "merge_states is not in this solver");
+  check_gf_solvable();
   for (auto &x : states) {
     if (use_cf) build_cf(*x, false, ws);
     else build_qmatrix(*x, false, ws);
@@ -476,6 +532,10 @@ void Instance::green_solve(Workspace &ws) {
       else build_qmatrix(*x, true, ws);
     }
   }
+  finish_gf();
+}
+
+void Instance::finish_gf() {
   gf_solved = true;
   green_average();
   // Green_function_density (src_ed/model_instance.hpp:657-675)

@@ -36,10 +36,26 @@ struct State {
   Sector sec;
   double energy = 0.0, weight = 0.0;
   DevBuf<double> psi;
-  LanczosResult lanczos;  // tridiagonal of the eigenvalue pass (replayed for psi)
-  bool dense = false;     // psi from full diagonalisation (small sector, non-factorized model)
+  LanczosResult lanczos;     // tridiagonal of the eigenvalue pass (replayed for psi)
+  bool dense = false;        // psi from full diagonalisation (small sector, non-factorized model)
+  std::vector<double> hpsi;  // dense: the eigenvector on the host until it is uploaded
   QMat q[2];   // [spin_down]
   CFSet cf[2];
+};
+
+// Eigenvalue pass of one target sector: the unit of work that batched drivers
+// spread over host threads (the selection of states needs all of them).
+struct SectorSolve {
+  Sector sec;
+  size_t dim = 0;
+  bool dense = false;
+  std::vector<double> w, U;  // dense: all eigenvalues (ascending) and eigenvectors
+  LanczosResult lanczos;     // Lanczos: tridiagonal and lowest energy
+};
+
+// Hole (s = 0) or electron (s = 1) part of the Q-matrix of one state and spin.
+struct QPart {
+  std::vector<double> e, V;
 };
 
 struct Instance {
@@ -64,6 +80,21 @@ struct Instance {
 
   std::pair<double, std::string> low_energy_states(Workspace &ws);
   void green_solve(Workspace &ws);
+
+  // The steps of low_energy_states and green_solve, for drivers that run the
+  // sectors, states and Q-matrix halves of many instances concurrently. A
+  // single instance runs them in this order on one thread.
+  void check_solvable() const;
+  size_t sector_dim(const Sector &s) const;
+  void solve_sector(const Sector &s, SectorSolve &out, Workspace &ws);
+  void select_states(std::vector<SectorSolve> &r);  // every sector, in target order
+  void state_vector(State &st, Workspace &ws);
+  void finish_gs() { gs_solved = true; }
+  void check_gf_solvable() const;
+  void qmatrix_part(State &st, bool spin_down, int s, QPart &out, Workspace &ws);
+  void qmatrix_combine(State &st, bool spin_down, QPart (&parts)[2], Workspace &ws);
+  void build_cf(State &st, bool spin_down, Workspace &ws);
+  void finish_gf();
   // G(z) for nz frequencies: out[k*n*n + b + a*n] (column-major blocks)
   void green_function(const cplx *z, int nz, bool spin_down, cplx *out, Workspace &ws);
   void self_energy(const cplx *z, int nz, bool spin_down, cplx *out, Workspace &ws);
@@ -74,8 +105,8 @@ struct Instance {
 
  private:
   void build_qmatrix(State &st, bool spin_down, Workspace &ws);
-  void build_cf(State &st, bool spin_down, Workspace &ws);
   void compute_weights();
+  std::string where(const Sector &s) const;
   void green_average();
   // fills phi = c^{pm}_{orb, spin} |psi> on the target sector of H
   void apply_cdag(const State &st, int pm, int spin, int orb, const SectorOp &H, double *y,

@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(512) k_hv_rows(HvOperator op, const double *__
       }
       const size_t I = (size_t)d * du + u;
       acc *= xs;
-      for (int s = 0; s < sub.n; ++s) acc -= sub.c[s] * sub.z[s][I];
+      for (int s = 0; s < sub.n; ++s) acc -= (sub.cdev ? sub.cdev[s] : sub.c[s]) * sub.z[s][I];
       y[I] = acc;
     }
   }
@@ -398,8 +398,9 @@ __global__ void __launch_bounds__(1024) k_hv_rows2(HvOperator op, const double *
       a0 *= xs;
       a1 *= xs;
       for (int s = 0; s < sub.n; ++s) {
-        a0 -= sub.c[s] * sub.z[s][I0];
-        if (two) a1 -= sub.c[s] * sub.z[s][I0 + du];
+        const double cs = sub.cdev ? sub.cdev[s] : sub.c[s];
+        a0 -= cs * sub.z[s][I0];
+        if (two) a1 -= cs * sub.z[s][I0 + du];
       }
       y[I0] = a0;
       if (two) y[I0 + du] = a1;
@@ -560,6 +561,105 @@ __global__ void k_axpby(size_t D, double a, double *y, double b, const double *x
     nrm[0] += v * v;
   }
   if (norm) block_reduce_store<1>(nrm, partials, 1);
+}
+
+__global__ void k_axpy_dev(size_t D, double *y, const double *x, const double *a_dev, double *partials) {
+  const double b = -*a_dev;
+  double nrm[1] = {0.0};
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
+    const double v = y[I] + b * x[I];
+    y[I] = v;
+    nrm[0] += v * v;
+  }
+  block_reduce_store<1>(nrm, partials, 1);
+}
+
+__global__ void k_lanczos_advance(size_t D, double *y, LanczosScalars ls) {
+  const double b = sqrt(*ls.b2_cur);
+  const double z = (b > 0.0) ? 1.0 / b : 0.0;
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x)
+    y[I] *= z;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const int j = *ls.j;
+    ls.alpha_hist[j] = *ls.alpha_cur;
+    ls.beta_hist[j] = b;
+    *ls.beta_prev = b;
+    *ls.j = j + 1;
+  }
+}
+
+// Sum over the CTA in a fixed order (warp shuffles, then warp 0 over the warp
+// sums); every thread gets the total. sm: at least 33 doubles of shared memory.
+__device__ __forceinline__ double cta_sum(double v, double *sm) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();  // previous use of sm is complete
+  if (lane == 0) sm[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double t = lane < nw ? sm[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0) sm[32] = t;
+  }
+  __syncthreads();
+  return sm[32];
+}
+
+// A chunk of ground-state Lanczos steps of one small sector in one CTA: H.v
+// (diagonal, up and down hops gathered straight from L1/L2), alpha, the
+// orthogonalisation, beta and the normalisation, with CTA barriers in place of
+// kernel boundaries. v[0..2] rotate as (v_{j-1}, v_j, w) -> (v_j, w, v_{j-1}).
+__global__ void __launch_bounds__(1024) k_lanczos_cta(HvOperator op, double *v0, double *v1, double *v2,
+                                                       LanczosScalars ls, int nsteps) {
+  __shared__ double sm[33];
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const uint32_t D = du * dd;
+  double *vp = v0, *vc = v1, *w = v2;
+  for (int step = 0; step < nsteps; ++step) {
+    const double bprev = *ls.beta_prev;
+    double sa = 0.0;
+    for (uint32_t I = threadIdx.x; I < D; I += blockDim.x) {
+      const uint32_t u = I % du, d = I / du;
+      const double x = vc[I];
+      double acc = (op.up.diag[u] + op.dn.diag[d] + inter_term(op.inter, op.up.bits[u], op.dn.bits[d])) * x;
+      const double *row = vc + (size_t)d * du;
+      for (int k = 0; k < op.up.cnt[u]; ++k) {
+        const uint32_t e = op.up.ell[(size_t)k * du + u];
+        acc += op.up.vals[e & 255u] * row[e >> 8];
+      }
+      for (int k = 0; k < op.dn.cnt[d]; ++k) {
+        const uint32_t e = op.dn.ell[(size_t)k * dd + d];
+        acc += op.dn.vals[e & 255u] * vc[(size_t)(e >> 8) * du + u];
+      }
+      acc -= bprev * vp[I];
+      w[I] = acc;
+      sa += x * acc;
+    }
+    const double a = cta_sum(sa, sm);  // alpha_j = <v_j, w>
+    double sb = 0.0;
+    for (uint32_t I = threadIdx.x; I < D; I += blockDim.x) {
+      const double t = w[I] - a * vc[I];
+      w[I] = t;
+      sb += t * t;
+    }
+    const double b = sqrt(cta_sum(sb, sm));  // beta_j = |w|
+    const double z = (b > 0.0) ? 1.0 / b : 0.0;
+    for (uint32_t I = threadIdx.x; I < D; I += blockDim.x) w[I] *= z;
+    if (threadIdx.x == 0) {
+      const int j = *ls.j;
+      ls.alpha_hist[j] = a;
+      ls.beta_hist[j] = b;
+      *ls.alpha_cur = a;
+      *ls.b2_cur = b * b;
+      *ls.beta_prev = b;
+      *ls.j = j + 1;
+    }
+    __syncthreads();  // v_{j+1} and beta_j visible to the whole CTA
+    double *t = vp;
+    vp = vc;
+    vc = w;
+    w = t;
+  }
 }
 
 __global__ void k_swap_scale(size_t D, double *q, double *p, double beta) {
@@ -825,6 +925,24 @@ int launch_axpby(size_t D, double a, double *y, double b, const double *x, int n
   k_axpby<<<grid, kThreads, 0, s>>>(D, a, y, b, x, norm, r.partials);
   QED_LAUNCH();
   return grid;
+}
+
+int launch_axpy_dev(size_t D, double *y, const double *x, const double *a_dev, Reducer &r, cudaStream_t s) {
+  int grid = std::min(grid_for(D, device_sms(), 4), r.max_blocks);
+  k_axpy_dev<<<grid, kThreads, 0, s>>>(D, y, x, a_dev, r.partials);
+  QED_LAUNCH();
+  return grid;
+}
+
+void launch_lanczos_advance(size_t D, double *y, const LanczosScalars &ls, cudaStream_t s) {
+  k_lanczos_advance<<<grid_for(D, device_sms(), 4), kThreads, 0, s>>>(D, y, ls);
+  QED_LAUNCH();
+}
+
+void launch_lanczos_cta(const HvOperator &op, double *vprev, double *vcur, double *w, const LanczosScalars &ls,
+                        int nsteps, cudaStream_t s) {
+  k_lanczos_cta<<<1, 1024, 0, s>>>(op, vprev, vcur, w, ls, nsteps);
+  QED_LAUNCH();
 }
 
 void launch_swap_scale(size_t D, double *q, double *p, double beta, cudaStream_t s) {

@@ -48,6 +48,7 @@ struct SubList {
   int n = 0;
   double c[32];
   const double *z[32];
+  const double *cdev = nullptr;  // if set, the coefficients are read from device memory cdev[k]
 };
 
 // Deterministic two-stage reductions: kernels write per-block partial sums,
@@ -81,6 +82,31 @@ void launch_cdag_gather(int L, int spin, int a, int pm, const uint32_t *tgt_up_b
 // (Hamiltonian_Dense, src_ed/Hamiltonian/Hamiltonian_Dense.hpp:60-88). h must
 // hold D*D doubles; it is overwritten.
 void launch_dense_hamiltonian(const HvOperator &op, double *h, cudaStream_t s);
+
+// ---- device-resident Lanczos step ------------------------------------------
+// Scalars of a ground-state Lanczos run kept in device memory, so that a chunk
+// of iterations runs without host round trips (LanczosEigenvalue,
+// src_ed/Hamiltonian/Lanczos.hpp:41-97, one step = w = H v_j - beta_{j-1} v_{j-1};
+// alpha_j = <v_j, w>; w -= alpha_j v_j; beta_j = |w|; v_{j+1} = w / beta_j).
+struct LanczosScalars {
+  double *alpha_cur = nullptr;   // alpha_j (finalised <v_j, w>)
+  double *b2_cur = nullptr;      // |w - alpha_j v_j|^2
+  double *beta_prev = nullptr;   // beta_j, read by the next row pass as its subtraction coefficient
+  double *alpha_hist = nullptr;  // alpha_j, beta_j appended at index *j
+  double *beta_hist = nullptr;
+  int *j = nullptr;
+};
+// y -= (*a_dev) x, with |y|^2 block partials in r.partials; returns the grid size.
+int launch_axpy_dev(size_t D, double *y, const double *x, const double *a_dev, Reducer &r, cudaStream_t s);
+// y *= 1 / sqrt(*b2_cur) (0 if that is 0); records alpha_j, beta_j and advances *j.
+void launch_lanczos_advance(size_t D, double *y, const LanczosScalars &ls, cudaStream_t s);
+// nsteps whole Lanczos steps of a sector of at most kLanczosCtaMaxDim states in
+// one CTA (one launch instead of six per step). On entry vprev = v_{j-1},
+// vcur = v_j, w = scratch; after n steps the roles have rotated n times as
+// (vprev, vcur, w) <- (vcur, w, vprev).
+constexpr size_t kLanczosCtaMaxDim = 65536;
+void launch_lanczos_cta(const HvOperator &op, double *vprev, double *vcur, double *w, const LanczosScalars &ls,
+                        int nsteps, cudaStream_t s);
 
 // ---- H.v ------------------------------------------------------------------
 // Row pass: y = (diag + up hops) x - sum_k sub.c[k] sub.z[k]   (x scaled by xs)

@@ -9,6 +9,7 @@
 
 #include "eigen.hpp"
 #include "options.hpp"
+#include "profile.hpp"
 
 namespace qed {
 
@@ -137,6 +138,7 @@ SpinTable view(const HalfTables &h) {
 }  // namespace
 
 SectorOp::SectorOp(const SpinData &t, const Sector &s, Workspace &ws) : sec(s), L(t.n) {
+  PhaseScope ps(kPhSectorSetup);
   if (s.N >= Sector::odd || s.S >= Sector::odd)
     fail(QED_ERR_UNSUPPORTED, "sector " + s.name() + " does not conserve N and S");
   if ((s.N + s.S) % 2) fail(QED_ERR_ARGUMENT, "sector " + s.name() + " is not valid");
@@ -210,55 +212,98 @@ void start_vector(size_t D, uint64_t seed, double *v, Workspace &ws) {
 // within 1e3 of the tolerance the O(j^2) QL last-row method (the reference's
 // dstev result) decides the stop, so the iteration count does not depend on
 // the fast estimate.
+//
+// The recurrence itself runs on the device in chunks: alpha_j, beta_j stay in
+// device memory (the row pass reads beta_{j-1} from there), and the host reads
+// a whole chunk of (alpha, beta) once, then applies the Ritz test step by step
+// in the reference's order. Steps computed past the stopping step are dropped,
+// so the tridiagonal, the energy and the iteration count are those of the
+// one-step-at-a-time recurrence.
 LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed) {
+  PhaseScope ps(kPhGsLanczos);
   LanczosResult res;
   const size_t D = H.D;
   const double accur = opt_double("accur_lanczos");
   const long max_iter = opt_int("max_iter_lanczos");
   cudaStream_t s = ws.stream;
+  constexpr int kChunk = 16;
+  static_assert(2 * kChunk <= Reducer::kMaxRed, "chunk read back through the pinned reduction buffer");
   DevBuf<double> A(D), B(D), C(D);
   start_vector(D, seed, B.p, ws);
+  QED_CUDA(cudaMemsetAsync(A.p, 0, D * sizeof(double), s));  // v_{-1} = 0
+  const size_t cap = (size_t)std::max<long>(max_iter, 1) + 2 * kChunk;
+  DevBuf<double> sc(3 + 2 * cap);
+  DevBuf<int> jd(1);
+  QED_CUDA(cudaMemsetAsync(sc.p, 0, 3 * sizeof(double), s));
+  QED_CUDA(cudaMemsetAsync(jd.p, 0, sizeof(int), s));
+  LanczosScalars ls;
+  ls.alpha_cur = sc.p;
+  ls.b2_cur = sc.p + 1;
+  ls.beta_prev = sc.p + 2;
+  ls.alpha_hist = sc.p + 3;
+  ls.beta_hist = sc.p + 3 + cap;
+  ls.j = jd.p;
+  SubList sub;  // w = H v_j - beta_{j-1} v_{j-1}, beta from device memory
+  sub.n = 1;
+  sub.cdev = ls.beta_prev;
   double *pa = A.p, *pb = B.p, *pc = C.p;
   std::vector<double> &alpha = res.alpha, &beta = res.beta;
-  double ritz = 2.0 * accur;
   double lambda0 = 0.0;
   double upper = std::numeric_limits<double>::infinity();  // Cauchy interlacing bound
-  int nb = 0;
-  while (ritz > accur) {
-    // w = H v_j - beta_{j-1} v_{j-1}
-    SubList sub;
-    if (!beta.empty()) {
-      sub.n = 1;
-      sub.c[0] = beta.back();
+  size_t launched = 0;
+  // a first short chunk: tiny sectors stop after about D steps
+  int chunk = (int)std::min<size_t>(std::max<size_t>(D, 2), 8);
+  bool stop = false;
+  while (!stop) {
+    if (launched + chunk > cap) fail(QED_ERR_INTERNAL, "Lanczos history overflow");
+    if (D <= kLanczosCtaMaxDim) launch_lanczos_cta(H.op, pa, pb, pc, ls, chunk, s);
+    for (int k = 0; k < chunk; ++k) {
+      if (D <= kLanczosCtaMaxDim) {  // the CTA kernel above ran the step
+        double *t = pa;
+        pa = pb;
+        pb = pc;
+        pc = t;
+        continue;
+      }
       sub.z[0] = pa;
+      launch_hv_rows(H.op, pb, 1.0, pc, sub, s);
+      int nb = launch_hv_cols(H.op, pb, 1.0, pc, 1, ws.red, s);
+      launch_finalize(ws.red.partials, nb, 1, ls.alpha_cur, s);      // alpha_j = <v_j, w>
+      nb = launch_axpy_dev(D, pc, pb, ls.alpha_cur, ws.red, s);      // w -= alpha_j v_j
+      launch_finalize(ws.red.partials, nb, 1, ls.b2_cur, s);          // |w|^2
+      launch_lanczos_advance(D, pc, ls, s);                           // v_{j+1} = w / beta_j
+      double *t = pa;  // v_{j-1} <- v_j <- v_{j+1}
+      pa = pb;
+      pb = pc;
+      pc = t;
     }
-    launch_hv_rows(H.op, pb, 1.0, pc, sub, s);
-    nb = launch_hv_cols(H.op, pb, 1.0, pc, 1, ws.red, s);
-    const double a = ws.sums(nb, 1)[0];  // alpha_j = <v_j, w>
-    nb = launch_axpby(D, 1.0, pc, -a, pb, 1, ws.red, s);
-    const double b = std::sqrt(ws.sums(nb, 1)[0]);  // beta_j = |w - alpha_j v_j|
-    alpha.push_back(a);
-    beta.push_back(b);
-    double last = 1.0;
-    tridiag_lowest_fast((int)alpha.size(), alpha.data(), beta.data(), upper, &lambda0, &last, nullptr);
-    upper = lambda0;
-    ritz = std::fabs(last * b);
-    if (ritz < 1e3 * accur) {
-      if (!tridiag_lowest_last((int)alpha.size(), alpha.data(), beta.data(), &lambda0, &last))
-        fail(QED_ERR_LANCZOS, "tridiagonal eigensolver did not converge");
-      ritz = std::fabs(last * b);
+    QED_CUDA(cudaMemcpyAsync(ws.host, ls.alpha_hist + launched, chunk * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+    QED_CUDA(cudaMemcpyAsync(ws.host + kChunk, ls.beta_hist + launched, chunk * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+    ws.sync();
+    launched += chunk;
+    for (int k = 0; k < chunk && !stop; ++k) {
+      const double a = ws.host[k], b = ws.host[kChunk + k];
+      alpha.push_back(a);
+      beta.push_back(b);
+      double last = 1.0;
+      tridiag_lowest_fast((int)alpha.size(), alpha.data(), beta.data(), upper, &lambda0, &last, nullptr);
+      upper = lambda0;
+      double ritz = std::fabs(last * b);
+      if (ritz < 1e3 * accur) {
+        if (!tridiag_lowest_last((int)alpha.size(), alpha.data(), beta.data(), &lambda0, &last))
+          fail(QED_ERR_LANCZOS, "tridiagonal eigensolver did not converge");
+        ritz = std::fabs(last * b);
+      }
+      if ((long)alpha.size() > max_iter)
+        fail(QED_ERR_LANCZOS, "Lanczos procedure exceeded " + std::to_string(max_iter) + " iterations");
+      if (!(ritz > accur)) stop = true;
     }
-    if ((long)alpha.size() > max_iter)
-      fail(QED_ERR_LANCZOS, "Lanczos procedure exceeded " + std::to_string(max_iter) + " iterations");
-    if (ritz > accur) {
-      launch_scale(D, pc, 1.0 / b, s);  // v_{j+1}
-      std::swap(pa, pb);                // v_{j-1} <- v_j
-      std::swap(pb, pc);                // v_j <- v_{j+1}
-    }
+    chunk = kChunk;
   }
   res.energy = lambda0;
   res.iterations = (int)alpha.size();
-  ws.sync();
   return res;
 }
 
@@ -266,6 +311,7 @@ LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed) {
 // with the v_j regenerated from the same start vector and the stored alpha/beta.
 void lanczos_eigenvector(const SectorOp &H, Workspace &ws, const LanczosResult &res,
                          uint64_t seed, DevBuf<double> &psi) {
+  PhaseScope ps(kPhGsVector);
   const size_t D = H.D;
   cudaStream_t s = ws.stream;
   const std::vector<double> &alpha = res.alpha, &beta = res.beta;
@@ -309,6 +355,7 @@ LanczosResult lanczos_ground_state(const SectorOp &H, Workspace &ws, DevBuf<doub
 
 void dense_eigensystem(const SectorOp &H, Workspace &ws, std::vector<double> &w,
                        std::vector<double> &U) {
+  PhaseScope ps(kPhDense);
   const size_t D = H.D;
   DevBuf<double> h(D * D);
   launch_dense_hamiltonian(H.op, h.p, ws.stream);
@@ -412,6 +459,7 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
   int j = 0;
   int nd = 0;
   VecList ys;
+  PhaseScope ps_loop(kPhBandLoop);
   for (j = 0; j < M0; ++j) {
     if (phi_alive && j >= p) {  // P(k, j) is only used for j < p (Q = P U over k < p)
       for (auto &f : phi) f.release();
@@ -505,6 +553,7 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
     for (int k = 0; k < nd; ++k) T(j, I[k]) = T(I[k], j);
     // step (12): convergence test on the lowest eigenvalue of the projected matrix
     if (j >= 4 * p && j % p == 0) {
+      PhaseScope ps_check(kPhBandCheck);
       std::vector<double> Hpr((size_t)j * j), ev;
       for (int c = 0; c < j; ++c)
         for (int r = 0; r < j; ++r) Hpr[(size_t)r + (size_t)j * c] = T(r, c);
@@ -523,6 +572,7 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
   ws.sync();
   Mout = j;
   if (j == 0) return false;
+  PhaseScope ps_eig(kPhBandEig);
   // projected eigensystem and Q = P U, summed over the first p Lanczos vectors
   std::vector<double> Hpr((size_t)j * j), U;
   for (int c = 0; c < j; ++c)

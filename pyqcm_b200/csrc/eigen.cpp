@@ -271,16 +271,27 @@ bool sym_eig(int n, const std::vector<double> &A, std::vector<double> &w, std::v
   return true;
 }
 
-bool band_eigenvalues(int n, int b, std::vector<double> A, std::vector<double> &w) {
-  w.assign(n, 0.0);
-  if (n == 0) return true;
-  if (b < 1) b = 1;
-  auto a = [&](int i, int j) -> double & { return A[(size_t)i + (size_t)n * j]; };
-  // symmetrise from the lower triangle and clear everything outside the band
+namespace {
+// Reduces the symmetric band matrix A (column-major n x n, half-bandwidth b,
+// lower triangle used) to tridiagonal form in place by Givens rotations with
+// bulge chasing (H. R. Schwarz, Numer. Math. 12, 1968). Every rotation of rows
+// and columns (p, p+1) is also passed to rot(p, c, s), so that a caller can
+// accumulate the transformation. On return d, e hold the tridiagonal.
+template <class Rot>
+void band_to_tridiagonal(int n, int b, const std::vector<double> &A, std::vector<double> &d, std::vector<double> &e,
+                         Rot &&rot) {
+  // Work array: the band |i - j| <= B = b + 2 (the band, the bulge at b + 1 and
+  // the reach of one rotation), column j at offset (i - j + B). Nothing outside
+  // it is ever read or written, and it stays cache-resident.
+  const int B = b + 2, W = 2 * B + 1;
+  std::vector<double> ab((size_t)W * n, 0.0);
+  auto a = [&](int i, int j) -> double & { return ab[(size_t)(i - j + B) + (size_t)W * j]; };
+  // symmetric band from the lower triangle of A
   for (int j = 0; j < n; ++j)
-    for (int i = 0; i < n; ++i) {
-      if (std::abs(i - j) > b) a(i, j) = 0.0;
-      else if (i < j) a(i, j) = a(j, i);
+    for (int i = j; i < std::min(n, j + b + 1); ++i) {
+      const double x = A[(size_t)i + (size_t)n * j];
+      a(i, j) = x;
+      a(j, i) = x;
     }
   // rotation in the (p, p+1) plane: A <- G A G^T, G = [[c, s], [-s, c]];
   // rows/columns p, p+1 have nonzeros only within [p-b-1, p+b+2]
@@ -297,6 +308,7 @@ bool band_eigenvalues(int n, int b, std::vector<double> A, std::vector<double> &
       a(i, p) = c * x + s * y;
       a(i, q) = -s * x + c * y;
     }
+    rot(p, c, s);
   };
   auto zero_with = [&](int p, int col) {  // zero a(p+1, col) using rows p, p+1
     const double f = a(p, col), g = a(p + 1, col);
@@ -318,11 +330,59 @@ bool band_eigenvalues(int n, int b, std::vector<double> A, std::vector<double> &
       }
     }
   }
-  std::vector<double> d(n), e(n, 0.0);
+  d.assign(n, 0.0);
+  e.assign(n, 0.0);
   for (int i = 0; i < n; ++i) d[i] = a(i, i);
   for (int i = 0; i + 1 < n; ++i) e[i] = a(i + 1, i);
+}
+}  // namespace
+
+bool band_eigenvalues(int n, int b, std::vector<double> A, std::vector<double> &w) {
+  w.assign(n, 0.0);
+  if (n == 0) return true;
+  if (b < 1) b = 1;
+  std::vector<double> d, e;
+  band_to_tridiagonal(n, b, A, d, e, [](int, double, double) {});
   if (!tridiag_eig(n, d, e, nullptr)) return false;
   w = d;
+  return true;
+}
+
+bool band_eig_rows(int n, int b, std::vector<double> A, int m, std::vector<double> &w, std::vector<double> &Z) {
+  w.assign(n, 0.0);
+  Z.assign((size_t)m * n, 0.0);
+  if (n == 0) return true;
+  if (b < 1) b = 1;
+  m = std::min(m, n);
+  // rows 0..m-1 of the accumulated orthogonal transformation, column-major m x n
+  std::vector<double> Q((size_t)m * n, 0.0);
+  for (int r = 0; r < m; ++r) Q[r + (size_t)m * r] = 1.0;
+  auto rot_cols = [&](int i, double c, double s) {  // columns (i, i+1) <- (c x + s y, -s x + c y)
+    double *x = Q.data() + (size_t)m * i, *y = x + m;
+    for (int r = 0; r < m; ++r) {
+      const double u = x[r], v = y[r];
+      x[r] = c * u + s * v;
+      y[r] = -s * u + c * v;
+    }
+  };
+  std::vector<double> d, e;
+  band_to_tridiagonal(n, b, A, d, e, rot_cols);
+  bool ok = ql_implicit(n, d.data(), e.data(), [&](int i, double c, double s) {
+    double *ci = Q.data() + (size_t)m * i, *cj = ci + m;
+    for (int r = 0; r < m; ++r) {
+      const double f = cj[r];
+      cj[r] = s * ci[r] + c * f;
+      ci[r] = c * ci[r] - s * f;
+    }
+  });
+  if (!ok) return false;
+  std::vector<int> idx(n);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return d[x] < d[y]; });
+  for (int k = 0; k < n; ++k) {
+    w[k] = d[idx[k]];
+    std::copy(Q.data() + (size_t)m * idx[k], Q.data() + (size_t)m * (idx[k] + 1), Z.data() + (size_t)m * k);
+  }
   return true;
 }
 

@@ -48,6 +48,13 @@ bool sym_eig(int n, const std::vector<double> &A, std::vector<double> &w, std::v
 // 12, 1968), O(n^2 b), then QL. Used for the band-Lanczos convergence test.
 bool band_eigenvalues(int n, int b, std::vector<double> A, std::vector<double> &w);
 
+// Eigenvalues (ascending) of the same band matrix and the first m rows of its
+// eigenvector matrix, Z column-major m x n (column k <-> w[k]): the band
+// reduction and the QL rotations are accumulated on those m rows only, O(n^2 b)
+// instead of the O(n^3) of a full eigensystem. The band-Lanczos Q-matrix needs
+// only the first p rows (Q = P U with P zero beyond the p start vectors).
+bool band_eig_rows(int n, int b, std::vector<double> A, int m, std::vector<double> &w, std::vector<double> &Z);
+
 // In-place inverse of a complex n x n column-major matrix (Gauss-Jordan with
 // partial pivoting). Returns false if singular.
 bool complex_inverse(int n, std::complex<double> *a);

@@ -577,13 +577,21 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
   std::vector<double> Hpr((size_t)j * j), U;
   for (int c = 0; c < j; ++c)
     for (int r = 0; r < j; ++r) Hpr[(size_t)r + (size_t)j * c] = T(r, c);
-  if (!sym_eig(j, Hpr, evals, &U)) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
   const int kmax = std::min(p, j);
+  // only rows k < p of the eigenvectors enter Q; without deflation the
+  // projected matrix is banded (half-bandwidth p)
+  int ldu = j;
+  if (nd == 0) {
+    if (!band_eig_rows(j, p, Hpr, kmax, evals, U)) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
+    ldu = kmax;
+  } else if (!sym_eig(j, Hpr, evals, &U)) {
+    fail(QED_ERR_INTERNAL, "projected eigensolver failed");
+  }
   Q.assign((size_t)p * j, 0.0);
   for (int m = 0; m < j; ++m)
     for (int i = 0; i < p; ++i) {
       double acc = 0.0;
-      for (int k = 0; k < kmax; ++k) acc += P[(size_t)i + (size_t)p * k] * U[(size_t)k + (size_t)j * m];
+      for (int k = 0; k < kmax; ++k) acc += P[(size_t)i + (size_t)p * k] * U[(size_t)k + (size_t)ldu * m];
       Q[(size_t)i + (size_t)p * m] = acc;
     }
   return true;

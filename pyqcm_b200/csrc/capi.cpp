@@ -596,10 +596,10 @@ int qed_hamiltonian_diag(qed_hamiltonian *h, double *d) {
     std::lock_guard<std::mutex> hl(h->m);
     // diagonal = H applied to unit vectors is wasteful; rebuild it from the tables on the host
     const SectorOp &H = *h->H;
-    std::vector<double> du(H.up.dim), dd(H.dn.dim);
+    std::vector<double> du(H.up->dim), dd(H.dn->dim);
     Workspace &w = ws();
-    H.up.diag.download(du.data(), du.size(), w.stream);
-    H.dn.diag.download(dd.data(), dd.size(), w.stream);
+    H.up->diag.download(du.data(), du.size(), w.stream);
+    H.dn->diag.download(dd.data(), dd.size(), w.stream);
     std::vector<double> vin;
     if (H.op.inter.mode >= 2) {
       vin.resize(H.vinter.n);
@@ -607,9 +607,9 @@ int qed_hamiltonian_diag(qed_hamiltonian *h, double *d) {
     }
     w.sync();
     const int n = H.L;
-    for (uint32_t b = 0; b < H.dn.dim; ++b)
-      for (uint32_t a = 0; a < H.up.dim; ++a) {
-        uint32_t up = H.up.hbits[a], dn = H.dn.hbits[b];
+    for (uint32_t b = 0; b < H.dn->dim; ++b)
+      for (uint32_t a = 0; a < H.up->dim; ++a) {
+        uint32_t up = H.up->hbits[a], dn = H.dn->hbits[b];
         double s = du[a] + dd[b];
         const auto &it = H.op.inter;
         if (it.mode == 1) s += it.u * __builtin_popcount(up & dn);
@@ -620,7 +620,7 @@ int qed_hamiltonian_diag(qed_hamiltonian *h, double *d) {
               for (int c = 0; c < n; ++c)
                 if (up >> c & 1u) s += vin[(size_t)r * n + c];
         }
-        d[a + (size_t)H.up.dim * b] = s;
+        d[a + (size_t)H.up->dim * b] = s;
       }
   });
 }

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <numeric>
 
 namespace qed {
@@ -192,6 +193,68 @@ void tridiag_lowest_fast(int n, const double *alpha, const double *beta, double 
     for (int i = 0; i < n; ++i) (*vec)[i] = u[i] / nrm;
   }
   (void)scale;
+}
+
+void tridiag_lowest_track(int n, const double *alpha, const double *beta, RitzTracker &tr, double *lambda0,
+                          double *last) {
+  auto fallback = [&] {
+    const double upper = ((int)tr.vec.size() == n - 1 && n > 1) ? tr.lambda : std::numeric_limits<double>::infinity();
+    tridiag_lowest_fast(n, alpha, beta, upper, lambda0, last, &tr.vec);
+    tr.lambda = *lambda0;
+    tr.last = *last;
+  };
+  if (n <= 2 || (int)tr.vec.size() != n - 1) return fallback();
+  double tnorm = 0.0;
+  for (int i = 0; i < n; ++i)
+    tnorm = std::max(tnorm, std::fabs(alpha[i]) + (i ? std::fabs(beta[i - 1]) : 0.0) +
+                                (i + 1 < n ? std::fabs(beta[i]) : 0.0));
+  const double r = std::fabs(beta[n - 2] * tr.last);
+  if (!(r <= 1e-2 * tnorm)) return fallback();
+  const double sigma = tr.lambda - r - 1e-13 * tnorm;
+  // LDL^T of T - sigma: all pivots positive <=> no eigenvalue below sigma
+  std::vector<double> dpiv(n), l(n, 0.0);
+  dpiv[0] = alpha[0] - sigma;
+  if (!(dpiv[0] > 0.0)) return fallback();
+  for (int i = 0; i + 1 < n; ++i) {
+    l[i] = beta[i] / dpiv[i];
+    dpiv[i + 1] = alpha[i + 1] - sigma - beta[i] * l[i];
+    if (!(dpiv[i + 1] > 0.0)) return fallback();
+  }
+  std::vector<double> x(n), y(n);
+  for (int i = 0; i + 1 < n; ++i) x[i] = tr.vec[i];
+  x[n - 1] = 0.0;
+  double rho = tr.lambda;
+  for (int it = 0; it < 4; ++it) {
+    // y = (T - sigma)^{-1} x
+    y[0] = x[0];
+    for (int i = 1; i < n; ++i) y[i] = x[i] - l[i - 1] * y[i - 1];
+    for (int i = 0; i < n; ++i) y[i] /= dpiv[i];
+    for (int i = n - 2; i >= 0; --i) y[i] -= l[i] * y[i + 1];
+    double nrm = 0.0;
+    for (int i = 0; i < n; ++i) nrm += y[i] * y[i];
+    nrm = std::sqrt(nrm);
+    for (int i = 0; i < n; ++i) x[i] = y[i] / nrm;
+    // Rayleigh quotient and residual of x
+    double num = 0.0, res2 = 0.0;
+    for (int i = 0; i < n; ++i) {
+      double tx = alpha[i] * x[i];
+      if (i) tx += beta[i - 1] * x[i - 1];
+      if (i + 1 < n) tx += beta[i] * x[i + 1];
+      y[i] = tx;
+      num += x[i] * tx;
+    }
+    rho = num;
+    for (int i = 0; i < n; ++i) res2 += (y[i] - rho * x[i]) * (y[i] - rho * x[i]);
+    if (std::sqrt(res2) <= 1e-14 * tnorm) {
+      *lambda0 = rho;
+      *last = x[n - 1];
+      tr.lambda = rho;
+      tr.last = x[n - 1];
+      tr.vec = x;
+      return;
+    }
+  }
+  fallback();
 }
 
 bool sym_eig(int n, const std::vector<double> &A, std::vector<double> &w, std::vector<double> *V) {

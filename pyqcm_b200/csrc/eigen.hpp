@@ -37,6 +37,23 @@ bool tridiag_lowest_last(int n, const double *alpha, const double *beta, double 
 void tridiag_lowest_fast(int n, const double *alpha, const double *beta, double upper,
                          double *lambda0, double *last, std::vector<double> *vec);
 
+// Incremental version for a growing Lanczos tridiagonal: called with n = 1, 2,
+// 3, ... on the same alpha/beta arrays (beta[n-2] couples the newest row). The
+// previous eigenvector [u; 0] has Rayleigh quotient lambda_prev and residual
+// r = |beta[n-2] u_last| for T_n, so T_n has an eigenvalue in
+// [lambda_prev - r, lambda_prev]; if T_n - sigma (sigma just below that
+// interval) is positive definite (all LDL^T pivots > 0, i.e. a Sturm count of
+// zero) that eigenvalue is the lowest and a few steps of inverse iteration from
+// [u; 0] give it with its eigenvector in O(n). Otherwise, or if the iteration
+// does not reach a residual of 1e-14 ||T||, it falls back to
+// tridiag_lowest_fast.
+struct RitzTracker {
+  double lambda = 0.0, last = 0.0;
+  std::vector<double> vec;  // eigenvector of the previous call
+};
+void tridiag_lowest_track(int n, const double *alpha, const double *beta, RitzTracker &tr, double *lambda0,
+                          double *last);
+
 // Dense symmetric eigenproblem, A column-major n x n (lower triangle used).
 // w receives eigenvalues ascending; V (if non-null) the eigenvectors.
 bool sym_eig(int n, const std::vector<double> &A, std::vector<double> &w, std::vector<double> *V);

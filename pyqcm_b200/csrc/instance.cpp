@@ -194,7 +194,7 @@ size_t Instance::sector_dim(const Sector &s) const {
 void Instance::solve_sector(const Sector &s, SectorSolve &out, Workspace &ws) {
   out.sec = s;
   try {
-    SectorOp H(terms, s, ws);
+    SectorOp H(terms, s, ws, &tables);
     out.dim = H.D;
     if (H.D == 0) return;
     if (!model->factorized && (long)H.D < opt_int("max_dim_full")) {
@@ -273,7 +273,7 @@ void Instance::state_vector(State &st, Workspace &ws) {
       st.hpsi = std::vector<double>();
       return;
     }
-    SectorOp H(terms, st.sec, ws);
+    SectorOp H(terms, st.sec, ws, &tables);
     lanczos_eigenvector(H, ws, st.lanczos, (uint64_t)opt_int("seed"), st.psi);
   } catch (const Error &e) {
     fail(e.code, std::string(e.what()) + where(st.sec));
@@ -328,7 +328,7 @@ void Instance::apply_cdag(const State &st, int pm, int spin, int orb, const Sect
   const int L = model->n_orb;
   const int src_nup = st.sec.Nup(), src_ndn = st.sec.Ndw();
   const uint32_t du_s = (uint32_t)((src_nup < 0 || src_nup > L) ? 0 : binom(L, src_nup));
-  launch_cdag_gather(L, spin, orb, pm, H.up.bits.p, H.up.dim, H.dn.bits.p, H.dn.dim, src_nup, src_ndn,
+  launch_cdag_gather(L, spin, orb, pm, H.up->bits.p, H.up->dim, H.dn->bits.p, H.dn->dim, src_nup, src_ndn,
                      du_s, st.psi.p, y, coef, accumulate ? 1 : 0, ws.stream);
 }
 
@@ -387,7 +387,7 @@ void Instance::qmatrix_part(State &st, bool spin_down, int s, QPart &out, Worksp
   out.V.clear();
   Sector tsec = shift_sector(st.sec, pm, spin);
   if (!sector_is_valid(tsec, model->n_orb)) return;
-  SectorOp H(terms, tsec, ws);
+  SectorOp H(terms, tsec, ws, &tables);
   if (H.D == 0) return;
   std::vector<DevBuf<double>> phi;
   phi.reserve(p);
@@ -484,7 +484,7 @@ void Instance::build_cf(State &st, bool spin_down, Workspace &ws) {
   for (int pm = -1; pm < 2; pm += 2) {
     Sector tsec = shift_sector(st.sec, pm, spin_down ? 1 : 0);
     if (!sector_is_valid(tsec, model->n_orb)) continue;
-    SectorOp H(terms, tsec, ws);
+    SectorOp H(terms, tsec, ws, &tables);
     if (H.D == 0) continue;
     DevBuf<double> psi(H.D), q(H.D);
     for (int o1 = 0; o1 < n; ++o1)

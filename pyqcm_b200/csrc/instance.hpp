@@ -71,6 +71,7 @@ struct Instance {
   double GS_energy = 0.0, E0 = 0.0, SEF_bath = 0.0, GF_density = 0.0;
   std::vector<std::shared_ptr<State>> states;
   SpinData terms;
+  HalfCache tables;  // spin tables shared by the sectors of this instance
   std::vector<double> tc[2], tb[2], tcb[2];  // cluster, bath (diagonalised), cluster-bath
   std::vector<cplx> Mave[2];
   std::mutex mtx;

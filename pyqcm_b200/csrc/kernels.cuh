@@ -104,7 +104,7 @@ void launch_lanczos_advance(size_t D, double *y, const LanczosScalars &ls, cudaS
 // one CTA (one launch instead of six per step). On entry vprev = v_{j-1},
 // vcur = v_j, w = scratch; after n steps the roles have rotated n times as
 // (vprev, vcur, w) <- (vcur, w, vprev).
-constexpr size_t kLanczosCtaMaxDim = 65536;
+constexpr size_t kLanczosCtaMaxDim = 8192;
 void launch_lanczos_cta(const HvOperator &op, double *vprev, double *vcur, double *w, const LanczosScalars &ls,
                         int nsteps, cudaStream_t s);
 

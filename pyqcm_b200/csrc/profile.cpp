@@ -10,7 +10,8 @@ namespace qed {
 namespace {
 const char *kNames[kPhCount] = {"sector setup",       "GS Lanczos (eigenvalue)", "GS Lanczos (eigenvector)",
                                 "dense sectors",      "c/c+ start vectors",      "band Lanczos recurrence",
-                                "band Lanczos checks", "band projected eigensystem", "continued fractions"};
+                                "band Lanczos checks", "band projected eigensystem", "continued fractions",
+                                "GS Ritz tests (in GS eigenvalue)"};
 
 struct Totals {
   std::atomic<long long> ns[kPhCount];

@@ -16,6 +16,7 @@ enum Phase {
   kPhBandCheck,     // band Lanczos convergence checks (host eigenvalues)
   kPhBandEig,       // projected eigensystem and Q = P U
   kPhCf,            // continued-fraction Lanczos
+  kPhRitz,          // ground-state Lanczos: host Ritz tests (inside kPhGsLanczos)
   kPhCount
 };
 

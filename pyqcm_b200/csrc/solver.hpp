@@ -42,15 +42,24 @@ struct HalfTables {
   int nvals = 0, width = 0;
 };
 
+// Per-instance cache of the spin tables: a sector (N_up, N_dn) uses the up
+// table of N_up and the down table of N_dn, so the sectors of one instance
+// share them. Thread-safe; tables live until the cache is destroyed.
+struct HalfCache {
+  std::mutex m;
+  std::map<std::pair<int, int>, std::shared_ptr<const HalfTables>> tab;  // (spin, N)
+};
+
 struct SectorOp {
   Sector sec;
   int L = 0;
-  HalfTables up, dn;
+  std::shared_ptr<const HalfTables> up, dn;
   DevBuf<double> vinter;
   HvOperator op;
   size_t D = 0;
-  // Builds all tables for `sec` from the collected terms, on `ws.stream`.
-  SectorOp(const SpinData &terms, const Sector &sec, Workspace &ws);
+  // Builds (or takes from `cache`) the tables for `sec` from the collected
+  // terms, on `ws.stream`.
+  SectorOp(const SpinData &terms, const Sector &sec, Workspace &ws, HalfCache *cache = nullptr);
   // y = H x (device vectors)
   void apply(const double *x, double *y, Workspace &ws) const;
 };

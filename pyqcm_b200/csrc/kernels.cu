@@ -255,6 +255,7 @@ __global__ void k_dense_hamiltonian(HvOperator op, double *__restrict__ h) {
 template <bool SMEM>
 __global__ void __launch_bounds__(512) k_hv_rows(HvOperator op, const double *__restrict__ x,
                                                   double xs, double *y, SubList sub) {
+  if (op.skip && *op.skip) return;
   extern __shared__ double xsm[];
   __shared__ double vals[256];
   const uint32_t du = op.up.dim, dd = op.dn.dim;
@@ -291,6 +292,7 @@ template <int VEC, int R>
 __global__ void __launch_bounds__(kThreads) k_hv_cols(HvOperator op, const double *__restrict__ x,
                                                        double xs, double *y, int red_mask,
                                                        double *partials) {
+  if (op.skip && *op.skip) return;
   __shared__ double vals[256];
   const uint32_t du = op.up.dim, dd = op.dn.dim;
   for (int i = threadIdx.x; i < op.dn.nvals; i += blockDim.x) vals[i] = op.dn.vals[i];
@@ -353,6 +355,7 @@ __global__ void __launch_bounds__(kThreads) k_hv_cols(HvOperator op, const doubl
 template <int UNROLL>
 __global__ void __launch_bounds__(1024) k_hv_rows2(HvOperator op, const double *__restrict__ x,
                                                    double xs, double *y, SubList sub) {
+  if (op.skip && *op.skip) return;
   extern __shared__ double2 xs2[];
   __shared__ double vals[256];
   const uint32_t du = op.up.dim, dd = op.dn.dim;
@@ -422,6 +425,7 @@ template <int VEC, bool CG>
 __global__ void __launch_bounds__(kThreads) k_hv_cols2(HvOperator op, const double *__restrict__ x,
                                                         double xs, double *y, int red_mask,
                                                         double *partials) {
+  if (op.skip && *op.skip) return;
   __shared__ double cval[kColsR][kMaxHops];
   __shared__ uint32_t cidx[kColsR][kMaxHops];
   __shared__ int ccnt[kColsR];
@@ -510,6 +514,8 @@ __global__ void __launch_bounds__(kThreads) k_hv_cols2(HvOperator op, const doub
 template <int G>
 __global__ void k_dots(size_t D, double *x, double xs, int write_x, VecList ys, int first,
                        double *partials) {
+  if (ys.skip && *ys.skip) return;
+  if (ys.xsdev && first == 0) xs = *ys.xsdev;
   double acc[G];
 #pragma unroll
   for (int g = 0; g < G; ++g) acc[g] = 0.0;
@@ -540,11 +546,12 @@ __global__ void k_dots(size_t D, double *x, double xs, int write_x, VecList ys, 
 
 __global__ void k_multi_axpy(size_t D, const double *x, double xs, VecList ys, int norm_first,
                              double *partials) {
+  if (ys.skip && *ys.skip) return;
   double nrm[1] = {0.0};
   for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
     const double xv = x[I] * xs;
     for (int i = 0; i < ys.n; ++i) {
-      double v = ys.v[i][I] - ys.c[i] * xv;
+      double v = ys.v[i][I] - (ys.cdev ? ys.cdev[i] : ys.c[i]) * xv;
       ys.v[i][I] = v;
       if (i == 0 && norm_first) nrm[0] += v * v;
     }
@@ -563,7 +570,9 @@ __global__ void k_axpby(size_t D, double a, double *y, double b, const double *x
   if (norm) block_reduce_store<1>(nrm, partials, 1);
 }
 
-__global__ void k_axpy_dev(size_t D, double *y, const double *x, const double *a_dev, double *partials) {
+__global__ void k_axpy_dev(size_t D, double *y, const double *x, const double *a_dev, double *partials,
+                           const int *skip) {
+  if (skip && *skip) return;
   const double b = -*a_dev;
   double nrm[1] = {0.0};
   for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
@@ -691,6 +700,38 @@ __global__ void k_random(size_t D, uint64_t seed, double *y, double *partials) {
     nrm[0] += v * v;
   }
   block_reduce_store<1>(nrm, partials, 1);
+}
+
+__global__ void k_scale_dev(size_t D, double *y, const double *a_dev, const int *skip) {
+  if (skip && *skip) return;
+  const double a = *a_dev;
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x)
+    y[I] *= a;
+}
+
+// Band-Lanczos norm step: z = sqrt(sum of partials); below the deflation
+// tolerance it raises *flag (step + 1) and leaves everything else alone,
+// otherwise it stores z and 1/z.
+__global__ void k_finalize_norm(const double *partials, int nblocks, double dtol, double *z_out,
+                                double *inv_out, int *flag, int step) {
+  __shared__ double sm[kThreads];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[(size_t)b * Reducer::kMaxRed];
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && *flag == 0) {
+    const double z = sqrt(sm[0]);
+    if (z < dtol) {
+      *flag = step + 1;
+    } else {
+      *z_out = z;
+      *inv_out = 1.0 / z;
+    }
+  }
 }
 
 __global__ void k_scale(size_t D, double *y, double a) {
@@ -927,9 +968,10 @@ int launch_axpby(size_t D, double a, double *y, double b, const double *x, int n
   return grid;
 }
 
-int launch_axpy_dev(size_t D, double *y, const double *x, const double *a_dev, Reducer &r, cudaStream_t s) {
+int launch_axpy_dev(size_t D, double *y, const double *x, const double *a_dev, Reducer &r, cudaStream_t s,
+                    const int *skip) {
   int grid = std::min(grid_for(D, device_sms(), 4), r.max_blocks);
-  k_axpy_dev<<<grid, kThreads, 0, s>>>(D, y, x, a_dev, r.partials);
+  k_axpy_dev<<<grid, kThreads, 0, s>>>(D, y, x, a_dev, r.partials, skip);
   QED_LAUNCH();
   return grid;
 }
@@ -955,6 +997,17 @@ int launch_random(size_t D, uint64_t seed, double *y, Reducer &r, cudaStream_t s
   k_random<<<grid, kThreads, 0, s>>>(D, seed, y, r.partials);
   QED_LAUNCH();
   return grid;
+}
+
+void launch_scale_dev(size_t D, double *y, const double *a_dev, const int *skip, cudaStream_t s) {
+  k_scale_dev<<<grid_for(D, device_sms(), 4), kThreads, 0, s>>>(D, y, a_dev, skip);
+  QED_LAUNCH();
+}
+
+void launch_finalize_norm(const double *partials, int nblocks, double dtol, double *z_out, double *inv_out,
+                          int *flag, int step, cudaStream_t s) {
+  k_finalize_norm<<<1, kThreads, 0, s>>>(partials, nblocks, dtol, z_out, inv_out, flag, step);
+  QED_LAUNCH();
 }
 
 void launch_scale(size_t D, double *y, double a, cudaStream_t s) {

@@ -40,6 +40,7 @@ struct HvOperator {
   SpinTable up, dn;
   InterSpin inter;
   int num_sms = 148;
+  const int *skip = nullptr;  // if set and *skip != 0 (device), the H.v passes do nothing
 };
 
 // List of (coefficient, vector) pairs subtracted in the row pass epilogue:
@@ -97,7 +98,8 @@ struct LanczosScalars {
   int *j = nullptr;
 };
 // y -= (*a_dev) x, with |y|^2 block partials in r.partials; returns the grid size.
-int launch_axpy_dev(size_t D, double *y, const double *x, const double *a_dev, Reducer &r, cudaStream_t s);
+int launch_axpy_dev(size_t D, double *y, const double *x, const double *a_dev, Reducer &r, cudaStream_t s,
+                    const int *skip = nullptr);
 // y *= 1 / sqrt(*b2_cur) (0 if that is 0); records alpha_j, beta_j and advances *j.
 void launch_lanczos_advance(size_t D, double *y, const LanczosScalars &ls, cudaStream_t s);
 // nsteps whole Lanczos steps of a sector of at most kLanczosCtaMaxDim states in
@@ -122,6 +124,9 @@ struct VecList {
   int n = 0;
   double *v[kMaxVec];
   double c[kMaxVec];
+  const double *cdev = nullptr;   // multi_axpy: coefficients from device memory
+  const double *xsdev = nullptr;  // dots: scale of x from device memory
+  const int *skip = nullptr;      // if set and *skip != 0 (device), the kernel does nothing
 };
 // out[i] = sum (xs*x) . y_i  (y_i = list.v[i]); if write_x, x *= xs in place.
 int launch_dots(size_t D, double *x, double xs, int write_x, const VecList &ys, Reducer &r,
@@ -137,6 +142,11 @@ void launch_swap_scale(size_t D, double *q, double *p, double beta, cudaStream_t
 // y = seeded normal random entries (counter-based), out[0] = |y|^2
 int launch_random(size_t D, uint64_t seed, double *y, Reducer &r, cudaStream_t s);
 void launch_scale(size_t D, double *y, double a, cudaStream_t s);
+// y *= *a_dev unless *skip
+void launch_scale_dev(size_t D, double *y, const double *a_dev, const int *skip, cudaStream_t s);
+// Norm step of a device-resident band-Lanczos step (see k_finalize_norm).
+void launch_finalize_norm(const double *partials, int nblocks, double dtol, double *z_out, double *inv_out,
+                          int *flag, int step, cudaStream_t s);
 // Reduction kernels return their block count; finalize_sums adds the per-block
 // partials of `nred` slots in a fixed order into r.out and copies them to
 // r.host (the caller synchronises the stream before reading r.host).

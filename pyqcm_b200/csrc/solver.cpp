@@ -478,10 +478,116 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
   int nd = 0;
   VecList ys;
   PhaseScope ps_loop(kPhBandLoop);
+  // step (12): convergence test on the lowest eigenvalue of the projected matrix
+  auto converged_at = [&](int jc) {
+    PhaseScope ps_check(kPhBandCheck);
+    std::vector<double> Hpr((size_t)jc * jc), ev;
+    for (int c = 0; c < jc; ++c)
+      for (int r = 0; r < jc; ++r) Hpr[(size_t)r + (size_t)jc * c] = T(r, c);
+    // without deflation t is banded (half-bandwidth p): O(j^2 p) instead of O(j^3)
+    const bool ok = (nd == 0) ? band_eigenvalues(jc, p, Hpr, ev) : sym_eig(jc, Hpr, ev, nullptr);
+    if (!ok) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
+    double test = std::fabs(ev[0] - ev_old);
+    ev_old = ev[0];
+    if (jc > 1 && ev[1] - ev[0] < min_gap && no_degenerate)
+      fail(QED_ERR_LANCZOS, "band Lanczos: the gap between the first two eigenvalues is smaller than " +
+                                std::to_string(min_gap));
+    return test < accur_bl;
+  };
+  // Device-resident steps: while nothing has been deflated (nd == 0) and the
+  // window is in steady state (j > pc: every step releases v_{j-pc-1} and
+  // takes its slot for v_{j+pc}), a chunk of steps runs with all scalars in
+  // device memory and no host round trip: z and 1/z (with the deflation test),
+  // the window dots, T(j, j) and the subtraction coefficients of the row pass.
+  // A step whose z falls below accur_deflation raises a device flag; it and
+  // every later step of the chunk then do nothing, and the host redoes that
+  // step on the host path (which deflates). The host reads the chunk's
+  // T entries once and fills T exactly as the step-by-step path does.
+  constexpr int kRec = 34;          // z, window dots (<= 31), T(j, j)
+  constexpr int kBandChunk = 32;
+  DevBuf<double> drec((size_t)kRec * (M0p + 1)), dinv(1);
+  DevBuf<int> dflag(1);
+  std::vector<double> hrec;
+  int host_step = -1;
   for (j = 0; j < M0; ++j) {
     if (phi_alive && j >= p) {  // P(k, j) is only used for j < p (Q = P U over k < p)
       for (auto &f : phi) f.release();
       phi_alive = false;
+    }
+    if (nd == 0 && j >= p && j > pc && j != host_step) {
+      int je = std::min(M0 - 1, j + kBandChunk - 1);
+      int chk = std::max(j, 4 * p);
+      chk = ((chk + p - 1) / p) * p;  // first convergence test at or after j
+      if (chk <= je) je = chk;
+      const std::vector<int> free0 = pool.free_list, v0 = v;
+      QED_CUDA(cudaMemsetAsync(dflag.p, 0, sizeof(int), s));
+      HvOperator op = H.op;
+      op.skip = dflag.p;
+      auto slots = [&](int jj) {  // steady-state window move of step jj
+        pool.put(v[jj - pc - 1]);
+        v[jj - pc - 1] = -1;
+        v[jj + pc] = pool.get();
+      };
+      for (int jj = j; jj <= je; ++jj) {
+        double *rec = drec.p + (size_t)kRec * jj;
+        double *vj = pool.p(v[jj]);
+        VecList one;  // (3)-(4): z = |v_j| and the deflation test
+        one.n = 1;
+        one.v[0] = vj;
+        one.skip = dflag.p;
+        int nb = launch_dots(D, vj, 1.0, 0, one, ws.red, s);
+        launch_finalize_norm(ws.red.partials, nb, accur_deflation, rec, dinv.p, dflag.p, jj, s);
+        VecList win;  // (5)-(6): v_j /= z; t_k = <v_j, v_k>; v_k -= t_k v_j
+        win.skip = dflag.p;
+        win.xsdev = dinv.p;
+        for (int k = jj + 1; k < jj + pc; ++k) win.v[win.n++] = pool.p(v[k]);
+        if (win.n) {
+          nb = launch_dots(D, vj, 1.0, 1, win, ws.red, s);
+          launch_finalize(ws.red.partials, nb, win.n, rec + 1, s);
+          win.cdev = rec + 1;
+          launch_multi_axpy(D, vj, 1.0, win, 0, ws.red, s);
+        } else {
+          launch_scale_dev(D, vj, dinv.p, dflag.p, s);
+        }
+        // (7)-(8): w = H v_j - sum_{k=j-pc}^{j-1} T(j, k) v_k, T(j, k) = rec[k - j + pc]
+        slots(jj);
+        double *w = pool.p(v[jj + pc]);
+        SubList sub;
+        sub.cdev = rec;
+        for (int k = jj - pc; k < jj; ++k) sub.z[sub.n++] = pool.p(v[k]);
+        launch_hv_rows(op, vj, 1.0, w, sub, s);
+        nb = launch_hv_cols(op, vj, 1.0, w, 1, ws.red, s);
+        launch_finalize(ws.red.partials, nb, 1, rec + pc, s);  // (10): T(j, j) = <v_j, w>
+        launch_axpy_dev(D, w, vj, rec + pc, ws.red, s, dflag.p);
+      }
+      const int n = je - j + 1;
+      hrec.resize((size_t)kRec * n);
+      QED_CUDA(cudaMemcpyAsync(hrec.data(), drec.p + (size_t)kRec * j, hrec.size() * sizeof(double),
+                               cudaMemcpyDeviceToHost, s));
+      int flag = 0;
+      QED_CUDA(cudaMemcpyAsync(&flag, dflag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      ws.sync();
+      const int jd = flag ? flag - 1 : je + 1;  // first step not done on the device
+      if (jd <= je) {  // the window moves of the skipped steps are undone
+        pool.free_list = free0;
+        v = v0;
+        for (int jj = j; jj < jd; ++jj) slots(jj);
+      }
+      for (int jj = j; jj < jd; ++jj) {
+        const double *r = hrec.data() + (size_t)kRec * (jj - j);
+        T(jj, jj - pc) = r[0];
+        for (int k = jj + 1; k < jj + pc; ++k) T(jj, k - pc) = r[k - jj];
+        for (int k = jj - pc; k < jj; ++k) T(k, jj) = T(jj, k);
+        T(jj, jj) = r[pc];
+      }
+      if (jd <= je) {
+        host_step = jd;
+        j = jd - 1;
+        continue;
+      }
+      j = je;
+      if (j >= 4 * p && j % p == 0 && converged_at(j)) break;
+      continue;
     }
     // step (3): z = |v_j|
     ys.n = 1;
@@ -569,23 +675,7 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
     launch_axpby(D, 1.0, w, -wjj, pool.p(v[j]), 0, ws.red, s);
     T(j, j) = wjj;
     for (int k = 0; k < nd; ++k) T(j, I[k]) = T(I[k], j);
-    // step (12): convergence test on the lowest eigenvalue of the projected matrix
-    if (j >= 4 * p && j % p == 0) {
-      PhaseScope ps_check(kPhBandCheck);
-      std::vector<double> Hpr((size_t)j * j), ev;
-      for (int c = 0; c < j; ++c)
-        for (int r = 0; r < j; ++r) Hpr[(size_t)r + (size_t)j * c] = T(r, c);
-      // without deflation t is banded (half-bandwidth p): O(j^2 p) instead of O(j^3)
-      const bool ok = (nd == 0) ? band_eigenvalues(j, p, Hpr, ev) : sym_eig(j, Hpr, ev, nullptr);
-      if (!ok) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
-      double test = std::fabs(ev[0] - ev_old);
-      ev_old = ev[0];
-      bool converged = test < accur_bl;
-      if (j > 1 && ev[1] - ev[0] < min_gap && no_degenerate)
-        fail(QED_ERR_LANCZOS, "band Lanczos: the gap between the first two eigenvalues is smaller than " +
-                                  std::to_string(min_gap));
-      if (converged) break;
-    }
+    if (j >= 4 * p && j % p == 0 && converged_at(j)) break;
   }
   ws.sync();
   Mout = j;

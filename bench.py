@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--solve", action="store_true", help="also time a full ground state of the 4x4 cluster")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the batched-solve metrics reported beside the H.v line")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: warm-up and timed H.v only (no e2e, clocks or CPU baseline)")
     ap.add_argument("--sector", default=None, help="sector of the 4x4 cluster to use (default R0:N16:S0)")
@@ -186,6 +188,8 @@ def run_reference(args, world, rank):
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
                              "sample": f"{steps} full H.v application(s) of the 4x4 sector; the reference's H.v has no threading"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if world == 1 and not args.no_secondary:
+        line["secondary"] = secondary_lines("reference")
     print(json.dumps(line), flush=True)
 
 
@@ -292,6 +296,8 @@ def run_ours(args, world, rank, local):
     }
     if solve:
         line["solve"] = solve
+    if world == 1 and not args.no_secondary:
+        line["secondary"] = secondary_lines("ours")
     print(json.dumps(line), flush=True)
 
 
@@ -316,21 +322,26 @@ def _ref_solve_one(payload):
     return e
 
 
-def run_batch_workload(args, world, rank, local):
-    """ED solves/s: each instance = ground state over its listed sectors + Green function."""
+BATCH_WORKLOADS = {
+    "batch": "independent Hubbard clusters (2x2, 2x3, 2x4, chain 8, chain 10; U~U[0,12], mu~U[0,U], "
+             "Neel field M~U[0,0.3]; every (N_up,N_dn) sector), ground state + band-Lanczos Green function",
+    "baths": "2x2 plaquette + 8 bath orbitals, U=8, R0:N12:S0 (dim 853776), random baths; ground state + "
+             "4x4 band-Lanczos Green function",
+}
+
+
+def batch_line(workload, batch, threads, steps, warmup, impl, world=1, rank=0, local=0, gpus=1):
+    """ED solves/s on one of the batched workloads; returns the JSON dict (None on ranks > 0)."""
     metric = "ED solves/s"
-    wl = ("independent Hubbard clusters (2x2, 2x3, 2x4, chain 8, chain 10; U~U[0,12], mu~U[0,U], "
-          "Neel field M~U[0,0.3]; every (N_up,N_dn) sector), ground state + band-Lanczos Green function"
-          if args.workload == "batch" else
-          "2x2 plaquette + 8 bath orbitals, U=8, R0:N12:S0 (dim 853776), random baths; ground state + "
-          "4x4 band-Lanczos Green function")
-    probs = batch_problems(args, rank, world)
-    if args.impl == "reference":
+    wl = BATCH_WORKLOADS[workload]
+    ns = argparse.Namespace(workload=workload, batch=batch)
+    probs = batch_problems(ns, rank, world)
+    if impl == "reference":
         if rank != 0:
-            return
+            return None
         import multiprocessing as mp
         cores = os.cpu_count() or 8
-        n = min(len(probs), max(cores, 8 if args.workload == "batch" else 2))
+        n = min(len(probs), cores)
         sample = probs[:n]
         ctx = mp.get_context("spawn")
         t0 = time.perf_counter()
@@ -338,15 +349,14 @@ def run_batch_workload(args, world, rank, local):
             pool.map(_ref_solve_one, [(p, 9100 + i, "L") for i, p in enumerate(sample)], chunksize=1)
         dt = time.perf_counter() - t0
         v = n / dt
-        line = {"metric": metric, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+        return {"metric": metric, "value": v, "unit": "solves/s", "n_gpus": gpus, "steps": 1, "warmup": 0,
                 "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic", "impl": "reference",
                 "config": {"workload": wl, "instances_per_step": n},
                 "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "reference",
-                                 "sample": f"{n} instances, one process per core (the reference's ED is single-threaded per instance)"},
+                                 "sample": f"the first {n} instances, one process per core (the reference's ED "
+                                           "is single-threaded per instance)"},
                 "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return
     import torch
     import pyqcm_b200 as qed
     torch.cuda.set_device(local)
@@ -359,30 +369,49 @@ def run_batch_workload(args, world, rank, local):
             qed.load_problem(p, base + i, model_name=f"bw_{p.name}_{base + i}", fmt="F")
             labels.append(base + i)
         t0 = time.perf_counter()
-        qed.ground_state_solve_batch(labels, threads=args.threads)
-        qed.Green_function_solve_batch(labels, threads=args.threads)
+        qed.ground_state_solve_batch(labels, threads=threads)
+        qed.Green_function_solve_batch(labels, threads=threads)
         G = [qed.Green_function(1j * np.pi / 50, label=l) for l in labels]  # results back on the host
         dt = time.perf_counter() - t0
         for l in labels:
             qed.erase_model_instance(l)
         return dt, G
 
-    for w in range(max(0, min(args.warmup, 1))):
+    for w in range(max(0, min(warmup, 1))):
         one_step(200000 + 10000 * w)
-    steps = max(1, min(args.steps, 3))
+    steps = max(1, min(steps, 3))
     times = [one_step(300000 + 10000 * k)[0] for k in range(steps)]
     dt = sum(times) / steps
     dt = max_over_ranks([dt], world, device=f"cuda:{local}")[0]
-    if rank == 0:
-        total = args.batch
-        line = {"metric": metric, "value": total / dt, "unit": "solves/s", "n_gpus": world, "steps": steps,
-                "warmup": min(args.warmup, 1), "ms_per_step": dt * 1e3, "higher_is_better": True,
-                "scaling": "weak" if world > 1 else "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": {"workload": wl, "instances_per_step": total,
-                                                "host_threads": args.threads or os.cpu_count()},
-                "e2e": {"value": total / dt, "unit": "solves/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 16 * args.batch,
-                        "path": "qed_ground_state_solve_batch + qed_Green_function_solve_batch + G(z) read back"}}
+    if rank != 0:
+        return None
+    return {"metric": metric, "value": batch / dt, "unit": "solves/s", "n_gpus": world, "steps": steps,
+            "warmup": min(warmup, 1), "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": wl, "instances_per_step": batch,
+                                            "host_threads": threads or os.cpu_count()},
+            "e2e": {"value": batch / dt, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 16 * batch,
+                    "path": "qed_ground_state_solve_batch + qed_Green_function_solve_batch + G(z) read back"}}
+
+
+SECONDARY = (("batch", 64), ("baths", 16))
+
+
+def secondary_lines(impl):
+    """The batched-solve metrics reported beside the H.v line of the default run."""
+    out = []
+    for wl, n in SECONDARY:
+        line = batch_line(wl, n, 0, 2, 1, impl)
+        if line:
+            out.append(line)
+    return out
+
+
+def run_batch_workload(args, world, rank, local):
+    line = batch_line(args.workload, args.batch, args.threads, args.steps, args.warmup, args.impl,
+                      world, rank, local, args.gpus)
+    if line:
         print(json.dumps(line), flush=True)
 
 

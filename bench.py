@@ -261,7 +261,14 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e, sec = qed.ground_state_solve(label + 100)
-        solve = {"ground_state_seconds": time.perf_counter() - t0, "E0": e, "sector": sec}
+        t1 = time.perf_counter()
+        qed.Green_function_solve(label + 100)
+        G = qed.Green_function(W.matsubara(256), label=label + 100)
+        t2 = time.perf_counter()
+        solve = {"ground_state_seconds": t1 - t0, "E0": e, "sector": sec,
+                 "green_function_seconds": t2 - t1, "G_iw0_00": [G[0, 0, 0].real, G[0, 0, 0].imag],
+                 "what": "4x4 ground state (Lanczos) + band-Lanczos (p=16) Green function on 256 Matsubara "
+                         "frequencies, beta=50"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import ref

@@ -739,6 +739,172 @@ __global__ void k_scale(size_t D, double *y, double a) {
     y[I] *= a;
 }
 
+// ------------------------------------------------ block (p-vector) kernels ----
+// A block holds p vectors interleaved: element (I, c) at I * p + c. P (a power
+// of two, p <= P <= 16) threads serve one basis state, thread c its column c,
+// so every gather of the block H.v reads the p values of one state at once.
+
+__global__ void k_interleave(size_t D, int p, BlockSrc src, double *x) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < D * p; t += (size_t)gridDim.x * blockDim.x)
+    x[t] = src.v[t % p][t / p];
+}
+
+// Up-spin hops, diagonal and the X2 M2 term of a block H.v, rows pass: kRowParts
+// CTAs share one dn-row (each a quarter of its up strings), so the rows in
+// flight (grid / kRowParts, about 37 on a B200) keep their gather targets
+// (du * p * 8 bytes each) resident in L2; each hop gathers the p values of one
+// state (one 128-byte line for p = 16); one hop-table read serves p vectors.
+constexpr int kRowParts = 4;
+template <int P>
+__global__ void __launch_bounds__(1024) k_block_up(HvOperator op, int p, const double *__restrict__ X,
+                                                    double *__restrict__ Y, const double *__restrict__ X2,
+                                                    const double *__restrict__ M2, double s2) {
+  __shared__ double uvals[256], m2[P * P];
+  for (int i = threadIdx.x; i < op.up.nvals; i += blockDim.x) uvals[i] = op.up.vals[i];
+  if (X2)
+    for (int i = threadIdx.x; i < p * p; i += blockDim.x) m2[i] = M2[i];
+  __syncthreads();
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const int c = threadIdx.x % P, g = threadIdx.x / P, G = blockDim.x / P;
+  if (c >= p) return;  // no barrier below
+  const int part = blockIdx.x % kRowParts;
+  const uint32_t uchunk = (du + kRowParts - 1) / kRowParts;
+  const uint32_t ub = part * uchunk, ue = min(du, ub + uchunk);
+  for (uint32_t d = blockIdx.x / kRowParts; d < dd; d += gridDim.x / kRowParts) {
+    const size_t rowb = (size_t)d * du;
+    const double ddg = op.dn.diag[d];
+    const uint32_t dnb = op.dn.bits[d];
+    for (uint32_t u = ub + g; u < ue; u += G) {
+      const size_t I = rowb + u;
+      double acc = (op.up.diag[u] + ddg + inter_term(op.inter, op.up.bits[u], dnb)) * X[I * p + c];
+      const int cu = op.up.cnt[u];
+      for (int k = 0; k < cu; ++k) {
+        const uint32_t e = __ldg(op.up.ell + (size_t)k * du + u);
+        acc += uvals[e & 255u] * X[(rowb + (e >> 8)) * p + c];
+      }
+      if (X2) {
+        double t = 0.0;
+        for (int i = 0; i < p; ++i) t += X2[I * p + i] * m2[i * p + c];
+        acc += s2 * t;
+      }
+      Y[I * p + c] = acc;
+    }
+  }
+}
+
+// Down-spin hops of a block H.v, Y += (dn hops) X: work items (chunk of
+// kThreads / P up strings, dn-row d) in chunk-major order, so the chunk's
+// columns of X for all rows (dd * chunk * p * 8 bytes) stay in L2 while its
+// rows are processed; every hop reads one contiguous segment.
+template <int P>
+__global__ void __launch_bounds__(kThreads) k_block_dn(HvOperator op, int p, const double *__restrict__ X,
+                                                        double *__restrict__ Y) {
+  __shared__ double dvals[256];
+  for (int i = threadIdx.x; i < op.dn.nvals; i += blockDim.x) dvals[i] = op.dn.vals[i];
+  __syncthreads();
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  constexpr int C = kThreads / P;
+  const int c = threadIdx.x % P, g = threadIdx.x / P;
+  const uint32_t nch = (du + C - 1) / C;
+  const size_t items = (size_t)nch * dd;
+  for (size_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const uint32_t ch = (uint32_t)(it / dd), d = (uint32_t)(it % dd);
+    const uint32_t u = ch * C + g;
+    if (u >= du || c >= p) continue;
+    double acc = 0.0;
+    const int cd = op.dn.cnt[d];
+    for (int k = 0; k < cd; ++k) {
+      const uint32_t e = __ldg(op.dn.ell + (size_t)k * dd + d);
+      acc += dvals[e & 255u] * X[((size_t)(e >> 8) * du + u) * p + c];
+    }
+    Y[((size_t)d * du + u) * p + c] += acc;
+  }
+}
+
+// Block partial sums of X^T Y: partials[b * ld + i * p + c] = sum over this
+// block's states of X[I][i] Y[I][c] (fixed order).
+template <int P>
+__device__ __forceinline__ void block_gram_store(const double (&acc)[P], int p, double *partials, int ld) {
+  __shared__ double sm[kThreads * (P + 1)];
+  constexpr int G = kThreads / P;
+  const int c = threadIdx.x % P, g = threadIdx.x / P;
+#pragma unroll
+  for (int i = 0; i < P; ++i) sm[(g * P + c) * (P + 1) + i] = acc[i];
+  __syncthreads();
+  for (int t = threadIdx.x; t < p * p; t += blockDim.x) {
+    const int i = t / p, cc = t % p;
+    double s = 0.0;
+    for (int gg = 0; gg < G; ++gg) s += sm[(gg * P + cc) * (P + 1) + i];
+    partials[(size_t)blockIdx.x * ld + t] = s;
+  }
+}
+
+template <int P>
+__global__ void __launch_bounds__(kThreads) k_block_gram(size_t D, int p, const double *__restrict__ X,
+                                                          const double *__restrict__ Y, double *partials, int ld) {
+  constexpr int G = kThreads / P;
+  const int c = threadIdx.x % P, g = threadIdx.x / P;
+  double acc[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) acc[i] = 0.0;
+  if (c < p)
+    for (size_t I = (size_t)blockIdx.x * G + g; I < D; I += (size_t)gridDim.x * G) {
+      const double y = Y[I * p + c];
+#pragma unroll
+      for (int i = 0; i < P; ++i)
+        if (i < p) acc[i] += X[I * p + i] * y;
+    }
+  block_gram_store<P>(acc, p, partials, ld);
+}
+
+// Y = a Y + s1 X1 M1 (M1 p x p row-major, device; Y != X1); optionally the
+// block partials of Y^T Y of the result (gram != 0).
+template <int P>
+__global__ void __launch_bounds__(kThreads) k_block_muladd(size_t D, int p, double a, double *Y, double s1,
+                                                            const double *__restrict__ X1,
+                                                            const double *__restrict__ M1, int gram,
+                                                            double *partials, int ld) {
+  __shared__ double m1[P * P];
+  for (int i = threadIdx.x; i < p * p; i += blockDim.x) m1[i] = M1[i];
+  __syncthreads();
+  constexpr int G = kThreads / P;
+  const int c = threadIdx.x % P, g = threadIdx.x / P;
+  const unsigned gmask = (P == 32) ? 0xffffffffu : (((1u << P) - 1u) << ((threadIdx.x & 31) / P * P));
+  double acc[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) acc[i] = 0.0;
+  for (size_t I0 = (size_t)blockIdx.x * G; I0 < D; I0 += (size_t)gridDim.x * G) {
+    const size_t I = I0 + g;
+    double v = 0.0;
+    if (I < D && c < p) {
+      double t = 0.0;
+      for (int i = 0; i < p; ++i) t += X1[I * p + i] * m1[i * p + c];
+      v = (a != 0.0 ? a * Y[I * p + c] : 0.0) + s1 * t;
+      Y[I * p + c] = v;
+    }
+    if (gram) {  // the group's p results are in its lanes: acc[i] += v_i * v_c
+#pragma unroll
+      for (int i = 0; i < P; ++i) acc[i] += __shfl_sync(gmask, v, i, P) * v;
+    }
+  }
+  if (gram) block_gram_store<P>(acc, p, partials, ld);
+}
+
+// out[slot] = sum over blocks of partials[b * ld + slot], slot < n, fixed order.
+__global__ void k_finalize_ld(const double *partials, int nblocks, int ld, double *out) {
+  __shared__ double sm[kThreads];
+  const int slot = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[(size_t)b * ld + slot];
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[slot] = sm[0];
+}
+
 // -------------------------------------------------------- Green functions ----
 
 // G(z) of a Lehmann representation for a batch of frequencies: one CTA per
@@ -984,6 +1150,71 @@ void launch_lanczos_advance(size_t D, double *y, const LanczosScalars &ls, cudaS
 void launch_lanczos_cta(const HvOperator &op, double *vprev, double *vcur, double *w, const LanczosScalars &ls,
                         int nsteps, cudaStream_t s) {
   k_lanczos_cta<<<1, 1024, 0, s>>>(op, vprev, vcur, w, ls, nsteps);
+  QED_LAUNCH();
+}
+
+namespace {
+int block_pow2(int p) {
+  int P = 1;
+  while (P < p) P <<= 1;
+  return P;
+}
+int block_grid(size_t D, int P, int max_blocks) {
+  const size_t G = kThreads / P;
+  size_t g = (D + G - 1) / G;
+  const size_t cap = (size_t)device_sms() * 8;
+  if (g > cap) g = cap;
+  if (g > (size_t)max_blocks) g = (size_t)max_blocks;
+  return (int)std::max<size_t>(g, 1);
+}
+}  // namespace
+
+void launch_interleave(size_t D, int p, const BlockSrc &src, double *x, cudaStream_t s) {
+  k_interleave<<<grid_for(D * p, device_sms(), 8), kThreads, 0, s>>>(D, p, src, x);
+  QED_LAUNCH();
+}
+
+#define QED_BLOCK_DISPATCH(P, CALL)                                       \
+  switch (P) {                                                            \
+    case 1: { constexpr int PP = 1; CALL; } break;                        \
+    case 2: { constexpr int PP = 2; CALL; } break;                        \
+    case 4: { constexpr int PP = 4; CALL; } break;                        \
+    case 8: { constexpr int PP = 8; CALL; } break;                        \
+    case 16: { constexpr int PP = 16; CALL; } break;                      \
+    default: fail(QED_ERR_UNSUPPORTED, "block of more than 16 vectors");  \
+  }
+
+void launch_block_hv(const HvOperator &op, int p, const double *X, double *Y, const double *X2, const double *M2,
+                     double s2, cudaStream_t s) {
+  const int P = block_pow2(p);
+  const int sms = device_sms();
+  const int up_grid = std::max(kRowParts, (sms / kRowParts) * kRowParts);
+  QED_BLOCK_DISPATCH(P, (k_block_up<PP><<<up_grid, 1024, 0, s>>>(op, p, X, Y, X2, M2, s2)));
+  QED_LAUNCH();
+  QED_BLOCK_DISPATCH(P, (k_block_dn<PP><<<sms * 8, kThreads, 0, s>>>(op, p, X, Y)));
+  QED_LAUNCH();
+}
+
+int launch_block_gram(size_t D, int p, const double *X, const double *Y, double *partials, int ld, int max_blocks,
+                      cudaStream_t s) {
+  const int P = block_pow2(p);
+  const int grid = block_grid(D, P, max_blocks);
+  QED_BLOCK_DISPATCH(P, (k_block_gram<PP><<<grid, kThreads, 0, s>>>(D, p, X, Y, partials, ld)));
+  QED_LAUNCH();
+  return grid;
+}
+
+int launch_block_muladd(size_t D, int p, double a, double *Y, double s1, const double *X1, const double *M1,
+                        int gram, double *partials, int ld, int max_blocks, cudaStream_t s) {
+  const int P = block_pow2(p);
+  const int grid = block_grid(D, P, max_blocks);
+  QED_BLOCK_DISPATCH(P, (k_block_muladd<PP><<<grid, kThreads, 0, s>>>(D, p, a, Y, s1, X1, M1, gram, partials, ld)));
+  QED_LAUNCH();
+  return grid;
+}
+
+void launch_finalize_ld(const double *partials, int nblocks, int ld, int n, double *out, cudaStream_t s) {
+  k_finalize_ld<<<n, kThreads, 0, s>>>(partials, nblocks, ld, out);
   QED_LAUNCH();
 }
 

@@ -110,6 +110,27 @@ constexpr size_t kLanczosCtaMaxDim = 8192;
 void launch_lanczos_cta(const HvOperator &op, double *vprev, double *vcur, double *w, const LanczosScalars &ls,
                         int nsteps, cudaStream_t s);
 
+// ---- blocks of p vectors (interleaved: element (I, c) at I * p + c) --------
+// These serve the block form of the band-Lanczos recurrence, where one table
+// read of the H.v serves p right-hand sides.
+struct BlockSrc {
+  const double *v[32];
+};
+// x = the p vectors src.v[0..p) interleaved
+void launch_interleave(size_t D, int p, const BlockSrc &src, double *x, cudaStream_t s);
+// Y = H X + s2 X2 M2 (X2, M2 optional; M2 p x p row-major in device memory):
+// a row pass (diagonal, up hops, X2 term) and a chunk-major down-hop pass
+void launch_block_hv(const HvOperator &op, int p, const double *X, double *Y, const double *X2, const double *M2,
+                     double s2, cudaStream_t s);
+// per-block partials of X^T Y (p x p row-major) at partials[b * ld]; returns the block count
+int launch_block_gram(size_t D, int p, const double *X, const double *Y, double *partials, int ld, int max_blocks,
+                      cudaStream_t s);
+// Y = a Y + s1 X1 M1 (Y and X1 distinct); if gram, also the partials of Y^T Y
+int launch_block_muladd(size_t D, int p, double a, double *Y, double s1, const double *X1, const double *M1,
+                        int gram, double *partials, int ld, int max_blocks, cudaStream_t s);
+// out[0..n) = fixed-order sums of partials with row stride ld
+void launch_finalize_ld(const double *partials, int nblocks, int ld, int n, double *out, cudaStream_t s);
+
 // ---- H.v ------------------------------------------------------------------
 // Row pass: y = (diag + up hops) x - sum_k sub.c[k] sub.z[k]   (x scaled by xs)
 void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,

@@ -49,6 +49,9 @@ struct Table {
     i["max_iter_BL"] = 600;
     i["max_iter_CF"] = 400;
     i["max_iter_lanczos"] = 1000;
+    // solver option (not in the reference): band-Lanczos sectors with at least
+    // this many states run the block form of the recurrence (p vectors per H.v)
+    i["block_lanczos_min_dim"] = 100000;
     i["seed"] = 0;
     i["GF_lookup_depth"] = 64;
     c["Hamiltonian_format"] = 'E';

@@ -11,7 +11,8 @@ namespace {
 const char *kNames[kPhCount] = {"sector setup",       "GS Lanczos (eigenvalue)", "GS Lanczos (eigenvector)",
                                 "dense sectors",      "c/c+ start vectors",      "band Lanczos recurrence",
                                 "band Lanczos checks", "band projected eigensystem", "continued fractions",
-                                "GS Ritz tests (in GS eigenvalue)"};
+                                "GS Ritz tests (in GS eigenvalue)", "block Lanczos recurrence",
+                                "block Lanczos fallbacks"};
 
 struct Totals {
   std::atomic<long long> ns[kPhCount];

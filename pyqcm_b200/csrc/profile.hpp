@@ -17,6 +17,8 @@ enum Phase {
   kPhBandEig,       // projected eigensystem and Q = P U
   kPhCf,            // continued-fraction Lanczos
   kPhRitz,          // ground-state Lanczos: host Ritz tests (inside kPhGsLanczos)
+  kPhBlockLoop,     // block form of the band-Lanczos recurrence
+  kPhBlockFallback, // block recurrence abandoned for the band one (count)
   kPhCount
 };
 

@@ -439,6 +439,190 @@ struct VecPool {
 
 }  // namespace
 
+namespace {
+
+// Upper-triangular R with G = R^T R (G p x p row-major symmetric); false if a
+// pivot is not positive. Rinv receives R^{-1} (upper triangular, row-major).
+bool cholesky_upper(int p, const double *G, std::vector<double> &R, std::vector<double> &Rinv) {
+  R.assign((size_t)p * p, 0.0);
+  for (int i = 0; i < p; ++i) {
+    double d = G[i * p + i];
+    for (int k = 0; k < i; ++k) d -= R[k * p + i] * R[k * p + i];
+    if (!(d > 0.0)) return false;
+    const double rii = std::sqrt(d);
+    R[i * p + i] = rii;
+    for (int j = i + 1; j < p; ++j) {
+      double t = G[i * p + j];
+      for (int k = 0; k < i; ++k) t -= R[k * p + i] * R[k * p + j];
+      R[i * p + j] = t / rii;
+    }
+  }
+  Rinv.assign((size_t)p * p, 0.0);
+  for (int i = p - 1; i >= 0; --i) {  // back substitution, row by row from the bottom
+    Rinv[i * p + i] = 1.0 / R[i * p + i];
+    for (int j = i + 1; j < p; ++j) {
+      double t = 0.0;
+      for (int k = i + 1; k <= j; ++k) t += R[i * p + k] * Rinv[k * p + j];
+      Rinv[i * p + j] = -t / R[i * p + i];
+    }
+  }
+  return true;
+}
+
+// Block form of the band-Lanczos recurrence for large sectors: V_0 = QR(phi),
+// W = H V_k - V_{k-1} B_k^T, A_k = V_k^T W, W -= V_k A_k, W = V_{k+1} B_{k+1}
+// (Cholesky QR, twice). Without deflation band Lanczos builds, in exact
+// arithmetic, the same Krylov space one vector at a time (the candidates of its
+// window are H v orthogonalised against the band), and its projected matrix is
+// this block tridiagonal T with upper-triangular B blocks, i.e. banded with
+// half-bandwidth p. Its dimension only stops at multiples of p (the convergence
+// test runs at j % p == 0, and M0 is a multiple of p), so the stopping rule is
+// the same. Returns false, leaving phi intact, when a QR pivot falls below 1e-4
+// (a deflation the band algorithm must handle) or p > 16; the caller then runs
+// the band recurrence.
+bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
+                           std::vector<double> &evals, std::vector<double> &Q, int &Mout) {
+  const size_t D = H.D;
+  const int p = (int)phi.size();
+  if (p < 1 || p > 16) return false;
+  cudaStream_t s = ws.stream;
+  int M0 = (int)(14 * p * std::log(1.0 * D));
+  if (!(M0 > 1)) fail(QED_ERR_INTERNAL, "Assertion failed: M>1 in build_Q_matrix");
+  double accur_bl = opt_double("accur_band_lanczos");
+  if (accur_bl < 0.0) accur_bl = 0.0;
+  const long max_iter_BL = opt_int("max_iter_BL");
+  const double min_gap = opt_double("band_lanczos_minimum_gap");
+  const bool no_degenerate = opt_bool("no_degenerate_BL");
+  if (M0 > max_iter_BL) M0 = (int)max_iter_BL;
+  M0 = (M0 / p + 1) * p - p;  // bandLanczos: M0p - pc with pc = p
+  if (M0 < p) return false;
+  constexpr double kPivotMin = 1e-4;
+  const int pp = p * p;
+  const int max_blocks = 4096;
+  DevBuf<double> part((size_t)max_blocks * pp), dsmall(4 * (size_t)pp);
+  double *dG = dsmall.p, *dM = dsmall.p + pp, *dB = dsmall.p + 2 * pp;
+  std::vector<double> hG(pp), R1, R1i, R2, R2i;
+  auto gram_to_host = [&](int nb) {
+    launch_finalize_ld(part.p, nb, pp, pp, dG, s);
+    QED_CUDA(cudaMemcpyAsync(hG.data(), dG, pp * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ws.sync();
+  };
+  auto upload = [&](double *dst, const std::vector<double> &h) {
+    QED_CUDA(cudaMemcpyAsync(dst, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  };
+  // Cholesky QR, twice: X (its gram already in hG) -> tmp -> out; B = R2 R1
+  auto cholqr2 = [&](const double *X, double *tmp, double *out, std::vector<double> &B) {
+    if (!cholesky_upper(p, hG.data(), R1, R1i)) return false;
+    for (int i = 0; i < p; ++i)
+      if (R1[i * p + i] < kPivotMin) return false;
+    upload(dM, R1i);
+    int nb = launch_block_muladd(D, p, 0.0, tmp, 1.0, X, dM, 1, part.p, pp, max_blocks, s);
+    gram_to_host(nb);
+    if (!cholesky_upper(p, hG.data(), R2, R2i)) return false;
+    upload(dM, R2i);
+    launch_block_muladd(D, p, 0.0, out, 1.0, tmp, dM, 0, part.p, pp, max_blocks, s);
+    B.assign(pp, 0.0);
+    for (int i = 0; i < p; ++i)
+      for (int j = i; j < p; ++j) {
+        double t = 0.0;
+        for (int k = i; k <= j; ++k) t += R2[i * p + k] * R1[k * p + j];
+        B[i * p + j] = t;
+      }
+    return true;
+  };
+  const size_t bl = D * (size_t)p;
+  DevBuf<double> b0(bl), b1(bl), b2(bl);
+  double *Vprev = b0.p, *Vk = b1.p, *W = b2.p;
+  // V_0 = QR(phi) and P = phi^T V_0
+  BlockSrc src;
+  for (int i = 0; i < p; ++i) src.v[i] = phi[i].p;
+  launch_interleave(D, p, src, W, s);  // W holds X0 = phi
+  std::vector<double> B;
+  int nb = launch_block_gram(D, p, W, W, part.p, pp, max_blocks, s);
+  gram_to_host(nb);
+  if (!cholqr2(W, Vprev, Vk, B)) return false;
+  nb = launch_block_gram(D, p, W, Vk, part.p, pp, max_blocks, s);  // P(k, i) = <phi_k, v_i>
+  gram_to_host(nb);
+  const std::vector<double> P(hG);  // row-major [k][i]
+  std::vector<double> t((size_t)M0 * M0, 0.0);
+  auto T = [&](int r, int c) -> double & { return t[(size_t)r + (size_t)M0 * c]; };
+  std::vector<double> Bk;  // B of the QR that produced V_k (none for k = 0)
+  double ev_old = 1e12;
+  int jdim = 0;
+  PhaseScope ps_loop(kPhBlockLoop);
+  for (int k = 0;; ++k) {
+    // W = H V_k - V_{k-1} B_k^T
+    if (k > 0) {
+      std::vector<double> Bt(pp);
+      for (int i = 0; i < p; ++i)
+        for (int c = 0; c < p; ++c) Bt[i * p + c] = Bk[c * p + i];
+      upload(dB, Bt);
+      launch_block_hv(H.op, p, Vk, W, Vprev, dB, -1.0, s);
+    } else {
+      launch_block_hv(H.op, p, Vk, W, nullptr, nullptr, 0.0, s);
+    }
+    // A_k = V_k^T W ; W -= V_k A_k (with the gram of the result for the QR)
+    nb = launch_block_gram(D, p, Vk, W, part.p, pp, max_blocks, s);
+    launch_finalize_ld(part.p, nb, pp, pp, dM, s);
+    QED_CUDA(cudaMemcpyAsync(hG.data(), dM, pp * sizeof(double), cudaMemcpyDeviceToHost, s));
+    nb = launch_block_muladd(D, p, 1.0, W, -1.0, Vk, dM, 1, part.p, pp, max_blocks, s);
+    ws.sync();
+    const std::vector<double> A(hG);
+    for (int i = 0; i < p; ++i)
+      for (int c = 0; c < p; ++c) T(k * p + i, k * p + c) = 0.5 * (A[i * p + c] + A[c * p + i]);
+    jdim = (k + 1) * p;
+    if (jdim >= M0) {
+      jdim = M0;
+      break;
+    }
+    if (jdim >= 4 * p) {  // bandLanczos step (12) at j = jdim, on the leading jdim x jdim block
+      PhaseScope ps_check(kPhBandCheck);
+      std::vector<double> Hpr((size_t)jdim * jdim), ev;
+      for (int c = 0; c < jdim; ++c)
+        for (int r = 0; r < jdim; ++r) Hpr[(size_t)r + (size_t)jdim * c] = T(r, c);
+      if (!band_eigenvalues(jdim, p, Hpr, ev)) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
+      const double test = std::fabs(ev[0] - ev_old);
+      ev_old = ev[0];
+      if (jdim > 1 && ev[1] - ev[0] < min_gap && no_degenerate)
+        fail(QED_ERR_LANCZOS, "band Lanczos: the gap between the first two eigenvalues is smaller than " +
+                                  std::to_string(min_gap));
+      if (test < accur_bl) break;
+    }
+    // W = V_{k+1} B_{k+1} (through V_{k-1}'s buffer, no longer needed)
+    gram_to_host(nb);
+    std::vector<double> Bn;
+    if (!cholqr2(W, Vprev, W, Bn)) return false;
+    for (int r = 0; r < p; ++r)
+      for (int c = r; c < p; ++c) {
+        T((k + 1) * p + r, k * p + c) = Bn[r * p + c];
+        T(k * p + c, (k + 1) * p + r) = Bn[r * p + c];
+      }
+    double *nv = W;  // V_{k+1}
+    W = Vprev;
+    Vprev = Vk;
+    Vk = nv;
+    Bk = Bn;
+  }
+  ws.sync();
+  for (auto &f : phi) f.release();
+  Mout = jdim;
+  PhaseScope ps_eig(kPhBandEig);
+  std::vector<double> Hpr((size_t)jdim * jdim), U;
+  for (int c = 0; c < jdim; ++c)
+    for (int r = 0; r < jdim; ++r) Hpr[(size_t)r + (size_t)jdim * c] = T(r, c);
+  if (!band_eig_rows(jdim, p, Hpr, p, evals, U)) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
+  Q.assign((size_t)p * jdim, 0.0);
+  for (int m = 0; m < jdim; ++m)
+    for (int i = 0; i < p; ++i) {
+      double acc = 0.0;
+      for (int kk = 0; kk < p; ++kk) acc += P[(size_t)i * p + kk] * U[(size_t)kk + (size_t)p * m];
+      Q[(size_t)i + (size_t)p * m] = acc;
+    }
+  return true;
+}
+
+}  // namespace
+
 bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
                           std::vector<double> &evals, std::vector<double> &Q, int &Mout) {
   const size_t D = H.D;
@@ -447,6 +631,10 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
   if (D == 0 || p == 0) {
     Mout = 0;
     return false;
+  }
+  if ((long)D >= opt_int("block_lanczos_min_dim")) {
+    if (block_lanczos_qmatrix(H, ws, phi, evals, Q, Mout)) return true;
+    if (profiling()) profile_add(kPhBlockFallback, 0.0);
   }
   // number of iterations (Hamiltonian::build_Q_matrix, Hamiltonian_base.hpp:236-239)
   int M0 = (int)(14 * p * std::log(1.0 * D));

@@ -247,3 +247,24 @@ def test_dense_path_keeps_degenerate_states(qed, oracle, fresh):
         if fmt == "S":
             assert np.max(np.abs(G[fmt] - oracle.green_function(label, z))) < GF_TOL
     assert np.max(np.abs(G["F"] - G["S"])) > 1e-6
+
+
+@pytest.mark.parametrize("case", [0, 2, 4])
+def test_block_lanczos_green_function(qed, oracle, fresh, case):
+    """The block form of the band-Lanczos recurrence (p vectors per H.v), forced
+    on sectors below its default threshold, against the reference's band Lanczos."""
+    name, mk = GS_CASES[case]
+    suffix, label = fresh()
+    set_both(qed, oracle, GF_method="L")
+    qed.set_global_parameter("block_lanczos_min_dim", 1000)
+    try:
+        load_both(qed, oracle, mk(), suffix, label, fmt="F")
+        z = W.matsubara(256)
+        G1 = qed.Green_function(z, label=label)
+        G1d = qed.Green_function(z, spin_down=True, label=label) if qed.mixing(label) & 4 else None
+    finally:
+        qed.set_global_parameter("block_lanczos_min_dim", 100000)
+    G2 = oracle.green_function(label, z)
+    assert np.max(np.abs(G1 - G2)) < GF_TOL, name
+    if G1d is not None:
+        assert np.max(np.abs(G1d - oracle.green_function(label, z, spin_down=True))) < GF_TOL, name

@@ -750,13 +750,15 @@ __global__ void k_interleave(size_t D, int p, BlockSrc src, double *x) {
 }
 
 // Up-spin hops, diagonal and the X2 M2 term of a block H.v, rows pass: kRowParts
-// CTAs share one dn-row (each a quarter of its up strings), so the rows in
-// flight (grid / kRowParts, about 37 on a B200) keep their gather targets
+// CTAs share one dn-row (each an eighth of its up strings), so the rows in
+// flight (grid / kRowParts, about 18 on a B200) keep their gather targets
 // (du * p * 8 bytes each) resident in L2; each hop gathers the p values of one
-// state (one 128-byte line for p = 16); one hop-table read serves p vectors.
-constexpr int kRowParts = 4;
+// state (one 128-byte line for p = 16); one hop-table read serves p vectors;
+// four hops are in flight per thread.
+constexpr int kRowParts = 8;
+constexpr int kUpThreads = 1024;
 template <int P>
-__global__ void __launch_bounds__(1024) k_block_up(HvOperator op, int p, const double *__restrict__ X,
+__global__ void __launch_bounds__(kUpThreads) k_block_up(HvOperator op, int p, const double *__restrict__ X,
                                                     double *__restrict__ Y, const double *__restrict__ X2,
                                                     const double *__restrict__ M2, double s2) {
   __shared__ double uvals[256], m2[P * P];
@@ -778,10 +780,26 @@ __global__ void __launch_bounds__(1024) k_block_up(HvOperator op, int p, const d
       const size_t I = rowb + u;
       double acc = (op.up.diag[u] + ddg + inter_term(op.inter, op.up.bits[u], dnb)) * X[I * p + c];
       const int cu = op.up.cnt[u];
-      for (int k = 0; k < cu; ++k) {
+      // four hops in flight: table entries first, then the four gathers
+      double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      int k = 0;
+      for (; k + 4 <= cu; k += 4) {
+        const uint32_t e0 = __ldg(op.up.ell + (size_t)k * du + u);
+        const uint32_t e1 = __ldg(op.up.ell + (size_t)(k + 1) * du + u);
+        const uint32_t e2 = __ldg(op.up.ell + (size_t)(k + 2) * du + u);
+        const uint32_t e3 = __ldg(op.up.ell + (size_t)(k + 3) * du + u);
+        const double x0 = X[(rowb + (e0 >> 8)) * p + c], x1 = X[(rowb + (e1 >> 8)) * p + c];
+        const double x2 = X[(rowb + (e2 >> 8)) * p + c], x3 = X[(rowb + (e3 >> 8)) * p + c];
+        acc += uvals[e0 & 255u] * x0;
+        a1 += uvals[e1 & 255u] * x1;
+        a2 += uvals[e2 & 255u] * x2;
+        a3 += uvals[e3 & 255u] * x3;
+      }
+      for (; k < cu; ++k) {
         const uint32_t e = __ldg(op.up.ell + (size_t)k * du + u);
         acc += uvals[e & 255u] * X[(rowb + (e >> 8)) * p + c];
       }
+      acc += (a1 + a2) + a3;
       if (X2) {
         double t = 0.0;
         for (int i = 0; i < p; ++i) t += X2[I * p + i] * m2[i * p + c];
@@ -800,8 +818,9 @@ template <int P>
 __global__ void __launch_bounds__(kThreads) k_block_dn(HvOperator op, int p, const double *__restrict__ X,
                                                         double *__restrict__ Y) {
   __shared__ double dvals[256];
+  __shared__ double hv[256];      // the row's hop values
+  __shared__ size_t hoff[256];    // and source-row offsets (e >> 8) * du
   for (int i = threadIdx.x; i < op.dn.nvals; i += blockDim.x) dvals[i] = op.dn.vals[i];
-  __syncthreads();
   const uint32_t du = op.up.dim, dd = op.dn.dim;
   constexpr int C = kThreads / P;
   const int c = threadIdx.x % P, g = threadIdx.x / P;
@@ -809,15 +828,29 @@ __global__ void __launch_bounds__(kThreads) k_block_dn(HvOperator op, int p, con
   const size_t items = (size_t)nch * dd;
   for (size_t it = blockIdx.x; it < items; it += gridDim.x) {
     const uint32_t ch = (uint32_t)(it / dd), d = (uint32_t)(it % dd);
-    const uint32_t u = ch * C + g;
-    if (u >= du || c >= p) continue;
-    double acc = 0.0;
     const int cd = op.dn.cnt[d];
-    for (int k = 0; k < cd; ++k) {
+    __syncthreads();  // dvals ready; previous item's hop list consumed
+    for (int k = threadIdx.x; k < cd; k += blockDim.x) {
       const uint32_t e = __ldg(op.dn.ell + (size_t)k * dd + d);
-      acc += dvals[e & 255u] * X[((size_t)(e >> 8) * du + u) * p + c];
+      hv[k] = dvals[e & 255u];
+      hoff[k] = (size_t)(e >> 8) * du;
     }
-    Y[((size_t)d * du + u) * p + c] += acc;
+    __syncthreads();
+    const uint32_t u = ch * C + g;
+    if (u < du && c < p) {
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      int k = 0;
+      for (; k + 4 <= cd; k += 4) {
+        const double x0 = X[(hoff[k] + u) * p + c], x1 = X[(hoff[k + 1] + u) * p + c];
+        const double x2 = X[(hoff[k + 2] + u) * p + c], x3 = X[(hoff[k + 3] + u) * p + c];
+        a0 += hv[k] * x0;
+        a1 += hv[k + 1] * x1;
+        a2 += hv[k + 2] * x2;
+        a3 += hv[k + 3] * x3;
+      }
+      for (; k < cd; ++k) a0 += hv[k] * X[(hoff[k] + u) * p + c];
+      Y[((size_t)d * du + u) * p + c] += (a0 + a1) + (a2 + a3);
+    }
   }
 }
 
@@ -850,9 +883,19 @@ __global__ void __launch_bounds__(kThreads) k_block_gram(size_t D, int p, const 
   if (c < p)
     for (size_t I = (size_t)blockIdx.x * G + g; I < D; I += (size_t)gridDim.x * G) {
       const double y = Y[I * p + c];
+      if (p == P && P >= 2) {  // the state's row of X as 16-byte loads
+        const double2 *x2 = reinterpret_cast<const double2 *>(X + I * p);
 #pragma unroll
-      for (int i = 0; i < P; ++i)
-        if (i < p) acc[i] += X[I * p + i] * y;
+        for (int i = 0; i < P / 2; ++i) {
+          const double2 v = x2[i];
+          acc[2 * i] += v.x * y;
+          acc[2 * i + 1] += v.y * y;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < P; ++i)
+          if (i < p) acc[i] += X[I * p + i] * y;
+      }
     }
   block_gram_store<P>(acc, p, partials, ld);
 }
@@ -878,7 +921,17 @@ __global__ void __launch_bounds__(kThreads) k_block_muladd(size_t D, int p, doub
     double v = 0.0;
     if (I < D && c < p) {
       double t = 0.0;
-      for (int i = 0; i < p; ++i) t += X1[I * p + i] * m1[i * p + c];
+      if (p == P && P >= 2) {  // the state's row of X1 as 16-byte loads
+        const double2 *x2 = reinterpret_cast<const double2 *>(X1 + I * p);
+#pragma unroll
+        for (int i = 0; i < P / 2; ++i) {
+          const double2 xv = x2[i];
+          t += xv.x * m1[2 * i * p + c];
+          t += xv.y * m1[(2 * i + 1) * p + c];
+        }
+      } else {
+        for (int i = 0; i < p; ++i) t += X1[I * p + i] * m1[i * p + c];
+      }
       v = (a != 0.0 ? a * Y[I * p + c] : 0.0) + s1 * t;
       Y[I * p + c] = v;
     }
@@ -1189,7 +1242,7 @@ void launch_block_hv(const HvOperator &op, int p, const double *X, double *Y, co
   const int P = block_pow2(p);
   const int sms = device_sms();
   const int up_grid = std::max(kRowParts, (sms / kRowParts) * kRowParts);
-  QED_BLOCK_DISPATCH(P, (k_block_up<PP><<<up_grid, 1024, 0, s>>>(op, p, X, Y, X2, M2, s2)));
+  QED_BLOCK_DISPATCH(P, (k_block_up<PP><<<up_grid, kUpThreads, 0, s>>>(op, p, X, Y, X2, M2, s2)));
   QED_LAUNCH();
   QED_BLOCK_DISPATCH(P, (k_block_dn<PP><<<sms * 8, kThreads, 0, s>>>(op, p, X, Y)));
   QED_LAUNCH();

@@ -121,6 +121,14 @@ int qed_hybridization_function(int label, int spin_down, int nz, const double *z
 /* ED::Green_function_average (src_ed/qcm_ED.hpp:146): <c^+_b c_a>, dim x dim complex. */
 int qed_Green_function_average(int label, int spin_down, double *M);
 
+/* ED::cluster_averages (src_ed/qcm_ED.hpp:113 -> src_ed/model_instance.hpp:149-173,
+ * 340-345): for each operator of the instance, in name order, its ground-state
+ * average and variance (divided by the number of sites for cluster operators).
+ * cap is the capacity of ave and var; *n receives the number of operators;
+ * names receives the operator names, each followed by '\n', in a buffer of
+ * names_size bytes. Solves the ground state first if needed. */
+int qed_cluster_averages(int label, int cap, int *n, double *ave, double *var, char *names, int names_size);
+
 /* ED::Potthoff_functional (src_ed/qcm_ED.hpp:222; SEF_bath + E0, src_ed/qcm_ED.cpp:330-334). */
 int qed_Potthoff_functional(int label, double *omega);
 

@@ -192,6 +192,18 @@ def green_function_average(label, spin_down=False):
     return out.T.copy()
 
 
+def cluster_averages(label):
+    """ED::cluster_averages: [(operator name, average, variance), ...]."""
+    cap = 256
+    n = C.c_int(0)
+    ave = np.zeros(cap)
+    var = np.zeros(cap)
+    buf = C.create_string_buffer(1 << 16)
+    _check(lib().ref_cluster_averages(label, cap, C.byref(n), _dp(ave), _dp(var), buf, len(buf)))
+    names = buf.value.decode().split("\n")[: n.value]
+    return [(names[i], float(ave[i]), float(var[i])) for i in range(n.value)]
+
+
 def potthoff(label):
     w = C.c_double()
     _check(lib().ref_potthoff(label, C.byref(w)))

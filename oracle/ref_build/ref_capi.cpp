@@ -178,6 +178,24 @@ int ref_green_function_average(int label, int spin_down, double *out) {
   });
 }
 
+// cluster_averages: n operators (name, average, variance); names '\n'-separated.
+int ref_cluster_averages(int label, int cap, int *n, double *ave, double *var, char *names, int names_size) {
+  return guarded([&] {
+    auto a = ED::cluster_averages((size_t)label);
+    if ((int)a.size() > cap) throw qcm_error("ref_cluster_averages: capacity too small");
+    *n = (int)a.size();
+    std::string all;
+    for (size_t i = 0; i < a.size(); ++i) {
+      ave[i] = std::get<1>(a[i]);
+      var[i] = std::get<2>(a[i]);
+      all += std::get<0>(a[i]);
+      all += '\n';
+    }
+    if ((int)all.size() + 1 > names_size) throw qcm_error("ref_cluster_averages: name buffer too small");
+    std::memcpy(names, all.c_str(), all.size() + 1);
+  });
+}
+
 int ref_potthoff(int label, double *omega) {
   return guarded([&] { *omega = ED::Potthoff_functional((size_t)label); });
 }

@@ -79,6 +79,7 @@ def lib():
         "qed_hybridization_function": [C.c_int, C.c_int, C.c_int, dp, dp],
         "qed_Green_function_average": [C.c_int, C.c_int, dp],
         "qed_Potthoff_functional": [C.c_int, dp],
+        "qed_cluster_averages": [C.c_int, C.c_int, ip, dp, dp, C.c_char_p, C.c_int],
         "qed_qmatrix": [C.c_int, C.c_int, ip, ip, dp, dp],
         "qed_cf_coefficients": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, ip, dp, dp],
         "qed_ground_state_vector": [C.c_int, lp, dp],
@@ -254,6 +255,19 @@ def Green_function_average(spin_down: bool = False, label: int = 0):
     out = np.zeros((n, n), dtype=np.complex128)
     _check(lib().qed_Green_function_average(label, int(spin_down), _dp(out.view(np.float64))))
     return out.T.copy()
+
+
+def cluster_averages(label: int = 0):
+    """ED::cluster_averages: [(operator name, average, variance), ...] in name order."""
+    cap = 256
+    n = C.c_int(0)
+    ave = np.zeros(cap)
+    var = np.zeros(cap)
+    buf = C.create_string_buffer(1 << 16)
+    _check(lib().qed_cluster_averages(label, cap, C.byref(n), ave.ctypes.data_as(C.POINTER(C.c_double)),
+                                      var.ctypes.data_as(C.POINTER(C.c_double)), buf, len(buf)))
+    names = buf.value.decode().split("\n")[: n.value]
+    return [(names[i], float(ave[i]), float(var[i])) for i in range(n.value)]
 
 
 def Potthoff_functional(label: int = 0) -> float:

@@ -179,8 +179,9 @@ int batch_ground_states(BatchSet &b, int threads) {
       tasks.push_back({(double)I->sector_dim(sp->sec), [I, sp] { I->state_vector(*sp, ws()); }});
     }
   if ((rc = run_tasks(tasks, threads)) != QED_OK) return rc;
-  for (Instance *I : todo) I->finish_gs();
-  return QED_OK;
+  return guarded([&] {
+    for (Instance *I : todo) I->finish_gs(ws());
+  });
 }
 
 // Green functions of a batch: each Q-matrix half (state, spin, hole/electron)
@@ -422,6 +423,27 @@ int qed_Green_function_average(int label, int spin_down, double *M) {
     I->green_solve(ws());
     const auto &src = I->Mave[(spin_down && (I->mix & mixing::up_down)) ? 1 : 0];
     std::memcpy(M, src.data(), src.size() * sizeof(cplx));
+  });
+}
+
+int qed_cluster_averages(int label, int cap, int *n, double *ave, double *var, char *names, int names_size) {
+  return guarded([&] {
+    if (!n || !ave || !var || !names) fail(QED_ERR_ARGUMENT, "null argument");
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    I->low_energy_states(ws());
+    const auto &a = I->averages;
+    if ((int)a.size() > cap) fail(QED_ERR_ARGUMENT, "qed_cluster_averages: capacity too small");
+    std::string all;
+    for (size_t i = 0; i < a.size(); ++i) {
+      ave[i] = std::get<1>(a[i]);
+      var[i] = std::get<2>(a[i]);
+      all += std::get<0>(a[i]);
+      all += '\n';
+    }
+    if ((int)all.size() + 1 > names_size) fail(QED_ERR_ARGUMENT, "qed_cluster_averages: name buffer too small");
+    std::memcpy(names, all.c_str(), all.size() + 1);
+    *n = (int)a.size();
   });
 }
 

@@ -281,6 +281,41 @@ void Instance::state_vector(State &st, Workspace &ws) {
   st.lanczos = LanczosResult();
 }
 
+// cluster_averages (src_ed/model_instance.hpp:149-173): for each operator O of
+// the instance, sum over states of weight * <psi|O|psi> and weight * |O psi|^2
+// (HS_Hermitian_operator::expectation_value, src_ed/Operators/HS_Hermitian_operator.hpp:46-52),
+// variance = second - first^2; operators on cluster orbitals only (target 1)
+// are scaled by norm = 1/n_sites (-1/n_sites for "mu"), Hermitian_operator.hpp:41-43.
+// O psi is one H.v with the operator's own tables and the <x,y>, <y,y>
+// reductions of the column pass.
+void Instance::finish_gs(Workspace &ws) {
+  averages.clear();
+  for (auto &v : value) {
+    const Operator &op = *model->term.at(v.first);
+    const SpinData t = collect_terms(*model, {{v.first, 1.0}});
+    double ave = 0.0, var = 0.0;
+    for (auto &st : states) {
+      SectorOp O(t, st->sec, ws);
+      if (O.D == 0) continue;
+      DevBuf<double> y(O.D);
+      SubList none;
+      launch_hv_rows(O.op, st->psi.p, 1.0, y.p, none, ws.stream);
+      const int nb = launch_hv_cols(O.op, st->psi.p, 1.0, y.p, 3, ws.red, ws.stream);
+      const double *r = ws.sums(nb, 2);
+      ave += st->weight * r[0];
+      var += st->weight * r[1];
+    }
+    var -= ave * ave;
+    if (op.target == 1) {
+      const double norm = (v.first == "mu" ? -1.0 : 1.0) / model->n_sites;
+      ave *= norm;
+      var *= norm * norm;
+    }
+    averages.emplace_back(v.first, ave, var);
+  }
+  gs_solved = true;
+}
+
 // low_energy_states (src_ed/model_instance.hpp:245-347)
 std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
   if (gs_solved) return {GS_energy, gs_string()};
@@ -290,7 +325,7 @@ std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
   for (auto &s : target_sectors) solve_sector(s, r[i++], ws);
   select_states(r);
   for (auto &x : states) state_vector(*x, ws);
-  finish_gs();
+  finish_gs(ws);
   return {GS_energy, gs_string()};
 }
 

@@ -8,6 +8,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "model.hpp"
@@ -74,6 +75,9 @@ struct Instance {
   HalfCache tables;  // spin tables shared by the sectors of this instance
   std::vector<double> tc[2], tb[2], tcb[2];  // cluster, bath (diagonalised), cluster-bath
   std::vector<cplx> Mave[2];
+  // cluster_averages: (operator, average, variance) for every operator of the
+  // instance, in name order (model_instance::averages, src_ed/model_instance.hpp:340-345)
+  std::vector<std::tuple<std::string, double, double>> averages;
   std::mutex mtx;
 
   Instance(int label, std::shared_ptr<Model> m, std::map<std::string, double> value,
@@ -90,7 +94,8 @@ struct Instance {
   void solve_sector(const Sector &s, SectorSolve &out, Workspace &ws);
   void select_states(std::vector<SectorSolve> &r);  // every sector, in target order
   void state_vector(State &st, Workspace &ws);
-  void finish_gs() { gs_solved = true; }
+  // the operator averages of the selected states, then gs_solved
+  void finish_gs(Workspace &ws);
   void check_gf_solvable() const;
   void qmatrix_part(State &st, bool spin_down, int s, QPart &out, Workspace &ws);
   void qmatrix_combine(State &st, bool spin_down, QPart (&parts)[2], Workspace &ws);

@@ -268,3 +268,23 @@ def test_block_lanczos_green_function(qed, oracle, fresh, case):
     assert np.max(np.abs(G1 - G2)) < GF_TOL, name
     if G1d is not None:
         assert np.max(np.abs(G1d - oracle.green_function(label, z, spin_down=True))) < GF_TOL, name
+
+
+@pytest.mark.parametrize("case", list(range(len(GS_CASES))) + [100])
+def test_cluster_averages(qed, oracle, fresh, case):
+    """ED::cluster_averages: ground-state average and variance of every operator
+    (cluster operators divided by the number of sites, 'mu' with a minus sign)."""
+    if case == 100:  # dense path, two-fold degenerate ground state
+        name, mk, fmt = "plaq_N3_degenerate", lambda: W.hubbard_cluster(2, 2, U=4.0, mu=1.0, n_up=2, n_dn=1), "S"
+    else:
+        (name, mk), fmt = GS_CASES[case], "F"
+    suffix, label = fresh()
+    set_both(qed, oracle, GF_method="L")
+    load_both(qed, oracle, mk(), suffix, label, fmt=fmt)
+    a1 = qed.cluster_averages(label)
+    oracle.ground_state(label)
+    a2 = oracle.cluster_averages(label)
+    assert [x[0] for x in a1] == [x[0] for x in a2], name
+    for (n, v1, s1), (_, v2, s2) in zip(a1, a2):
+        assert abs(v1 - v2) < 1e-9 * max(1.0, abs(v2)), (name, n, v1, v2)
+        assert abs(s1 - s2) < 1e-8 * max(1.0, abs(s2)), (name, n, s1, s2)

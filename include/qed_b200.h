@@ -129,6 +129,42 @@ int qed_Green_function_average(int label, int spin_down, double *M);
  * names_size bytes. Solves the ground state first if needed. */
 int qed_cluster_averages(int label, int cap, int *n, double *ave, double *var, char *names, int names_size);
 
+/* ED::model_size (src_ed/qcm_ED.hpp:42): sites, bath orbitals, group elements (1). */
+int qed_model_size(const char *model, int *n_sites, int *n_bath, int *n_elements);
+
+/* ED::exists (src_ed/qcm_ED.hpp:66): *found = 1 if the model has the operator. */
+int qed_operator_exists(const char *model, const char *op, int *found);
+
+/* ED::matrix_elements (src_ed/qcm_ED.hpp:308): the operator's type ("one_body" or
+ * "interaction", into a buffer of type_size bytes) and its stored elements
+ * (r, c, v) after the reference's normalisation; cap is the capacity of r, c, v. */
+int qed_matrix_elements(const char *model, const char *op, char *type, int type_size, int cap, int *n, int *r,
+                        int *c, double *v);
+
+/* ED::complex_HS (src_ed/qcm_ED.hpp:94): always 0 (real Hilbert space). */
+int qed_complex_HS(int label, int *flag);
+
+/* ED::Green_function_density (src_ed/qcm_ED.hpp:152): the density from the
+ * solved Green function (0 before Green_function_solve). */
+int qed_Green_function_density(int label, double *density);
+
+/* ED::hopping_matrix (src_ed/qcm_ED.hpp:174): the cluster one-body matrix,
+ * n_sites x n_sites complex, column-major (spin down only differs for up_down mixing). */
+int qed_hopping_matrix(int label, int spin_down, double *H);
+
+/* ED::hopping_matrix_full (src_ed/qcm_ED.hpp:175): cluster + bath one-body matrix,
+ * d x d complex with d = n_sites + n_bath (written to *d), column-major; diag
+ * selects the diagonalised bath. H may be NULL to query d. */
+int qed_hopping_matrix_full(int label, int spin_down, int diag, int *d, double *H);
+
+/* ED::interactions (src_ed/qcm_ED.hpp:180): (r, c, v * value) for every element of
+ * the instance's interaction operators; cap is the capacity of r, c, v. */
+int qed_interactions(int label, int cap, int *n, int *r, int *c, double *v);
+
+/* ED::tr_sigma_inf (src_ed/qcm_ED.hpp:252): trace of the self-energy at infinite
+ * frequency, extrapolated from three large imaginary frequencies. */
+int qed_tr_sigma_inf(int label, double *value);
+
 /* ED::Potthoff_functional (src_ed/qcm_ED.hpp:222; SEF_bath + E0, src_ed/qcm_ED.cpp:330-334). */
 int qed_Potthoff_functional(int label, double *omega);
 

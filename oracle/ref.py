@@ -192,6 +192,67 @@ def green_function_average(label, spin_down=False):
     return out.T.copy()
 
 
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def model_size(model):
+    a, b, c = C.c_int(), C.c_int(), C.c_int()
+    _check(lib().ref_model_size(model.encode(), C.byref(a), C.byref(b), C.byref(c)))
+    return a.value, b.value, c.value
+
+
+def exists(model, op):
+    f = C.c_int()
+    _check(lib().ref_exists(model.encode(), op.encode(), C.byref(f)))
+    return bool(f.value)
+
+
+def matrix_elements(model, op):
+    cap = 1 << 14
+    r, c, v = np.zeros(cap, np.int32), np.zeros(cap, np.int32), np.zeros(cap)
+    n = C.c_int()
+    t = C.create_string_buffer(64)
+    _check(lib().ref_matrix_elements(model.encode(), op.encode(), t, len(t), cap, C.byref(n), _ip(r), _ip(c), _dp(v)))
+    return t.value.decode(), [(int(r[i]), int(c[i]), float(v[i])) for i in range(n.value)]
+
+
+def gf_density(label):
+    d = C.c_double()
+    _check(lib().ref_gf_density(label, C.byref(d)))
+    return d.value
+
+
+def _square(fn, *args):
+    d = C.c_int()
+    _check(fn(*args, C.byref(d), None))
+    buf = np.zeros(2 * d.value * d.value)
+    _check(fn(*args, C.byref(d), _dp(buf)))
+    return (buf[0::2] + 1j * buf[1::2]).reshape(d.value, d.value).T.copy()
+
+
+def hopping_matrix(label, spin_down=False):
+    return _square(lib().ref_hopping_matrix, label, int(spin_down))
+
+
+def hopping_matrix_full(label, spin_down=False, diag=False):
+    return _square(lib().ref_hopping_matrix_full, label, int(spin_down), int(diag))
+
+
+def interactions(label):
+    cap = 1 << 14
+    r, c, v = np.zeros(cap, np.int32), np.zeros(cap, np.int32), np.zeros(cap)
+    n = C.c_int()
+    _check(lib().ref_interactions(label, cap, C.byref(n), _ip(r), _ip(c), _dp(v)))
+    return [(int(r[i]), int(c[i]), float(v[i])) for i in range(n.value)]
+
+
+def tr_sigma_inf(label):
+    d = C.c_double()
+    _check(lib().ref_tr_sigma_inf(label, C.byref(d)))
+    return d.value
+
+
 def cluster_averages(label):
     """ED::cluster_averages: [(operator name, average, variance), ...]."""
     cap = 256

@@ -196,6 +196,72 @@ int ref_cluster_averages(int label, int cap, int *n, double *ave, double *var, c
   });
 }
 
+int ref_model_size(const char *name, int *ns, int *nb, int *ne) {
+  return guarded([&] {
+    auto t = ED::model_size(name);
+    *ns = (int)std::get<0>(t);
+    *nb = (int)std::get<1>(t);
+    *ne = (int)std::get<2>(t);
+  });
+}
+
+int ref_exists(const char *model, const char *op, int *found) {
+  return guarded([&] { *found = ED::exists(model, op) ? 1 : 0; });
+}
+
+int ref_matrix_elements(const char *model, const char *op, char *type, int type_size, int cap, int *n, int *r,
+                        int *c, double *v) {
+  return guarded([&] {
+    auto m = ED::matrix_elements(model, op);
+    if ((int)m.first.size() + 1 > type_size || (int)m.second.size() > cap)
+      throw qcm_error("ref_matrix_elements: buffer too small");
+    std::memcpy(type, m.first.c_str(), m.first.size() + 1);
+    for (size_t i = 0; i < m.second.size(); ++i) {
+      r[i] = (int)m.second[i].r;
+      c[i] = (int)m.second[i].c;
+      v[i] = m.second[i].v.real();
+    }
+    *n = (int)m.second.size();
+  });
+}
+
+int ref_gf_density(int label, double *d) {
+  return guarded([&] { *d = ED::Green_function_density((size_t)label); });
+}
+
+int ref_hopping_matrix(int label, int spin_down, int *d, double *H) {
+  return guarded([&] {
+    auto g = ED::hopping_matrix(spin_down != 0, (size_t)label);
+    *d = (int)g.r;
+    if (H) put_complex(g, H);
+  });
+}
+
+int ref_hopping_matrix_full(int label, int spin_down, int diag, int *d, double *H) {
+  return guarded([&] {
+    auto g = ED::hopping_matrix_full(spin_down != 0, diag != 0, (size_t)label);
+    *d = (int)g.r;
+    if (H) put_complex(g, H);
+  });
+}
+
+int ref_interactions(int label, int cap, int *n, int *r, int *c, double *v) {
+  return guarded([&] {
+    auto V = ED::interactions((size_t)label);
+    if ((int)V.size() > cap) throw qcm_error("ref_interactions: capacity too small");
+    for (size_t i = 0; i < V.size(); ++i) {
+      r[i] = std::get<0>(V[i]);
+      c[i] = std::get<1>(V[i]);
+      v[i] = std::get<2>(V[i]);
+    }
+    *n = (int)V.size();
+  });
+}
+
+int ref_tr_sigma_inf(int label, double *value) {
+  return guarded([&] { *value = ED::tr_sigma_inf((size_t)label); });
+}
+
 int ref_potthoff(int label, double *omega) {
   return guarded([&] { *omega = ED::Potthoff_functional((size_t)label); });
 }

@@ -80,6 +80,15 @@ def lib():
         "qed_Green_function_average": [C.c_int, C.c_int, dp],
         "qed_Potthoff_functional": [C.c_int, dp],
         "qed_cluster_averages": [C.c_int, C.c_int, ip, dp, dp, C.c_char_p, C.c_int],
+        "qed_model_size": [C.c_char_p, ip, ip, ip],
+        "qed_operator_exists": [C.c_char_p, C.c_char_p, ip],
+        "qed_matrix_elements": [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_int, ip, ip, ip, dp],
+        "qed_complex_HS": [C.c_int, ip],
+        "qed_Green_function_density": [C.c_int, dp],
+        "qed_hopping_matrix": [C.c_int, C.c_int, dp],
+        "qed_hopping_matrix_full": [C.c_int, C.c_int, C.c_int, ip, dp],
+        "qed_interactions": [C.c_int, C.c_int, ip, ip, ip, dp],
+        "qed_tr_sigma_inf": [C.c_int, dp],
         "qed_qmatrix": [C.c_int, C.c_int, ip, ip, dp, dp],
         "qed_cf_coefficients": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, ip, dp, dp],
         "qed_ground_state_vector": [C.c_int, lp, dp],
@@ -255,6 +264,88 @@ def Green_function_average(spin_down: bool = False, label: int = 0):
     out = np.zeros((n, n), dtype=np.complex128)
     _check(lib().qed_Green_function_average(label, int(spin_down), _dp(out.view(np.float64))))
     return out.T.copy()
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _dpp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def model_size(model: str):
+    """ED::model_size: (n_sites, n_bath, number of group elements)."""
+    a, b, c = C.c_int(), C.c_int(), C.c_int()
+    _check(lib().qed_model_size(model.encode(), C.byref(a), C.byref(b), C.byref(c)))
+    return a.value, b.value, c.value
+
+
+def exists(model: str, op: str) -> bool:
+    """ED::exists: whether the model defines the operator."""
+    f = C.c_int()
+    _check(lib().qed_operator_exists(model.encode(), op.encode(), C.byref(f)))
+    return bool(f.value)
+
+
+def matrix_elements(model: str, op: str):
+    """ED::matrix_elements: (type, [(r, c, v), ...]) of an operator, 0-based orbitals."""
+    cap = 1 << 14
+    r, c, v = np.zeros(cap, np.int32), np.zeros(cap, np.int32), np.zeros(cap)
+    n = C.c_int()
+    t = C.create_string_buffer(64)
+    _check(lib().qed_matrix_elements(model.encode(), op.encode(), t, len(t), cap, C.byref(n), _ip(r), _ip(c), _dpp(v)))
+    return t.value.decode(), [(int(r[i]), int(c[i]), float(v[i])) for i in range(n.value)]
+
+
+def complex_HS(label: int = 0) -> bool:
+    f = C.c_int()
+    _check(lib().qed_complex_HS(label, C.byref(f)))
+    return bool(f.value)
+
+
+def Green_function_density(label: int = 0) -> float:
+    d = C.c_double()
+    _check(lib().qed_Green_function_density(label, C.byref(d)))
+    return d.value
+
+
+def _square_complex(nrow, call):
+    out = np.zeros((nrow, nrow), dtype=np.complex128)
+    buf = np.zeros(2 * nrow * nrow)
+    call(_dpp(buf))
+    out[:] = (buf[0::2] + 1j * buf[1::2]).reshape(nrow, nrow).T  # column-major
+    return out
+
+
+def hopping_matrix(spin_down: bool = False, label: int = 0):
+    """ED::hopping_matrix: the cluster one-body matrix (n_sites x n_sites, complex)."""
+    n = Green_function_dimension(label)
+    return _square_complex(n, lambda p: _check(lib().qed_hopping_matrix(label, int(spin_down), p)))
+
+
+def hopping_matrix_full(spin_down: bool = False, diag: bool = False, label: int = 0):
+    """ED::hopping_matrix_full: cluster + bath one-body matrix ((n_sites + n_bath)^2, complex)."""
+    d = C.c_int()
+    _check(lib().qed_hopping_matrix_full(label, int(spin_down), int(diag), C.byref(d), None))
+    return _square_complex(d.value, lambda p: _check(lib().qed_hopping_matrix_full(label, int(spin_down), int(diag),
+                                                                                   C.byref(d), p)))
+
+
+def interactions(label: int = 0):
+    """ED::interactions: [(r, c, v * value), ...] of the instance's interaction operators."""
+    cap = 1 << 14
+    r, c, v = np.zeros(cap, np.int32), np.zeros(cap, np.int32), np.zeros(cap)
+    n = C.c_int()
+    _check(lib().qed_interactions(label, cap, C.byref(n), _ip(r), _ip(c), _dpp(v)))
+    return [(int(r[i]), int(c[i]), float(v[i])) for i in range(n.value)]
+
+
+def tr_sigma_inf(label: int = 0) -> float:
+    """ED::tr_sigma_inf: trace of the self-energy at infinite frequency."""
+    d = C.c_double()
+    _check(lib().qed_tr_sigma_inf(label, C.byref(d)))
+    return d.value
 
 
 def cluster_averages(label: int = 0):

@@ -447,6 +447,121 @@ int qed_cluster_averages(int label, int cap, int *n, double *ave, double *var, c
   });
 }
 
+int qed_model_size(const char *model, int *n_sites, int *n_bath, int *n_elements) {
+  return guarded([&] {
+    std::shared_ptr<Model> m;
+    {
+      std::lock_guard<std::mutex> l(g_reg);
+      auto it = g_models.find(model ? model : "");
+      if (it == g_models.end()) fail(QED_ERR_ARGUMENT, "model " + std::string(model ? model : "") + " does not exist!");
+      m = it->second;
+    }
+    *n_sites = m->n_sites;
+    *n_bath = m->n_bath;
+    *n_elements = 1;
+  });
+}
+
+int qed_operator_exists(const char *model, const char *op, int *found) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> l(g_reg);
+    auto it = g_models.find(model ? model : "");
+    if (it == g_models.end()) fail(QED_ERR_ARGUMENT, "model " + std::string(model ? model : "") + " does not exist!");
+    *found = it->second->term.count(op ? op : "") ? 1 : 0;
+  });
+}
+
+int qed_matrix_elements(const char *model, const char *op, char *type, int type_size, int cap, int *n, int *r,
+                        int *c, double *v) {
+  return guarded([&] {
+    std::shared_ptr<Operator> o;
+    {
+      std::lock_guard<std::mutex> l(g_reg);
+      auto it = g_models.find(model ? model : "");
+      if (it == g_models.end())
+        fail(QED_ERR_ARGUMENT, "The model " + std::string(model ? model : "") + " is not defined. Check spelling.");
+      auto jt = it->second->term.find(op ? op : "");
+      if (jt == it->second->term.end())
+        fail(QED_ERR_ARGUMENT, "operator " + std::string(op ? op : "") + " is not defined in model . Check spelling.");
+      o = jt->second;
+    }
+    const std::string t = o->is_interaction ? "interaction" : "one_body";
+    if ((int)t.size() + 1 > type_size || (int)o->elements.size() > cap)
+      fail(QED_ERR_ARGUMENT, "qed_matrix_elements: buffer too small");
+    std::memcpy(type, t.c_str(), t.size() + 1);
+    for (size_t i = 0; i < o->elements.size(); ++i) {
+      r[i] = o->elements[i].r;
+      c[i] = o->elements[i].c;
+      v[i] = o->elements[i].v;
+    }
+    *n = (int)o->elements.size();
+  });
+}
+
+int qed_complex_HS(int label, int *flag) {
+  return guarded([&] {
+    instance(label);
+    *flag = 0;
+  });
+}
+
+int qed_Green_function_density(int label, double *density) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    *density = I->GF_density;
+  });
+}
+
+namespace {
+void put_real_as_complex(const std::vector<double> &h, double *out) {
+  for (size_t i = 0; i < h.size(); ++i) {
+    out[2 * i] = h[i];
+    out[2 * i + 1] = 0.0;
+  }
+}
+}  // namespace
+
+int qed_hopping_matrix(int label, int spin_down, double *H) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    put_real_as_complex(I->hopping_matrix(spin_down != 0), H);
+  });
+}
+
+int qed_hopping_matrix_full(int label, int spin_down, int diag, int *d, double *H) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    *d = I->model->n_orb;
+    if (H) put_real_as_complex(I->hopping_matrix_full(spin_down != 0, diag != 0), H);
+  });
+}
+
+int qed_interactions(int label, int cap, int *n, int *r, int *c, double *v) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    const auto V = I->interactions();
+    if ((int)V.size() > cap) fail(QED_ERR_ARGUMENT, "qed_interactions: capacity too small");
+    for (size_t i = 0; i < V.size(); ++i) {
+      r[i] = V[i].r;
+      c[i] = V[i].c;
+      v[i] = V[i].v;
+    }
+    *n = (int)V.size();
+  });
+}
+
+int qed_tr_sigma_inf(int label, double *value) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    *value = I->tr_sigma_inf(ws());
+  });
+}
+
 int qed_Potthoff_functional(int label, double *omega) {
   return guarded([&] {
     auto I = instance(label);

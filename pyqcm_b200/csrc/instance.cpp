@@ -129,6 +129,8 @@ void Instance::set_hopping_matrix() {
     for (int a = 0; a < ns; ++a)
       for (int b = 0; b < nb; ++b) tcb[sp][a + (size_t)ns * b] = t[(size_t)a * no + ns + b];
     if (nb) {
+      tb_nd[sp] = tb[sp];
+      tcb_nd[sp] = tcb[sp];
       bool diag = true;
       for (int a = 0; a < nb; ++a)
         for (int b = 0; b < nb; ++b)
@@ -155,6 +157,82 @@ void Instance::set_hopping_matrix() {
   }
   if (mix == mixing::normal) SEF_bath *= 2.0;
   hopping_solved = true;
+}
+
+std::vector<double> Instance::hopping_matrix(bool spin_down) const {
+  return tc[(spin_down && (mix & mixing::up_down)) ? 1 : 0];
+}
+
+// The (n_sites + n_bath)^2 one-body matrix: cluster block, bath block (diagonal
+// form when diag, as given otherwise), cluster-bath block and its transpose.
+// With diag, the cluster-bath columns carry the bath eigenvectors, whose signs
+// are a convention of the eigensolver.
+std::vector<double> Instance::hopping_matrix_full(bool spin_down, bool diag) const {
+  // the reference keeps spin-down matrices only for up_down mixing (its call
+  // fails on the empty ones otherwise)
+  if (spin_down && !(mix & mixing::up_down))
+    fail(QED_ERR_ARGUMENT, "hopping_matrix_full: no spin-down one-body matrices without up_down mixing");
+  const int ns = model->n_sites, nb = model->n_bath, d = ns + nb;
+  // likewise it keeps the undiagonalised bath matrices only when there is a bath
+  if (!diag && nb == 0)
+    fail(QED_ERR_ARGUMENT, "hopping_matrix_full: no undiagonalised bath matrices in a model without bath");
+  const int sp = spin_down ? 1 : 0;
+  const std::vector<double> &B = diag ? tb[sp] : tb_nd[sp], &CB = diag ? tcb[sp] : tcb_nd[sp];
+  std::vector<double> H((size_t)d * d, 0.0);
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b < ns; ++b) H[a + (size_t)d * b] = tc[sp][a + (size_t)ns * b];
+  for (int a = 0; a < nb; ++a)
+    for (int b = 0; b < nb; ++b) H[(ns + a) + (size_t)d * (ns + b)] = B[a + (size_t)nb * b];
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b < nb; ++b) {
+      H[a + (size_t)d * (ns + b)] = CB[a + (size_t)ns * b];
+      H[(ns + b) + (size_t)d * a] = CB[a + (size_t)ns * b];
+    }
+  return H;
+}
+
+std::vector<Element> Instance::interactions() const {
+  std::vector<Element> V;
+  for (auto &x : value) {
+    const Operator &op = *model->term.at(x.first);
+    if (!op.is_interaction) continue;
+    for (auto &e : op.elements) V.push_back({e.r, e.c, e.v * x.second});
+  }
+  return V;
+}
+
+// Trace of the self-energy at infinite frequency: Re tr Sigma(i / x) at
+// x = 1e-5, 2e-5, 3e-5 (both spins, or twice the up one for normal mixing),
+// extrapolated to x = 0 by the interpolating polynomial through the three
+// points (Lagrange form; the reference uses Neville's scheme for the same
+// polynomial, src_ed/model_instance.cpp:186-222).
+double Instance::tr_sigma_inf(Workspace &ws) {
+  const int n = dim_GF;
+  constexpr int kNW = 3;
+  double x[kNW], S[kNW];
+  std::vector<cplx> z(kNW), sig((size_t)kNW * n * n);
+  for (int i = 0; i < kNW; ++i) {
+    x[i] = (i + 1) * 1.0e-5;
+    z[i] = cplx(0.0, 1.0 / x[i]);
+  }
+  for (int sd = 0; sd < ((mix & mixing::up_down) ? 2 : 1); ++sd) {
+    self_energy(z.data(), kNW, sd == 1, sig.data(), ws);
+    for (int i = 0; i < kNW; ++i) {
+      double t = 0.0;
+      for (int j = 0; j < n; ++j) t += sig[(size_t)i * n * n + j + (size_t)n * j].real();
+      S[i] = (sd == 0) ? t : S[i] + t;
+    }
+  }
+  if (mix == mixing::normal)
+    for (int i = 0; i < kNW; ++i) S[i] *= 2.0;
+  double s0 = 0.0;
+  for (int i = 0; i < kNW; ++i) {
+    double w = 1.0;
+    for (int j = 0; j < kNW; ++j)
+      if (j != i) w *= (0.0 - x[j]) / (x[i] - x[j]);
+    s0 += w * S[i];
+  }
+  return s0;
 }
 
 std::string Instance::gs_string() const {

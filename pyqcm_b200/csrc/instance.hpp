@@ -74,6 +74,7 @@ struct Instance {
   SpinData terms;
   HalfCache tables;  // spin tables shared by the sectors of this instance
   std::vector<double> tc[2], tb[2], tcb[2];  // cluster, bath (diagonalised), cluster-bath
+  std::vector<double> tb_nd[2], tcb_nd[2];   // bath and cluster-bath before the bath diagonalisation
   std::vector<cplx> Mave[2];
   // cluster_averages: (operator, average, variance) for every operator of the
   // instance, in name order (model_instance::averages, src_ed/model_instance.hpp:340-345)
@@ -106,6 +107,14 @@ struct Instance {
   void self_energy(const cplx *z, int nz, bool spin_down, cplx *out, Workspace &ws);
   void hybridization(const cplx *z, int nz, bool spin_down, cplx *out);
   double potthoff(Workspace &ws);
+  // model_instance::hopping_matrix / hopping_matrix_full (src_ed/model_instance.cpp:13-16,
+  // src_ed/model_instance.hpp:1491-1523): column-major, real parts (real Hilbert space)
+  std::vector<double> hopping_matrix(bool spin_down) const;
+  std::vector<double> hopping_matrix_full(bool spin_down, bool diag) const;
+  // model_instance::interactions (src_ed/model_instance.hpp:1528-1541)
+  std::vector<Element> interactions() const;
+  // model_instance::tr_sigma_inf (src_ed/model_instance.hpp:1279-1312)
+  double tr_sigma_inf(Workspace &ws);
   std::string gs_string() const;
   void set_hopping_matrix();
 

@@ -288,3 +288,18 @@ def test_cluster_averages(qed, oracle, fresh, case):
     for (n, v1, s1), (_, v2, s2) in zip(a1, a2):
         assert abs(v1 - v2) < 1e-9 * max(1.0, abs(v2)), (name, n, v1, v2)
         assert abs(s1 - s2) < 1e-8 * max(1.0, abs(s2)), (name, n, s1, s2)
+
+
+@pytest.mark.parametrize("case", [2, 3])
+def test_tr_sigma_inf_and_gf_density(qed, oracle, fresh, case):
+    """ED::tr_sigma_inf (self-energy trace extrapolated from |z| ~ 1e5; the
+    extrapolation amplifies round-off, hence 1e-6) and ED::Green_function_density."""
+    name, mk = GS_CASES[case]
+    suffix, label = fresh()
+    set_both(qed, oracle, GF_method="L")
+    load_both(qed, oracle, mk(), suffix, label, fmt="F")
+    qed.Green_function_solve(label)
+    oracle.green_solve(label)
+    assert abs(qed.Green_function_density(label) - oracle.gf_density(label)) < 1e-8, name
+    s1, s2 = qed.tr_sigma_inf(label), oracle.tr_sigma_inf(label)
+    assert abs(s1 - s2) < 1e-6 * max(1.0, abs(s2)), (name, s1, s2)

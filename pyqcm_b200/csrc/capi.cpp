@@ -17,11 +17,31 @@
 
 using namespace qed;
 
+// mult_add pipeline: x goes up in kMultAddChunks row blocks, each block's row
+// pass starting as soon as its copy lands; H x comes back in the same blocks and
+// the host adds each block into y while the next one is in flight.
+constexpr int kMultAddChunks = 8;
+
 struct qed_hamiltonian {
   std::unique_ptr<SectorOp> H;
   DevBuf<double> x, y;
   DevBuf<double> partials;  // per-block partial sums of apply_dots_device
   std::mutex m;             // calls on one handle are serialised
+  // mult_add staging: device H x, pinned host copy of it, copy stream, events
+  DevBuf<double> z;
+  double *hz = nullptr;
+  size_t hz_n = 0;
+  cudaStream_t copy = nullptr;
+  cudaEvent_t ev_in[kMultAddChunks] = {}, ev_out[kMultAddChunks] = {};
+  ~qed_hamiltonian() {
+    if (copy) cudaStreamSynchronize(copy);
+    for (int k = 0; k < kMultAddChunks; ++k) {
+      if (ev_in[k]) cudaEventDestroy(ev_in[k]);
+      if (ev_out[k]) cudaEventDestroy(ev_out[k]);
+    }
+    if (copy) cudaStreamDestroy(copy);
+    if (hz) cudaFreeHost(hz);
+  }
 };
 
 namespace {
@@ -650,24 +670,77 @@ int qed_hamiltonian_create(int label, const char *sector, qed_hamiltonian **h, l
   });
 }
 
+// y += H x with host vectors (Hamiltonian::mult_add). Only x crosses to the
+// device and only H x comes back: x in row blocks on a copy stream, each
+// block's row pass (diagonal + up-spin hops, on a view of the down-spin tables
+// shifted to the block) waiting for its own copy; the column pass once all of x
+// is there; H x back in row blocks, and host threads adding each block into y
+// as soon as it has landed.
 int qed_hamiltonian_mult_add(qed_hamiltonian *h, const double *x, double *y) {
   return guarded([&] {
     if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
     std::lock_guard<std::mutex> hl(h->m);
     const size_t D = h->H->D;
     if (!D) return;
-    if (h->x.n < D) { h->x.alloc(D); h->y.alloc(D); }
     Workspace &w = ws();
-    h->x.upload(x, D, w.stream);
-    h->y.upload(y, D, w.stream);
-    // y += H x : row pass writes H_rows x + y, column pass adds the rest
-    SubList sub;
-    sub.n = 1;
-    sub.c[0] = -1.0;
-    sub.z[0] = h->y.p;
-    launch_hv_rows(h->H->op, h->x.p, 1.0, h->y.p, sub, w.stream);
-    launch_hv_cols(h->H->op, h->x.p, 1.0, h->y.p, 0, w.red, w.stream);
-    h->y.download(y, D, w.stream);
+    if (!h->copy) {
+      QED_CUDA(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking));
+      for (int k = 0; k < kMultAddChunks; ++k) {
+        QED_CUDA(cudaEventCreateWithFlags(&h->ev_in[k], cudaEventDisableTiming));
+        QED_CUDA(cudaEventCreateWithFlags(&h->ev_out[k], cudaEventDisableTiming));
+      }
+    }
+    if (h->x.n < D) h->x.alloc(D);
+    if (h->z.n < D) h->z.alloc(D);
+    if (h->hz_n < D) {
+      if (h->hz) QED_CUDA(cudaFreeHost(h->hz));
+      h->hz = nullptr;
+      QED_CUDA(cudaMallocHost(&h->hz, D * sizeof(double)));
+      h->hz_n = D;
+    }
+    w.sync();  // buffers allocated on w.stream are ready for the copy stream
+    const HvOperator &op = h->H->op;
+    const uint32_t du = op.up.dim, dd = op.dn.dim;
+    size_t off[kMultAddChunks + 1];
+    for (int k = 0; k <= kMultAddChunks; ++k) off[k] = (size_t)du * (size_t)((uint64_t)dd * k / kMultAddChunks);
+    SubList none;
+    for (int k = 0; k < kMultAddChunks; ++k) {
+      const size_t n = off[k + 1] - off[k];
+      if (n) QED_CUDA(cudaMemcpyAsync(h->x.p + off[k], x + off[k], n * sizeof(double), cudaMemcpyHostToDevice, h->copy));
+      QED_CUDA(cudaEventRecord(h->ev_in[k], h->copy));
+      QED_CUDA(cudaStreamWaitEvent(w.stream, h->ev_in[k], 0));
+      if (!n) continue;
+      HvOperator blk = op;  // rows [r0, r1) of the sector
+      const uint32_t r0 = (uint32_t)(off[k] / du), r1 = (uint32_t)(off[k + 1] / du);
+      blk.dn.bits += r0;
+      blk.dn.diag += r0;
+      blk.dn.dim = r1 - r0;
+      launch_hv_rows(blk, h->x.p + off[k], 1.0, h->z.p + off[k], none, w.stream);
+    }
+    launch_hv_cols(op, h->x.p, 1.0, h->z.p, 0, w.red, w.stream);
+    for (int k = 0; k < kMultAddChunks; ++k) {
+      const size_t n = off[k + 1] - off[k];
+      if (n) QED_CUDA(cudaMemcpyAsync(h->hz + off[k], h->z.p + off[k], n * sizeof(double), cudaMemcpyDeviceToHost, w.stream));
+      QED_CUDA(cudaEventRecord(h->ev_out[k], w.stream));
+    }
+    int nt = (int)std::thread::hardware_concurrency();
+    nt = std::max(1, std::min(nt, 16));
+    std::atomic<int> bad{0};
+    auto add = [&](int t) {
+      for (int k = 0; k < kMultAddChunks; ++k) {
+        if (cudaEventSynchronize(h->ev_out[k]) != cudaSuccess) {
+          bad = 1;
+          return;
+        }
+        const size_t n = off[k + 1] - off[k], a = off[k] + n * t / nt, b = off[k] + n * (t + 1) / nt;
+        for (size_t i = a; i < b; ++i) y[i] += h->hz[i];
+      }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(add, t);
+    add(0);
+    for (auto &th : pool) th.join();
+    if (bad) fail(QED_ERR_CUDA, "qed_hamiltonian_mult_add: device work failed");
     w.sync();
   });
 }

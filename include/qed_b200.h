@@ -165,6 +165,16 @@ int qed_interactions(int label, int cap, int *n, int *r, int *c, double *v);
  * frequency, extrapolated from three large imaginary frequencies. */
 int qed_tr_sigma_inf(int label, double *value);
 
+/* ED::susceptibility (src_ed/qcm_ED.hpp:202 -> src_ed/model_instance.hpp:1027-1061):
+ * the dynamical susceptibility of operator op at nw complex frequencies w
+ * (re, im pairs) into chi (re, im pairs). */
+int qed_susceptibility(int label, const char *op, int nw, const double *w, double *chi);
+
+/* ED::susceptibility_poles (src_ed/qcm_ED.hpp:213 -> src_ed/model_instance.hpp:1070-1115):
+ * poles (e > 1e-8) and residues (> 1e-6) of the susceptibility, poles closer
+ * than 1e-4 merged; cap is the capacity of e and r. */
+int qed_susceptibility_poles(int label, const char *op, int cap, int *n, double *e, double *r);
+
 /* ED::Potthoff_functional (src_ed/qcm_ED.hpp:222; SEF_bath + E0, src_ed/qcm_ED.cpp:330-334). */
 int qed_Potthoff_functional(int label, double *omega);
 

@@ -253,6 +253,21 @@ def tr_sigma_inf(label):
     return d.value
 
 
+def susceptibility(label, op, w):
+    w = np.ascontiguousarray(np.atleast_1d(np.asarray(w, dtype=np.complex128)))
+    chi = np.zeros(len(w), dtype=np.complex128)
+    _check(lib().ref_susceptibility(label, op.encode(), len(w), _dp(w.view(np.float64)), _dp(chi.view(np.float64))))
+    return chi
+
+
+def susceptibility_poles(label, op):
+    cap = 1 << 14
+    e, r = np.zeros(cap), np.zeros(cap)
+    n = C.c_int()
+    _check(lib().ref_susceptibility_poles(label, op.encode(), cap, C.byref(n), _dp(e), _dp(r)))
+    return [(float(e[i]), float(r[i])) for i in range(n.value)]
+
+
 def cluster_averages(label):
     """ED::cluster_averages: [(operator name, average, variance), ...]."""
     cap = 256

@@ -262,6 +262,30 @@ int ref_tr_sigma_inf(int label, double *value) {
   return guarded([&] { *value = ED::tr_sigma_inf((size_t)label); });
 }
 
+int ref_susceptibility(int label, const char *op, int nw, const double *w, double *chi) {
+  return guarded([&] {
+    std::vector<Complex> z(nw);
+    for (int i = 0; i < nw; ++i) z[i] = Complex(w[2 * i], w[2 * i + 1]);
+    auto c = ED::susceptibility(op, z, (size_t)label);
+    for (int i = 0; i < nw; ++i) {
+      chi[2 * i] = c[i].real();
+      chi[2 * i + 1] = c[i].imag();
+    }
+  });
+}
+
+int ref_susceptibility_poles(int label, const char *op, int cap, int *n, double *e, double *r) {
+  return guarded([&] {
+    auto p = ED::susceptibility_poles(op, (size_t)label);
+    if ((int)p.size() > cap) throw qcm_error("ref_susceptibility_poles: capacity too small");
+    for (size_t i = 0; i < p.size(); ++i) {
+      e[i] = p[i].first;
+      r[i] = p[i].second;
+    }
+    *n = (int)p.size();
+  });
+}
+
 int ref_potthoff(int label, double *omega) {
   return guarded([&] { *omega = ED::Potthoff_functional((size_t)label); });
 }

@@ -89,6 +89,8 @@ def lib():
         "qed_hopping_matrix_full": [C.c_int, C.c_int, C.c_int, ip, dp],
         "qed_interactions": [C.c_int, C.c_int, ip, ip, ip, dp],
         "qed_tr_sigma_inf": [C.c_int, dp],
+        "qed_susceptibility": [C.c_int, C.c_char_p, C.c_int, dp, dp],
+        "qed_susceptibility_poles": [C.c_int, C.c_char_p, C.c_int, ip, dp, dp],
         "qed_qmatrix": [C.c_int, C.c_int, ip, ip, dp, dp],
         "qed_cf_coefficients": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, ip, dp, dp],
         "qed_ground_state_vector": [C.c_int, lp, dp],
@@ -346,6 +348,23 @@ def tr_sigma_inf(label: int = 0) -> float:
     d = C.c_double()
     _check(lib().qed_tr_sigma_inf(label, C.byref(d)))
     return d.value
+
+
+def susceptibility(op: str, w, label: int = 0):
+    """ED::susceptibility: dynamical susceptibility of operator op at the complex frequencies w."""
+    w = np.ascontiguousarray(np.atleast_1d(np.asarray(w, dtype=np.complex128)))
+    chi = np.zeros(len(w), dtype=np.complex128)
+    _check(lib().qed_susceptibility(label, op.encode(), len(w), _dpp(w.view(np.float64)), _dpp(chi.view(np.float64))))
+    return chi
+
+
+def susceptibility_poles(op: str, label: int = 0):
+    """ED::susceptibility_poles: [(pole, residue), ...]."""
+    cap = 1 << 14
+    e, r = np.zeros(cap), np.zeros(cap)
+    n = C.c_int()
+    _check(lib().qed_susceptibility_poles(label, op.encode(), cap, C.byref(n), _dpp(e), _dpp(r)))
+    return [(float(e[i]), float(r[i])) for i in range(n.value)]
 
 
 def cluster_averages(label: int = 0):

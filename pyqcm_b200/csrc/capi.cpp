@@ -582,6 +582,30 @@ int qed_tr_sigma_inf(int label, double *value) {
   });
 }
 
+int qed_susceptibility(int label, const char *op, int nw, const double *w, double *chi) {
+  return guarded([&] {
+    if (!op || (nw > 0 && (!w || !chi))) fail(QED_ERR_ARGUMENT, "null argument");
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    I->susceptibility(op, reinterpret_cast<const cplx *>(w), nw, reinterpret_cast<cplx *>(chi), ws());
+  });
+}
+
+int qed_susceptibility_poles(int label, const char *op, int cap, int *n, double *e, double *r) {
+  return guarded([&] {
+    if (!op || !n || !e || !r) fail(QED_ERR_ARGUMENT, "null argument");
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    const auto p = I->susceptibility_poles(op, ws());
+    if ((int)p.size() > cap) fail(QED_ERR_ARGUMENT, "qed_susceptibility_poles: capacity too small");
+    for (size_t i = 0; i < p.size(); ++i) {
+      e[i] = p[i].first;
+      r[i] = p[i].second;
+    }
+    *n = (int)p.size();
+  });
+}
+
 int qed_Potthoff_functional(int label, double *omega) {
   return guarded([&] {
     auto I = instance(label);

@@ -235,6 +235,94 @@ double Instance::tr_sigma_inf(Workspace &ws) {
   return s0;
 }
 
+std::vector<Instance::SusQ> Instance::susceptibility_qmatrices(const std::string &opname, Workspace &ws) {
+  if (!model->term.count(opname)) fail(QED_ERR_ARGUMENT, "Operator " + opname + " is not defined in the model.");
+  if (!value.count(opname))
+    fail(QED_ERR_ARGUMENT, "operator " + opname + " is not activated in instance " + std::to_string(label));
+  if (!gs_solved) low_energy_states(ws);
+  const SpinData t = collect_terms(*model, {{opname, 1.0}});
+  std::vector<SusQ> out;
+  for (auto &sec : target_sectors)
+    for (auto &st : states) {
+      if (!(st->sec == sec)) continue;
+      SectorOp H(terms, sec, ws, &tables);
+      if (H.D == 0) continue;
+      SectorOp O(t, sec, ws);
+      std::vector<DevBuf<double>> b(1);
+      b[0].alloc(H.D);
+      SubList none;
+      launch_hv_rows(O.op, st->psi.p, 1.0, b[0].p, none, ws.stream);  // b = O psi
+      launch_hv_cols(O.op, st->psi.p, 1.0, b[0].p, 0, ws.red, ws.stream);
+      SusQ q;
+      q.st = st.get();
+      int M = 0;
+      bool ok;
+      if (!model->factorized && (long)H.D < opt_int("max_dim_full")) {
+        std::vector<double> U, ph(H.D);
+        dense_eigensystem(H, ws, q.e, U);
+        b[0].download(ph.data(), H.D, ws.stream);
+        ws.sync();
+        M = (int)H.D;
+        q.V.assign(M, 0.0);
+        for (int k = 0; k < M; ++k) {
+          double acc = 0.0;
+          for (size_t j = 0; j < H.D; ++j) acc += ph[j] * U[(size_t)k * H.D + j];
+          q.V[k] = acc;
+        }
+        ok = true;
+      } else {
+        ok = band_lanczos_qmatrix(H, ws, b, q.e, q.V, M);
+      }
+      if (!ok || M == 0) continue;
+      q.e.resize(M);
+      q.V.resize(M);
+      for (auto &x : q.e) x -= st->energy;
+      out.push_back(std::move(q));
+    }
+  return out;
+}
+
+void Instance::susceptibility(const std::string &opname, const cplx *w, int nw, cplx *chi, Workspace &ws) {
+  const auto qs = susceptibility_qmatrices(opname, ws);
+  DevBuf<double> dz(2 * (size_t)std::max(nw, 1)), dG(2 * (size_t)std::max(nw, 1));
+  dz.upload(reinterpret_cast<const double *>(w), 2 * (size_t)nw, ws.stream);
+  QED_CUDA(cudaMemsetAsync(dG.p, 0, dG.bytes(), ws.stream));
+  std::vector<DevBuf<double>> keep;
+  for (auto &q : qs) {
+    std::vector<double> V(q.V);
+    const double sw = std::sqrt(q.st->weight);
+    for (auto &x : V) x *= sw;
+    keep.emplace_back(q.e.size());
+    keep.back().upload(q.e, ws.stream);
+    keep.emplace_back(V.size());
+    keep.back().upload(V, ws.stream);
+    launch_qmatrix_gf(1, (int)q.e.size(), keep[keep.size() - 2].p, keep.back().p, nw, dz.p, dG.p, ws.stream);
+  }
+  dG.download(reinterpret_cast<double *>(chi), 2 * (size_t)nw, ws.stream);
+  ws.sync();
+}
+
+std::vector<std::pair<double, double>> Instance::susceptibility_poles(const std::string &opname, Workspace &ws) {
+  const auto qs = susceptibility_qmatrices(opname, ws);
+  std::vector<std::pair<double, double>> chi, chi2;
+  for (auto &q : qs)
+    for (size_t i = 0; i < q.e.size(); ++i) {
+      if (q.e[i] < 1e-8) continue;
+      const double r = q.V[i] * q.V[i] * q.st->weight;
+      if (r > 1e-6) chi.push_back({q.e[i], r});
+    }
+  for (auto &x : chi) {  // poles closer than 1e-4 are merged, in order of appearance
+    size_t j = 0;
+    for (; j < chi2.size(); ++j)
+      if (std::fabs(chi2[j].first - x.first) < 1e-4) {
+        chi2[j].second += x.second;
+        break;
+      }
+    if (j == chi2.size()) chi2.push_back(x);
+  }
+  return chi2;
+}
+
 std::string Instance::gs_string() const {
   if (!is_correlated) return "uncorrelated";
   std::map<Sector, double, SectorLess> ws;

@@ -115,10 +115,21 @@ struct Instance {
   std::vector<Element> interactions() const;
   // model_instance::tr_sigma_inf (src_ed/model_instance.hpp:1279-1312)
   double tr_sigma_inf(Workspace &ws);
+  // model_instance::susceptibility / susceptibility_poles (src_ed/model_instance.hpp:1027-1115):
+  // chi(w) = sum over states of weight * sum_i |<i|O|psi>|^2 / (w - (E_i - E0)),
+  // from the Lehmann representation of O|psi> in the state's own sector
+  void susceptibility(const std::string &op, const cplx *w, int nw, cplx *chi, Workspace &ws);
+  std::vector<std::pair<double, double>> susceptibility_poles(const std::string &op, Workspace &ws);
   std::string gs_string() const;
   void set_hopping_matrix();
 
  private:
+  // Q-matrix (p = 1) of O|psi> for every state: poles shifted by the state energy
+  struct SusQ {
+    const State *st;
+    std::vector<double> e, V;
+  };
+  std::vector<SusQ> susceptibility_qmatrices(const std::string &op, Workspace &ws);
   void build_qmatrix(State &st, bool spin_down, Workspace &ws);
   void compute_weights();
   std::string where(const Sector &s) const;

@@ -303,3 +303,32 @@ def test_tr_sigma_inf_and_gf_density(qed, oracle, fresh, case):
     assert abs(qed.Green_function_density(label) - oracle.gf_density(label)) < 1e-8, name
     s1, s2 = qed.tr_sigma_inf(label), oracle.tr_sigma_inf(label)
     assert abs(s1 - s2) < 1e-6 * max(1.0, abs(s2)), (name, s1, s2)
+
+
+@pytest.mark.parametrize("case,op", [(2, "M"), (2, "t"), (0, "U"), (3, "mu")])
+def test_susceptibility(qed, oracle, fresh, case, op):
+    """ED::susceptibility and susceptibility_poles (Lehmann representation of
+    O|psi> by band Lanczos with one start vector). With a single start vector the
+    recurrence stops as soon as its lowest Ritz value (the ground state itself)
+    changes by less than 1e-12 between steps, a test that round-off can pass one
+    step earlier or later in either code, which moves the unconverged high
+    poles: the tolerance is 1e-5 here instead of the 1e-8 of the Green functions,
+    and 1e-4 on the poles of residue above 0.05 (the reference's own small poles
+    for chain8 / U move by 2e-5 when only its random seed changes; those of
+    plaq8b / mu with residue 0.03 by 1e-3 between the two codes)."""
+    name, mk = GS_CASES[case]
+    suffix, label = fresh()
+    set_both(qed, oracle, GF_method="L")
+    load_both(qed, oracle, mk(), suffix, label, fmt="F")
+    w = np.array([0.3 + 0.05j, 1.0 + 0.1j, 2.5 + 0.2j, 1j, 6.0 + 0.5j])
+    c1 = qed.susceptibility(op, w, label=label)
+    oracle.ground_state(label)
+    c2 = oracle.susceptibility(label, op, w)
+    assert np.max(np.abs(c1 - c2)) < 1e-5 * max(1.0, np.max(np.abs(c2))), (name, op)
+    p1 = qed.susceptibility_poles(op, label=label)
+    p2 = oracle.susceptibility_poles(label, op)
+    big1 = [x for x in p1 if x[1] > 0.05]
+    big2 = [x for x in p2 if x[1] > 0.05]
+    assert len(big1) == len(big2), (name, op)
+    for (e1, r1), (e2, r2) in zip(sorted(big1), sorted(big2)):
+        assert abs(e1 - e2) < 1e-4 and abs(r1 - r2) < 1e-4 * max(1.0, r2), (name, op, e1, e2, r1, r2)

@@ -175,6 +175,10 @@ int qed_susceptibility(int label, const char *op, int nw, const double *w, doubl
  * than 1e-4 merged; cap is the capacity of e and r. */
 int qed_susceptibility_poles(int label, const char *op, int cap, int *n, double *e, double *r);
 
+/* ED::fidelity (src_ed/qcm_ED.hpp:244 -> src_ed/model_instance.hpp:1258-1271): the sum
+ * over state pairs of the two instances in the same sector of w1 w2 |<psi1|psi2>|^2. */
+int qed_fidelity(int label1, int label2, double *fidelity);
+
 /* ED::Potthoff_functional (src_ed/qcm_ED.hpp:222; SEF_bath + E0, src_ed/qcm_ED.cpp:330-334). */
 int qed_Potthoff_functional(int label, double *omega);
 

@@ -268,6 +268,12 @@ def susceptibility_poles(label, op):
     return [(float(e[i]), float(r[i])) for i in range(n.value)]
 
 
+def fidelity(l1, l2):
+    d = C.c_double()
+    _check(lib().ref_fidelity(l1, l2, C.byref(d)))
+    return d.value
+
+
 def cluster_averages(label):
     """ED::cluster_averages: [(operator name, average, variance), ...]."""
     cap = 256

@@ -286,6 +286,10 @@ int ref_susceptibility_poles(int label, const char *op, int cap, int *n, double 
   });
 }
 
+int ref_fidelity(int l1, int l2, double *f) {
+  return guarded([&] { *f = ED::fidelity(l1, l2); });
+}
+
 int ref_potthoff(int label, double *omega) {
   return guarded([&] { *omega = ED::Potthoff_functional((size_t)label); });
 }

@@ -90,6 +90,7 @@ def lib():
         "qed_interactions": [C.c_int, C.c_int, ip, ip, ip, dp],
         "qed_tr_sigma_inf": [C.c_int, dp],
         "qed_susceptibility": [C.c_int, C.c_char_p, C.c_int, dp, dp],
+        "qed_fidelity": [C.c_int, C.c_int, dp],
         "qed_susceptibility_poles": [C.c_int, C.c_char_p, C.c_int, ip, dp, dp],
         "qed_qmatrix": [C.c_int, C.c_int, ip, ip, dp, dp],
         "qed_cf_coefficients": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, ip, dp, dp],
@@ -365,6 +366,13 @@ def susceptibility_poles(op: str, label: int = 0):
     n = C.c_int()
     _check(lib().qed_susceptibility_poles(label, op.encode(), cap, C.byref(n), _dpp(e), _dpp(r)))
     return [(float(e[i]), float(r[i])) for i in range(n.value)]
+
+
+def fidelity(label1: int, label2: int) -> float:
+    """ED::fidelity: sum over same-sector state pairs of w1 w2 |<psi1|psi2>|^2."""
+    d = C.c_double()
+    _check(lib().qed_fidelity(label1, label2, C.byref(d)))
+    return d.value
 
 
 def cluster_averages(label: int = 0):

@@ -606,6 +606,37 @@ int qed_susceptibility_poles(int label, const char *op, int cap, int *n, double 
   });
 }
 
+int qed_fidelity(int label1, int label2, double *fidelity) {
+  return guarded([&] {
+    if (!fidelity) fail(QED_ERR_ARGUMENT, "null argument");
+    auto I1 = instance(label1), I2 = instance(label2);
+    // both instances locked, in label order
+    std::unique_lock<std::mutex> la, lb;
+    if (I1 == I2) {
+      la = std::unique_lock<std::mutex>(I1->mtx);
+    } else {
+      Instance *first = label1 < label2 ? I1.get() : I2.get(), *second = label1 < label2 ? I2.get() : I1.get();
+      la = std::unique_lock<std::mutex>(first->mtx);
+      lb = std::unique_lock<std::mutex>(second->mtx);
+    }
+    Workspace &w = ws();
+    I1->low_energy_states(w);
+    I2->low_energy_states(w);
+    double z = 0.0;
+    for (auto &s1 : I1->states)
+      for (auto &s2 : I2->states) {
+        if (!(s1->sec == s2->sec) || s1->psi.n != s2->psi.n || s1->psi.n == 0) continue;
+        VecList one;
+        one.n = 1;
+        one.v[0] = s2->psi.p;
+        const int nb = launch_dots(s1->psi.n, s1->psi.p, 1.0, 0, one, w.red, w.stream);
+        const double zz = w.sums(nb, 1)[0];
+        z += zz * zz * s1->weight * s2->weight;
+      }
+    *fidelity = z;
+  });
+}
+
 int qed_Potthoff_functional(int label, double *omega) {
   return guarded([&] {
     auto I = instance(label);

@@ -332,3 +332,19 @@ def test_susceptibility(qed, oracle, fresh, case, op):
     assert len(big1) == len(big2), (name, op)
     for (e1, r1), (e2, r2) in zip(sorted(big1), sorted(big2)):
         assert abs(e1 - e2) < 1e-4 and abs(r1 - r2) < 1e-4 * max(1.0, r2), (name, op, e1, e2, r1, r2)
+
+
+def test_fidelity(qed, oracle, fresh):
+    """ED::fidelity between two instances of one model at nearby parameters: the
+    overlap of ground states does not depend on their signs or normalisation
+    conventions beyond those of the reference (both Lanczos vectors, weight 1)."""
+    mk = lambda U: W.hubbard_cluster(4, 2, U=U, mu=1.7, M=0.25, name="fid")
+    labels = []
+    for U in (5.0, 5.3):
+        suffix, label = fresh()
+        load_both(qed, oracle, mk(U), "_fid" + suffix, label, fmt="F")
+        labels.append(label)
+    f1 = qed.fidelity(*labels)
+    f2 = oracle.fidelity(*labels)
+    assert abs(f1 - f2) < 1e-9, (f1, f2)
+    assert abs(qed.fidelity(labels[0], labels[0]) - oracle.fidelity(labels[0], labels[0])) < 1e-9

@@ -118,8 +118,11 @@ int qed_self_energy(int label, int spin_down, int nz, const double *z, double *S
 /* ED::hybridization_function (src_ed/qcm_ED.hpp:210 -> src_ed/model_instance.hpp:1004-1018), batched. */
 int qed_hybridization_function(int label, int spin_down, int nz, const double *z, double *H);
 
-/* ED::Green_function_average (src_ed/qcm_ED.hpp:146): <c^+_b c_a>, dim x dim complex. */
+/* ED::Green_function_average (src_ed/qcm_ED.hpp:146): <c^+_b c_a>, d x d complex,
+ * d from qed_Green_function_average_dimension: the number of cluster sites, or
+ * cluster + bath orbitals for an uncorrelated instance (as the reference returns). */
 int qed_Green_function_average(int label, int spin_down, double *M);
+int qed_Green_function_average_dimension(int label, int *d);
 
 /* ED::cluster_averages (src_ed/qcm_ED.hpp:113 -> src_ed/model_instance.hpp:149-173,
  * 340-345): for each operator of the instance, in name order, its ground-state

@@ -186,7 +186,9 @@ def hybridization_function(label, z, spin_down=False):
 
 
 def green_function_average(label, spin_down=False):
-    n = gf_dim(label)
+    d = C.c_int()
+    _check(lib().ref_green_function_average_dim(label, int(spin_down), C.byref(d)))
+    n = d.value
     out = np.zeros((n, n), dtype=np.complex128)
     _check(lib().ref_green_function_average(label, int(spin_down), _dp(out.view(np.float64))))
     return out.T.copy()

@@ -178,6 +178,10 @@ int ref_green_function_average(int label, int spin_down, double *out) {
   });
 }
 
+int ref_green_function_average_dim(int label, int spin_down, int *d) {
+  return guarded([&] { *d = (int)ED::Green_function_average(spin_down != 0, (size_t)label).r; });
+}
+
 // cluster_averages: n operators (name, average, variance); names '\n'-separated.
 int ref_cluster_averages(int label, int cap, int *n, double *ave, double *var, char *names, int names_size) {
   return guarded([&] {

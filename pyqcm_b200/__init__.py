@@ -78,6 +78,7 @@ def lib():
         "qed_self_energy": [C.c_int, C.c_int, C.c_int, dp, dp],
         "qed_hybridization_function": [C.c_int, C.c_int, C.c_int, dp, dp],
         "qed_Green_function_average": [C.c_int, C.c_int, dp],
+        "qed_Green_function_average_dimension": [C.c_int, ip],
         "qed_Potthoff_functional": [C.c_int, dp],
         "qed_cluster_averages": [C.c_int, C.c_int, ip, dp, dp, C.c_char_p, C.c_int],
         "qed_model_size": [C.c_char_p, ip, ip, ip],
@@ -263,7 +264,9 @@ def hybridization_function(z, spin_down: bool = False, label: int = 0):
 
 
 def Green_function_average(spin_down: bool = False, label: int = 0):
-    n = Green_function_dimension(label)
+    d = C.c_int()
+    _check(lib().qed_Green_function_average_dimension(label, C.byref(d)))
+    n = d.value
     out = np.zeros((n, n), dtype=np.complex128)
     _check(lib().qed_Green_function_average(label, int(spin_down), _dp(out.view(np.float64))))
     return out.T.copy()

@@ -167,11 +167,14 @@ struct BatchSet {
 int batch_ground_states(BatchSet &b, int threads) {
   std::vector<Instance *> todo;
   int rc = guarded([&] {
-    for (auto &I : b.inst)
-      if (!I->gs_solved) {
-        I->check_solvable();
-        todo.push_back(I.get());
+    for (auto &I : b.inst) {
+      if (I->gs_solved) continue;
+      if (!I->is_correlated) {  // the one-body problem: nothing to spread over threads
+        I->low_energy_states(ws());
+        continue;
       }
+      todo.push_back(I.get());
+    }
   });
   if (rc != QED_OK || todo.empty()) return rc;
   std::vector<std::vector<SectorSolve>> res(todo.size());
@@ -441,8 +444,16 @@ int qed_Green_function_average(int label, int spin_down, double *M) {
     auto I = instance(label);
     std::lock_guard<std::mutex> li(I->mtx);
     I->green_solve(ws());
-    const auto &src = I->Mave[(spin_down && (I->mix & mixing::up_down)) ? 1 : 0];
+    const int sd = (spin_down && (I->mix & mixing::up_down)) ? 1 : 0;
+    const auto &src = I->is_correlated ? I->Mave[sd] : I->Mfull[sd];
     std::memcpy(M, src.data(), src.size() * sizeof(cplx));
+  });
+}
+
+int qed_Green_function_average_dimension(int label, int *d) {
+  return guarded([&] {
+    auto I = instance(label);
+    *d = I->is_correlated ? I->dim_GF : I->model->n_orb;
   });
 }
 

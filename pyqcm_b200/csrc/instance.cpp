@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <iomanip>
+#include <limits>
 #include <sstream>
 
 #include "eigen.hpp"
@@ -342,10 +343,102 @@ std::string Instance::where(const Sector &s) const {
          "', sector '" + s.name() + "'";
 }
 
-void Instance::check_solvable() const {
-  if (!is_correlated)
-    fail(QED_ERR_UNSUPPORTED, "uncorrelated instances (no interaction term) are solved by the one-body "
-                              "path, which is not in this solver");
+// one_body_solve (src_ed/model_instance.hpp:1164-1256): without interaction the
+// cluster + bath problem is one-body. Per spin, the (n_sites + n_bath)^2
+// one-body matrix (bath diagonalised) is diagonalised; the Q-matrix holds all
+// its poles with the cluster components of the eigenvectors, the ground-state
+// energy is the sum of the negative one-body energies, and M_ab = <c+_b c_a> is
+// the sum over occupied orbitals. Reproduced as the reference has it: the
+// spin-down branch adds the spin-up negative energies again, and only the
+// spin-up Q-matrix is checked for unitarity. The operator averages come from M
+// (one_body_operator::average_from_GF, src_ed/Operators/one_body_operator.hpp:420-440);
+// their variances are undefined (NaN), as in the reference.
+void Instance::one_body_solve(Workspace &ws) {
+  const int ns = model->n_sites, nb = model->n_bath, d = ns + nb;
+  use_cf = false;  // the one-body Green function is a Q-matrix (GF_format_BL)
+  states.clear();
+  auto st = std::make_shared<State>();
+  double gs = 0.0;
+  std::vector<double> Mocc[2];
+  const int nsp = (mix & mixing::up_down) ? 2 : 1;
+  std::vector<double> eup;
+  for (int sp = 0; sp < nsp; ++sp) {
+    std::vector<double> H((size_t)d * d, 0.0), e, U;
+    for (int a = 0; a < ns; ++a)
+      for (int b = 0; b < ns; ++b) H[a + (size_t)d * b] = tc[sp][a + (size_t)ns * b];
+    for (int a = 0; a < nb; ++a)
+      for (int b = 0; b < nb; ++b) H[(ns + a) + (size_t)d * (ns + b)] = tb[sp][a + (size_t)nb * b];
+    for (int a = 0; a < ns; ++a)
+      for (int b = 0; b < nb; ++b) {
+        H[a + (size_t)d * (ns + b)] = tcb[sp][a + (size_t)ns * b];
+        H[(ns + b) + (size_t)d * a] = tcb[sp][a + (size_t)ns * b];
+      }
+    if (!sym_eig(d, H, e, &U)) fail(QED_ERR_INTERNAL, "one-body eigensolver failed");
+    QMat &q = st->q[sp];
+    q.L = ns;
+    q.M = d;
+    q.e = e;
+    q.V.assign((size_t)d * ns, 0.0);
+    for (int k = 0; k < d; ++k)
+      for (int i = 0; i < ns; ++i) q.V[(size_t)k * ns + i] = U[i + (size_t)d * k];
+    Mocc[sp].assign((size_t)d * d, 0.0);
+    for (int a = 0; a < d; ++a)
+      for (int b = 0; b < d; ++b) {
+        double m = 0.0;
+        for (int r = 0; r < d; ++r)
+          if (e[r] < 0.0) m += U[a + (size_t)d * r] * U[b + (size_t)d * r];
+        Mocc[sp][b + (size_t)d * a] = m;
+      }
+    if (sp == 0) eup = e;
+    for (double x : eup)
+      if (x < 0.0) gs += x;
+    if (sp == 0) {  // Q.check_norm(1e-6)
+      double ztot = 0.0;
+      for (int i = 0; i < ns; ++i) {
+        double z = 0.0;
+        for (int k = 0; k < d; ++k) z += q.V[(size_t)k * ns + i] * q.V[(size_t)k * ns + i];
+        ztot += (z - 1.0) * (z - 1.0);
+        for (int j = 0; j < i; ++j) {
+          double zz = 0.0;
+          for (int k = 0; k < d; ++k) zz += q.V[(size_t)k * ns + i] * q.V[(size_t)k * ns + j];
+          ztot += 2.0 * zz * zz;
+        }
+      }
+      if (ztot > 1e-6) fail(QED_ERR_QMATRIX, "Q-matrix does not satisfy unitary condition by " + std::to_string(ztot));
+    }
+    q.de.upload(q.e, ws.stream);
+    q.dV.upload(q.V, ws.stream);
+  }
+  ws.sync();
+  for (int sp = 0; sp < nsp; ++sp) Mfull[sp].assign(Mocc[sp].begin(), Mocc[sp].end());
+  if (mix == mixing::normal) gs *= 2.0;
+  GS_energy = gs;
+  E0 = gs;
+  st->energy = gs;
+  st->weight = 1.0;
+  states.push_back(st);
+  // cluster_averages from M: trace of M times the operator's one-body block
+  averages.clear();
+  const int no = model->n_orb;
+  for (auto &v : value) {
+    const Operator &op = *model->term.at(v.first);
+    double ave = std::numeric_limits<double>::quiet_NaN();
+    if (!op.is_interaction) {
+      ave = 0.0;
+      for (int sp = 0; sp < nsp; ++sp)
+        for (auto &x : op.elements) {
+          const bool down = x.r >= no;
+          if (down != (sp == 1) || (x.c >= no) != down) continue;
+          const int r = x.r - (down ? no : 0), c = x.c - (down ? no : 0);
+          ave += Mocc[sp][r + (size_t)d * c] * x.v;
+        }
+      if (mix == mixing::normal) ave *= 2.0;
+      if (op.target == 1) ave *= (v.first == "mu" ? -1.0 : 1.0) / ns;
+    }
+    averages.emplace_back(v.first, ave, std::numeric_limits<double>::quiet_NaN());
+  }
+  gs_solved = true;
+  finish_gf();
 }
 
 size_t Instance::sector_dim(const Sector &s) const {
@@ -485,7 +578,10 @@ void Instance::finish_gs(Workspace &ws) {
 // low_energy_states (src_ed/model_instance.hpp:245-347)
 std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
   if (gs_solved) return {GS_energy, gs_string()};
-  check_solvable();
+  if (!is_correlated) {
+    one_body_solve(ws);
+    return {GS_energy, gs_string()};
+  }
   std::vector<SectorSolve> r(target_sectors.size());
   size_t i = 0;
   for (auto &s : target_sectors) solve_sector(s, r[i++], ws);

@@ -76,6 +76,9 @@ struct Instance {
   std::vector<double> tc[2], tb[2], tcb[2];  // cluster, bath (diagonalised), cluster-bath
   std::vector<double> tb_nd[2], tcb_nd[2];   // bath and cluster-bath before the bath diagonalisation
   std::vector<cplx> Mave[2];
+  // uncorrelated instances: <c+_b c_a> over cluster and bath orbitals, which is
+  // what the reference's Green_function_average returns for them
+  std::vector<cplx> Mfull[2];
   // cluster_averages: (operator, average, variance) for every operator of the
   // instance, in name order (model_instance::averages, src_ed/model_instance.hpp:340-345)
   std::vector<std::tuple<std::string, double, double>> averages;
@@ -90,7 +93,9 @@ struct Instance {
   // The steps of low_energy_states and green_solve, for drivers that run the
   // sectors, states and Q-matrix halves of many instances concurrently. A
   // single instance runs them in this order on one thread.
-  void check_solvable() const;
+  // uncorrelated instances (no interaction operator): one_body_solve
+  // (src_ed/model_instance.hpp:1164-1256), the one-body problem in full
+  void one_body_solve(Workspace &ws);
   size_t sector_dim(const Sector &s) const;
   void solve_sector(const Sector &s, SectorSolve &out, Workspace &ws);
   void select_states(std::vector<SectorSolve> &r);  // every sector, in target order

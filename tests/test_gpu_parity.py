@@ -348,3 +348,44 @@ def test_fidelity(qed, oracle, fresh):
     f2 = oracle.fidelity(*labels)
     assert abs(f1 - f2) < 1e-9, (f1, f2)
     assert abs(qed.fidelity(labels[0], labels[0]) - oracle.fidelity(labels[0], labels[0])) < 1e-9
+
+
+def _uncorrelated(p):
+    p.operators.pop("U")
+    p.params.pop("U")
+    return p
+
+
+UNCORRELATED = [
+    ("free2x3_neel", lambda: _uncorrelated(W.hubbard_cluster(3, 2, U=4.0, mu=0.7, M=0.2, name="free23"))),
+    ("free_chain6", lambda: _uncorrelated(W.hubbard_cluster(6, 1, U=4.0, mu=0.4, name="free6"))),
+    ("free_plaq8b", lambda: _uncorrelated(W.plaquette_bath(np.linspace(-1.5, 1.5, 8), np.linspace(0.2, 0.9, 8),
+                                                           name="freepb"))),
+]
+
+
+@pytest.mark.parametrize("case", range(len(UNCORRELATED)))
+def test_uncorrelated_one_body_path(qed, oracle, fresh, case):
+    """Instances without an interaction operator: one_body_solve (ground-state
+    energy from the occupied one-body levels, the Q-matrix of the one-body
+    problem, averages from <c+ c>)."""
+    name, mk = UNCORRELATED[case]
+    suffix, label = fresh()
+    set_both(qed, oracle, GF_method="L")
+    load_both(qed, oracle, mk(), suffix, label, fmt="F")
+    e1, s1 = qed.ground_state_solve(label)
+    e2, s2 = oracle.ground_state(label)
+    assert s1 == s2 == "uncorrelated"
+    assert abs(e1 - e2) <= 1e-12 * max(1.0, abs(e2)), (name, e1, e2)
+    z = W.matsubara(64)
+    assert np.max(np.abs(qed.Green_function(z, label=label) - oracle.green_function(label, z))) < 1e-12
+    if qed.mixing(label) & 4:
+        assert np.max(np.abs(qed.Green_function(z, spin_down=True, label=label)
+                             - oracle.green_function(label, z, spin_down=True))) < 1e-12
+    assert abs(qed.Potthoff_functional(label) - oracle.potthoff(label)) < 1e-12
+    assert np.max(np.abs(qed.Green_function_average(label=label) - oracle.green_function_average(label))) < 1e-12
+    a1, a2 = qed.cluster_averages(label), oracle.cluster_averages(label)
+    assert [x[0] for x in a1] == [x[0] for x in a2]
+    for (n, v1, s1_), (_, v2, s2_) in zip(a1, a2):
+        assert abs(v1 - v2) < 1e-12, (name, n, v1, v2)
+        assert np.isnan(s1_) and np.isnan(s2_)

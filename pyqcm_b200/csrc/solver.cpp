@@ -478,13 +478,13 @@ bool cholesky_upper(int p, const double *G, std::vector<double> &R, std::vector<
 // half-bandwidth p. Its dimension only stops at multiples of p (the convergence
 // test runs at j % p == 0, and M0 is a multiple of p), so the stopping rule is
 // the same. Returns false, leaving phi intact, when a QR pivot falls below 1e-4
-// (a deflation the band algorithm must handle) or p > 16; the caller then runs
-// the band recurrence.
+// (a deflation the band algorithm must handle), for p > 16 and for p = 1; the
+// caller then runs the band recurrence.
 bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
                            std::vector<double> &evals, std::vector<double> &Q, int &Mout) {
   const size_t D = H.D;
   const int p = (int)phi.size();
-  if (p < 1 || p > 16) return false;
+  if (p < 2 || p > 16) return false;  // one start vector: nothing to amortise
   cudaStream_t s = ws.stream;
   int M0 = (int)(14 * p * std::log(1.0 * D));
   if (!(M0 > 1)) fail(QED_ERR_INTERNAL, "Assertion failed: M>1 in build_Q_matrix");

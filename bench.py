@@ -42,7 +42,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--solve", action="store_true", help="also time a full ground state of the 4x4 cluster")
+    ap.add_argument("--solve", action="store_true", help="time the full 4x4 solve also for N > 1")
+    ap.add_argument("--no-solve", action="store_true",
+                    help="skip the full 4x4 ground state + Green function timed by default at N = 1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the batched-solve metrics reported beside the H.v line")
@@ -255,7 +257,7 @@ def run_ours(args, world, rank, local):
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     ms, e2e_s = max_over_ranks([ms, e2e_s], world, device=f"cuda:{local}")
     solve = None
-    if args.solve:
+    if (args.solve or world == 1) and not args.no_solve:
         qed.set_global_parameter("GF_method", "L")
         qed.load_problem(prob, label + 100, model_name="bench_sq4x4", fmt="F")
         torch.cuda.synchronize()
@@ -269,6 +271,13 @@ def run_ours(args, world, rank, local):
                  "green_function_seconds": t2 - t1, "G_iw0_00": [G[0, 0, 0].real, G[0, 0, 0].imag],
                  "what": "4x4 ground state (Lanczos) + band-Lanczos (p=16) Green function on 256 Matsubara "
                          "frequencies, beta=50"}
+        fx = os.path.join(ROOT, "tests", "golden", "sq4x4_gs.json")
+        if os.path.exists(fx):  # the reference's own ground state of this sector
+            with open(fx) as f:
+                r = json.load(f)
+            solve["reference_ground_state"] = {"E0": r["E0"], "seconds": r["seconds"], "threads": r["threads"],
+                                               "where": "one core of the build host (fixture tests/golden/sq4x4_gs.json)"}
+            solve["E0_rel_diff"] = abs(e - r["E0"]) / abs(r["E0"])
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import ref

@@ -2,13 +2,16 @@
 ED (the compiled oracle, oracle/_ref) on the synthetic workloads.
 
     python tests/golden/make_golden.py            # small cases (seconds)
-    python tests/golden/make_golden.py --big      # 4x4 ground state (about 2 h on one core)
+    python tests/golden/make_golden.py --big      # 4x4 ground state (about 1.5 h on one core)
+    python tests/golden/make_golden.py --sq4x3    # 4x3 ground state + Green function (minutes)
 
 Fixtures:
   small_cases.npz : names, E0, G (256 Matsubara points, beta = 50) for
                     chain8 (band Lanczos and continued fraction), 2x3 with t',
                     2x4 with a Neel field (both spins), plaquette + 8 bath, chain10
   sq4x4_gs.json   : ground-state energy and sector of the 4x4 cluster (t'=0.3, U=8)
+  sq4x3_gf.npz    : 4x3 cluster (t'=0.3, U=8, half filling, dim 853776): E0, Potthoff
+                    functional and G on 64 Matsubara points (band Lanczos, p = 12)
 """
 import json
 import os
@@ -67,8 +70,24 @@ def big():
     print(out)
 
 
+def sq4x3():
+    prob = W.hubbard_cluster(4, 3, t=-1.0, tp=0.3, U=8.0, mu=4.0, name="sq4x3")
+    ref.set_param("GF_method", "L")
+    ref.load_problem(prob, 700, model_name="golden_sq4x3", fmt="F")
+    t = time.time()
+    e, sec = ref.ground_state(700)
+    z = W.matsubara(64)
+    G = ref.green_function(700, z)
+    om = ref.potthoff(700)
+    np.savez_compressed(os.path.join(HERE, "sq4x3_gf.npz"), E0=e, sector=sec, G=G, z=z, omega=om,
+                        seconds=time.time() - t)
+    print(e, sec, om, time.time() - t)
+
+
 if __name__ == "__main__":
     if "--big" in sys.argv:
         big()
+    elif "--sq4x3" in sys.argv:
+        sq4x3()
     else:
         small()

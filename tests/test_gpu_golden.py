@@ -53,3 +53,22 @@ def test_sq4x4_ground_state_against_fixture(qed, fresh):
     e, sec = qed.ground_state_solve(label)
     assert abs(e - ref["E0"]) <= 1e-10 * abs(ref["E0"])
     assert sec == ref["sector"]
+
+
+def test_sq4x3_green_function_against_fixture(qed, fresh):
+    """4x3 cluster (dim 853776, 12 start vectors): the block band-Lanczos path
+    against the reference's band Lanczos, E0 at 1e-10 and G(i w_n) at 1e-8."""
+    path = os.path.join(GOLDEN, "sq4x3_gf.npz")
+    if not os.path.exists(path):
+        pytest.skip("4x3 fixture not generated yet")
+    g = np.load(path, allow_pickle=False)
+    suffix, label = fresh()
+    qed.set_global_parameter("GF_method", "L")
+    qed.load_problem(W.hubbard_cluster(4, 3, t=-1.0, tp=0.3, U=8.0, mu=4.0, name="sq4x3"), label,
+                     model_name="gold_sq4x3" + suffix, fmt="F")
+    e, sec = qed.ground_state_solve(label)
+    assert abs(e - float(g["E0"])) <= 1e-10 * abs(float(g["E0"]))
+    assert sec == str(g["sector"])
+    G = qed.Green_function(g["z"], label=label)
+    assert np.max(np.abs(G - g["G"])) < 1e-8
+    assert abs(qed.Potthoff_functional(label) - float(g["omega"])) < 1e-9

@@ -202,9 +202,13 @@ int batch_ground_states(BatchSet &b, int threads) {
       tasks.push_back({(double)I->sector_dim(sp->sec), [I, sp] { I->state_vector(*sp, ws()); }});
     }
   if ((rc = run_tasks(tasks, threads)) != QED_OK) return rc;
-  return guarded([&] {
-    for (Instance *I : todo) I->finish_gs(ws());
-  });
+  tasks.clear();
+  for (Instance *I : todo) {  // operator averages, one task per instance
+    double cost = 0.0;
+    for (auto &st : I->states) cost += (double)I->sector_dim(st->sec);
+    tasks.push_back({cost * (double)I->value.size(), [I] { I->finish_gs(ws()); }});
+  }
+  return run_tasks(tasks, threads);
 }
 
 // Green functions of a batch: each Q-matrix half (state, spin, hole/electron)

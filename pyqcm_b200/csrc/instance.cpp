@@ -248,7 +248,7 @@ std::vector<Instance::SusQ> Instance::susceptibility_qmatrices(const std::string
       if (!(st->sec == sec)) continue;
       SectorOp H(terms, sec, ws, &tables);
       if (H.D == 0) continue;
-      SectorOp O(t, sec, ws);
+      SectorOp O(t, sec, ws, &op_tables[opname]);
       std::vector<DevBuf<double>> b(1);
       b[0].alloc(H.D);
       SubList none;
@@ -548,13 +548,14 @@ void Instance::state_vector(State &st, Workspace &ws) {
 // O psi is one H.v with the operator's own tables and the <x,y>, <y,y>
 // reductions of the column pass.
 void Instance::finish_gs(Workspace &ws) {
+  PhaseScope ps(kPhAverages);
   averages.clear();
   for (auto &v : value) {
     const Operator &op = *model->term.at(v.first);
     const SpinData t = collect_terms(*model, {{v.first, 1.0}});
     double ave = 0.0, var = 0.0;
     for (auto &st : states) {
-      SectorOp O(t, st->sec, ws);
+      SectorOp O(t, st->sec, ws, &op_tables[v.first]);
       if (O.D == 0) continue;
       DevBuf<double> y(O.D);
       SubList none;

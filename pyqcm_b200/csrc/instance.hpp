@@ -73,6 +73,7 @@ struct Instance {
   std::vector<std::shared_ptr<State>> states;
   SpinData terms;
   HalfCache tables;  // spin tables shared by the sectors of this instance
+  std::map<std::string, HalfCache> op_tables;  // the same for each operator alone (averages, susceptibility)
   std::vector<double> tc[2], tb[2], tcb[2];  // cluster, bath (diagonalised), cluster-bath
   std::vector<double> tb_nd[2], tcb_nd[2];   // bath and cluster-bath before the bath diagonalisation
   std::vector<cplx> Mave[2];

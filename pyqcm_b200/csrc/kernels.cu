@@ -30,6 +30,9 @@ void ensure_binom() {
     for (int n = 0; n <= 32; ++n)
       for (int k = 0; k <= 32; ++k) h[n][k] = (uint32_t)binom(n, k);
     QED_CUDA(cudaMemcpyToSymbol(c_binom, h, sizeof(h)));
+    // the copy runs on the legacy stream, which the solver's non-blocking
+    // streams do not wait for: finish it before any kernel reads the table
+    QED_CUDA(cudaDeviceSynchronize());
   });
 }
 
@@ -810,6 +813,57 @@ __global__ void __launch_bounds__(kUpThreads) k_block_up(HvOperator op, int p, c
   }
 }
 
+// The same rows pass when one dn-row of X (du * p doubles) fits in shared
+// memory: a CTA stages its row with coalesced loads and gathers the hops from
+// shared memory. Thread t of the row handles entry (u, c) = (t / p, t % p), so
+// the p threads of a state share its table entries (one broadcast load).
+constexpr size_t kBlockRowSmemMax = 200 * 1024;
+__global__ void __launch_bounds__(1024) k_block_up_smem(HvOperator op, int p, const double *__restrict__ X,
+                                                        double *__restrict__ Y, const double *__restrict__ X2,
+                                                        const double *__restrict__ M2, double s2) {
+  extern __shared__ double xs[];  // [du * p]
+  __shared__ double uvals[256], m2[256];
+  for (int i = threadIdx.x; i < op.up.nvals; i += blockDim.x) uvals[i] = op.up.vals[i];
+  if (X2)
+    for (int i = threadIdx.x; i < p * p; i += blockDim.x) m2[i] = M2[i];
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const uint32_t n = du * (uint32_t)p;  // entries of one row (du * p * 8 bytes fit in shared memory)
+  for (uint32_t d = blockIdx.x; d < dd; d += gridDim.x) {
+    const size_t rowb = (size_t)d * du;
+    const double *xr = X + rowb * p;
+    __syncthreads();  // the previous row's gathers are done
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) xs[i] = xr[i];
+    __syncthreads();
+    const double ddg = op.dn.diag[d];
+    const uint32_t dnb = op.dn.bits[d];
+    for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
+      const uint32_t u = t / p, c = t - u * p;
+      double acc = (op.up.diag[u] + ddg + inter_term(op.inter, op.up.bits[u], dnb)) * xs[t];
+      const int cu = op.up.cnt[u];
+      double a1 = 0.0;
+      int k = 0;
+      for (; k + 2 <= cu; k += 2) {
+        const uint32_t e0 = __ldg(op.up.ell + (size_t)k * du + u);
+        const uint32_t e1 = __ldg(op.up.ell + (size_t)(k + 1) * du + u);
+        acc += uvals[e0 & 255u] * xs[(e0 >> 8) * p + c];
+        a1 += uvals[e1 & 255u] * xs[(e1 >> 8) * p + c];
+      }
+      if (k < cu) {
+        const uint32_t e = __ldg(op.up.ell + (size_t)k * du + u);
+        acc += uvals[e & 255u] * xs[(e >> 8) * p + c];
+      }
+      acc += a1;
+      if (X2) {
+        const double *x2 = X2 + (rowb + u) * p;
+        double s = 0.0;
+        for (int i = 0; i < p; ++i) s += x2[i] * m2[i * p + c];
+        acc += s2 * s;
+      }
+      Y[rowb * p + t] = acc;
+    }
+  }
+}
+
 // Down-spin hops of a block H.v, Y += (dn hops) X: work items (chunk of
 // kThreads / P up strings, dn-row d) in chunk-major order, so the chunk's
 // columns of X for all rows (dd * chunk * p * 8 bytes) stay in L2 while its
@@ -956,6 +1010,62 @@ __global__ void k_finalize_ld(const double *partials, int nblocks, int ld, doubl
     __syncthreads();
   }
   if (threadIdx.x == 0) out[slot] = sm[0];
+}
+
+// Cholesky factor of a p x p Gram matrix (p <= 16, row-major): R upper
+// triangular with G = R^T R, and R^{-1}; the kernel exists so that the block
+// recurrence needs no host round trip for its QR. One CTA of 256 threads,
+// thread (r, c) owning entry r * p + c: p right-looking elimination steps in
+// shared memory (each entry receives the same subtractions, in the same order,
+// as the row-by-row host factorisation), then one back substitution per column
+// of R^{-1}. A diagonal that is not positive, or a pivot below pivot_min, sets
+// *fail_flag = 1 and zeroes R^{-1}. With Rprev given, also B = R Rprev (upper
+// triangular) into B_out and its transpose into Bt_out.
+__global__ void __launch_bounds__(256) k_block_chol(int p, const double *G, double pivot_min, double *R,
+                                                    double *Rinv, const double *Rprev, double *B_out,
+                                                    double *Bt_out, double *fail_flag) {
+  __shared__ double a[256], ri[256];
+  __shared__ int bad;
+  const int t = threadIdx.x, pp = p * p;
+  const int r = t / p, c = t - (t / p) * p;  // valid for t < pp
+  if (t < pp) a[t] = G[t];
+  if (t == 0) bad = 0;
+  __syncthreads();
+  for (int i = 0; i < p; ++i) {
+    __syncthreads();                // the updates of step i - 1 are done
+    const double d = a[i * p + i];  // fully updated by steps 0..i-1
+    const bool ok = d > 0.0;
+    const double rii = ok ? sqrt(d) : 1.0;
+    if (t == 0 && (!ok || rii < pivot_min)) bad = 1;
+    __syncthreads();  // everyone has read a[i][i]
+    if (t < pp && r == i) a[t] = (c == i) ? rii : (c > i ? a[t] / rii : 0.0);
+    __syncthreads();  // row i of R is final
+    if (t < pp && r > i && c >= r) a[t] -= a[i * p + r] * a[i * p + c];
+  }
+  __syncthreads();
+  // R^{-1}: column c by back substitution from row c up (thread c)
+  if (t < p) {
+    for (int i = t; i >= 0; --i) {
+      double acc = 0.0;
+      for (int k = i + 1; k <= t; ++k) acc += a[i * p + k] * ri[k * p + t];
+      ri[i * p + t] = (i == t) ? 1.0 / a[i * p + i] : -acc / a[i * p + i];
+    }
+    for (int i = t + 1; i < p; ++i) ri[i * p + t] = 0.0;
+  }
+  __syncthreads();
+  if (t < pp) {
+    const double rv = (c >= r) ? a[t] : 0.0;
+    R[t] = rv;
+    Rinv[t] = bad ? 0.0 : ri[t];
+    if (Rprev) {
+      double acc = 0.0;
+      for (int k = r; k <= c; ++k) acc += a[r * p + k] * Rprev[k * p + c];
+      const double b = (c >= r) ? acc : 0.0;
+      B_out[t] = b;
+      Bt_out[c * p + r] = b;
+    }
+  }
+  if (t == 0 && bad) *fail_flag = 1.0;
 }
 
 // -------------------------------------------------------- Green functions ----
@@ -1241,8 +1351,24 @@ void launch_block_hv(const HvOperator &op, int p, const double *X, double *Y, co
                      double s2, cudaStream_t s) {
   const int P = block_pow2(p);
   const int sms = device_sms();
-  const int up_grid = std::max(kRowParts, (sms / kRowParts) * kRowParts);
-  QED_BLOCK_DISPATCH(P, (k_block_up<PP><<<up_grid, kUpThreads, 0, s>>>(op, p, X, Y, X2, M2, s2)));
+  const size_t row_bytes = (size_t)op.up.dim * p * sizeof(double);
+  if (row_bytes <= kBlockRowSmemMax && op.dn.dim > 0) {
+    static const bool attr = [] {
+      QED_CUDA(cudaFuncSetAttribute(k_block_up_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kBlockRowSmemMax));
+      return true;
+    }();
+    (void)attr;
+    const uint32_t n = op.up.dim * (uint32_t)p;
+    const int threads = n >= 1024 ? 1024 : (int)((n + 31) / 32 * 32);
+    const int by_threads = std::max(1, 2048 / threads);
+    const int by_smem = std::max<int>(1, (int)((228 * 1024) / (row_bytes + 4 * 1024)));
+    const int grid = (int)std::min<size_t>(op.dn.dim, (size_t)sms * std::min(by_threads, by_smem));
+    k_block_up_smem<<<grid, threads, row_bytes, s>>>(op, p, X, Y, X2, M2, s2);
+  } else {
+    const int up_grid = std::max(kRowParts, (sms / kRowParts) * kRowParts);
+    QED_BLOCK_DISPATCH(P, (k_block_up<PP><<<up_grid, kUpThreads, 0, s>>>(op, p, X, Y, X2, M2, s2)));
+  }
   QED_LAUNCH();
   QED_BLOCK_DISPATCH(P, (k_block_dn<PP><<<sms * 8, kThreads, 0, s>>>(op, p, X, Y)));
   QED_LAUNCH();
@@ -1268,6 +1394,13 @@ int launch_block_muladd(size_t D, int p, double a, double *Y, double s1, const d
 
 void launch_finalize_ld(const double *partials, int nblocks, int ld, int n, double *out, cudaStream_t s) {
   k_finalize_ld<<<n, kThreads, 0, s>>>(partials, nblocks, ld, out);
+  QED_LAUNCH();
+}
+
+void launch_block_chol(int p, const double *G, double pivot_min, double *R, double *Rinv, const double *Rprev,
+                       double *B_out, double *Bt_out, double *fail_flag, cudaStream_t s) {
+  if (p < 1 || p > 16) fail(QED_ERR_ARGUMENT, "launch_block_chol: block size outside [1, 16]");
+  k_block_chol<<<1, 256, 0, s>>>(p, G, pivot_min, R, Rinv, Rprev, B_out, Bt_out, fail_flag);
   QED_LAUNCH();
 }
 

@@ -130,6 +130,10 @@ int launch_block_muladd(size_t D, int p, double a, double *Y, double s1, const d
                         int gram, double *partials, int ld, int max_blocks, cudaStream_t s);
 // out[0..n) = fixed-order sums of partials with row stride ld
 void launch_finalize_ld(const double *partials, int nblocks, int ld, int n, double *out, cudaStream_t s);
+// G = R^T R on the device (p <= 16): R, R^{-1}; *fail = 1 if G is not positive
+// definite or a pivot is below pivot_min; with Rprev, B = R Rprev and B^T
+void launch_block_chol(int p, const double *G, double pivot_min, double *R, double *Rinv, const double *Rprev,
+                       double *B_out, double *Bt_out, double *fail_flag, cudaStream_t s);
 
 // ---- H.v ------------------------------------------------------------------
 // Row pass: y = (diag + up hops) x - sum_k sub.c[k] sub.z[k]   (x scaled by xs)

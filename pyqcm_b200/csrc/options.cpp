@@ -49,9 +49,15 @@ struct Table {
     i["max_iter_BL"] = 600;
     i["max_iter_CF"] = 400;
     i["max_iter_lanczos"] = 1000;
-    // solver option (not in the reference): band-Lanczos sectors with at least
-    // this many states run the block form of the recurrence (p vectors per H.v)
-    i["block_lanczos_min_dim"] = 100000;
+    // solver options (not in the reference): band-Lanczos sectors with at least
+    // block_lanczos_min_dim states and at least block_lanczos_min_p start
+    // vectors run the block form of the recurrence (p vectors per H.v). Measured
+    // on a B200 (Green function of one instance, band against block form): p = 8,
+    // 4900 states 83 / 57 ms; p = 10, 63504 states 107 / 68 ms; p = 12, 853776
+    // states 588 / 432 ms; p = 4, 16 concurrent 853776-state instances, 32.8 / 32.7
+    // solves/s. Smaller p and sectors were not measured.
+    i["block_lanczos_min_dim"] = 1000;
+    i["block_lanczos_min_p"] = 4;
     i["seed"] = 0;
     i["GF_lookup_depth"] = 64;
     c["Hamiltonian_format"] = 'E';

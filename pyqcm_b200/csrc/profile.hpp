@@ -19,6 +19,7 @@ enum Phase {
   kPhRitz,          // ground-state Lanczos: host Ritz tests (inside kPhGsLanczos)
   kPhBlockLoop,     // block form of the band-Lanczos recurrence
   kPhBlockFallback, // block recurrence abandoned for the band one (count)
+  kPhAverages,      // operator averages of the ground state (cluster_averages)
   kPhCount
 };
 

@@ -40,6 +40,7 @@ Workspace::~Workspace() {
   out.release();
   if (stream) cudaStreamSynchronize(stream);
   if (host) cudaFreeHost(host);
+  if (pin) cudaFreeHost(pin);
   if (tls_stream == stream) tls_stream = nullptr;
   if (stream) cudaStreamDestroy(stream);
 }
@@ -51,6 +52,18 @@ const double *Workspace::sums(int nblocks, int nred) {
 }
 
 void Workspace::sync() { QED_CUDA(cudaStreamSynchronize(stream)); }
+
+double *Workspace::pinned(size_t n) {
+  if (n > pin_n) {
+    sync();  // the old buffer may still be a copy's destination
+    if (pin) cudaFreeHost(pin);
+    pin = nullptr;
+    pin_n = 0;
+    QED_CUDA(cudaMallocHost(&pin, n * sizeof(double)));
+    pin_n = n;
+  }
+  return pin;
+}
 
 // ------------------------------------------------------------- SectorOp ------
 
@@ -499,8 +512,8 @@ bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<
   constexpr double kPivotMin = 1e-4;
   const int pp = p * p;
   const int max_blocks = 4096;
-  DevBuf<double> part((size_t)max_blocks * pp), dsmall(4 * (size_t)pp);
-  double *dG = dsmall.p, *dM = dsmall.p + pp, *dB = dsmall.p + 2 * pp;
+  DevBuf<double> part((size_t)max_blocks * pp), dsmall(2 * (size_t)pp);
+  double *dG = dsmall.p, *dM = dsmall.p + pp;
   std::vector<double> hG(pp), R1, R1i, R2, R2i;
   auto gram_to_host = [&](int nb) {
     launch_finalize_ld(part.p, nb, pp, pp, dG, s);
@@ -546,28 +559,63 @@ bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<
   const std::vector<double> P(hG);  // row-major [k][i]
   std::vector<double> t((size_t)M0 * M0, 0.0);
   auto T = [&](int r, int c) -> double & { return t[(size_t)r + (size_t)M0 * c]; };
-  std::vector<double> Bk;  // B of the QR that produced V_k (none for k = 0)
+  // The steps run on the device with their QR: the p x p Cholesky factors are
+  // computed by k_block_chol, so a step needs no host value. Step k leaves
+  // rec_k = [A_k | B_{k+1} | QR failed] in device memory; the host reads it
+  // once, fills T and runs the convergence test while step k + 1, enqueued
+  // beforehand, runs on the GPU. A step enqueued past the stopping point is
+  // discarded.
+  const int nsteps = M0 / p;  // the last step (jdim = M0) needs no QR
+  const int ldr = 2 * pp + 1;
+  DevBuf<double> drec((size_t)ldr * nsteps), dqr(5 * (size_t)pp);
+  QED_CUDA(cudaMemsetAsync(drec.p, 0, drec.bytes(), s));
+  double *dR1 = dqr.p, *dR1i = dqr.p + pp, *dR2 = dqr.p + 2 * pp, *dR2i = dqr.p + 3 * pp, *dBt = dqr.p + 4 * pp;
+  double *hrec = ws.pinned(2 * (size_t)ldr);
+  cudaEvent_t ev[2];
+  QED_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  QED_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  struct Events {
+    cudaEvent_t *e;
+    ~Events() {
+      cudaEventDestroy(e[0]);
+      cudaEventDestroy(e[1]);
+    }
+  } ev_guard{ev};
+  auto enqueue = [&](int k) {
+    // W = H V_k - V_{k-1} B_k^T
+    if (k > 0)
+      launch_block_hv(H.op, p, Vk, W, Vprev, dBt, -1.0, s);
+    else
+      launch_block_hv(H.op, p, Vk, W, nullptr, nullptr, 0.0, s);
+    // A_k = V_k^T W ; W -= V_k A_k (with the gram of the result for the QR)
+    double *rk = drec.p + (size_t)ldr * k;
+    int nbk = launch_block_gram(D, p, Vk, W, part.p, pp, max_blocks, s);
+    launch_finalize_ld(part.p, nbk, pp, pp, rk, s);
+    nbk = launch_block_muladd(D, p, 1.0, W, -1.0, Vk, rk, 1, part.p, pp, max_blocks, s);
+    if ((k + 1) * p < M0) {
+      // W = V_{k+1} B_{k+1}, Cholesky QR twice, through V_{k-1}'s buffer
+      launch_finalize_ld(part.p, nbk, pp, pp, dG, s);
+      launch_block_chol(p, dG, kPivotMin, dR1, dR1i, nullptr, nullptr, nullptr, rk + 2 * pp, s);
+      nbk = launch_block_muladd(D, p, 0.0, Vprev, 1.0, W, dR1i, 1, part.p, pp, max_blocks, s);
+      launch_finalize_ld(part.p, nbk, pp, pp, dG, s);
+      launch_block_chol(p, dG, 0.0, dR2, dR2i, dR1, rk + pp, dBt, rk + 2 * pp, s);
+      launch_block_muladd(D, p, 0.0, W, 1.0, Vprev, dR2i, 0, part.p, pp, max_blocks, s);
+    }
+    QED_CUDA(cudaMemcpyAsync(hrec + (size_t)ldr * (k & 1), rk, ldr * sizeof(double), cudaMemcpyDeviceToHost, s));
+    QED_CUDA(cudaEventRecord(ev[k & 1], s));
+    double *nv = W;  // V_{k+1}
+    W = Vprev;
+    Vprev = Vk;
+    Vk = nv;
+  };
   double ev_old = 1e12;
   int jdim = 0;
   PhaseScope ps_loop(kPhBlockLoop);
+  enqueue(0);
   for (int k = 0;; ++k) {
-    // W = H V_k - V_{k-1} B_k^T
-    if (k > 0) {
-      std::vector<double> Bt(pp);
-      for (int i = 0; i < p; ++i)
-        for (int c = 0; c < p; ++c) Bt[i * p + c] = Bk[c * p + i];
-      upload(dB, Bt);
-      launch_block_hv(H.op, p, Vk, W, Vprev, dB, -1.0, s);
-    } else {
-      launch_block_hv(H.op, p, Vk, W, nullptr, nullptr, 0.0, s);
-    }
-    // A_k = V_k^T W ; W -= V_k A_k (with the gram of the result for the QR)
-    nb = launch_block_gram(D, p, Vk, W, part.p, pp, max_blocks, s);
-    launch_finalize_ld(part.p, nb, pp, pp, dM, s);
-    QED_CUDA(cudaMemcpyAsync(hG.data(), dM, pp * sizeof(double), cudaMemcpyDeviceToHost, s));
-    nb = launch_block_muladd(D, p, 1.0, W, -1.0, Vk, dM, 1, part.p, pp, max_blocks, s);
-    ws.sync();
-    const std::vector<double> A(hG);
+    if ((k + 1) * p < M0) enqueue(k + 1);  // runs while the host handles step k
+    QED_CUDA(cudaEventSynchronize(ev[k & 1]));
+    const double *A = hrec + (size_t)ldr * (k & 1);
     for (int i = 0; i < p; ++i)
       for (int c = 0; c < p; ++c) T(k * p + i, k * p + c) = 0.5 * (A[i * p + c] + A[c * p + i]);
     jdim = (k + 1) * p;
@@ -577,31 +625,29 @@ bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<
     }
     if (jdim >= 4 * p) {  // bandLanczos step (12) at j = jdim, on the leading jdim x jdim block
       PhaseScope ps_check(kPhBandCheck);
-      std::vector<double> Hpr((size_t)jdim * jdim), ev;
+      std::vector<double> Hpr((size_t)jdim * jdim), evs;
       for (int c = 0; c < jdim; ++c)
         for (int r = 0; r < jdim; ++r) Hpr[(size_t)r + (size_t)jdim * c] = T(r, c);
-      if (!band_eigenvalues(jdim, p, Hpr, ev)) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
-      const double test = std::fabs(ev[0] - ev_old);
-      ev_old = ev[0];
-      if (jdim > 1 && ev[1] - ev[0] < min_gap && no_degenerate)
+      if (!band_eigenvalues(jdim, p, Hpr, evs)) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
+      const double test = std::fabs(evs[0] - ev_old);
+      ev_old = evs[0];
+      if (jdim > 1 && evs[1] - evs[0] < min_gap && no_degenerate) {
+        ws.sync();
         fail(QED_ERR_LANCZOS, "band Lanczos: the gap between the first two eigenvalues is smaller than " +
                                   std::to_string(min_gap));
+      }
       if (test < accur_bl) break;
     }
-    // W = V_{k+1} B_{k+1} (through V_{k-1}'s buffer, no longer needed)
-    gram_to_host(nb);
-    std::vector<double> Bn;
-    if (!cholqr2(W, Vprev, W, Bn)) return false;
+    if (A[2 * pp] != 0.0) {  // a QR pivot below kPivotMin: the band recurrence takes over
+      ws.sync();
+      return false;
+    }
+    const double *Bn = A + pp;
     for (int r = 0; r < p; ++r)
       for (int c = r; c < p; ++c) {
         T((k + 1) * p + r, k * p + c) = Bn[r * p + c];
         T(k * p + c, (k + 1) * p + r) = Bn[r * p + c];
       }
-    double *nv = W;  // V_{k+1}
-    W = Vprev;
-    Vprev = Vk;
-    Vk = nv;
-    Bk = Bn;
   }
   ws.sync();
   for (auto &f : phi) f.release();
@@ -632,7 +678,7 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
     Mout = 0;
     return false;
   }
-  if ((long)D >= opt_int("block_lanczos_min_dim")) {
+  if ((long)D >= opt_int("block_lanczos_min_dim") && p >= opt_int("block_lanczos_min_p")) {
     if (block_lanczos_qmatrix(H, ws, phi, evals, Q, Mout)) return true;
     if (profiling()) profile_add(kPhBlockFallback, 0.0);
   }

@@ -23,8 +23,12 @@ struct Workspace {
   Reducer red;
   DevBuf<double> partials, out;
   double *host = nullptr;
+  double *pin = nullptr;  // pinned host staging, grown on demand
+  size_t pin_n = 0;
   Workspace();
   ~Workspace();
+  // pinned host buffer of at least n doubles (contents not kept on growth)
+  double *pinned(size_t n);
   // finalize + wait: returns host pointer with nred sums
   const double *sums(int nblocks, int nred);
   void sync();

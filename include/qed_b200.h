@@ -112,6 +112,22 @@ int qed_Green_function_dimension(int label, int *dim);
  * dim x dim complex, column-major, evaluated on the GPU. */
 int qed_Green_function(int label, int spin_down, int nz, const double *z, double *G);
 
+/* The wavevector sum of the self-energy-functional integrand on a fixed grid, per
+ * frequency: lattice_model_instance::SEF_integrand_k (src_qcm/lattice_model_instance.cpp:618-640)
+ * under QCM::k_integral_grid (src_util/integrate.cpp:177-240), as Potthoff_functional's
+ * discrete-grid path uses them (src_qcm/lattice_model_instance.cpp:520-545).
+ * For each of the nw frequencies w[i] (the point i*w[i] on the imaginary axis):
+ *   I_w[i] = 1/Nk sum_k log |det(V(k) G(i w[i]) - 1)|,  k = (a/nkx, b/nky, c/nkz),
+ *   V(k) = V0 + sum_e v[e] exp(2 pi i k.R[e]) at row r[e], column c[e]   (set_V, src_qcm/CPT.cpp:22-64),
+ * with G the cluster Green function of ED instance `label` (spin_down selects the
+ * down block under up_down mixing), V0 dim x dim complex column-major (the
+ * k-independent part of V), R[3 e..3 e + 2] integer superlattice coordinates and
+ * v[e] complex (interleaved). G and the nw x Nk determinants are computed on the GPU;
+ * dim (at most 16) must be the cluster's Green-function dimension. */
+int qed_sef_integrand_grid(int label, int spin_down, int dim, const double *V0, int nel, const int *r, const int *c,
+                           const int *R, const double *v, int nw, const double *w, int nkx, int nky, int nkz,
+                           double *I_w);
+
 /* ED::self_energy (src_ed/qcm_ED.hpp:180 -> src_ed/model_instance.hpp:683-700), batched. */
 int qed_self_energy(int label, int spin_down, int nz, const double *z, double *S);
 

@@ -75,6 +75,33 @@ def lib():
             f = getattr(L, name)
             f.argtypes = args
             f.restype = C.c_int
+        cpp = C.POINTER(C.c_char_p)
+        sig.update({
+            "ref_qcm_great_reset": [],
+            "ref_qcm_add_cluster": [lp, C.c_int, lp, C.c_int, C.c_int],
+            "ref_qcm_add_system": [C.c_char_p, C.c_int],
+            "ref_qcm_lattice_model": [C.c_char_p, C.c_int, lp, lp],
+            "ref_qcm_hopping_operator": [C.c_char_p, lp, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int],
+            "ref_qcm_interaction_operator": [C.c_char_p, lp, C.c_double, C.c_int, C.c_int, C.c_char_p],
+            "ref_qcm_density_wave": [C.c_char_p, C.c_char_p, dp, lp, C.c_double, C.c_int, C.c_double],
+            "ref_qcm_set_target_sectors": [C.c_int, cpp],
+            "ref_qcm_set_parameters": [C.c_int, cpp, dp, C.c_int, cpp, dp, cpp],
+            "ref_qcm_set_parameter": [C.c_char_p, C.c_double],
+            "ref_qcm_new_model_instance": [C.c_int],
+            "ref_qcm_erase_instance": [C.c_int],
+            "ref_qcm_dims": [ip, ip, ip],
+            "ref_qcm_set_wavevector_grid": [C.c_int, C.c_int, C.c_int],
+            "ref_qcm_frequency_grid": [C.c_int, dp, dp],
+            "ref_qcm_potthoff": [C.c_int, dp],
+            "ref_qcm_cluster_hopping": [C.c_int, C.c_int, C.c_int, ip, dp],
+            "ref_qcm_V_superdual": [C.c_int, C.c_int, C.c_double, C.c_double, dp, ip, dp],
+            "ref_qcm_cluster_gf": [C.c_int, C.c_int, C.c_double, C.c_double, ip, dp],
+            "ref_qcm_ed_label": [C.c_int, C.c_int],
+        })
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
         L.ref_hv_create.argtypes = [C.c_int, C.c_char_p, lp]
         L.ref_hv_create.restype = C.c_void_p
         L.ref_hv_destroy.argtypes = [C.c_void_p]
@@ -363,3 +390,101 @@ class RefHamiltonian:
         if getattr(self, "h", None):
             lib().ref_hv_destroy(self.h)
             self.h = None
+
+
+# ------------------------------------------------------------ lattice layer --
+# The reference's lattice layer (namespace QCM, src_qcm) holds ONE lattice model
+# per process (src_qcm/QCM.cpp:34); load_lattice starts from QCM::great_reset,
+# which also clears the ED models and instances (src_qcm/QCM.cpp:81-92).
+
+def _strs(xs):
+    return (C.c_char_p * max(1, len(xs)))(*[x.encode() for x in xs])
+
+
+def _longs(xs):
+    xs = [int(v) for v in xs]
+    return (C.c_long * max(1, len(xs)))(*xs)
+
+
+def load_lattice(prob, label: int = 0, cluster_name: str = "clus"):
+    """Builds `prob` (a workloads.LatticeProblem) the way pyqcm does
+    (cluster_model -> cluster -> lattice_model -> operators -> set_target_sectors
+    -> set_parameters, pyqcm/__init__.py:107-600) and creates instance `label`."""
+    L = lib()
+    _check(L.ref_qcm_great_reset())
+    new_model(cluster_name, prob.n_sites, 0)
+    pos = [c for s in prob.sites for c in s]
+    _check(L.ref_qcm_add_cluster(_longs([0, 0, 0]), prob.n_sites, _longs(pos), -1, 0))
+    _check(L.ref_qcm_add_system(cluster_name.encode(), 0))
+    sl = [c for v in prob.superlattice for c in v]
+    _check(L.ref_qcm_lattice_model(prob.name.encode(), len(prob.superlattice), _longs(sl), None))
+    for name in prob.interactions:
+        _check(L.ref_qcm_interaction_operator(name.encode(), None, 1.0, 1, 1, b"Hubbard"))
+    for name, link, amp in prob.hoppings:
+        _check(L.ref_qcm_hopping_operator(name.encode(), _longs(link), float(amp), 1, 1, 1, 0))
+    for name, typ, Q in prob.density_waves:
+        q = np.asarray(Q, dtype=np.float64)
+        _check(L.ref_qcm_density_wave(name.encode(), typ.encode(), _dp(q), None, 1.0, 0, 0.0))
+    _check(L.ref_qcm_set_target_sectors(1, _strs([prob.sectors])))
+    names = list(prob.params)
+    vals = np.array([prob.params[k] for k in names], dtype=np.float64)
+    en = [e[0] for e in prob.equiv]
+    em = np.array([e[1] for e in prob.equiv] or [0.0], dtype=np.float64)
+    er = [e[2] for e in prob.equiv]
+    _check(L.ref_qcm_set_parameters(len(names), _strs(names), _dp(vals), len(en), _strs(en), _dp(em), _strs(er)))
+    _check(L.ref_qcm_new_model_instance(label))
+
+
+def lattice_new_instance(label: int, **values):
+    """Sets independent parameters, then creates lattice instance `label`."""
+    for k, v in values.items():
+        _check(lib().ref_qcm_set_parameter(k.encode(), float(v)))
+    _check(lib().ref_qcm_new_model_instance(label))
+
+
+def lattice_dims():
+    m, d, n = C.c_int(), C.c_int(), C.c_int()
+    _check(lib().ref_qcm_dims(C.byref(m), C.byref(d), C.byref(n)))
+    return m.value, d.value, n.value
+
+
+def set_grids(freqs, weights, nk):
+    f = np.ascontiguousarray(freqs, dtype=np.float64)
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    _check(lib().ref_qcm_frequency_grid(len(f), _dp(f), _dp(w)))
+    nk = tuple(nk) + (1,) * (3 - len(tuple(nk)))
+    _check(lib().ref_qcm_set_wavevector_grid(*[int(v) for v in nk]))
+
+
+def lattice_potthoff(label: int) -> float:
+    om = C.c_double()
+    _check(lib().ref_qcm_potthoff(label, C.byref(om)))
+    return om.value
+
+
+def _cmat(fn, *args):
+    d = C.c_int()
+    _check(fn(*args, C.byref(d), None))
+    out = np.zeros(2 * d.value * d.value)
+    _check(fn(*args, C.byref(d), _dp(out)))
+    n = d.value
+    return (out[0::2] + 1j * out[1::2]).reshape(n, n, order="F")
+
+
+def lattice_cluster_hopping(label: int, spin_down=False, clus=0):
+    return _cmat(lib().ref_qcm_cluster_hopping, label, clus, int(spin_down))
+
+
+def lattice_V(label: int, w: complex, k, spin_down=False):
+    """V(k) at frequency w for k in the superdual basis (fractions of the reduced zone)."""
+    kk = np.zeros(3)
+    kk[:len(k)] = k
+    return _cmat(lib().ref_qcm_V_superdual, label, int(spin_down), w.real, w.imag, _dp(kk))
+
+
+def lattice_cluster_gf(label: int, w: complex, spin_down=False):
+    return _cmat(lib().ref_qcm_cluster_gf, label, int(spin_down), w.real, w.imag)
+
+
+def lattice_ed_label(label: int, s: int = 0) -> int:
+    return lib().ref_qcm_ed_label(label, s)

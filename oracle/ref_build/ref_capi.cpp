@@ -22,8 +22,17 @@
 #include "qcm_ED.hpp"
 #include "model_instance.hpp"
 #include "global_parameter.hpp"
+#include "QCM.hpp"
+#include "lattice_model.hpp"
+#include "lattice_model_instance.hpp"
 
 namespace QCM { void global_parameter_init(); }
+
+// Globals of the reference's lattice layer (src_qcm/QCM.cpp:34-41).
+extern shared_ptr<lattice_model> qcm_model;
+extern map<int, unique_ptr<lattice_model_instance>> lattice_model_instances;
+extern vector<double> grid_freqs;
+extern vector<double> grid_weights;
 
 // Globals defined by the reference at src_ed/qcm_ED.cpp:25-26.
 extern map<string, shared_ptr<model>> models;
@@ -68,7 +77,11 @@ int ref_last_error(char *buf, int n) {
 }
 
 int ref_init(void) {
-  return guarded([] { QCM::global_parameter_init(); });
+  return guarded([] {
+    // QCM::qcm_init (src_python/qcm_lib.cpp:61-63) without the OpenMP banner
+    if (!qcm_model) qcm_model = make_shared<lattice_model>();
+    QCM::global_parameter_init();
+  });
 }
 
 int ref_set_int(const char *name, long v) {
@@ -417,5 +430,152 @@ int ref_hv_bench(void *h, int reps, double *checksum) {
 }
 
 void ref_hv_destroy(void *h) { delete (hv_handle *)h; }
+
+// ---- lattice layer (namespace QCM), argument conventions of the Python
+// binding src_python/qcm_wrap.hpp:57-260 (orbital labels from 1, vectors as
+// 3 integers, the unit cell defaulting to the identity) --------------------
+
+int ref_qcm_great_reset(void) {
+  return guarded([] { QCM::great_reset(); });
+}
+
+int ref_qcm_add_cluster(const long *cpos, int n, const long *pos, int ref, int conj) {
+  return guarded([&] {
+    vector<vector3D<int64_t>> p(n);
+    for (int i = 0; i < n; ++i) p[i] = vector3D<int64_t>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+    QCM::add_cluster(vector3D<int64_t>(cpos[0], cpos[1], cpos[2]), p, ref, conj != 0);
+  });
+}
+
+int ref_qcm_add_system(const char *name, int clus) {
+  return guarded([&] { QCM::add_system(name, clus); });
+}
+
+int ref_qcm_lattice_model(const char *name, int nvec, const long *super, const long *unit) {
+  return guarded([&] {
+    vector<int64_t> sl(super, super + 3 * nvec), uc(3 * nvec, 0);
+    if (unit)
+      uc.assign(unit, unit + 3 * nvec);
+    else
+      for (int i = 0; i < nvec; ++i) uc[4 * i] = 1;
+    QCM::new_lattice_model(name, sl, uc);
+  });
+}
+
+int ref_qcm_hopping_operator(const char *name, const long *link, double amp, int orb1, int orb2, int tau,
+                             int sigma) {
+  return guarded([&] {
+    vector3D<int64_t> lk(link[0], link[1], link[2]);
+    QCM::hopping_operator(name, lk, amp, orb1, orb2, tau, sigma);
+  });
+}
+
+int ref_qcm_interaction_operator(const char *name, const long *link, double amp, int orb1, int orb2,
+                                 const char *type) {
+  return guarded([&] {
+    vector3D<int64_t> lk(0, 0, 0);
+    if (link) lk = vector3D<int64_t>(link[0], link[1], link[2]);
+    QCM::interaction_operator(name, lk, amp, orb1, orb2, type);
+  });
+}
+
+int ref_qcm_density_wave(const char *name, const char *type, const double *Q, const long *link, double amp,
+                         int orb, double phase) {
+  return guarded([&] {
+    vector3D<int64_t> lk(0, 0, 0);
+    if (link) lk = vector3D<int64_t>(link[0], link[1], link[2]);
+    QCM::density_wave(name, lk, Complex(amp, 0.0), orb, vector3D<double>(Q[0], Q[1], Q[2]), phase, type);
+  });
+}
+
+int ref_qcm_set_target_sectors(int n, const char **sectors) {
+  return guarded([&] {
+    if ((size_t)n != qcm_model->nsys)
+      throw qcm_error("number of sector strings differs from the number of systems");
+    qcm_model->sector_strings.assign(sectors, sectors + n);
+  });
+}
+
+int ref_qcm_set_parameters(int nv, const char **names, const double *values, int ne, const char **enames,
+                           const double *mult, const char **refs) {
+  return guarded([&] {
+    vector<pair<string, double>> v;
+    for (int i = 0; i < nv; ++i) v.push_back({names[i], values[i]});
+    vector<tuple<string, double, string>> e;
+    for (int i = 0; i < ne; ++i) e.push_back({enames[i], mult[i], refs[i]});
+    QCM::set_parameters(v, e);
+  });
+}
+
+int ref_qcm_set_parameter(const char *name, double value) {
+  return guarded([&] { QCM::set_parameter(name, value); });
+}
+
+int ref_qcm_new_model_instance(int label) {
+  return guarded([&] { QCM::new_model_instance(label); });
+}
+
+int ref_qcm_erase_instance(int label) {
+  return guarded([&] { QCM::erase_lattice_model_instance((size_t)label); });
+}
+
+int ref_qcm_dims(int *mixing, int *dim_gf, int *nsys) {
+  return guarded([&] {
+    *mixing = QCM::mixing();
+    *dim_gf = (int)QCM::Green_function_dimension();
+    *nsys = (int)qcm_model->nsys;
+  });
+}
+
+int ref_qcm_set_wavevector_grid(int nkx, int nky, int nkz) {
+  return guarded([&] { QCM::set_wavevector_grid(nkx, nky, nkz); });
+}
+
+int ref_qcm_frequency_grid(int n, const double *freqs, const double *weights) {
+  return guarded([&] {
+    grid_freqs.assign(freqs, freqs + n);
+    grid_weights.assign(weights, weights + n);
+  });
+}
+
+int ref_qcm_potthoff(int label, double *omega) {
+  return guarded([&] { *omega = QCM::Potthoff_functional(label); });
+}
+
+// cluster one-body matrix of cluster `clus` (dim x dim complex, column-major)
+int ref_qcm_cluster_hopping(int label, int clus, int spin_down, int *dim, double *out) {
+  return guarded([&] {
+    auto h = QCM::cluster_hopping_matrix((size_t)clus, spin_down != 0, label);
+    *dim = (int)h.r;
+    if (out) put_complex(h, out);
+  });
+}
+
+// V(k) = t(k) - t' (src_qcm/CPT.cpp:22-64) at a wavevector given in the
+// superdual basis (fractions of the reduced zone, as the grid integral uses)
+int ref_qcm_V_superdual(int label, int spin_down, double w_re, double w_im, const double *k, int *dim,
+                        double *out) {
+  return guarded([&] {
+    auto &inst = *lattice_model_instances.at(label);
+    Green_function G = inst.cluster_Green_function(Complex(w_re, w_im), false, spin_down != 0);
+    Green_function_k M(G, vector3D<double>(k[0], k[1], k[2]));
+    inst.set_V(M);
+    *dim = (int)M.V.r;
+    if (out) put_complex(M.V, out);
+  });
+}
+
+// the cluster Green function the lattice layer uses (remixed), dim x dim
+int ref_qcm_cluster_gf(int label, int spin_down, double w_re, double w_im, int *dim, double *out) {
+  return guarded([&] {
+    auto &inst = *lattice_model_instances.at(label);
+    Green_function G = inst.cluster_Green_function(Complex(w_re, w_im), false, spin_down != 0);
+    *dim = (int)G.G.r;
+    if (out) put_complex(G.G.build_matrix(), out);
+  });
+}
+
+// ED label of system s of lattice instance `label` (nsys * label + s)
+int ref_qcm_ed_label(int label, int s) { return (int)(qcm_model->nsys * (size_t)label + (size_t)s); }
 
 }  // extern "C"

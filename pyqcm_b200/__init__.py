@@ -105,6 +105,8 @@ def lib():
         "qed_halfbasis": [C.c_int, C.c_int, up, lp],
         "qed_halfbasis_rank": [C.c_int, C.c_int, C.c_long, up, up],
         "qed_destroy_table": [C.c_int, C.c_int, C.c_int, C.c_int, lp, ip],
+        "qed_sef_integrand_grid": [C.c_int, C.c_int, C.c_int, dp, C.c_int, ip, ip, ip, dp, C.c_int, dp,
+                                   C.c_int, C.c_int, C.c_int, dp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -395,6 +397,27 @@ def Potthoff_functional(label: int = 0) -> float:
     w = C.c_double()
     _check(lib().qed_Potthoff_functional(label, C.byref(w)))
     return w.value
+
+
+def sef_integrand_grid(V0, r, c, R, v, w, nk, spin_down: bool = False, label: int = 0):
+    """Per frequency w[i]: 1/Nk sum_k log|det(V(k) G(i w[i]) - 1)| on the k grid nk
+    (see qed_sef_integrand_grid). V0: k-independent part of V (dim x dim);
+    (r, c, R, v): inter-cluster elements, R in superlattice coordinates."""
+    V0 = np.asfortranarray(V0, dtype=np.complex128)
+    dim = V0.shape[0]
+    n = len(r)
+    ri = np.ascontiguousarray(r, dtype=np.int32)
+    ci = np.ascontiguousarray(c, dtype=np.int32)
+    Ri = np.ascontiguousarray(np.reshape(R, (-1, 3)), dtype=np.int32) if n else np.zeros((1, 3), np.int32)
+    vv = np.ascontiguousarray(v, dtype=np.complex128) if n else np.zeros(1, np.complex128)
+    ww = np.ascontiguousarray(w, dtype=np.float64)
+    nk = tuple(int(x) for x in nk) + (1,) * (3 - len(tuple(nk)))
+    out = np.zeros(len(ww))
+    v0 = V0.ravel(order="F").view(np.float64)
+    _check(lib().qed_sef_integrand_grid(label, int(spin_down), dim, _dp(v0), n, _ip(ri if n else np.zeros(1, np.int32)),
+                                        _ip(ci if n else np.zeros(1, np.int32)), _ip(Ri), _dp(vv.view(np.float64)),
+                                        len(ww), _dp(ww), nk[0], nk[1], nk[2], _dp(out)))
+    return out
 
 
 def qmatrix(spin_down: bool = False, label: int = 0, capacity: int = 1 << 16):

@@ -946,6 +946,31 @@ void Instance::green_function(const cplx *z, int nz, bool spin_down, cplx *out, 
   }
 }
 
+void Instance::green_function_device(const cplx *z, int nz, bool spin_down, double *dG, Workspace &ws) {
+  if (spin_down && !(mix & mixing::up_down || mix == 0))
+    fail(QED_ERR_ARGUMENT, "spin_down=True impossible with Hilbert space mixing " + std::to_string(mix));
+  if (!gf_solved) green_solve(ws);
+  const int n = model->n_sites;
+  const int sd = (spin_down && (mix & mixing::up_down)) ? 1 : 0;
+  const size_t nn = (size_t)n * n;
+  if (nz <= 0) return;
+  if (use_cf) {  // continued fractions: evaluated by green_function, then uploaded
+    std::vector<cplx> G(nn * nz);
+    green_function(z, nz, spin_down, G.data(), ws);
+    QED_CUDA(cudaMemcpyAsync(dG, G.data(), G.size() * sizeof(cplx), cudaMemcpyHostToDevice, ws.stream));
+    ws.sync();
+    return;
+  }
+  DevBuf<double> dz(2 * (size_t)nz);
+  dz.upload(reinterpret_cast<const double *>(z), 2 * (size_t)nz, ws.stream);
+  QED_CUDA(cudaMemsetAsync(dG, 0, 2 * nn * nz * sizeof(double), ws.stream));
+  for (auto &st : states) {
+    const QMat &q = st->q[sd];
+    launch_qmatrix_gf(n, q.M, q.de.p, q.dV.p, nz, dz.p, dG, ws.stream);
+  }
+  ws.sync();
+}
+
 // hybridization_function (src_ed/model_instance.hpp:1004-1018)
 void Instance::hybridization(const cplx *z, int nz, bool spin_down, cplx *out) {
   const int n = model->n_sites, nb = model->n_bath;

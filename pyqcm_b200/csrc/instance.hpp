@@ -110,6 +110,8 @@ struct Instance {
   void finish_gf();
   // G(z) for nz frequencies: out[k*n*n + b + a*n] (column-major blocks)
   void green_function(const cplx *z, int nz, bool spin_down, cplx *out, Workspace &ws);
+  // the same into device memory (n_sites^2 * nz complex, column-major per z)
+  void green_function_device(const cplx *z, int nz, bool spin_down, double *dG, Workspace &ws);
   void self_energy(const cplx *z, int nz, bool spin_down, cplx *out, Workspace &ws);
   void hybridization(const cplx *z, int nz, bool spin_down, cplx *out);
   double potthoff(Workspace &ws);

@@ -1113,6 +1113,105 @@ __global__ void k_qmatrix_gf(int L, int M, const double *e, const double *V, int
   }
 }
 
+// Integrand of the self-energy functional on a (frequency, wavevector) grid
+// (lattice_model_instance::SEF_integrand_k, src_qcm/lattice_model_instance.cpp:618-640,
+// summed as in Potthoff_functional's grid path, :520-545): for each frequency
+// w and each k = (i/nkx, j/nky, l/nkz) of the reduced zone,
+//   V(k) = V0 + sum_e v_e exp(2 pi i k.R_e) at (r_e, c_e)   (set_V, src_qcm/CPT.cpp:22-64)
+//   I(w, k) = log |det(V(k) G(iw) - 1)|.
+// One thread per (w, k): V(k), V G - 1 and its LU factorisation with partial
+// pivoting live in the thread's local memory (n <= 16 complex); each CTA adds
+// its threads' values in a fixed order into partials[w * nblk + block].
+constexpr int kSefMaxN = 16;
+constexpr int kSefThreads = 128;
+__global__ void __launch_bounds__(kSefThreads) k_sef_logdet(int n, const double *__restrict__ G,
+                                                            const double *__restrict__ V0, int nel,
+                                                            const int *__restrict__ er, const int *__restrict__ ec,
+                                                            const double *__restrict__ eR,
+                                                            const double *__restrict__ ev, int nkx, int nky, int nkz,
+                                                            double *partials) {
+  __shared__ double red[kSefThreads];
+  const int iw = blockIdx.y;
+  const long nk = (long)nkx * nky * nkz;
+  const long kid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double val = 0.0;
+  if (kid < nk) {
+    const int ix = (int)(kid / ((long)nky * nkz)), iy = (int)((kid / nkz) % nky), iz = (int)(kid % nkz);
+    const double kx = (double)ix / nkx, ky = (double)iy / nky, kz = (double)iz / nkz;
+    double vr[kSefMaxN * kSefMaxN], vi[kSefMaxN * kSefMaxN];  // column-major n x n
+    for (int t = 0; t < n * n; ++t) {
+      vr[t] = V0[2 * t];
+      vi[t] = V0[2 * t + 1];
+    }
+    for (int e = 0; e < nel; ++e) {
+      double s, c;
+      sincospi(2.0 * (kx * eR[3 * e] + ky * eR[3 * e + 1] + kz * eR[3 * e + 2]), &s, &c);
+      const double ar = ev[2 * e], ai = ev[2 * e + 1];
+      const int t = er[e] + n * ec[e];
+      vr[t] += ar * c - ai * s;
+      vi[t] += ar * s + ai * c;
+    }
+    // M = V G - 1 (column-major); G of this frequency, column-major
+    const double *g = G + 2 * (size_t)iw * n * n;
+    double mr[kSefMaxN * kSefMaxN], mi[kSefMaxN * kSefMaxN];
+    for (int b = 0; b < n; ++b)
+      for (int a = 0; a < n; ++a) {
+        double sr = (a == b) ? -1.0 : 0.0, si = 0.0;
+        for (int c = 0; c < n; ++c) {
+          const double xr = vr[a + n * c], xi = vi[a + n * c];
+          const double yr = g[2 * (c + n * b)], yi = g[2 * (c + n * b) + 1];
+          sr += xr * yr - xi * yi;
+          si += xr * yi + xi * yr;
+        }
+        mr[a + n * b] = sr;
+        mi[a + n * b] = si;
+      }
+    // LU with partial pivoting: log |det M| = sum log |u_jj|
+    double logdet = 0.0;
+    for (int j = 0; j < n; ++j) {
+      int piv = j;
+      double best = hypot(mr[j + n * j], mi[j + n * j]);
+      for (int r = j + 1; r < n; ++r) {
+        const double m = hypot(mr[r + n * j], mi[r + n * j]);
+        if (m > best) {
+          best = m;
+          piv = r;
+        }
+      }
+      if (piv != j)
+        for (int c = 0; c < n; ++c) {
+          double t = mr[j + n * c];
+          mr[j + n * c] = mr[piv + n * c];
+          mr[piv + n * c] = t;
+          t = mi[j + n * c];
+          mi[j + n * c] = mi[piv + n * c];
+          mi[piv + n * c] = t;
+        }
+      logdet += log(best);
+      if (best == 0.0) break;
+      const double pr = mr[j + n * j], pi = mi[j + n * j];
+      const double d = pr * pr + pi * pi;
+      const double ir = pr / d, ii = -pi / d;  // 1 / pivot
+      for (int r = j + 1; r < n; ++r) {
+        const double lr = mr[r + n * j] * ir - mi[r + n * j] * ii;
+        const double li = mr[r + n * j] * ii + mi[r + n * j] * ir;
+        for (int c = j + 1; c < n; ++c) {
+          mr[r + n * c] -= lr * mr[j + n * c] - li * mi[j + n * c];
+          mi[r + n * c] -= lr * mi[j + n * c] + li * mr[j + n * c];
+        }
+      }
+    }
+    val = logdet;
+  }
+  red[threadIdx.x] = val;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int t = 0; t < blockDim.x; ++t) s += red[t];
+    partials[(size_t)iw * gridDim.x + blockIdx.x] = s;
+  }
+}
+
 // Jacobi continued fractions, backward recursion (continued_fraction::evaluate,
 // src_ed/continued_fraction.cpp:52-57); one thread per (fraction, frequency).
 __global__ void k_cf_eval(int nf, const int *off, const int *len, const double *a, const double *b,
@@ -1395,6 +1494,19 @@ int launch_block_muladd(size_t D, int p, double a, double *Y, double s1, const d
 void launch_finalize_ld(const double *partials, int nblocks, int ld, int n, double *out, cudaStream_t s) {
   k_finalize_ld<<<n, kThreads, 0, s>>>(partials, nblocks, ld, out);
   QED_LAUNCH();
+}
+
+int launch_sef_logdet(int n, int nw, const double *G, const double *V0, int nel, const int *er, const int *ec,
+                      const double *eR, const double *ev, int nkx, int nky, int nkz, double *partials,
+                      cudaStream_t s) {
+  if (n < 1 || n > kSefMaxN) fail(QED_ERR_UNSUPPORTED, "SEF grid integrand: Green function dimension above 16");
+  const long nk = (long)nkx * nky * nkz;
+  const int nblk = (int)((nk + kSefThreads - 1) / kSefThreads);
+  if (nw <= 0 || nk <= 0) return nblk;
+  if (nw > 65535) fail(QED_ERR_ARGUMENT, "SEF grid integrand: more than 65535 frequencies");
+  k_sef_logdet<<<dim3(nblk, nw), kSefThreads, 0, s>>>(n, G, V0, nel, er, ec, eR, ev, nkx, nky, nkz, partials);
+  QED_LAUNCH();
+  return nblk;
 }
 
 void launch_block_chol(int p, const double *G, double pivot_min, double *R, double *Rinv, const double *Rprev,

@@ -130,6 +130,12 @@ int launch_block_muladd(size_t D, int p, double a, double *Y, double s1, const d
                         int gram, double *partials, int ld, int max_blocks, cudaStream_t s);
 // out[0..n) = fixed-order sums of partials with row stride ld
 void launch_finalize_ld(const double *partials, int nblocks, int ld, int n, double *out, cudaStream_t s);
+// log |det(V(k) G(iw) - 1)| on the (w, k) grid, V(k) = V0 + sum_e v_e exp(2 pi i k.R_e)
+// at (r_e, c_e); G: nw column-major n x n complex matrices. Writes, per w, the
+// per-CTA sums partials[w * nblk + b] and returns nblk (n <= 16).
+int launch_sef_logdet(int n, int nw, const double *G, const double *V0, int nel, const int *er, const int *ec,
+                      const double *eR, const double *ev, int nkx, int nky, int nkz, double *partials,
+                      cudaStream_t s);
 // G = R^T R on the device (p <= 16): R, R^{-1}; *fail = 1 if G is not positive
 // definite or a pivot is below pivot_min; with Rprev, B = R Rprev and B^T
 void launch_block_chol(int p, const double *G, double pivot_min, double *R, double *Rinv, const double *Rprev,

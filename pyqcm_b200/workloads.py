@@ -161,3 +161,68 @@ def random_baths(n: int = 256, seed: int = 4242):
     """Seeded bath-parameter points for the 2x2 + 8-bath cluster."""
     rng = np.random.default_rng(seed)
     return [plaquette_bath(rng.uniform(-2, 2, 8), rng.uniform(0, 1, 8)) for _ in range(n)]
+
+
+# ------------------------------------------------------------------ lattices --
+
+@dataclass
+class LatticeProblem:
+    """A lattice model tiled by one cluster, in the vocabulary of pyqcm's
+    lattice_model (pyqcm/__init__.py: cluster_model, cluster, lattice_model,
+    hopping_operator, interaction_operator, density_wave, set_parameters).
+
+    sites: cluster site positions (integer 3-vectors); superlattice: the
+    superlattice vectors (their number is the spatial dimension);
+    hoppings: (name, link, amplitude); interactions: Hubbard operator names;
+    density_waves: (name, type, Q in multiples of pi); params: independent
+    parameter values; equiv: (name, multiplier, reference) dependences, as in
+    pyqcm's "name = multiplier * reference" syntax. Cluster (Weiss) parameters
+    carry the suffix _1."""
+    name: str
+    sites: list
+    superlattice: list
+    hoppings: list = field(default_factory=list)
+    interactions: list = field(default_factory=list)
+    density_waves: list = field(default_factory=list)
+    sectors: str = "R0"
+    params: dict = field(default_factory=dict)
+    equiv: list = field(default_factory=list)
+
+    @property
+    def n_sites(self) -> int:
+        return len(self.sites)
+
+
+def square_lattice_vca(nx: int, ny: int, U: float = 8.0, M1: float = 0.1, mu1: float | None = None,
+                       t: float = 1.0, mu: float | None = None, name: str | None = None) -> LatticeProblem:
+    """Square lattice (nearest-neighbour hopping -t) tiled by an nx x ny cluster,
+    Hubbard U, chemical potential mu (U/2 by default, half filling) and a Neel
+    Weiss field M on the cluster only (M_1, density wave of type Z at Q = (pi, pi)).
+    mu1, when given, is a separate cluster chemical potential mu_1 (else mu_1 = mu)."""
+    n = nx * ny
+    sites = [(x, y, 0) for y in range(ny) for x in range(nx)]
+    params = {"t": t, "U": U, "mu": U / 2 if mu is None else mu, "M": 0.0, "M_1": M1}
+    equiv = [("t_1", 1.0, "t"), ("U_1", 1.0, "U")]
+    if mu1 is None:
+        equiv.append(("mu_1", 1.0, "mu"))
+    else:
+        params["mu_1"] = mu1
+    return LatticeProblem(name or f"sq{nx}x{ny}_vca", sites, [(nx, 0, 0), (0, ny, 0)],
+                          hoppings=[("t", (1, 0, 0), -1.0), ("t", (0, 1, 0), -1.0)], interactions=["U"],
+                          density_waves=[("M", "Z", (1.0, 1.0, 0.0))], sectors=f"R0:N{n}:S0",
+                          params=params, equiv=equiv)
+
+
+def regular_frequency_grid(wc: float, n1: int, n2: int):
+    """Uniform grid of n1 points on [0, wc] and n2 points uniform in 1/w on
+    [0, 1/wc] (midpoint rule), weights including the 1/pi of the imaginary-axis
+    integral: the grid of pyqcm's regular_frequency_grid (pyqcm/__init__.py:3069-3089)."""
+    w = np.zeros(n1 + n2)
+    p = np.zeros(n1 + n2)
+    dw = wc / n1
+    w[:n1] = np.linspace(0.5 * dw, wc - 0.5 * dw, n1)
+    p[:n1] = dw / np.pi
+    dw = 1.0 / (n2 * wc)
+    w[n1:] = np.flip(1.0 / np.linspace(0.5 * dw, 1.0 / wc - 0.5 * dw, n2))
+    p[n1:] = w[n1:] * w[n1:] * dw / np.pi
+    return w, p

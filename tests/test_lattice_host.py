@@ -1,0 +1,35 @@
+"""Lattice layer (VCA) host logic against the reference's own lattice layer
+(the compiled oracle): the cluster's ED operators, the cluster one-body matrix
+and V(k) = t(k) - t' on a few wavevectors. No GPU calls."""
+import numpy as np
+import pytest
+
+from pyqcm_b200 import workloads as W
+
+
+@pytest.mark.parametrize("geom", [(2, 2, 0.1, None), (2, 4, 0.05, 3.7), (4, 2, 0.2, None)])
+def test_lattice_operators_and_V_match_reference(qed, oracle, geom):
+    from pyqcm_b200 import lattice as LT
+    nx, ny, M1, mu1 = geom
+    prob = W.square_lattice_vca(nx, ny, U=8.0, M1=M1, mu1=mu1)
+    oracle.set_param("GF_method", "L")
+    oracle.load_lattice(prob, 0)
+    M = LT.LatticeModel(prob)
+    mix, dim_gf, nsys = oracle.lattice_dims()
+    assert (mix, dim_gf, nsys) == (M.mixing, M.n, 1)
+    for op in ("t", "mu", "U"):
+        assert sorted(oracle.matrix_elements("clus", op)[1]) == sorted(qed.matrix_elements(M.cluster_model, op)[1]), op
+    I = M.instance(900 + nx * 10 + ny)
+    rng = np.random.default_rng(5)
+    for sd in (False, True):
+        Hc = qed.hopping_matrix(spin_down=sd, label=I.label)
+        assert np.max(np.abs(Hc - oracle.lattice_cluster_hopping(0, sd))) < 1e-14
+        for k in [(0.0, 0.0), (0.5, 0.5), tuple(rng.uniform(0, 1, 2))]:
+            assert np.max(np.abs(I.V(k, sd) - oracle.lattice_V(0, 0.5j, k, sd))) < 1e-13, (sd, k)
+
+
+def test_frequency_grid_weights():
+    """The midpoint grid integrates 1/pi * int_0^inf dw/(1 + w^2) = 1/2 closely."""
+    w, p = W.regular_frequency_grid(2.0, 200, 200)
+    assert abs(np.sum(p / (1 + w * w)) - 0.5) < 1e-4
+    assert np.all(np.diff(w) > 0)

@@ -272,6 +272,32 @@ int qed_halfbasis_rank(int L, int N, long n, const unsigned *strings, unsigned *
  * fermion phase bit per source state. */
 int qed_destroy_table(int L, int n_up, int n_dn, int a, long *target, int *phase);
 
+/* ---- VCA surrogate network ---------------------------------------------------
+ * No counterpart in the reference (its VCA, pyqcm/vca.py, evaluates the Potthoff
+ * functional by ED at every point). A multilayer perceptron n_in -> W -> W -> W -> 1
+ * (GELU) trained by Adam on Omega values this solver computes; it proposes the
+ * starting point of the ED Newton-Raphson search. BF16 weights and activations in
+ * the tensor-core products, FP32 accumulation, FP32 master weights and moments.
+ * Parameter layout (FP32, qed_mlp_layout gives the 8 block offsets and the padded
+ * input width k_in): W1 [W][k_in] (columns >= n_in zero), b1 [W], W2 [W][W], b2,
+ * W3 [W][W], b3, w4 [W], b4 [1]. Errors: qed_mlp_last_error. */
+int qed_mlp_create(int n_in, int width, unsigned long long seed, void **handle);
+void qed_mlp_destroy(void *handle);
+int qed_mlp_last_error(char *buf, int len);
+int qed_mlp_num_params(void *handle, long *n);
+int qed_mlp_layout(void *handle, long *offsets9);
+int qed_mlp_get_params(void *handle, float *params);
+int qed_mlp_set_params(void *handle, const float *params);
+/* y[rows] for x[rows][n_in] (host arrays) */
+int qed_mlp_forward(void *handle, int rows, const float *x, float *y);
+/* gradients of the mean squared error over rows (a multiple of 16) into grads
+ * (the parameter layout) and the loss */
+int qed_mlp_gradients(void *handle, int rows, const float *x, const float *t, float *grads, float *loss);
+/* `epochs` passes of Adam (lr; beta1 0.9, beta2 0.999, eps 1e-8) over shuffled
+ * batches (a multiple of 16 rows); per epoch, the loss of its last batch */
+int qed_mlp_train(void *handle, int rows, const float *x, const float *t, int epochs, int batch, float lr,
+                  unsigned long long seed, float *epoch_loss);
+
 #ifdef __cplusplus
 }
 #endif

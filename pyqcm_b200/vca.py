@@ -22,11 +22,13 @@ from pyqcm_b200 import lattice as LT
 
 
 class OmegaEvaluator:
-    """Omega at batches of points of the variational parameters `varia`."""
+    """Omega at batches of points of the variational parameters `varia` (or of
+    any point -> parameter-values map `to_values`)."""
 
     def __init__(self, model: LT.LatticeModel, varia, freqs, weights, nk, fixed=None, threads: int = 0,
-                 label0: int = 700000):
+                 label0: int = 700000, to_values=None):
         self.model = model
+        self.to_values = to_values
         self.varia = list(varia)
         self.freqs = np.asarray(freqs, dtype=np.float64)
         self.weights = np.asarray(weights, dtype=np.float64)
@@ -43,7 +45,10 @@ class OmegaEvaluator:
         insts = []
         for x in X:
             vals = dict(self.fixed)
-            vals.update({k: float(v) for k, v in zip(self.varia, x)})
+            if self.to_values is not None:
+                vals.update(self.to_values(x))
+            else:
+                vals.update({k: float(v) for k, v in zip(self.varia, x)})
             self.label += 1
             insts.append(self.model.instance(self.label, **vals))
         labels = [I.label for I in insts]
@@ -101,15 +106,48 @@ def nr_quadratic_fit(func, x, step):
     return val, grad, hess
 
 
-def newton_raphson(func, start, step, accur, gtol: float = 1e-4, max_iteration: int = 30):
+def central_fit(func, x, step):
+    """Value, gradient and Hessian at x from the full 3^n central-difference
+    stencil (x + {-1, 0, 1} step_i in every direction): gradient and Hessian are
+    exact for cubic terms along each axis, where the 1 + 2n + n(n-1)/2 point fit
+    lets them leak through its single off-diagonal point. The 3^n points are
+    one batch of concurrent GPU solves."""
+    x = np.asarray(x, dtype=np.float64)
+    n = len(x)
+    s = np.asarray(step, dtype=np.float64)
+    offs = np.array(np.meshgrid(*[[-1, 0, 1]] * n, indexing="ij")).reshape(n, -1).T
+    y = func(x + offs * s)
+    idx = {tuple(o): i for i, o in enumerate(offs)}
+    e = lambda *o: y[idx[tuple(o)]]
+    z = [0] * n
+    f0 = e(*z)
+    grad = np.zeros(n)
+    hess = np.zeros((n, n))
+    for i in range(n):
+        p, m = list(z), list(z)
+        p[i], m[i] = 1, -1
+        grad[i] = (e(*p) - e(*m)) / (2 * s[i])
+        hess[i, i] = (e(*p) + e(*m) - 2 * f0) / (s[i] * s[i])
+        for j in range(i):
+            q = [list(z) for _ in range(4)]
+            for k, (a, b) in enumerate(((1, 1), (1, -1), (-1, 1), (-1, -1))):
+                q[k][i], q[k][j] = a, b
+            hess[i, j] = hess[j, i] = (e(*q[0]) - e(*q[1]) - e(*q[2]) + e(*q[3])) / (4 * s[i] * s[j])
+    return f0, grad, hess
+
+
+def newton_raphson(func, start, step, accur, gtol: float = 1e-4, max_iteration: int = 30, stencil: str = "central"):
     """Newton-Raphson search for a stationary point (_newton_raphson, pyqcm/vca.py:318-410).
-    Returns (x, Omega at x from the last fit, gradient, Hessian, iterations)."""
+    stencil "reference" fits the reference's 1 + 2n + n(n-1)/2 points;
+    "central" (the default here) uses the 3^n central differences of central_fit.
+    Returns (x, Omega at the last fit point, gradient, Hessian, iterations)."""
+    fit = nr_quadratic_fit if stencil == "reference" else central_fit
     x = np.array(start, dtype=np.float64)
     step0 = np.array(step, dtype=np.float64)
     step = step0.copy()
     accur = np.asarray(accur, dtype=np.float64)
     for it in range(1, max_iteration + 1):
-        val, grad, hess = nr_quadratic_fit(func, x, step)
+        val, grad, hess = fit(func, x, step)
         if np.linalg.norm(grad) < gtol:
             return x, val, grad, hess, it
         dx = -np.linalg.solve(hess, grad)
@@ -120,3 +158,62 @@ def newton_raphson(func, start, step, accur, gtol: float = 1e-4, max_iteration: 
         if np.all(np.abs(dx) <= accur):
             return x, val, grad, hess, it
     raise RuntimeError(f"VCA Newton-Raphson: no convergence after {max_iteration} iterations")
+
+
+# ------------------------------------------------------------ surrogate path --
+
+def vca_values(x):
+    """(U, M', dmu) -> lattice parameters: mu = U/2, M_1 = M', mu_1 = U/2 + dmu."""
+    U, M, dmu = (float(v) for v in x)
+    return {"U": U, "mu": U / 2, "M_1": M, "mu_1": U / 2 + dmu}
+
+
+class SurrogateVCA:
+    """Potthoff functional surrogate over (U, M', dmu) in a box, trained on ED data.
+
+    Features of a point: (U scaled to [-1, 1], M' scaled to [-1, 1], dmu scaled to
+    [-1, 1], the square of the scaled M'); the target is Omega standardised by
+    the training mean and deviation. `propose(U)` returns the stationary point of
+    the surrogate at that U (Newton-Raphson on the network), which the ED search
+    then refines."""
+
+    def __init__(self, box, width: int = 256, seed: int = 0):
+        from pyqcm_b200 import surrogate as S
+        self.box = np.asarray(box, dtype=np.float64)  # [[lo, hi] for U, M', dmu]
+        self.net = S.MLP(n_in=4, width=width, seed=seed)
+        self.mean = 0.0
+        self.scale = 1.0
+
+    def features(self, X):
+        X = np.atleast_2d(np.asarray(X, dtype=np.float64))
+        lo, hi = self.box[:, 0], self.box[:, 1]
+        s = 2.0 * (X - lo) / (hi - lo) - 1.0
+        return np.c_[s, s[:, 1] ** 2].astype(np.float32)
+
+    def fit(self, X, y, epochs: int = 400, batch: int = 256, lr: float = 1e-3, seed: int = 0):
+        y = np.asarray(y, dtype=np.float64)
+        self.mean = float(np.mean(y))
+        self.scale = float(np.std(y)) or 1.0
+        return self.net.train(self.features(X), ((y - self.mean) / self.scale).astype(np.float32),
+                              epochs=epochs, batch=batch, lr=lr, seed=seed)
+
+    def __call__(self, X):
+        return self.net(self.features(X)).astype(np.float64) * self.scale + self.mean
+
+    def propose(self, U, start, step, accur=(2e-3, 2e-3)):
+        """Stationary point of the surrogate at U. The network's BF16 activations
+        resolve about 1e-3 of the box, so the quadratic fits keep steps of that
+        order (accur); the ED search refines the proposal."""
+        f = lambda P: self(np.c_[np.full(len(P), U), P])
+        try:
+            x, _, _, _, _ = newton_raphson(f, start, step, accur, gtol=0.0, max_iteration=40)
+        except (RuntimeError, np.linalg.LinAlgError):
+            return np.asarray(start, dtype=np.float64)
+        lo, hi = self.box[1:, 0], self.box[1:, 1]
+        return np.clip(x, lo, hi)
+
+
+def training_points(n: int, box, seed: int = 0):
+    rng = np.random.default_rng(seed)
+    box = np.asarray(box, dtype=np.float64)
+    return box[:, 0] + (box[:, 1] - box[:, 0]) * rng.random((n, len(box)))

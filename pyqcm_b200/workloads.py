@@ -194,7 +194,8 @@ class LatticeProblem:
 
 
 def square_lattice_vca(nx: int, ny: int, U: float = 8.0, M1: float = 0.1, mu1: float | None = None,
-                       t: float = 1.0, mu: float | None = None, name: str | None = None) -> LatticeProblem:
+                       t: float = 1.0, mu: float | None = None, name: str | None = None,
+                       superlattice=None) -> LatticeProblem:
     """Square lattice (nearest-neighbour hopping -t) tiled by an nx x ny cluster,
     Hubbard U, chemical potential mu (U/2 by default, half filling) and a Neel
     Weiss field M on the cluster only (M_1, density wave of type Z at Q = (pi, pi)).
@@ -207,10 +208,19 @@ def square_lattice_vca(nx: int, ny: int, U: float = 8.0, M1: float = 0.1, mu1: f
         equiv.append(("mu_1", 1.0, "mu"))
     else:
         params["mu_1"] = mu1
-    return LatticeProblem(name or f"sq{nx}x{ny}_vca", sites, [(nx, 0, 0), (0, ny, 0)],
+    sl = [tuple(v) for v in superlattice] if superlattice is not None else [(nx, 0, 0), (0, ny, 0)]
+    return LatticeProblem(name or f"sq{nx}x{ny}_vca", sites, sl,
                           hoppings=[("t", (1, 0, 0), -1.0), ("t", (0, 1, 0), -1.0)], interactions=["U"],
                           density_waves=[("M", "Z", (1.0, 1.0, 0.0))], sectors=f"R0:N{n}:S0",
                           params=params, equiv=equiv)
+
+
+def vca_2x5(U: float = 8.0, M1: float = 0.1, dmu: float = 0.0) -> LatticeProblem:
+    """2x5 clusters tiling the square lattice (t = 1, amplitude -1), half filling
+    (mu = U/2), Neel Weiss field M_1 and cluster chemical potential mu_1 = U/2 + dmu.
+    The superlattice (2,0), (1,5) keeps Q = (pi, pi) commensurate with the tiling."""
+    return square_lattice_vca(2, 5, U=U, M1=M1, mu1=U / 2 + dmu, name="vca2x5",
+                              superlattice=[(2, 0, 0), (1, 5, 0)])
 
 
 def regular_frequency_grid(wc: float, n1: int, n2: int):

@@ -1,0 +1,36 @@
+"""Variational cluster approximation on the GPU: the Newton-Raphson search on
+ED Potthoff functionals, and the surrogate-guided search reaching the same
+stationary point."""
+import numpy as np
+import pytest
+
+from pyqcm_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _evaluator(qed, U=None):
+    from pyqcm_b200 import lattice as LT, vca
+    qed.set_global_parameter("GF_method", "L")
+    model = LT.LatticeModel(W.square_lattice_vca(2, 2, U=8.0, M1=0.1, mu1=4.0))
+    w, p = W.regular_frequency_grid(2.0, 24, 24)
+    return model, vca.OmegaEvaluator(model, [], w, p, (16, 16), to_values=vca.vca_values)
+
+
+def test_surrogate_guided_vca_reaches_the_ed_stationary_point(qed):
+    from pyqcm_b200 import vca
+    model, ev = _evaluator(qed)
+    U = 8.0
+    f_ed = lambda P: ev(np.c_[np.full(len(P), U), P])
+    acc = [2e-5, 2e-5]
+    x_ed, *_ = vca.newton_raphson(f_ed, [0.15, 0.0], [0.02, 0.02], acc)
+    box = [[7.0, 9.0], [0.0, 0.4], [-0.5, 0.5]]
+    X = vca.training_points(512, box, seed=1)
+    y = ev(X)
+    sur = vca.SurrogateVCA(box, width=256, seed=0)
+    sur.fit(X, y, epochs=400)
+    x0 = sur.propose(U, [0.2, 0.0], [0.02, 0.02])
+    x_s, *_ = vca.newton_raphson(f_ed, x0, [0.005, 0.005], acc)
+    om = ev(np.c_[[U, U], np.vstack([x_ed, x_s])])
+    assert abs(om[0] - om[1]) < 1e-8, (x_ed, x_s, om)
+    assert np.max(np.abs(x_ed - x_s)) < 1e-3

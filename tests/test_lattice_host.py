@@ -33,3 +33,14 @@ def test_frequency_grid_weights():
     w, p = W.regular_frequency_grid(2.0, 200, 200)
     assert abs(np.sum(p / (1 + w * w)) - 0.5) < 1e-4
     assert np.all(np.diff(w) > 0)
+
+
+def test_nr_fit_recovers_a_quadratic():
+    from pyqcm_b200 import vca
+    A = np.array([[2.0, 0.3], [0.3, -1.0]])
+    x0 = np.array([0.1, -0.2])
+    f = lambda X: np.array([0.5 * (x - x0) @ A @ (x - x0) + 3.0 for x in np.atleast_2d(X)])
+    val, g, H = vca.nr_quadratic_fit(f, np.array([0.3, 0.1]), [0.01, 0.01])
+    assert np.allclose(H, A, atol=1e-8) and np.allclose(g, A @ (np.array([0.3, 0.1]) - x0), atol=1e-8)
+    x, *_ = vca.newton_raphson(f, [0.3, 0.1], [0.01, 0.01], [1e-8, 1e-8])
+    assert np.allclose(x, x0, atol=1e-8)

@@ -51,9 +51,12 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: warm-up and timed H.v only (no e2e, clocks or CPU baseline)")
     ap.add_argument("--sector", default=None, help="sector of the 4x4 cluster to use (default R0:N16:S0)")
-    ap.add_argument("--workload", default="hv", choices=["hv", "batch", "baths"],
+    ap.add_argument("--workload", default="hv", choices=["hv", "batch", "baths", "vca"],
                     help="hv: H.v on the 4x4 cluster (default); batch: independent random clusters, "
-                         "every sector, ground state + Green function; baths: 2x2 + 8-bath points")
+                         "every sector, ground state + Green function; baths: 2x2 + 8-bath points; "
+                         "vca: 2x5-cluster VCA, surrogate-guided against ED-only")
+    ap.add_argument("--vca-points", type=int, default=4096, help="training points of the VCA surrogate")
+    ap.add_argument("--vca-epochs", type=int, default=400, help="training epochs of the VCA surrogate")
     ap.add_argument("--batch", type=int, default=64, help="instances per step for --workload batch/baths")
     ap.add_argument("--threads", type=int, default=0, help="host threads for batched solves (0 = all)")
     return ap.parse_args()
@@ -414,15 +417,19 @@ def batch_line(workload, batch, threads, steps, warmup, impl, world=1, rank=0, l
 
 
 SECONDARY = (("batch", 64), ("baths", 16))
+VCA_SECONDARY_POINTS = 1024
 
 
 def secondary_lines(impl):
-    """The batched-solve metrics reported beside the H.v line of the default run."""
+    """The batched-solve metrics (and, for this solver, the VCA line) reported
+    beside the H.v line of the default run."""
     out = []
     for wl, n in SECONDARY:
         line = batch_line(wl, n, 0, 2, 1, impl)
         if line:
             out.append(line)
+    if impl == "ours":
+        out.append(vca_line(VCA_SECONDARY_POINTS, 400, 0))
     return out
 
 
@@ -433,11 +440,80 @@ def run_batch_workload(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+VCA_WORKLOAD = ("VCA on the square lattice (t=1) tiled by 2x5 clusters (superlattice (2,0),(1,5)), "
+                "half filling mu=U/2; variational Neel Weiss field M' and cluster chemical potential shift "
+                "dmu; Omega from the ED ground state + band-Lanczos Green function (dim 63504) and a fixed "
+                "grid of 64 Matsubara frequencies x 64x64 wavevectors; Newton-Raphson (3x3 central stencil, "
+                "accuracy 2e-5) from (M', dmu) = (0.2, 0) with steps 0.02 (ED only) or from the surrogate's "
+                "stationary point with steps 0.005 (surrogate-guided)")
+
+
+def vca_line(n_points, epochs, threads, Us=(5.0, 7.0, 9.0), local=0):
+    """Surrogate-guided against ED-only VCA on the 2x5 cluster: training-data and
+    training cost, then per U the wall time of both searches to the same stationary point."""
+    import pyqcm_b200 as qed
+    from pyqcm_b200 import lattice as LT, vca
+    from pyqcm_b200 import workloads as W
+    qed.init(local)
+    qed.set_global_parameter("GF_method", "L")
+    model = LT.LatticeModel(W.vca_2x5())
+    w, p = W.regular_frequency_grid(2.0, 32, 32)
+    ev = vca.OmegaEvaluator(model, [], w, p, (64, 64), to_values=vca.vca_values, threads=threads)
+    box = [[4.0, 10.0], [0.0, 0.4], [-0.5, 0.5]]
+    X = vca.training_points(n_points, box, seed=2024)
+    t0 = time.perf_counter()
+    y = np.concatenate([ev(X[i:i + 256]) for i in range(0, len(X), 256)])
+    t_data = time.perf_counter() - t0
+    sur = vca.SurrogateVCA(box, width=256, seed=0)
+    t0 = time.perf_counter()
+    losses = sur.fit(X, y, epochs=epochs, batch=256, lr=1e-3, seed=0)
+    t_train = time.perf_counter() - t0
+    acc = [2e-5, 2e-5]
+    runs = []
+    for U in Us:
+        f_ed = lambda P, U=U: ev(np.c_[np.full(len(P), U), P])
+        n0 = ev.n_evals
+        t0 = time.perf_counter()
+        x_ed, _, _, _, it_ed = vca.newton_raphson(f_ed, [0.2, 0.0], [0.02, 0.02], acc)
+        t_ed = time.perf_counter() - t0
+        n_ed = ev.n_evals - n0
+        n0 = ev.n_evals
+        t0 = time.perf_counter()
+        x0 = sur.propose(U, [0.2, 0.0], [0.02, 0.02])
+        x_s, _, _, _, it_s = vca.newton_raphson(f_ed, x0, [0.005, 0.005], acc)
+        t_s = time.perf_counter() - t0
+        n_s = ev.n_evals - n0
+        x_poly = sur.propose(U, [0.2, 0.0], [0.02, 0.02], use_net=False)
+        om = ev(np.c_[[U, U], np.vstack([x_ed, x_s])])
+        runs.append({"U": U, "ed_only_s": t_ed, "surrogate_s": t_s, "ed_only_iterations": it_ed,
+                     "surrogate_iterations": it_s, "ed_only_omega_evals": n_ed, "surrogate_omega_evals": n_s,
+                     "x_ed_only": [float(v) for v in x_ed], "x_surrogate": [float(v) for v in x_s],
+                     "x_proposed": [float(v) for v in x0],
+                     "x_proposed_polynomial_only": [float(v) for v in x_poly], "omega": float(om[0]),
+                     "omega_abs_diff": float(abs(om[0] - om[1]))})
+    t_sur = sum(r["surrogate_s"] for r in runs)
+    t_ed = sum(r["ed_only_s"] for r in runs)
+    return {"metric": "VCA wall time, surrogate-guided (same stationary point as ED-only within 1e-8)",
+            "value": t_sur, "unit": "s", "n_gpus": 1, "steps": len(Us), "warmup": 0,
+            "ms_per_step": 1e3 * t_sur / len(Us), "higher_is_better": False, "scaling": "replicas",
+            "vs_baseline": None, "dtype": "f64 (ED, Omega); bf16 x bf16 -> f32 (surrogate)",
+            "data": "synthetic", "config": {"workload": VCA_WORKLOAD, "U": list(Us),
+                                            "training_points": n_points, "epochs": epochs},
+            "ed_only_seconds": t_ed, "speedup": t_ed / t_sur if t_sur > 0 else None,
+            "max_omega_abs_diff": max(r["omega_abs_diff"] for r in runs),
+            "training": {"data_seconds": t_data, "omega_per_second": n_points / t_data,
+                         "train_seconds": t_train, "first_loss": float(losses[0]), "last_loss": float(losses[-1])},
+            "runs": runs}
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     try:
-        if args.workload != "hv":
+        if args.workload == "vca":
+            if rank == 0:
+                print(json.dumps(vca_line(args.vca_points, args.vca_epochs, args.threads, local=local)), flush=True)
+        elif args.workload != "hv":
             run_batch_workload(args, world, rank, local)
         elif args.impl == "reference":
             run_reference(args, world, rank)

@@ -171,11 +171,16 @@ def vca_values(x):
 class SurrogateVCA:
     """Potthoff functional surrogate over (U, M', dmu) in a box, trained on ED data.
 
-    Features of a point: (U scaled to [-1, 1], M' scaled to [-1, 1], dmu scaled to
-    [-1, 1], the square of the scaled M'); the target is Omega standardised by
-    the training mean and deviation. `propose(U)` returns the stationary point of
-    the surrogate at that U (Newton-Raphson on the network), which the ED search
-    then refines."""
+    Omega varies across the box mostly with U (by about 1 per unit of U) and
+    only by 1e-4 to 1e-3 with the variational parameters, below what BF16
+    activations resolve on that scale. So the surrogate is a least-squares
+    polynomial of total degree 4 in the scaled coordinates (FP64, on the host)
+    plus the network fitted to its residual, standardised. Network features:
+    the three coordinates scaled to [-1, 1] and the square of the scaled M'.
+    `propose(U)` returns the stationary point of the surrogate at that U
+    (Newton-Raphson on the surrogate), which the ED search then refines."""
+
+    DEGREE = 4
 
     def __init__(self, box, width: int = 256, seed: int = 0):
         from pyqcm_b200 import surrogate as S
@@ -183,28 +188,49 @@ class SurrogateVCA:
         self.net = S.MLP(n_in=4, width=width, seed=seed)
         self.mean = 0.0
         self.scale = 1.0
+        self.coef = None
 
-    def features(self, X):
+    def _scaled(self, X):
         X = np.atleast_2d(np.asarray(X, dtype=np.float64))
         lo, hi = self.box[:, 0], self.box[:, 1]
-        s = 2.0 * (X - lo) / (hi - lo) - 1.0
+        return 2.0 * (X - lo) / (hi - lo) - 1.0
+
+    def features(self, X):
+        s = self._scaled(X)
         return np.c_[s, s[:, 1] ** 2].astype(np.float32)
+
+    def _poly(self, X):
+        s = self._scaled(X)
+        cols = [np.ones(len(s))]
+        for a in range(self.DEGREE + 1):
+            for b in range(self.DEGREE + 1 - a):
+                for c in range(self.DEGREE + 1 - a - b):
+                    if a + b + c:
+                        cols.append(s[:, 0] ** a * s[:, 1] ** b * s[:, 2] ** c)
+        return np.stack(cols, axis=1)
 
     def fit(self, X, y, epochs: int = 400, batch: int = 256, lr: float = 1e-3, seed: int = 0):
         y = np.asarray(y, dtype=np.float64)
-        self.mean = float(np.mean(y))
-        self.scale = float(np.std(y)) or 1.0
-        return self.net.train(self.features(X), ((y - self.mean) / self.scale).astype(np.float32),
+        A = self._poly(X)
+        self.coef = np.linalg.lstsq(A, y, rcond=None)[0]
+        r = y - A @ self.coef
+        self.mean = float(np.mean(r))
+        self.scale = float(np.std(r)) or 1.0
+        return self.net.train(self.features(X), ((r - self.mean) / self.scale).astype(np.float32),
                               epochs=epochs, batch=batch, lr=lr, seed=seed)
 
-    def __call__(self, X):
-        return self.net(self.features(X)).astype(np.float64) * self.scale + self.mean
+    def __call__(self, X, use_net: bool = True):
+        base = self._poly(X) @ self.coef
+        if not use_net:
+            return base
+        return base + self.net(self.features(X)).astype(np.float64) * self.scale + self.mean
 
-    def propose(self, U, start, step, accur=(2e-3, 2e-3)):
-        """Stationary point of the surrogate at U. The network's BF16 activations
-        resolve about 1e-3 of the box, so the quadratic fits keep steps of that
-        order (accur); the ED search refines the proposal."""
-        f = lambda P: self(np.c_[np.full(len(P), U), P])
+    def propose(self, U, start, step, accur=(2e-3, 2e-3), use_net: bool = True):
+        """Stationary point of the surrogate at U (use_net=False: of the polynomial
+        alone). The network's BF16 activations resolve about 1e-3 of the box, so
+        the quadratic fits keep steps of that order (accur); the ED search
+        refines the proposal."""
+        f = lambda P: self(np.c_[np.full(len(P), U), P], use_net=use_net)
         try:
             x, _, _, _, _ = newton_raphson(f, start, step, accur, gtol=0.0, max_iteration=40)
         except (RuntimeError, np.linalg.LinAlgError):

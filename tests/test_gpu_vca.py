@@ -23,14 +23,19 @@ def test_surrogate_guided_vca_reaches_the_ed_stationary_point(qed):
     U = 8.0
     f_ed = lambda P: ev(np.c_[np.full(len(P), U), P])
     acc = [2e-5, 2e-5]
+    n0 = ev.n_evals
     x_ed, *_ = vca.newton_raphson(f_ed, [0.15, 0.0], [0.02, 0.02], acc)
+    n_ed = ev.n_evals - n0
     box = [[7.0, 9.0], [0.0, 0.4], [-0.5, 0.5]]
     X = vca.training_points(512, box, seed=1)
     y = ev(X)
     sur = vca.SurrogateVCA(box, width=256, seed=0)
     sur.fit(X, y, epochs=400)
     x0 = sur.propose(U, [0.2, 0.0], [0.02, 0.02])
+    n0 = ev.n_evals
     x_s, *_ = vca.newton_raphson(f_ed, x0, [0.005, 0.005], acc)
+    n_s = ev.n_evals - n0
+    assert n_s < n_ed, (n_s, n_ed)  # what the trained surrogate saves: ED evaluations
     om = ev(np.c_[[U, U], np.vstack([x_ed, x_s])])
     assert abs(om[0] - om[1]) < 1e-8, (x_ed, x_s, om)
     assert np.max(np.abs(x_ed - x_s)) < 1e-3

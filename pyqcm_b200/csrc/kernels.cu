@@ -1290,11 +1290,12 @@ constexpr size_t kRowSmem2Max = 220 * 1024;  // below the 227 KB per-CTA limit
 }
 
 // Launch variant of the H.v passes (bit 0: column-pass gathers cached in L2
-// only; bit 1: row pass with four gathers in flight). QED_HV_VARIANT overrides.
+// only; bit 1: row pass with four gathers in flight). QED_HV_VARIANT overrides
+// the default 2 (on the 4x4 sector: 5.47 ms per H.v against 5.57 ms for 0).
 int hv_variant() {
   static const int v = [] {
     const char *e = getenv("QED_HV_VARIANT");
-    return e ? atoi(e) : 0;
+    return e ? atoi(e) : 2;
   }();
   return v;
 }

@@ -2,6 +2,7 @@
 // Hamiltonians, and the error convention (status code + per-thread message).
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cstring>
 #include <functional>
 #include <thread>
@@ -108,6 +109,60 @@ std::shared_ptr<Instance> instance(int label) {
 
 // Runs fn(i) for i in [0, n) on `threads` host threads (each with its own
 // Workspace / CUDA stream). Returns the status of the first failure.
+// Worker threads kept for the life of the process, so that each keeps its
+// Workspace (stream, reduction buffers, pinned staging) from one batch call to
+// the next. A batch call hands the pool one work loop that `extra` workers and
+// the calling thread run; batch calls from different host threads take turns.
+class WorkerPool {
+ public:
+  void run(int extra, const std::function<void()> &work) {
+    std::lock_guard<std::mutex> serial(run_mtx_);
+    {
+      std::lock_guard<std::mutex> l(m_);
+      while ((int)threads_ < extra) {
+        const int idx = (int)threads_++;
+        std::thread([this, idx] { loop(idx); }).detach();
+      }
+      job_ = work;
+      wanted_ = extra;
+      active_ = extra;
+      ++gen_;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> l(m_);
+    done_.wait(l, [&] { return active_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  void loop(int idx) {
+    uint64_t seen = 0;
+    std::unique_lock<std::mutex> l(m_);
+    for (;;) {
+      cv_.wait(l, [&] { return gen_ != seen; });
+      seen = gen_;
+      if (idx >= wanted_) continue;
+      std::function<void()> w = job_;
+      l.unlock();
+      w();
+      l.lock();
+      if (--active_ == 0) done_.notify_all();
+    }
+  }
+  std::mutex run_mtx_, m_;
+  std::condition_variable cv_, done_;
+  std::function<void()> job_;
+  size_t threads_ = 0;
+  int wanted_ = 0, active_ = 0;
+  uint64_t gen_ = 0;
+};
+
+WorkerPool &pool() {
+  static WorkerPool *p = new WorkerPool;  // never destroyed: its threads live until exit
+  return *p;
+}
+
 template <class F> int run_batch(int n, int threads, F &&fn) {
   if (n <= 0) return QED_OK;
   int hw = (int)std::thread::hardware_concurrency();
@@ -129,10 +184,7 @@ template <class F> int run_batch(int n, int threads, F &&fn) {
       }
     }
   };
-  std::vector<std::thread> pool;
-  for (int t = 1; t < threads; ++t) pool.emplace_back(work);
-  work();
-  for (auto &th : pool) th.join();
+  pool().run(threads - 1, work);
   if (first_code != QED_OK) t_err = first_msg;
   return first_code;
 }

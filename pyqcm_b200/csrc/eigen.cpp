@@ -411,6 +411,116 @@ bool band_eigenvalues(int n, int b, std::vector<double> A, std::vector<double> &
   return true;
 }
 
+namespace {
+// LDL^T of (A - s I), A symmetric with half-bandwidth b in lower band storage;
+// L in the same layout (unit diagonal implied). False on a pivot <= 0.
+bool band_ldlt(int n, int b, const std::vector<double> &B, double s, std::vector<double> &L, std::vector<double> &D) {
+  const int w = b + 1;
+  L.assign((size_t)n * w, 0.0);
+  D.assign(n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    const int j0 = std::max(0, i - b);
+    for (int j = j0; j < i; ++j) {
+      double v = B[(size_t)i * w + (i - j)];
+      for (int m = std::max(j0, j - b); m < j; ++m) v -= L[(size_t)i * w + (i - m)] * D[m] * L[(size_t)j * w + (j - m)];
+      L[(size_t)i * w + (i - j)] = v / D[j];
+    }
+    double d = B[(size_t)i * w] - s;
+    for (int m = j0; m < i; ++m) {
+      const double l = L[(size_t)i * w + (i - m)];
+      d -= l * l * D[m];
+    }
+    if (!(d > 0.0)) return false;
+    D[i] = d;
+  }
+  return true;
+}
+
+void band_ldlt_solve(int n, int b, const std::vector<double> &L, const std::vector<double> &D, std::vector<double> &x) {
+  const int w = b + 1;
+  for (int i = 0; i < n; ++i)
+    for (int m = std::max(0, i - b); m < i; ++m) x[i] -= L[(size_t)i * w + (i - m)] * x[m];
+  for (int i = 0; i < n; ++i) x[i] /= D[i];
+  for (int i = n - 1; i >= 0; --i)
+    for (int r = i + 1; r <= std::min(n - 1, i + b); ++r) x[i] -= L[(size_t)r * w + (r - i)] * x[r];
+}
+
+// x^T A x for A in lower band storage
+double band_quadratic(int n, int b, const std::vector<double> &B, const std::vector<double> &x) {
+  const int w = b + 1;
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double t = B[(size_t)i * w] * x[i];
+    for (int k = 1; k <= std::min(i, b); ++k) t += 2.0 * B[(size_t)i * w + k] * x[i - k];
+    s += t * x[i];
+  }
+  return s;
+}
+
+// inverse iteration on A - s I from x (normalised in place); Rayleigh quotient
+bool inverse_iteration(int n, int b, const std::vector<double> &B, double s, std::vector<double> &x, double *rq) {
+  std::vector<double> L, D;
+  if (!band_ldlt(n, b, B, s, L, D)) return false;
+  double prev = 0.0;
+  for (int it = 0; it < 80; ++it) {
+    band_ldlt_solve(n, b, L, D, x);
+    double nrm = 0.0;
+    for (double v : x) nrm += v * v;
+    nrm = std::sqrt(nrm);
+    if (!(nrm > 0.0) || !std::isfinite(nrm)) return false;
+    for (double &v : x) v /= nrm;
+    const double r = band_quadratic(n, b, B, x);
+    if (it >= 2 && std::fabs(r - prev) <= 1e-15 * (1.0 + std::fabs(r))) {
+      *rq = r;
+      return true;
+    }
+    prev = r;
+  }
+  return false;
+}
+}  // namespace
+
+bool band_lowest(int n, int b, const std::vector<double> &B, BandLowest &st, double *lambda) {
+  if (n <= 0 || b < 1) return false;
+  const int w = b + 1;
+  if (!st.valid || (int)st.x.size() > n) {
+    // cold start: all eigenvalues, then the eigenvector by inverse iteration
+    std::vector<double> A((size_t)n * n, 0.0), ev;
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k <= std::min(i, b); ++k) A[(size_t)i + (size_t)n * (i - k)] = A[(size_t)(i - k) + (size_t)n * i] = B[(size_t)i * w + k];
+    if (!band_eigenvalues(n, b, A, ev)) return false;
+    const double gap = n > 1 ? ev[1] - ev[0] : 1.0;
+    std::vector<double> x(n, 1.0);
+    double rq = 0.0;
+    st.valid = inverse_iteration(n, b, B, ev[0] - std::max(1e-3 * gap, 1e-12 * (1.0 + std::fabs(ev[0]))), x, &rq);
+    st.x = x;
+    st.lambda = ev[0];
+    st.drop = 0.0;
+    *lambda = ev[0];
+    return true;
+  }
+  std::vector<double> x(n, 0.0);
+  std::copy(st.x.begin(), st.x.end(), x.begin());
+  double delta = std::max(2.0 * st.drop, 1e-9 * (1.0 + std::fabs(st.lambda)));
+  double rq = 0.0;
+  bool ok = false;
+  for (int t = 0; t < 12 && !ok; ++t, delta *= 8.0) {
+    std::vector<double> y = x;
+    if (inverse_iteration(n, b, B, st.lambda - delta, y, &rq)) {
+      x = y;
+      ok = true;
+    }
+  }
+  if (!ok) return false;
+  std::vector<double> L, D;
+  if (!band_ldlt(n, b, B, rq - 1e-14 * (1.0 + std::fabs(rq)), L, D)) return false;  // certificate
+  st.drop = std::max(0.0, st.lambda - rq);
+  st.lambda = rq;
+  st.x = x;
+  *lambda = rq;
+  return true;
+}
+
 bool band_eig_rows(int n, int b, std::vector<double> A, int m, std::vector<double> &w, std::vector<double> &Z) {
   w.assign(n, 0.0);
   Z.assign((size_t)m * n, 0.0);

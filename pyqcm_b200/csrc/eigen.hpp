@@ -65,6 +65,23 @@ bool sym_eig(int n, const std::vector<double> &A, std::vector<double> &w, std::v
 // 12, 1968), O(n^2 b), then QL. Used for the band-Lanczos convergence test.
 bool band_eigenvalues(int n, int b, std::vector<double> A, std::vector<double> &w);
 
+// Lowest eigenvalue of a growing sequence of band matrices (each the leading
+// block of the next, as in the band-Lanczos convergence test), in lower band
+// storage B[i * (b + 1) + k] = A(i, i - k), k = 0..min(i, b). The first call
+// takes all eigenvalues (band_eigenvalues); later calls run inverse iteration
+// on A - s I (banded LDL^T, O(n b^2)) from the previous eigenvector, with the
+// shift s below the previous lowest eigenvalue (which, by interlacing, is not
+// below the new one), and certify the Rayleigh quotient r: the LDL^T of
+// A - (r - eps) I, eps = 1e-14 (1 + |r|), must have positive pivots, so the
+// lowest eigenvalue lies in [r - eps, r]. Returns false where that fails (the
+// caller then takes band_eigenvalues).
+struct BandLowest {
+  std::vector<double> x;  // eigenvector of the last call
+  double lambda = 0.0, drop = 0.0;
+  bool valid = false;
+};
+bool band_lowest(int n, int b, const std::vector<double> &B, BandLowest &st, double *lambda);
+
 // Eigenvalues (ascending) of the same band matrix and the first m rows of its
 // eigenvector matrix, Z column-major m x n (column k <-> w[k]): the band
 // reduction and the QL rotations are accumulated on those m rows only, O(n^2 b)

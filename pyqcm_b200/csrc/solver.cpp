@@ -42,6 +42,7 @@ Workspace::~Workspace() {
   if (stream) cudaStreamSynchronize(stream);
   if (host) cudaFreeHost(host);
   if (pin) cudaFreeHost(pin);
+  if (sync_ev) cudaEventDestroy(sync_ev);
   if (tls_stream == stream) tls_stream = nullptr;
   if (stream) cudaStreamDestroy(stream);
 }
@@ -52,7 +53,27 @@ const double *Workspace::sums(int nblocks, int nred) {
   return host;
 }
 
-void Workspace::sync() { QED_CUDA(cudaStreamSynchronize(stream)); }
+// Host waits: cudaStreamSynchronize (the device's scheduling policy, a spin
+// while few contexts are active), or with QED_SYNC=block a blocking-sync event,
+// which lets the waiting thread sleep so that more host threads than cores can
+// drive concurrent solves.
+static bool blocking_sync() {
+  static const bool b = [] {
+    const char *e = getenv("QED_SYNC");
+    return e && std::string(e) == "block";
+  }();
+  return b;
+}
+
+void Workspace::sync() {
+  if (!blocking_sync()) {
+    QED_CUDA(cudaStreamSynchronize(stream));
+    return;
+  }
+  if (!sync_ev) QED_CUDA(cudaEventCreateWithFlags(&sync_ev, cudaEventBlockingSync | cudaEventDisableTiming));
+  QED_CUDA(cudaEventRecord(sync_ev, stream));
+  QED_CUDA(cudaEventSynchronize(sync_ev));
+}
 
 double *Workspace::pinned(size_t n) {
   if (n > pin_n) {
@@ -338,11 +359,12 @@ void start_vector(size_t D, uint64_t seed, double *v, Workspace &ws) {
 // The Ritz test of LanczosEigenvalue (src_ed/Hamiltonian/Lanczos.hpp:73-90)
 // needs the lowest eigenvalue of the j x j tridiagonal and the last component
 // of its eigenvector at every step. Far from convergence both come from O(j)
-// updates (inverse iteration from the previous step's eigenvector, or Sturm
-// bisection + backward recurrence); once the residual estimate is within 8x
-// of the tolerance the O(j^2) QL last-row method (the reference's dstev
-// result) decides the stop, so the iteration count does not depend on the fast
-// estimate.
+// updates (inverse iteration from the previous step's eigenvector, certified by
+// an LDL^T inertia count, or Sturm bisection + backward recurrence), accurate
+// to about 1e-12 relative where the lowest eigenvalue is separated. Only when
+// that estimate lands within 0.1 % of the tolerance does the O(j^2) QL
+// last-row method (the reference's dstev result) decide the stop, so that the
+// iteration count does not hinge on the fast estimate's last digits.
 //
 // The recurrence itself runs on the device in chunks: alpha_j, beta_j stay in
 // device memory (the row pass reads beta_{j-1} from there), and the host reads
@@ -353,7 +375,7 @@ void start_vector(size_t D, uint64_t seed, double *v, Workspace &ws) {
 // The fast estimate agrees with the QL value to about 1 % near the tolerance
 // (O(j) inverse iteration converged to a residual of 1e-14 ||T||), so a gate of
 // 8x leaves a wide margin while the O(j^2) QL runs only on the last steps.
-constexpr double kQlGate = 8.0;
+constexpr double kQlBand = 1e-3;
 
 LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed) {
   PhaseScope ps(kPhGsLanczos);
@@ -427,7 +449,7 @@ LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed) {
       double last = 1.0;
       tridiag_lowest_track((int)alpha.size(), alpha.data(), beta.data(), tracker, &lambda0, &last);
       double ritz = std::fabs(last * b);
-      if (ritz < kQlGate * accur) {
+      if (std::fabs(ritz - accur) < kQlBand * accur) {
         if (!tridiag_lowest_last((int)alpha.size(), alpha.data(), beta.data(), &lambda0, &last))
           fail(QED_ERR_LANCZOS, "tridiagonal eigensolver did not converge");
         ritz = std::fabs(last * b);
@@ -715,6 +737,7 @@ bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<
   };
   double ev_old = 1e12;
   int jdim = 0;
+  BandLowest lowest;
   PhaseScope ps_loop(kPhBlockLoop);
   enqueue(0);
   for (int k = 0;; ++k) {
@@ -730,17 +753,29 @@ bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<
     }
     if (jdim >= 4 * p) {  // bandLanczos step (12) at j = jdim, on the leading jdim x jdim block
       PhaseScope ps_check(kPhBandCheck);
-      std::vector<double> Hpr((size_t)jdim * jdim), evs;
-      for (int c = 0; c < jdim; ++c)
-        for (int r = 0; r < jdim; ++r) Hpr[(size_t)r + (size_t)jdim * c] = T(r, c);
-      if (!band_eigenvalues(jdim, p, Hpr, evs)) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
-      const double test = std::fabs(evs[0] - ev_old);
-      ev_old = evs[0];
-      if (jdim > 1 && evs[1] - evs[0] < min_gap && no_degenerate) {
-        ws.sync();
-        fail(QED_ERR_LANCZOS, "band Lanczos: the gap between the first two eigenvalues is smaller than " +
-                                  std::to_string(min_gap));
+      double ev0 = 0.0;
+      bool fast = false;
+      if (!no_degenerate) {  // only the lowest eigenvalue is needed
+        std::vector<double> Bb((size_t)jdim * (p + 1), 0.0);
+        for (int i = 0; i < jdim; ++i)
+          for (int kk = 0; kk <= std::min(i, p); ++kk) Bb[(size_t)i * (p + 1) + kk] = T(i, i - kk);
+        fast = band_lowest(jdim, p, Bb, lowest, &ev0);
       }
+      if (!fast) {
+        std::vector<double> Hpr((size_t)jdim * jdim), evs;
+        for (int c = 0; c < jdim; ++c)
+          for (int r = 0; r < jdim; ++r) Hpr[(size_t)r + (size_t)jdim * c] = T(r, c);
+        if (!band_eigenvalues(jdim, p, Hpr, evs)) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
+        if (jdim > 1 && evs[1] - evs[0] < min_gap && no_degenerate) {
+          ws.sync();
+          fail(QED_ERR_LANCZOS, "band Lanczos: the gap between the first two eigenvalues is smaller than " +
+                                    std::to_string(min_gap));
+        }
+        ev0 = evs[0];
+        lowest.valid = false;
+      }
+      const double test = std::fabs(ev0 - ev_old);
+      ev_old = ev0;
       if (test < accur_bl) break;
     }
     if (A[2 * pp] != 0.0) {  // a QR pivot below kPivotMin: the band recurrence takes over
@@ -818,19 +853,35 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
   VecList ys;
   PhaseScope ps_loop(kPhBandLoop);
   // step (12): convergence test on the lowest eigenvalue of the projected matrix
+  // Without deflation t is banded (half-bandwidth p) and only its lowest
+  // eigenvalue is needed: band_lowest (warm-started inverse iteration, O(j p^2)
+  // per test, certified to 1e-14) with band_eigenvalues (O(j^2 p)) where it
+  // declines; after a deflation, the dense eigenvalues.
+  BandLowest lowest;
   auto converged_at = [&](int jc) {
     PhaseScope ps_check(kPhBandCheck);
-    std::vector<double> Hpr((size_t)jc * jc), ev;
-    for (int c = 0; c < jc; ++c)
-      for (int r = 0; r < jc; ++r) Hpr[(size_t)r + (size_t)jc * c] = T(r, c);
-    // without deflation t is banded (half-bandwidth p): O(j^2 p) instead of O(j^3)
-    const bool ok = (nd == 0) ? band_eigenvalues(jc, p, Hpr, ev) : sym_eig(jc, Hpr, ev, nullptr);
-    if (!ok) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
-    double test = std::fabs(ev[0] - ev_old);
-    ev_old = ev[0];
-    if (jc > 1 && ev[1] - ev[0] < min_gap && no_degenerate)
-      fail(QED_ERR_LANCZOS, "band Lanczos: the gap between the first two eigenvalues is smaller than " +
-                                std::to_string(min_gap));
+    double ev0 = 0.0;
+    bool fast = false;
+    if (nd == 0 && !no_degenerate) {
+      std::vector<double> Bb((size_t)jc * (p + 1), 0.0);
+      for (int i = 0; i < jc; ++i)
+        for (int kk = 0; kk <= std::min(i, p); ++kk) Bb[(size_t)i * (p + 1) + kk] = T(i, i - kk);
+      fast = band_lowest(jc, p, Bb, lowest, &ev0);
+    }
+    if (!fast) {
+      std::vector<double> Hpr((size_t)jc * jc), ev;
+      for (int c = 0; c < jc; ++c)
+        for (int r = 0; r < jc; ++r) Hpr[(size_t)r + (size_t)jc * c] = T(r, c);
+      const bool ok = (nd == 0) ? band_eigenvalues(jc, p, Hpr, ev) : sym_eig(jc, Hpr, ev, nullptr);
+      if (!ok) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
+      if (jc > 1 && ev[1] - ev[0] < min_gap && no_degenerate)
+        fail(QED_ERR_LANCZOS, "band Lanczos: the gap between the first two eigenvalues is smaller than " +
+                                  std::to_string(min_gap));
+      ev0 = ev[0];
+      lowest.valid = false;
+    }
+    double test = std::fabs(ev0 - ev_old);
+    ev_old = ev0;
     return test < accur_bl;
   };
   // Device-resident steps: while nothing has been deflated (nd == 0) and the

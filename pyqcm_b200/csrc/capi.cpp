@@ -188,6 +188,27 @@ template <class F> int run_batch(int n, int threads, F &&fn) {
   if (first_code != QED_OK) t_err = first_msg;
   return first_code;
 }
+// The batched eigenvalue pass spreads its per-sector Ritz tests over the pool.
+// Those tests run inside a batch call whose own work loop may hold the pool,
+// so they take a second, smaller pool of their own.
+WorkerPool &ritz_pool() {
+  static WorkerPool *p = new WorkerPool;
+  return *p;
+}
+
+const bool g_parallel_for_set = [] {
+  set_parallel_for([](int n, const std::function<void(int)> &fn) {
+    int hw = (int)std::thread::hardware_concurrency();
+    const int threads = std::max(1, std::min({hw > 0 ? hw : 8, n, 64}));
+    std::atomic<int> next{0};
+    auto work = [&] {
+      for (int i = next++; i < n; i = next++) fn(i);
+    };
+    ritz_pool().run(threads - 1, work);
+  });
+  return true;
+}();
+
 // Weighted tasks run longest-first (LPT) on the batch thread pool.
 struct Task {
   double cost;
@@ -231,6 +252,7 @@ int batch_ground_states(BatchSet &b, int threads) {
   if (rc != QED_OK || todo.empty()) return rc;
   std::vector<std::vector<SectorSolve>> res(todo.size());
   std::vector<Task> tasks;
+  DeferredSectors defer;  // small Lanczos sectors: one batched eigenvalue pass below
   for (size_t k = 0; k < todo.size(); ++k) {
     Instance *I = todo[k];
     res[k].resize(I->target_sectors.size());
@@ -238,11 +260,32 @@ int batch_ground_states(BatchSet &b, int threads) {
     for (auto &sec : I->target_sectors) {
       SectorSolve *out = &res[k][i++];
       Sector s = sec;
-      tasks.push_back({(double)I->sector_dim(s), [I, s, out] { I->solve_sector(s, *out, ws()); }});
+      tasks.push_back({(double)I->sector_dim(s), [I, s, out, &defer] { I->solve_sector(s, *out, ws(), &defer); }});
     }
   }
   if ((rc = run_tasks(tasks, threads)) != QED_OK) return rc;
+  // eigenvalue passes: every large sector as one task, all small sectors as one
+  // batched task, so that the batched launches overlap the large sectors' work
+  tasks.clear();
+  double small_cost = 0.0;
+  for (auto &it : defer.items) small_cost += (double)it.H->D;
+  if (!defer.items.empty())
+    tasks.push_back({small_cost, [&defer] { lanczos_energy_batch(defer.items, ws()); }});
+  for (auto &it : defer.large) {
+    LanczosBatchItem *p = &it;
+    tasks.push_back({(double)it.H->D, [p] {
+                       try {
+                         *p->out = lanczos_energy(*p->H, ws(), p->seed);
+                       } catch (const Error &e) {
+                         fail(e.code, std::string(e.what()) + p->where);
+                       }
+                     }});
+  }
+  if ((rc = run_tasks(tasks, threads)) != QED_OK) return rc;
   rc = guarded([&] {
+    defer.items.clear();
+    defer.large.clear();
+    defer.ops.clear();
     for (size_t k = 0; k < todo.size(); ++k) todo[k]->select_states(res[k]);
   });
   if (rc != QED_OK) return rc;

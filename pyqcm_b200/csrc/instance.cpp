@@ -450,15 +450,25 @@ size_t Instance::sector_dim(const Sector &s) const {
 // Eigenvalue pass of one sector: Hamiltonian_Dense::states
 // (src_ed/Hamiltonian/Hamiltonian_Dense.hpp:110-125) below max_dim_full in the
 // non-factorized formats, the Lanczos eigenvalue pass otherwise.
-void Instance::solve_sector(const Sector &s, SectorSolve &out, Workspace &ws) {
+void Instance::solve_sector(const Sector &s, SectorSolve &out, Workspace &ws, DeferredSectors *defer) {
   out.sec = s;
   try {
-    SectorOp H(terms, s, ws, &tables);
+    auto Hp = std::make_unique<SectorOp>(terms, s, ws, &tables);
+    SectorOp &H = *Hp;
     out.dim = H.D;
     if (H.D == 0) return;
     if (!model->factorized && (long)H.D < opt_int("max_dim_full")) {
       out.dense = true;
       dense_eigensystem(H, ws, out.w, out.U);
+    } else if (defer) {
+      LanczosBatchItem it;
+      it.H = Hp.get();
+      it.seed = (uint64_t)opt_int("seed");
+      it.out = &out.lanczos;
+      it.where = where(s);
+      std::lock_guard<std::mutex> l(defer->m);
+      (H.D <= kLanczosCtaMaxDim ? defer->items : defer->large).push_back(it);
+      defer->ops.push_back(std::move(Hp));
     } else {
       out.lanczos = lanczos_energy(H, ws, (uint64_t)opt_int("seed"));
     }

@@ -54,6 +54,16 @@ struct SectorSolve {
   LanczosResult lanczos;     // Lanczos: tridiagonal and lowest energy
 };
 
+// Small Lanczos sectors set aside by Instance::solve_sector for one
+// lanczos_energy_batch over a whole batch call.
+struct DeferredSectors {
+  std::mutex m;
+  std::vector<std::unique_ptr<SectorOp>> ops;
+  std::vector<LanczosBatchItem> items;  // at most kLanczosCtaMaxDim states: one batched pass
+  std::vector<LanczosBatchItem> large;  // the others: one task each
+};
+
+
 // Hole (s = 0) or electron (s = 1) part of the Q-matrix of one state and spin.
 struct QPart {
   std::vector<double> e, V;
@@ -98,7 +108,9 @@ struct Instance {
   // (src_ed/model_instance.hpp:1164-1256), the one-body problem in full
   void one_body_solve(Workspace &ws);
   size_t sector_dim(const Sector &s) const;
-  void solve_sector(const Sector &s, SectorSolve &out, Workspace &ws);
+  // defer: if given, a Lanczos sector is only prepared (its operator and result
+  // slot go to defer, with the small sectors apart)
+  void solve_sector(const Sector &s, SectorSolve &out, Workspace &ws, DeferredSectors *defer = nullptr);
   void select_states(std::vector<SectorSolve> &r);  // every sector, in target order
   void state_vector(State &st, Workspace &ws);
   // the operator averages of the selected states, then gs_solved

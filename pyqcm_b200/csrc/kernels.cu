@@ -617,31 +617,56 @@ __device__ __forceinline__ double cta_sum(double v, double *sm) {
   return sm[32];
 }
 
-// A chunk of ground-state Lanczos steps of one small sector in one CTA: H.v
-// (diagonal, up and down hops gathered straight from L1/L2), alpha, the
-// orthogonalisation, beta and the normalisation, with CTA barriers in place of
-// kernel boundaries. v[0..2] rotate as (v_{j-1}, v_j, w) -> (v_j, w, v_{j-1}).
-__global__ void __launch_bounds__(1024) k_lanczos_cta(HvOperator op, double *v0, double *v1, double *v2,
-                                                       LanczosScalars ls, int nsteps) {
+// One sector per CTA; the job descriptor is staged in shared memory.
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z);
+
+__global__ void __launch_bounds__(kLanczosJobThreads) k_lanczos_start_jobs(const LanczosJob *__restrict__ jobs) {
+  __shared__ LanczosJob J;
   __shared__ double sm[33];
-  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  if (threadIdx.x == 0) J = jobs[blockIdx.x];
+  __syncthreads();
+  const uint32_t D = J.op.up.dim * J.op.dn.dim;
+  double *vp = J.v[J.rot], *vc = J.v[(J.rot + 1) % 3];
+  const uint64_t key = splitmix64(J.seed ^ 0x5eedull);
+  double s2 = 0.0;
+  for (uint32_t I = threadIdx.x; I < D; I += blockDim.x) {
+    uint64_t h1 = splitmix64(key + 2 * (uint64_t)I), h2 = splitmix64(key + 2 * (uint64_t)I + 1);
+    double u1 = ((h1 >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    double u2 = (h2 >> 11) * (1.0 / 9007199254740992.0);
+    const double v = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+    vc[I] = v;
+    vp[I] = 0.0;
+    s2 += v * v;
+  }
+  const double nrm = sqrt(cta_sum(s2, sm));
+  const double z = nrm > 0.0 ? 1.0 / nrm : 0.0;
+  for (uint32_t I = threadIdx.x; I < D; I += blockDim.x) vc[I] *= z;
+  if (threadIdx.x == 0) *J.beta_prev = 0.0;
+}
+
+__global__ void __launch_bounds__(kLanczosJobThreads) k_lanczos_jobs(const LanczosJob *__restrict__ jobs) {
+  __shared__ LanczosJob J;
+  __shared__ double sm[33];
+  if (threadIdx.x == 0) J = jobs[blockIdx.x];
+  __syncthreads();
+  const uint32_t du = J.op.up.dim, dd = J.op.dn.dim;
   const uint32_t D = du * dd;
-  double *vp = v0, *vc = v1, *w = v2;
-  for (int step = 0; step < nsteps; ++step) {
-    const double bprev = *ls.beta_prev;
+  double *vp = J.v[J.rot], *vc = J.v[(J.rot + 1) % 3], *w = J.v[(J.rot + 2) % 3];
+  for (int step = 0; step < J.nsteps; ++step) {
+    const double bprev = *J.beta_prev;
     double sa = 0.0;
     for (uint32_t I = threadIdx.x; I < D; I += blockDim.x) {
       const uint32_t u = I % du, d = I / du;
       const double x = vc[I];
-      double acc = (op.up.diag[u] + op.dn.diag[d] + inter_term(op.inter, op.up.bits[u], op.dn.bits[d])) * x;
+      double acc = (J.op.up.diag[u] + J.op.dn.diag[d] + inter_term(J.op.inter, J.op.up.bits[u], J.op.dn.bits[d])) * x;
       const double *row = vc + (size_t)d * du;
-      for (int k = 0; k < op.up.cnt[u]; ++k) {
-        const uint32_t e = op.up.ell[(size_t)k * du + u];
-        acc += op.up.vals[e & 255u] * row[e >> 8];
+      for (int k = 0; k < J.op.up.cnt[u]; ++k) {
+        const uint32_t e = J.op.up.ell[(size_t)k * du + u];
+        acc += J.op.up.vals[e & 255u] * row[e >> 8];
       }
-      for (int k = 0; k < op.dn.cnt[d]; ++k) {
-        const uint32_t e = op.dn.ell[(size_t)k * dd + d];
-        acc += op.dn.vals[e & 255u] * vc[(size_t)(e >> 8) * du + u];
+      for (int k = 0; k < J.op.dn.cnt[d]; ++k) {
+        const uint32_t e = J.op.dn.ell[(size_t)k * dd + d];
+        acc += J.op.dn.vals[e & 255u] * vc[(size_t)(e >> 8) * du + u];
       }
       acc -= bprev * vp[I];
       w[I] = acc;
@@ -658,13 +683,9 @@ __global__ void __launch_bounds__(1024) k_lanczos_cta(HvOperator op, double *v0,
     const double z = (b > 0.0) ? 1.0 / b : 0.0;
     for (uint32_t I = threadIdx.x; I < D; I += blockDim.x) w[I] *= z;
     if (threadIdx.x == 0) {
-      const int j = *ls.j;
-      ls.alpha_hist[j] = a;
-      ls.beta_hist[j] = b;
-      *ls.alpha_cur = a;
-      *ls.b2_cur = b * b;
-      *ls.beta_prev = b;
-      *ls.j = j + 1;
+      J.out[step] = a;
+      J.out[kLanczosJobMaxSteps + step] = b;
+      *J.beta_prev = b;
     }
     __syncthreads();  // v_{j+1} and beta_j visible to the whole CTA
     double *t = vp;
@@ -1410,9 +1431,15 @@ void launch_lanczos_advance(size_t D, double *y, const LanczosScalars &ls, cudaS
   QED_LAUNCH();
 }
 
-void launch_lanczos_cta(const HvOperator &op, double *vprev, double *vcur, double *w, const LanczosScalars &ls,
-                        int nsteps, cudaStream_t s) {
-  k_lanczos_cta<<<1, 1024, 0, s>>>(op, vprev, vcur, w, ls, nsteps);
+void launch_lanczos_start_jobs(const LanczosJob *jobs, int njobs, cudaStream_t s) {
+  if (njobs <= 0) return;
+  k_lanczos_start_jobs<<<njobs, kLanczosJobThreads, 0, s>>>(jobs);
+  QED_LAUNCH();
+}
+
+void launch_lanczos_jobs(const LanczosJob *jobs, int njobs, cudaStream_t s) {
+  if (njobs <= 0) return;
+  k_lanczos_jobs<<<njobs, kLanczosJobThreads, 0, s>>>(jobs);
   QED_LAUNCH();
 }
 

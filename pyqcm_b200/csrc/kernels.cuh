@@ -102,13 +102,28 @@ int launch_axpy_dev(size_t D, double *y, const double *x, const double *a_dev, R
                     const int *skip = nullptr);
 // y *= 1 / sqrt(*b2_cur) (0 if that is 0); records alpha_j, beta_j and advances *j.
 void launch_lanczos_advance(size_t D, double *y, const LanczosScalars &ls, cudaStream_t s);
-// nsteps whole Lanczos steps of a sector of at most kLanczosCtaMaxDim states in
-// one CTA (one launch instead of six per step). On entry vprev = v_{j-1},
-// vcur = v_j, w = scratch; after n steps the roles have rotated n times as
-// (vprev, vcur, w) <- (vcur, w, vprev).
 constexpr size_t kLanczosCtaMaxDim = 8192;
-void launch_lanczos_cta(const HvOperator &op, double *vprev, double *vcur, double *w, const LanczosScalars &ls,
-                        int nsteps, cudaStream_t s);
+
+// Ground-state Lanczos of many small sectors in one launch, one CTA of kLanczosJobThreads threads per
+// sector (dimension at most kLanczosCtaMaxDim): the ground-state Lanczos
+// chunks of a whole batch of sectors advance together. Buffer roles of a job:
+// v_{j-1} = v[rot], v_j = v[(rot + 1) % 3], scratch = v[(rot + 2) % 3]; they
+// rotate once per step. out receives alpha then beta of the launch's steps
+// (2 * kLanczosJobMaxSteps doubles per job).
+constexpr int kLanczosJobThreads = 256;
+constexpr int kLanczosJobMaxSteps = 16;
+struct LanczosJob {
+  HvOperator op;
+  double *v[3];
+  double *beta_prev;  // beta_{j-1} (0 before the first step)
+  double *out;
+  unsigned long long seed;
+  int nsteps, rot;
+};
+// v_j = normalised random start vector (the values of launch_random for `seed`),
+// v_{j-1} = 0, beta_prev = 0, for every job
+void launch_lanczos_start_jobs(const LanczosJob *jobs, int njobs, cudaStream_t s);
+void launch_lanczos_jobs(const LanczosJob *jobs, int njobs, cudaStream_t s);
 
 // ---- blocks of p vectors (interleaved: element (I, c) at I * p + c) --------
 // These serve the block form of the band-Lanczos recurrence, where one table

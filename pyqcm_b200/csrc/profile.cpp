@@ -12,7 +12,8 @@ const char *kNames[kPhCount] = {"sector setup",       "GS Lanczos (eigenvalue)",
                                 "dense sectors",      "c/c+ start vectors",      "band Lanczos recurrence",
                                 "band Lanczos checks", "band projected eigensystem", "continued fractions",
                                 "GS Ritz tests (in GS eigenvalue)", "block Lanczos recurrence",
-                                "block Lanczos fallbacks", "ground-state operator averages"};
+                                "block Lanczos fallbacks", "ground-state operator averages",
+                                "GS batched small sectors"};
 
 struct Totals {
   std::atomic<long long> ns[kPhCount];

@@ -20,6 +20,7 @@ enum Phase {
   kPhBlockLoop,     // block form of the band-Lanczos recurrence
   kPhBlockFallback, // block recurrence abandoned for the band one (count)
   kPhAverages,      // operator averages of the ground state (cluster_averages)
+  kPhGsBatch,       // batched eigenvalue pass of small sectors (inside kPhGsLanczos)
   kPhCount
 };
 

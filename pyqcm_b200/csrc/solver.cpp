@@ -348,8 +348,29 @@ void SectorOp::apply(const double *x, double *y, Workspace &ws) const {
 
 namespace {
 // Random start vector, normalised (Hamiltonian::states -> random(),
-// src_util/vector_num.cpp:114-119); deterministic in `seed`.
+// src_util/vector_num.cpp:114-119); deterministic in `seed`. Small sectors take
+// it from the per-sector start kernel of the batched eigenvalue pass, so that
+// the eigenvector pass replays the same v_0.
 void start_vector(size_t D, uint64_t seed, double *v, Workspace &ws) {
+  if (D <= kLanczosCtaMaxDim) {
+    DevBuf<double> prev(D), bp(1);
+    LanczosJob J;
+    J.op.up.dim = (uint32_t)D;
+    J.op.dn.dim = 1;
+    J.v[0] = prev.p;
+    J.v[1] = v;
+    J.v[2] = prev.p;
+    J.beta_prev = bp.p;
+    J.out = nullptr;
+    J.seed = seed;
+    J.nsteps = 0;
+    J.rot = 0;
+    DevBuf<LanczosJob> dj(1);
+    dj.upload(&J, 1, ws.stream);
+    launch_lanczos_start_jobs(dj.p, 1, ws.stream);
+    ws.sync();
+    return;
+  }
   const int nb = launch_random(D, seed, v, ws.red, ws.stream);
   const double n2 = ws.sums(nb, 1)[0];
   launch_scale(D, v, 1.0 / std::sqrt(n2), ws.stream);
@@ -377,7 +398,138 @@ void start_vector(size_t D, uint64_t seed, double *v, Workspace &ws) {
 // 8x leaves a wide margin while the O(j^2) QL runs only on the last steps.
 constexpr double kQlBand = 1e-3;
 
+namespace {
+ParallelFor g_parallel_for;
+}  // namespace
+
+void set_parallel_for(ParallelFor f) { g_parallel_for = std::move(f); }
+
+void lanczos_energy_batch(std::vector<LanczosBatchItem> &items, Workspace &ws) {
+  PhaseScope ps(kPhGsLanczos);
+  const int n = (int)items.size();
+  if (!n) return;
+  PhaseScope ps_batch(n > 1 ? kPhGsBatch : kPhGsLanczos);
+  const double accur = opt_double("accur_lanczos");
+  const long max_iter = opt_int("max_iter_lanczos");
+  cudaStream_t s = ws.stream;
+  constexpr int kChunk = kLanczosJobMaxSteps;
+  // one arena for the three vectors of every sector (32-byte aligned blocks)
+  std::vector<size_t> off(n);
+  size_t tot = 0;
+  for (int i = 0; i < n; ++i) {
+    if (items[i].H->D > kLanczosCtaMaxDim) fail(QED_ERR_INTERNAL, "lanczos_energy_batch: sector too large");
+    off[i] = tot;
+    tot += 3 * ((items[i].H->D + 3) / 4 * 4);
+  }
+  DevBuf<double> arena(std::max<size_t>(tot, 1)), bprev(n), out((size_t)n * 2 * kChunk);
+  DevBuf<LanczosJob> djobs(n);
+  std::vector<LanczosJob> jobs(n);
+  struct Run {
+    RitzTracker tracker;
+    double lambda0 = 0.0;
+    int rot = 0, chunk = 0;
+  };
+  std::vector<Run> run(n);
+  for (int i = 0; i < n; ++i) {
+    const size_t D = items[i].H->D;
+    const size_t Dp = (D + 3) / 4 * 4;
+    LanczosJob &J = jobs[i];
+    J.op = items[i].H->op;
+    for (int r = 0; r < 3; ++r) J.v[r] = arena.p + off[i] + r * Dp;
+    J.beta_prev = bprev.p + i;
+    J.out = out.p + (size_t)i * 2 * kChunk;
+    J.seed = items[i].seed;
+    J.nsteps = 0;
+    J.rot = 0;
+    *items[i].out = LanczosResult();
+    // a first short chunk: tiny sectors stop after about D steps
+    run[i].chunk = (int)std::min<size_t>(std::max<size_t>(D, 2), 8);
+  }
+  djobs.upload(jobs.data(), n, s);
+  launch_lanczos_start_jobs(djobs.p, n, s);
+  std::vector<int> active(n);
+  for (int i = 0; i < n; ++i) active[i] = i;
+  std::vector<LanczosJob> batch;
+  std::vector<double> hout;
+  while (!active.empty()) {
+    const int na = (int)active.size();
+    batch.resize(na);
+    for (int a = 0; a < na; ++a) {
+      const int i = active[a];
+      batch[a] = jobs[i];
+      batch[a].nsteps = run[i].chunk;
+      batch[a].rot = run[i].rot;
+      batch[a].out = out.p + (size_t)a * 2 * kChunk;
+    }
+    djobs.upload(batch.data(), na, s);
+    launch_lanczos_jobs(djobs.p, na, s);
+    hout.resize((size_t)na * 2 * kChunk);
+    out.download(hout.data(), hout.size(), s);
+    ws.sync();
+    PhaseScope ps_ritz(kPhRitz);
+    std::vector<char> done(na, 0);
+    std::vector<std::string> err(na);
+    std::vector<int> code(na, 0);
+    auto test = [&](int a) {  // the Ritz tests of one sector's chunk, in step order
+      const int i = active[a];
+      Run &R = run[i];
+      LanczosResult &res = *items[i].out;
+      const double *ha = hout.data() + (size_t)a * 2 * kChunk, *hb = ha + kChunk;
+      bool stop = false;
+      try {
+        for (int k = 0; k < R.chunk && !stop; ++k) {
+          res.alpha.push_back(ha[k]);
+          res.beta.push_back(hb[k]);
+          double last = 1.0;
+          tridiag_lowest_track((int)res.alpha.size(), res.alpha.data(), res.beta.data(), R.tracker, &R.lambda0,
+                               &last);
+          double ritz = std::fabs(last * hb[k]);
+          if (std::fabs(ritz - accur) < kQlBand * accur) {
+            if (!tridiag_lowest_last((int)res.alpha.size(), res.alpha.data(), res.beta.data(), &R.lambda0, &last))
+              fail(QED_ERR_LANCZOS, "tridiagonal eigensolver did not converge" + items[i].where);
+            ritz = std::fabs(last * hb[k]);
+          }
+          if ((long)res.alpha.size() > max_iter)
+            fail(QED_ERR_LANCZOS, "Lanczos procedure exceeded " + std::to_string(max_iter) + " iterations" +
+                                      items[i].where);
+          if (!(ritz > accur)) stop = true;
+        }
+      } catch (const Error &e) {
+        code[a] = e.code;
+        err[a] = e.what();
+        return;
+      }
+      R.rot = (R.rot + R.chunk) % 3;
+      R.chunk = kChunk;
+      if (stop) {
+        res.energy = R.lambda0;
+        res.iterations = (int)res.alpha.size();
+        done[a] = 1;
+      }
+    };
+    if (g_parallel_for && na > 1)
+      g_parallel_for(na, test);
+    else
+      for (int a = 0; a < na; ++a) test(a);
+    std::vector<int> still;
+    for (int a = 0; a < na; ++a) {
+      if (code[a]) fail(code[a], err[a]);
+      if (!done[a]) still.push_back(active[a]);
+    }
+    active.swap(still);
+  }
+}
+
 LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed) {
+  if (H.D <= kLanczosCtaMaxDim) {
+    LanczosResult res;
+    std::vector<LanczosBatchItem> one(1);
+    one[0].H = &H;
+    one[0].seed = seed;
+    one[0].out = &res;
+    lanczos_energy_batch(one, ws);
+    return res;
+  }
   PhaseScope ps(kPhGsLanczos);
   LanczosResult res;
   const size_t D = H.D;
@@ -414,15 +566,7 @@ LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed) {
   bool stop = false;
   while (!stop) {
     if (launched + chunk > cap) fail(QED_ERR_INTERNAL, "Lanczos history overflow");
-    if (D <= kLanczosCtaMaxDim) launch_lanczos_cta(H.op, pa, pb, pc, ls, chunk, s);
     for (int k = 0; k < chunk; ++k) {
-      if (D <= kLanczosCtaMaxDim) {  // the CTA kernel above ran the step
-        double *t = pa;
-        pa = pb;
-        pb = pc;
-        pc = t;
-        continue;
-      }
       sub.z[0] = pa;
       launch_hv_rows(H.op, pb, 1.0, pc, sub, s);
       int nb = launch_hv_cols(H.op, pb, 1.0, pc, 1, ws.red, s);

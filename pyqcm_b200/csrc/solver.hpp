@@ -7,6 +7,7 @@
 // vector work runs in the kernels of kernels.cu, only the small tridiagonal /
 // banded projected problems are solved on the host.
 #pragma once
+#include <functional>
 #include <map>
 #include <memory>
 #include <vector>
@@ -81,6 +82,21 @@ struct LanczosResult {
   std::vector<double> alpha, beta;
 };
 LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed);
+// The eigenvalue pass of many sectors of at most kLanczosCtaMaxDim states at
+// once: one CTA per sector, all sectors advancing by chunks in one launch, the
+// Ritz test of each applied on the host after every chunk. Results are those
+// of lanczos_energy, which runs a single small sector through the same path.
+struct LanczosBatchItem {
+  const SectorOp *H = nullptr;
+  uint64_t seed = 0;
+  LanczosResult *out = nullptr;
+  std::string where;  // appended to error messages
+};
+void lanczos_energy_batch(std::vector<LanczosBatchItem> &items, Workspace &ws);
+// Host-side parallel loop used by lanczos_energy_batch for the per-sector Ritz
+// tests (the library's worker pool; a plain loop until one is installed).
+using ParallelFor = std::function<void(int n, const std::function<void(int)> &fn)>;
+void set_parallel_for(ParallelFor f);
 void lanczos_eigenvector(const SectorOp &H, Workspace &ws, const LanczosResult &res,
                          uint64_t seed, DevBuf<double> &psi);
 // Both passes.

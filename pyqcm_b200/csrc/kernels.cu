@@ -773,18 +773,21 @@ __global__ void k_interleave(size_t D, int p, BlockSrc src, double *x) {
     x[t] = src.v[t % p][t / p];
 }
 
-// Up-spin hops, diagonal and the X2 M2 term of a block H.v, rows pass: kRowParts
-// CTAs share one dn-row (each an eighth of its up strings), so the rows in
-// flight (grid / kRowParts, about 18 on a B200) keep their gather targets
-// (du * p * 8 bytes each) resident in L2; each hop gathers the p values of one
-// state (one 128-byte line for p = 16); one hop-table read serves p vectors;
-// four hops are in flight per thread.
-constexpr int kRowParts = 8;
+// Up-spin hops, diagonal and the X2 M2 term of a block H.v, rows pass: `parts`
+// CTAs share one dn-row (each a quarter of its up strings by default), so the
+// rows in flight (grid / parts: 74 on a B200 with two CTAs per SM) keep their
+// gather targets (du * p * 8 bytes each, 1.65 MB for the 4x4 sector at p = 16)
+// resident in L2; each hop gathers the p values of one state (one 128-byte line
+// for p = 16); one hop-table read serves p vectors; four hops are in flight per
+// thread. On the 4x4 Green function (p = 16): 8 parts x 1 CTA per SM 20.0-20.7 s,
+// 16 x 2 19.6 s, 4 x 2 18.6-19.2 s, 2 x 2 19.9 s, 4 x 3 19.9 s.
+constexpr int kRowParts = 4;
+constexpr int kUpCtasPerSm = 2;
 constexpr int kUpThreads = 1024;
 template <int P>
-__global__ void __launch_bounds__(kUpThreads) k_block_up(HvOperator op, int p, const double *__restrict__ X,
+__global__ void __launch_bounds__(kUpThreads, 2) k_block_up(HvOperator op, int p, const double *__restrict__ X,
                                                     double *__restrict__ Y, const double *__restrict__ X2,
-                                                    const double *__restrict__ M2, double s2) {
+                                                    const double *__restrict__ M2, double s2, int parts) {
   __shared__ double uvals[256], m2[P * P];
   for (int i = threadIdx.x; i < op.up.nvals; i += blockDim.x) uvals[i] = op.up.vals[i];
   if (X2)
@@ -793,10 +796,10 @@ __global__ void __launch_bounds__(kUpThreads) k_block_up(HvOperator op, int p, c
   const uint32_t du = op.up.dim, dd = op.dn.dim;
   const int c = threadIdx.x % P, g = threadIdx.x / P, G = blockDim.x / P;
   if (c >= p) return;  // no barrier below
-  const int part = blockIdx.x % kRowParts;
-  const uint32_t uchunk = (du + kRowParts - 1) / kRowParts;
+  const int part = blockIdx.x % parts;
+  const uint32_t uchunk = (du + parts - 1) / parts;
   const uint32_t ub = part * uchunk, ue = min(du, ub + uchunk);
-  for (uint32_t d = blockIdx.x / kRowParts; d < dd; d += gridDim.x / kRowParts) {
+  for (uint32_t d = blockIdx.x / parts; d < dd; d += gridDim.x / parts) {
     const size_t rowb = (size_t)d * du;
     const double ddg = op.dn.diag[d];
     const uint32_t dnb = op.dn.bits[d];
@@ -1493,8 +1496,14 @@ void launch_block_hv(const HvOperator &op, int p, const double *X, double *Y, co
     const int grid = (int)std::min<size_t>(op.dn.dim, (size_t)sms * std::min(by_threads, by_smem));
     k_block_up_smem<<<grid, threads, row_bytes, s>>>(op, p, X, Y, X2, M2, s2);
   } else {
-    const int up_grid = std::max(kRowParts, (sms / kRowParts) * kRowParts);
-    QED_BLOCK_DISPATCH(P, (k_block_up<PP><<<up_grid, kUpThreads, 0, s>>>(op, p, X, Y, X2, M2, s2)));
+    static const std::pair<int, int> cfg = [] {  // (CTAs per dn-row, CTAs per SM); QED_BLOCKUP="parts,mult"
+      int parts = kRowParts, mult = kUpCtasPerSm;
+      if (const char *e = getenv("QED_BLOCKUP")) sscanf(e, "%d,%d", &parts, &mult);
+      return std::make_pair(std::max(1, parts), std::max(1, mult));
+    }();
+    const int parts = cfg.first;
+    const int up_grid = std::max(parts, (sms * cfg.second / parts) * parts);
+    QED_BLOCK_DISPATCH(P, (k_block_up<PP><<<up_grid, kUpThreads, 0, s>>>(op, p, X, Y, X2, M2, s2, parts)));
   }
   QED_LAUNCH();
   QED_BLOCK_DISPATCH(P, (k_block_dn<PP><<<sms * 8, kThreads, 0, s>>>(op, p, X, Y)));

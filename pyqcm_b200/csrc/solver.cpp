@@ -42,7 +42,6 @@ Workspace::~Workspace() {
   if (stream) cudaStreamSynchronize(stream);
   if (host) cudaFreeHost(host);
   if (pin) cudaFreeHost(pin);
-  if (sync_ev) cudaEventDestroy(sync_ev);
   if (tls_stream == stream) tls_stream = nullptr;
   if (stream) cudaStreamDestroy(stream);
 }
@@ -53,27 +52,7 @@ const double *Workspace::sums(int nblocks, int nred) {
   return host;
 }
 
-// Host waits: cudaStreamSynchronize (the device's scheduling policy, a spin
-// while few contexts are active), or with QED_SYNC=block a blocking-sync event,
-// which lets the waiting thread sleep so that more host threads than cores can
-// drive concurrent solves.
-static bool blocking_sync() {
-  static const bool b = [] {
-    const char *e = getenv("QED_SYNC");
-    return e && std::string(e) == "block";
-  }();
-  return b;
-}
-
-void Workspace::sync() {
-  if (!blocking_sync()) {
-    QED_CUDA(cudaStreamSynchronize(stream));
-    return;
-  }
-  if (!sync_ev) QED_CUDA(cudaEventCreateWithFlags(&sync_ev, cudaEventBlockingSync | cudaEventDisableTiming));
-  QED_CUDA(cudaEventRecord(sync_ev, stream));
-  QED_CUDA(cudaEventSynchronize(sync_ev));
-}
+void Workspace::sync() { QED_CUDA(cudaStreamSynchronize(stream)); }
 
 double *Workspace::pinned(size_t n) {
   if (n > pin_n) {

@@ -25,7 +25,6 @@ struct Workspace {
   DevBuf<double> partials, out;
   double *host = nullptr;
   double *pin = nullptr;  // pinned host staging, grown on demand
-  cudaEvent_t sync_ev = nullptr;  // blocking-sync event (QED_SYNC=block)
   size_t pin_n = 0;
   Workspace();
   ~Workspace();

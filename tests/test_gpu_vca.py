@@ -39,3 +39,34 @@ def test_surrogate_guided_vca_reaches_the_ed_stationary_point(qed):
     om = ev(np.c_[[U, U], np.vstack([x_ed, x_s])])
     assert abs(om[0] - om[1]) < 1e-8, (x_ed, x_s, om)
     assert np.max(np.abs(x_ed - x_s)) < 1e-3
+
+
+def test_vca_stationary_point_matches_reference(qed, oracle):
+    """The same Newton-Raphson search on the reference's Potthoff functional (the
+    compiled lattice layer, CPU) and on this solver's (GPU): same stationary point,
+    same Omega there within 1e-8."""
+    from pyqcm_b200 import vca
+    model, ev = _evaluator(qed)
+    prob = model.prob
+    oracle.set_param("GF_method", "L")
+    oracle.load_lattice(prob, 0)
+    oracle.set_grids(ev.freqs, ev.weights, ev.nk)
+    U = 8.0
+    lab = [100]
+
+    def f_ref(P):
+        out = []
+        for x in np.atleast_2d(P):
+            lab[0] += 1
+            oracle.lattice_new_instance(lab[0], **vca.vca_values([U, *x]))
+            out.append(oracle.lattice_potthoff(lab[0]))
+        return np.array(out)
+
+    f_gpu = lambda P: ev(np.c_[np.full(len(P), U), P])
+    acc = [2e-5, 2e-5]
+    x_ref, *_ = vca.newton_raphson(f_ref, [0.15, 0.0], [0.02, 0.02], acc)
+    x_gpu, *_ = vca.newton_raphson(f_gpu, [0.15, 0.0], [0.02, 0.02], acc)
+    assert np.max(np.abs(x_ref - x_gpu)) < 1e-4, (x_ref, x_gpu)
+    om_ref = f_ref(np.array([x_ref]))[0]
+    om_gpu = f_gpu(np.array([x_gpu]))[0]
+    assert abs(om_ref - om_gpu) < 1e-8, (om_ref, om_gpu)

@@ -128,6 +128,18 @@ int qed_sef_integrand_grid(int label, int spin_down, int dim, const double *V0, 
                            const int *R, const double *v, int nw, const double *w, int nkx, int nky, int nkz,
                            double *I_w);
 
+/* The projected CPT Green function of the CDMFT host, per frequency:
+ * lattice_model_instance::projected_Green_function (src_qcm/CPT.cpp:283-346) with
+ * set_Gcpt (:76-86) and set_V (:22-64): Gproj(i w[i]) = average over the grid
+ * k = ((a + offset)/nkx, (b + offset)/nky, (c + offset)/nkz) of G (1 - V(k) G)^{-1},
+ * V(k) = V0_i + sum_e v[e] exp(2 pi i k.R[e]). V0: nw k-independent parts (dim x dim
+ * complex column-major each; with bath orbitals they hold -Gamma(i w[i])), elements as
+ * in qed_sef_integrand_grid; Gproj: nw dim x dim complex, column-major. The reference's
+ * grid is kgrid_side points per direction with offset 0.5. On the GPU; dim <= 16. */
+int qed_cpt_projected_green_function(int label, int spin_down, int dim, const double *V0, int nel, const int *r,
+                                     const int *c, const int *R, const double *v, int nw, const double *w,
+                                     int nkx, int nky, int nkz, double offset, double *Gproj);
+
 /* ED::self_energy (src_ed/qcm_ED.hpp:180 -> src_ed/model_instance.hpp:683-700), batched. */
 int qed_self_energy(int label, int spin_down, int nz, const double *z, double *S);
 

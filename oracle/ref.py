@@ -97,6 +97,10 @@ def lib():
             "ref_qcm_V_superdual": [C.c_int, C.c_int, C.c_double, C.c_double, dp, ip, dp],
             "ref_qcm_cluster_gf": [C.c_int, C.c_int, C.c_double, C.c_double, ip, dp],
             "ref_qcm_ed_label": [C.c_int, C.c_int],
+            "ref_qcm_cdmft_variational_set": [C.c_int, cpp],
+            "ref_qcm_cdmft_host": [C.c_int, C.c_int, dp, dp],
+            "ref_qcm_get_cdmft_host": [C.c_int, C.c_int, C.c_int, C.c_int, ip, dp],
+            "ref_qcm_cdmft_distance": [C.c_int, C.c_int, dp, C.c_int, dp],
         })
         for name, args in sig.items():
             f = getattr(L, name)
@@ -412,7 +416,9 @@ def load_lattice(prob, label: int = 0, cluster_name: str = "clus"):
     -> set_parameters, pyqcm/__init__.py:107-600) and creates instance `label`."""
     L = lib()
     _check(L.ref_qcm_great_reset())
-    new_model(cluster_name, prob.n_sites, 0)
+    new_model(cluster_name, prob.n_sites, getattr(prob, "n_bath", 0))
+    for op, (typ, el) in getattr(prob, "cluster_operators", {}).items():
+        new_operator(cluster_name, op, typ, el)
     pos = [c for s in prob.sites for c in s]
     _check(L.ref_qcm_add_cluster(_longs([0, 0, 0]), prob.n_sites, _longs(pos), -1, 0))
     _check(L.ref_qcm_add_system(cluster_name.encode(), 0))
@@ -488,3 +494,24 @@ def lattice_cluster_gf(label: int, w: complex, spin_down=False):
 
 def lattice_ed_label(label: int, s: int = 0) -> int:
     return lib().ref_qcm_ed_label(label, s)
+
+
+def cdmft_variational_set(names):
+    _check(lib().ref_qcm_cdmft_variational_set(len(names), _strs(names)))
+
+
+def cdmft_host(label, freqs, weights):
+    f = np.ascontiguousarray(freqs, dtype=np.float64)
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    _check(lib().ref_qcm_cdmft_host(label, len(f), _dp(f), _dp(w)))
+
+
+def get_cdmft_host(label, iw, spin_down=False, clus=0):
+    return _cmat(lib().ref_qcm_get_cdmft_host, label, int(spin_down), iw, clus)
+
+
+def cdmft_distance(label, p, clus=0):
+    v = np.ascontiguousarray(p, dtype=np.float64)
+    d = C.c_double()
+    _check(lib().ref_qcm_cdmft_distance(label, len(v), _dp(v), clus, C.byref(d)))
+    return d.value

@@ -575,6 +575,39 @@ int ref_qcm_cluster_gf(int label, int spin_down, double w_re, double w_im, int *
   });
 }
 
+// CDMFT (src_qcm/CPT.cpp:356-560): variational parameters of cluster 0, the
+// host function on a frequency grid, its matrices, and the distance
+int ref_qcm_cdmft_variational_set(int n, const char **names) {
+  return guarded([&] {
+    vector<vector<string>> v(1);
+    for (int i = 0; i < n; ++i) v[0].push_back(names[i]);
+    QCM::CDMFT_variational_set(v);
+  });
+}
+
+int ref_qcm_cdmft_host(int label, int n, const double *freqs, const double *weights) {
+  return guarded([&] {
+    vector<double> f(freqs, freqs + n), w(weights, weights + n);
+    QCM::CDMFT_host(f, w, label);
+  });
+}
+
+int ref_qcm_get_cdmft_host(int label, int spin_down, int iw, int clus, int *dim, double *out) {
+  return guarded([&] {
+    auto H = QCM::get_CDMFT_host(spin_down != 0, label);
+    const matrix<Complex> &m = H.at((size_t)iw).at((size_t)clus);
+    *dim = (int)m.r;
+    if (out) put_complex(m, out);
+  });
+}
+
+int ref_qcm_cdmft_distance(int label, int n, const double *p, int clus, double *d) {
+  return guarded([&] {
+    vector<double> v(p, p + n);
+    *d = QCM::CDMFT_distance(v, clus, label);
+  });
+}
+
 // ED label of system s of lattice instance `label` (nsys * label + s)
 int ref_qcm_ed_label(int label, int s) { return (int)(qcm_model->nsys * (size_t)label + (size_t)s); }
 

@@ -107,6 +107,8 @@ def lib():
         "qed_destroy_table": [C.c_int, C.c_int, C.c_int, C.c_int, lp, ip],
         "qed_sef_integrand_grid": [C.c_int, C.c_int, C.c_int, dp, C.c_int, ip, ip, ip, dp, C.c_int, dp,
                                    C.c_int, C.c_int, C.c_int, dp],
+        "qed_cpt_projected_green_function": [C.c_int, C.c_int, C.c_int, dp, C.c_int, ip, ip, ip, dp, C.c_int,
+                                             dp, C.c_int, C.c_int, C.c_int, C.c_double, dp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -418,6 +420,26 @@ def sef_integrand_grid(V0, r, c, R, v, w, nk, spin_down: bool = False, label: in
                                         _ip(ci if n else np.zeros(1, np.int32)), _ip(Ri), _dp(vv.view(np.float64)),
                                         len(ww), _dp(ww), nk[0], nk[1], nk[2], _dp(out)))
     return out
+
+
+def cpt_projected_green_function(V0, r, c, R, v, w, nk, offset=0.5, spin_down: bool = False, label: int = 0):
+    """Per frequency w[i]: grid average of G (1 - V(k) G)^{-1} (see
+    qed_cpt_projected_green_function); V0: (nw, dim, dim) k-independent parts."""
+    V0 = np.asarray(V0, dtype=np.complex128)
+    nw, dim = V0.shape[0], V0.shape[1]
+    v0 = np.ascontiguousarray(np.transpose(V0, (0, 2, 1))).view(np.float64)  # column-major blocks
+    n = len(r)
+    ri = np.ascontiguousarray(r if n else [0], dtype=np.int32)
+    ci = np.ascontiguousarray(c if n else [0], dtype=np.int32)
+    Ri = np.ascontiguousarray(np.reshape(R, (-1, 3)) if n else np.zeros((1, 3)), dtype=np.int32)
+    vv = np.ascontiguousarray(v if n else [0.0], dtype=np.complex128)
+    ww = np.ascontiguousarray(w, dtype=np.float64)
+    nk = tuple(int(x) for x in nk) + (1,) * (3 - len(tuple(nk)))
+    out = np.zeros(2 * dim * dim * nw)
+    _check(lib().qed_cpt_projected_green_function(label, int(spin_down), dim, _dp(v0), n, _ip(ri), _ip(ci), _ip(Ri),
+                                                  _dp(vv.view(np.float64)), nw, _dp(ww), nk[0], nk[1], nk[2],
+                                                  float(offset), _dp(out)))
+    return (out[0::2] + 1j * out[1::2]).reshape(nw, dim, dim).transpose(0, 2, 1)
 
 
 def qmatrix(spin_down: bool = False, label: int = 0, capacity: int = 1 << 16):

@@ -567,6 +567,44 @@ int qed_sef_integrand_grid(int label, int spin_down, int dim, const double *V0, 
   });
 }
 
+int qed_cpt_projected_green_function(int label, int spin_down, int dim, const double *V0, int nel, const int *r,
+                                     const int *c, const int *R, const double *v, int nw, const double *w,
+                                     int nkx, int nky, int nkz, double offset, double *Gproj) {
+  return guarded([&] {
+    if (nw < 0 || nel < 0 || nkx < 1 || nky < 1 || nkz < 1)
+      fail(QED_ERR_ARGUMENT, "qed_cpt_projected_green_function: bad sizes");
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    if (dim != I->model->n_sites)
+      fail(QED_ERR_ARGUMENT, "qed_cpt_projected_green_function: dim differs from the cluster's Green function dimension");
+    for (int e = 0; e < nel; ++e)
+      if (r[e] < 0 || r[e] >= dim || c[e] < 0 || c[e] >= dim)
+        fail(QED_ERR_ARGUMENT, "qed_cpt_projected_green_function: element index outside the Green function");
+    if (nw == 0) return;
+    Workspace &W = ws();
+    std::vector<cplx> z(nw);
+    for (int i = 0; i < nw; ++i) z[i] = cplx(0.0, w[i]);
+    const size_t nn = (size_t)dim * dim;
+    DevBuf<double> dG(2 * nn * nw), dV0(2 * nn * nw), dR(3 * (size_t)std::max(nel, 1)),
+        dv(2 * (size_t)std::max(nel, 1)), part((size_t)cpt_partials_size(dim, nw)), dP(2 * nn * nw);
+    DevBuf<int> dr(std::max(nel, 1)), dc(std::max(nel, 1));
+    I->green_function_device(z.data(), nw, spin_down != 0, dG.p, W);
+    dV0.upload(V0, 2 * nn * nw, W.stream);
+    if (nel) {
+      std::vector<double> Rd(3 * (size_t)nel);
+      for (size_t i = 0; i < Rd.size(); ++i) Rd[i] = (double)R[i];
+      dR.upload(Rd, W.stream);
+      dv.upload(v, 2 * (size_t)nel, W.stream);
+      dr.upload(r, nel, W.stream);
+      dc.upload(c, nel, W.stream);
+    }
+    launch_cpt_projected(dim, nw, dG.p, dV0.p, nel, dr.p, dc.p, dR.p, dv.p, nkx, nky, nkz, offset, part.p, dP.p,
+                         W.stream);
+    dP.download(Gproj, 2 * nn * nw, W.stream);
+    W.sync();
+  });
+}
+
 int qed_self_energy(int label, int spin_down, int nz, const double *z, double *S) {
   return guarded([&] {
     auto I = instance(label);

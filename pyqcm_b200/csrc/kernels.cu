@@ -1236,6 +1236,130 @@ __global__ void __launch_bounds__(kSefThreads) k_sef_logdet(int n, const double 
   }
 }
 
+// Projected CPT Green function on a wavevector grid, for the CDMFT host
+// (lattice_model_instance::projected_Green_function, src_qcm/CPT.cpp:283-346;
+// set_Gcpt, :76-86): for frequency w, the grid average of
+//   G_cpt(k) = G (1 - V(k) G)^{-1},  V(k) = V0(w) + sum_e v_e exp(2 pi i k.R_e),
+// k = ((a + off)/nkx, (b + off)/nky, (c + off)/nkz). One CTA per frequency;
+// thread t sums the k points t, t + blockDim.x, ... into its own n x n
+// accumulator (local memory, n <= 16) and writes it to partials[(w * T + t)];
+// k_cpt_reduce adds the T accumulators in a fixed order. (1 - V G) is inverted
+// by Gauss-Jordan elimination with partial pivoting.
+constexpr int kCptThreads = 64;
+__global__ void __launch_bounds__(kCptThreads) k_cpt_partial(int n, const double *__restrict__ G,
+                                                              const double *__restrict__ V0, int nel,
+                                                              const int *__restrict__ er, const int *__restrict__ ec,
+                                                              const double *__restrict__ eR,
+                                                              const double *__restrict__ ev, int nkx, int nky,
+                                                              int nkz, double off, double *partials) {
+  const int iw = blockIdx.x, T = blockDim.x;
+  const int nn = n * n;
+  const long nk = (long)nkx * nky * nkz;
+  const double *g = G + 2 * (size_t)iw * nn, *v0 = V0 + 2 * (size_t)iw * nn;
+  double sr[kSefMaxN * kSefMaxN], si[kSefMaxN * kSefMaxN];  // this thread's sum of G_cpt
+  double ar[kSefMaxN * kSefMaxN], ai[kSefMaxN * kSefMaxN];  // 1 - V G, then its inverse
+  double br[kSefMaxN * kSefMaxN], bi[kSefMaxN * kSefMaxN];  // V(k), then the identity being transformed
+  for (int t = 0; t < nn; ++t) sr[t] = si[t] = 0.0;
+  for (long kid = threadIdx.x; kid < nk; kid += T) {
+    const int ix = (int)(kid / ((long)nky * nkz)), iy = (int)((kid / nkz) % nky), iz = (int)(kid % nkz);
+    const double kx = (ix + off) / nkx, ky = (iy + off) / nky, kz = (iz + off) / nkz;
+    for (int t = 0; t < nn; ++t) {
+      br[t] = v0[2 * t];
+      bi[t] = v0[2 * t + 1];
+    }
+    for (int e = 0; e < nel; ++e) {
+      double s, c;
+      sincospi(2.0 * (kx * eR[3 * e] + ky * eR[3 * e + 1] + kz * eR[3 * e + 2]), &s, &c);
+      const int t = er[e] + n * ec[e];
+      br[t] += ev[2 * e] * c - ev[2 * e + 1] * s;
+      bi[t] += ev[2 * e] * s + ev[2 * e + 1] * c;
+    }
+    for (int b = 0; b < n; ++b)  // A = 1 - V G (column-major)
+      for (int a = 0; a < n; ++a) {
+        double xr = (a == b) ? 1.0 : 0.0, xi = 0.0;
+        for (int c = 0; c < n; ++c) {
+          const double vr = br[a + n * c], vi = bi[a + n * c];
+          const double gr = g[2 * (c + n * b)], gi = g[2 * (c + n * b) + 1];
+          xr -= vr * gr - vi * gi;
+          xi -= vr * gi + vi * gr;
+        }
+        ar[a + n * b] = xr;
+        ai[a + n * b] = xi;
+      }
+    for (int t = 0; t < nn; ++t) {  // B = identity
+      br[t] = (t % (n + 1) == 0) ? 1.0 : 0.0;
+      bi[t] = 0.0;
+    }
+    for (int j = 0; j < n; ++j) {  // Gauss-Jordan: A -> 1, B -> A^{-1}
+      int piv = j;
+      double best = hypot(ar[j + n * j], ai[j + n * j]);
+      for (int r = j + 1; r < n; ++r) {
+        const double m = hypot(ar[r + n * j], ai[r + n * j]);
+        if (m > best) {
+          best = m;
+          piv = r;
+        }
+      }
+      if (piv != j)
+        for (int c = 0; c < n; ++c) {
+          double t = ar[j + n * c]; ar[j + n * c] = ar[piv + n * c]; ar[piv + n * c] = t;
+          t = ai[j + n * c]; ai[j + n * c] = ai[piv + n * c]; ai[piv + n * c] = t;
+          t = br[j + n * c]; br[j + n * c] = br[piv + n * c]; br[piv + n * c] = t;
+          t = bi[j + n * c]; bi[j + n * c] = bi[piv + n * c]; bi[piv + n * c] = t;
+        }
+      const double pr = ar[j + n * j], pi = ai[j + n * j];
+      const double d = pr * pr + pi * pi;
+      const double qr = pr / d, qi = -pi / d;  // 1 / pivot
+      for (int c = 0; c < n; ++c) {  // row j /= pivot
+        double xr = ar[j + n * c], xi = ai[j + n * c];
+        ar[j + n * c] = xr * qr - xi * qi;
+        ai[j + n * c] = xr * qi + xi * qr;
+        xr = br[j + n * c];
+        xi = bi[j + n * c];
+        br[j + n * c] = xr * qr - xi * qi;
+        bi[j + n * c] = xr * qi + xi * qr;
+      }
+      for (int r = 0; r < n; ++r) {  // eliminate column j from the other rows
+        if (r == j) continue;
+        const double fr = ar[r + n * j], fi = ai[r + n * j];
+        if (fr == 0.0 && fi == 0.0) continue;
+        for (int c = 0; c < n; ++c) {
+          ar[r + n * c] -= fr * ar[j + n * c] - fi * ai[j + n * c];
+          ai[r + n * c] -= fr * ai[j + n * c] + fi * ar[j + n * c];
+          br[r + n * c] -= fr * br[j + n * c] - fi * bi[j + n * c];
+          bi[r + n * c] -= fr * bi[j + n * c] + fi * br[j + n * c];
+        }
+      }
+    }
+    for (int b = 0; b < n; ++b)  // sum += G A^{-1}
+      for (int a = 0; a < n; ++a) {
+        double xr = 0.0, xi = 0.0;
+        for (int c = 0; c < n; ++c) {
+          const double gr = g[2 * (a + n * c)], gi = g[2 * (a + n * c) + 1];
+          xr += gr * br[c + n * b] - gi * bi[c + n * b];
+          xi += gr * bi[c + n * b] + gi * br[c + n * b];
+        }
+        sr[a + n * b] += xr;
+        si[a + n * b] += xi;
+      }
+  }
+  double *out = partials + 2 * ((size_t)iw * T + threadIdx.x) * nn;
+  for (int t = 0; t < nn; ++t) {
+    out[2 * t] = sr[t];
+    out[2 * t + 1] = si[t];
+  }
+}
+
+// Gproj[w] = (sum over the T thread accumulators, in order) / nk
+__global__ void k_cpt_reduce(int nn, int T, long nk, const double *partials, double *Gproj) {
+  const int iw = blockIdx.x;
+  for (int t = threadIdx.x; t < 2 * nn; t += blockDim.x) {
+    double s = 0.0;
+    for (int q = 0; q < T; ++q) s += partials[2 * ((size_t)iw * T + q) * nn + t];
+    Gproj[2 * (size_t)iw * nn + t] = s / (double)nk;
+  }
+}
+
 // Jacobi continued fractions, backward recursion (continued_fraction::evaluate,
 // src_ed/continued_fraction.cpp:52-57); one thread per (fraction, frequency).
 __global__ void k_cf_eval(int nf, const int *off, const int *len, const double *a, const double *b,
@@ -1532,6 +1656,19 @@ void launch_finalize_ld(const double *partials, int nblocks, int ld, int n, doub
   k_finalize_ld<<<n, kThreads, 0, s>>>(partials, nblocks, ld, out);
   QED_LAUNCH();
 }
+
+void launch_cpt_projected(int n, int nw, const double *G, const double *V0, int nel, const int *er, const int *ec,
+                          const double *eR, const double *ev, int nkx, int nky, int nkz, double off,
+                          double *partials, double *Gproj, cudaStream_t s) {
+  if (n < 1 || n > kSefMaxN) fail(QED_ERR_UNSUPPORTED, "projected Green function: dimension above 16");
+  if (nw <= 0) return;
+  k_cpt_partial<<<nw, kCptThreads, 0, s>>>(n, G, V0, nel, er, ec, eR, ev, nkx, nky, nkz, off, partials);
+  QED_LAUNCH();
+  k_cpt_reduce<<<nw, 64, 0, s>>>(n * n, kCptThreads, (long)nkx * nky * nkz, partials, Gproj);
+  QED_LAUNCH();
+}
+
+int cpt_partials_size(int n, int nw) { return 2 * n * n * kCptThreads * nw; }
 
 int launch_sef_logdet(int n, int nw, const double *G, const double *V0, int nel, const int *er, const int *ec,
                       const double *eR, const double *ev, int nkx, int nky, int nkz, double *partials,

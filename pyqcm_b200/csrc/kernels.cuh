@@ -151,6 +151,13 @@ void launch_finalize_ld(const double *partials, int nblocks, int ld, int n, doub
 int launch_sef_logdet(int n, int nw, const double *G, const double *V0, int nel, const int *er, const int *ec,
                       const double *eR, const double *ev, int nkx, int nky, int nkz, double *partials,
                       cudaStream_t s);
+// Grid average of G (1 - V(k) G)^{-1} per frequency into Gproj (nw n x n
+// complex, column-major); V0 holds nw k-independent parts of V (one per
+// frequency); k = ((a + off)/nkx, ...). partials: cpt_partials_size(n, nw) doubles.
+void launch_cpt_projected(int n, int nw, const double *G, const double *V0, int nel, const int *er, const int *ec,
+                          const double *eR, const double *ev, int nkx, int nky, int nkz, double off,
+                          double *partials, double *Gproj, cudaStream_t s);
+int cpt_partials_size(int n, int nw);
 // G = R^T R on the device (p <= 16): R, R^{-1}; *fail = 1 if G is not positive
 // definite or a pivot is below pivot_min; with Rprev, B = R Rprev and B^T
 void launch_block_chol(int p, const double *G, double pivot_min, double *R, double *Rinv, const double *Rprev,

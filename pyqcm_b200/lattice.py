@@ -74,6 +74,8 @@ class LatticeModel:
     def __init__(self, prob, cluster_model: str | None = None):
         self.prob = prob
         self.n = prob.n_sites
+        self.n_bath = getattr(prob, "n_bath", 0)
+        self.n_orb = self.n + self.n_bath
         self.dim = len(prob.superlattice)
         self.sites = np.array(prob.sites, dtype=np.int64)
         self.S = np.array(prob.superlattice, dtype=np.int64)  # rows: superlattice vectors
@@ -146,15 +148,18 @@ class LatticeModel:
         return False
 
     def _define_cluster_model(self):
-        """The cluster's ED model: every operator restricted to the cluster
-        (neighbour 0), orbitals s (up) and s + n (down), as the reference's
+        """The cluster's ED model: its own operators (bath energies and
+        hybridisations), then every lattice operator restricted to the cluster
+        (neighbour 0), orbitals s (up) and s + n_orb (down), as the reference's
         lattice_model::build_cluster_operators names them."""
-        n = self.n
-        qed.new_model(self.cluster_model, n, 0)
+        no = self.n_orb
+        qed.new_model(self.cluster_model, self.n, self.n_bath)
+        for name, (typ, el) in getattr(self.prob, "cluster_operators", {}).items():
+            qed.new_operator(self.cluster_model, name, typ, el)
         for name in self.interactions:
-            qed.new_operator(self.cluster_model, name, "interaction", [(i, i + n, 1.0) for i in range(n)])
+            qed.new_operator(self.cluster_model, name, "interaction", [(i, i + no, 1.0) for i in range(self.n)])
         for name, E in self.elements.items():
-            el = [(s1 + n * sp1, s2 + n * sp2, v) for (s1, sp1, s2, sp2, R), v in sorted(E.items())
+            el = [(s1 + no * sp1, s2 + no * sp2, v) for (s1, sp1, s2, sp2, R), v in sorted(E.items())
                   if R == (0, 0, 0) and abs(v) > 1e-12]
             if el:
                 qed.new_operator(self.cluster_model, name, "one-body", el)
@@ -269,3 +274,70 @@ class LatticeInstance:
             omega_diag *= 2.0
         omega_diag *= 0.5
         return (omega_trace - omega_diag + omega_clus) / self.model.n
+
+
+# -------------------------------------------------------------------- CDMFT --
+
+def _blocks(model):
+    return (False, True) if model.mixing == 4 else (False,)
+
+
+def projected_green_function(inst: LatticeInstance, freqs, side: int = 32, spin_down: bool = False):
+    """Grid average of the CPT Green function per frequency (projected_Green_function,
+    src_qcm/CPT.cpp:283-346): side points per superlattice direction at offsets
+    (i + 0.5)/side; with bath orbitals V(k) carries -Gamma(iw) of the cluster."""
+    freqs = np.asarray(freqs, dtype=np.float64)
+    m = inst.model
+    H, inter = m.lattice_blocks(inst.values)
+    sd = 1 if (spin_down and m.mixing == 4) else 0
+    Hc = qed.hopping_matrix(spin_down=bool(sd), label=inst.label)
+    V0 = np.repeat((H[sd] - Hc)[None, :, :], len(freqs), axis=0).astype(np.complex128)
+    if m.n_bath:
+        V0 -= qed.hybridization_function(1j * freqs, spin_down=bool(sd), label=inst.label)
+    el = inter[sd]
+    nk = [side if i < m.dim else 1 for i in range(3)]
+    return qed.cpt_projected_green_function(V0, [e[0] for e in el], [e[1] for e in el], [e[2] for e in el],
+                                            [e[3] for e in el], freqs, nk, 0.5, spin_down=bool(sd),
+                                            label=inst.label)
+
+
+def CDMFT_host(inst: LatticeInstance, freqs, side: int = 32):
+    """Host function per spin block and frequency (lattice_model_instance::CDMFT_host,
+    src_qcm/CPT.cpp:356-425): G_host = Gproj^{-1} + Sigma_c(iw) + H_c - iw."""
+    freqs = np.asarray(freqs, dtype=np.float64)
+    out = []
+    for sd in _blocks(inst.model):
+        P = projected_green_function(inst, freqs, side, spin_down=sd)
+        S = qed.self_energy(1j * freqs, spin_down=sd, label=inst.label)
+        Hc = qed.hopping_matrix(spin_down=sd, label=inst.label)
+        eye = np.eye(inst.model.n)
+        out.append(np.linalg.inv(P) + S + Hc[None] - 1j * freqs[:, None, None] * eye[None])
+    return out
+
+
+def CDMFT_distance(model: LatticeModel, host, freqs, weights, varia, points, base_values, label0: int = 800000):
+    """Distance of the cluster hybridisation to the host for a batch of bath
+    points (lattice_model_instance::CDMFT_distance, src_qcm/CPT.cpp:519-560):
+    sum over frequencies and spin blocks of weight * |Gamma(iw) + G_host(iw)|^2,
+    doubled without spin asymmetry, times the frequency step, over dim^2. The
+    hybridisation needs no ground state: each point is only an ED instance."""
+    freqs = np.asarray(freqs, dtype=np.float64)
+    weights = np.asarray(weights, dtype=np.float64)
+    dw = freqs[1] - freqs[0]
+    dim = model.n
+    out = []
+    for k, p in enumerate(np.atleast_2d(points)):
+        vals = dict(base_values)
+        vals.update({v: float(x) for v, x in zip(varia, p)})
+        inst = model.instance(label0 + k, **vals)
+        try:
+            d = 0.0
+            for h, sd in zip(host, _blocks(model)):
+                g = qed.hybridization_function(1j * freqs, spin_down=sd, label=inst.label)
+                d += float(np.sum(weights[:, None, None] * np.abs(g + h) ** 2))
+        finally:
+            inst.erase()
+        if model.mixing == 0:
+            d *= 2.0
+        out.append(d * dw / (dim * dim))
+    return np.array(out)

@@ -187,6 +187,8 @@ class LatticeProblem:
     sectors: str = "R0"
     params: dict = field(default_factory=dict)
     equiv: list = field(default_factory=list)
+    n_bath: int = 0
+    cluster_operators: dict = field(default_factory=dict)  # name -> (type, [(r, c, v)]) on the cluster model
 
     @property
     def n_sites(self) -> int:
@@ -221,6 +223,27 @@ def vca_2x5(U: float = 8.0, M1: float = 0.1, dmu: float = 0.0) -> LatticeProblem
     The superlattice (2,0), (1,5) keeps Q = (pi, pi) commensurate with the tiling."""
     return square_lattice_vca(2, 5, U=U, M1=M1, mu1=U / 2 + dmu, name="vca2x5",
                               superlattice=[(2, 0, 0), (1, 5, 0)])
+
+
+def cdmft_2x2_bath(eps, hyb, U: float = 8.0, t: float = 1.0) -> LatticeProblem:
+    """Square lattice (hopping -t) tiled by 2x2 plaquettes, each with 8 bath
+    orbitals (two per site): bath energies eb{b}_1 = eps[b], hybridisations
+    tb{b}_1 = hyb[b] with cluster site b // 2, half filling (mu = U/2, sector
+    R0:N12:S0). The cluster model is that of plaquette_bath."""
+    ns, nb = 4, 8
+    L = ns + nb
+    sites = [(x, y, 0) for y in range(2) for x in range(2)]
+    cops = {}
+    params = {"t": t, "U": U, "mu": U / 2}
+    for b in range(nb):
+        cops[f"eb{b}"] = ("one-body", _both_spins(L, [(ns + b, ns + b, 1.0)]))
+        cops[f"tb{b}"] = ("one-body", _both_spins(L, [(b // 2, ns + b, 1.0)]))
+        params[f"eb{b}_1"] = float(eps[b])
+        params[f"tb{b}_1"] = float(hyb[b])
+    return LatticeProblem("cdmft2x2", sites, [(2, 0, 0), (0, 2, 0)], hoppings=[("t", (1, 0, 0), -1.0),
+                          ("t", (0, 1, 0), -1.0)], interactions=["U"], sectors="R0:N12:S0", params=params,
+                          equiv=[("t_1", 1.0, "t"), ("U_1", 1.0, "U"), ("mu_1", 1.0, "mu")], n_bath=nb,
+                          cluster_operators=cops)
 
 
 def regular_frequency_grid(wc: float, n1: int, n2: int):

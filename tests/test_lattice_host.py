@@ -44,3 +44,23 @@ def test_nr_fit_recovers_a_quadratic():
     assert np.allclose(H, A, atol=1e-8) and np.allclose(g, A @ (np.array([0.3, 0.1]) - x0), atol=1e-8)
     x, *_ = vca.newton_raphson(f, [0.3, 0.1], [0.01, 0.01], [1e-8, 1e-8])
     assert np.allclose(x, x0, atol=1e-8)
+
+
+def test_bath_lattice_model_matches_reference(qed, oracle):
+    """The CDMFT model (2x2 plaquettes with eight bath orbitals): the cluster's ED
+    operators, its one-body matrix and V(k) = t(k) - t' - Gamma(w) against the
+    reference's lattice layer."""
+    from pyqcm_b200 import lattice as LT
+    rng = np.random.default_rng(3)
+    prob = W.cdmft_2x2_bath(rng.uniform(-2, 2, 8), rng.uniform(0.2, 1, 8))
+    oracle.set_param("GF_method", "L")
+    oracle.load_lattice(prob, 0)
+    M = LT.LatticeModel(prob)
+    for op in ("t", "mu", "U", "eb3", "tb5"):
+        assert sorted(oracle.matrix_elements("clus", op)[1]) == sorted(qed.matrix_elements(M.cluster_model, op)[1]), op
+    I = M.instance(990)
+    assert np.max(np.abs(qed.hopping_matrix(label=I.label) - oracle.lattice_cluster_hopping(0))) < 1e-14
+    w = 0.5j
+    gamma = qed.hybridization_function(w, label=I.label)
+    for k in [(0.0, 0.0), (0.25, 0.5), tuple(rng.uniform(0, 1, 2))]:
+        assert np.max(np.abs(I.V(k) - gamma - oracle.lattice_V(0, w, k))) < 1e-13, k

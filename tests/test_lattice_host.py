@@ -64,3 +64,23 @@ def test_bath_lattice_model_matches_reference(qed, oracle):
     gamma = qed.hybridization_function(w, label=I.label)
     for k in [(0.0, 0.0), (0.25, 0.5), tuple(rng.uniform(0, 1, 2))]:
         assert np.max(np.abs(I.V(k) - gamma - oracle.lattice_V(0, w, k))) < 1e-13, k
+
+
+def test_tilted_superlattice_2x5_matches_reference(qed, oracle):
+    """The VCA bench's lattice: 2x5 clusters on the superlattice (2,0), (1,5), which
+    keeps the Neel vector commensurate; operators, H_c and V(k) against the reference."""
+    from pyqcm_b200 import lattice as LT
+    prob = W.vca_2x5(U=7.0, M1=0.12, dmu=0.1)
+    oracle.set_param("GF_method", "L")
+    oracle.load_lattice(prob, 0)
+    M = LT.LatticeModel(prob)
+    assert oracle.lattice_dims()[:2] == (M.mixing, M.n)
+    for op in ("t", "mu", "U"):  # (the Weiss field enters through H_c, compared below)
+        assert sorted(oracle.matrix_elements("clus", op)[1]) == sorted(qed.matrix_elements(M.cluster_model, op)[1]), op
+    I = M.instance(995)
+    rng = np.random.default_rng(9)
+    for sd in (False, True):
+        assert np.max(np.abs(qed.hopping_matrix(spin_down=sd, label=I.label) -
+                             oracle.lattice_cluster_hopping(0, sd))) < 1e-14
+        for k in [(0.0, 0.0), (0.3, 0.7), tuple(rng.uniform(0, 1, 2))]:
+            assert np.max(np.abs(I.V(k, sd) - oracle.lattice_V(0, 0.4j, k, sd))) < 1e-13, (sd, k)

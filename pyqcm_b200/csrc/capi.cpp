@@ -15,6 +15,7 @@
 #include "instance.hpp"
 #include "options.hpp"
 #include "qed_b200.h"
+#include "worker_pool.hpp"
 
 using namespace qed;
 
@@ -109,55 +110,6 @@ std::shared_ptr<Instance> instance(int label) {
 
 // Runs fn(i) for i in [0, n) on `threads` host threads (each with its own
 // Workspace / CUDA stream). Returns the status of the first failure.
-// Worker threads kept for the life of the process, so that each keeps its
-// Workspace (stream, reduction buffers, pinned staging) from one batch call to
-// the next. A batch call hands the pool one work loop that `extra` workers and
-// the calling thread run; batch calls from different host threads take turns.
-class WorkerPool {
- public:
-  void run(int extra, const std::function<void()> &work) {
-    std::lock_guard<std::mutex> serial(run_mtx_);
-    {
-      std::lock_guard<std::mutex> l(m_);
-      while ((int)threads_ < extra) {
-        const int idx = (int)threads_++;
-        std::thread([this, idx] { loop(idx); }).detach();
-      }
-      job_ = work;
-      wanted_ = extra;
-      active_ = extra;
-      ++gen_;
-    }
-    cv_.notify_all();
-    work();
-    std::unique_lock<std::mutex> l(m_);
-    done_.wait(l, [&] { return active_ == 0; });
-    job_ = nullptr;
-  }
-
- private:
-  void loop(int idx) {
-    uint64_t seen = 0;
-    std::unique_lock<std::mutex> l(m_);
-    for (;;) {
-      cv_.wait(l, [&] { return gen_ != seen; });
-      seen = gen_;
-      if (idx >= wanted_) continue;
-      std::function<void()> w = job_;
-      l.unlock();
-      w();
-      l.lock();
-      if (--active_ == 0) done_.notify_all();
-    }
-  }
-  std::mutex run_mtx_, m_;
-  std::condition_variable cv_, done_;
-  std::function<void()> job_;
-  size_t threads_ = 0;
-  int wanted_ = 0, active_ = 0;
-  uint64_t gen_ = 0;
-};
-
 WorkerPool &pool() {
   static WorkerPool *p = new WorkerPool;  // never destroyed: its threads live until exit
   return *p;

@@ -448,6 +448,26 @@ VCA_WORKLOAD = ("VCA on the square lattice (t=1) tiled by 2x5 clusters (superlat
                 "stationary point with steps 0.005 (surrogate-guided)")
 
 
+VCA_REF_POINT = (7.0, 0.15, 0.0)  # (U, M', dmu) of the reference's timed Omega evaluation
+
+
+def vca_reference_sample():
+    """One Potthoff-functional evaluation of the 2x5 VCA workload by the reference's
+    own lattice layer (the compiled oracle; ED ground state + Green function + the
+    fixed grid) on one host core: (seconds, Omega)."""
+    from oracle import ref
+    from pyqcm_b200 import vca
+    from pyqcm_b200 import workloads as W
+    U, M, dmu = VCA_REF_POINT
+    ref.set_param("GF_method", "L")
+    ref.load_lattice(W.vca_2x5(U=U, M1=M, dmu=dmu), 0)
+    w, p = W.regular_frequency_grid(2.0, 32, 32)
+    ref.set_grids(w, p, (64, 64))
+    t0 = time.perf_counter()
+    om = ref.lattice_potthoff(0)
+    return time.perf_counter() - t0, om
+
+
 def vca_line(n_points, epochs, threads, Us=(5.0, 7.0, 9.0), local=0):
     """Surrogate-guided against ED-only VCA on the 2x5 cluster: training-data and
     training cost, then per U the wall time of both searches to the same stationary point."""
@@ -493,6 +513,9 @@ def vca_line(n_points, epochs, threads, Us=(5.0, 7.0, 9.0), local=0):
                      "omega_abs_diff": float(abs(om[0] - om[1]))})
     t_sur = sum(r["surrogate_s"] for r in runs)
     t_ed = sum(r["ed_only_s"] for r in runs)
+    om_here = float(ev(np.array([VCA_REF_POINT]))[0])
+    t_ref, om_ref = vca_reference_sample()
+    n_ed = sum(r["ed_only_omega_evals"] for r in runs)
     return {"metric": "VCA wall time, surrogate-guided (same stationary point as ED-only within 1e-8)",
             "value": t_sur, "unit": "s", "n_gpus": 1, "steps": len(Us), "warmup": 0,
             "ms_per_step": 1e3 * t_sur / len(Us), "higher_is_better": False, "scaling": "replicas",
@@ -500,6 +523,12 @@ def vca_line(n_points, epochs, threads, Us=(5.0, 7.0, 9.0), local=0):
             "data": "synthetic", "config": {"workload": VCA_WORKLOAD, "U": list(Us),
                                             "training_points": n_points, "epochs": epochs},
             "ed_only_seconds": t_ed, "speedup": t_ed / t_sur if t_sur > 0 else None,
+            "cpu_baseline": {"value": t_ref * n_ed, "unit": "s", "cores": 1, "kind": "reference",
+                             "sample": f"one Potthoff-functional evaluation by the reference's compiled lattice "
+                                       f"layer at (U, M', dmu) = {VCA_REF_POINT} took {t_ref:.2f} s on one host "
+                                       f"core; value = that x the {n_ed} evaluations of the ED-only searches",
+                             "omega_reference": om_ref, "omega_this_solver": om_here,
+                             "omega_abs_diff": abs(om_ref - om_here)},
             "max_omega_abs_diff": max(r["omega_abs_diff"] for r in runs),
             "training": {"data_seconds": t_data, "omega_per_second": n_points / t_data,
                          "train_seconds": t_train, "first_loss": float(losses[0]), "last_loss": float(losses[-1])},

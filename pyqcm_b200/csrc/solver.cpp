@@ -294,10 +294,15 @@ void start_vector(size_t D, uint64_t seed, double *v, Workspace &ws) {
 constexpr double kQlBand = 1e-3;
 
 namespace {
-ParallelFor g_parallel_for;
+// constructed on first use: the library installs the hook from another
+// translation unit's static initialiser, which may run before this one's
+ParallelFor &parallel_for_hook() {
+  static ParallelFor f;
+  return f;
+}
 }  // namespace
 
-void set_parallel_for(ParallelFor f) { g_parallel_for = std::move(f); }
+void set_parallel_for(ParallelFor f) { parallel_for_hook() = std::move(f); }
 
 void lanczos_energy_batch(std::vector<LanczosBatchItem> &items, Workspace &ws) {
   PhaseScope ps(kPhGsLanczos);
@@ -393,6 +398,10 @@ void lanczos_energy_batch(std::vector<LanczosBatchItem> &items, Workspace &ws) {
         code[a] = e.code;
         err[a] = e.what();
         return;
+      } catch (const std::exception &e) {  // nothing may escape into a pool thread
+        code[a] = QED_ERR_INTERNAL;
+        err[a] = e.what();
+        return;
       }
       R.rot = (R.rot + R.chunk) % 3;
       R.chunk = kChunk;
@@ -402,8 +411,9 @@ void lanczos_energy_batch(std::vector<LanczosBatchItem> &items, Workspace &ws) {
         done[a] = 1;
       }
     };
-    if (g_parallel_for && na > 1)
-      g_parallel_for(na, test);
+    const ParallelFor &pf = parallel_for_hook();
+    if (pf && na > 1)
+      pf(na, test);
     else
       for (int a = 0; a < na; ++a) test(a);
     std::vector<int> still;

@@ -131,6 +131,12 @@ class LatticeModel:
         # lattice_model::density_wave (src_qcm/lattice_model.cpp:1149-1230), phase 0, amplitude 1
         if typ not in ("Z", "spin", "N", "cdw"):
             raise ValueError(f"density wave of type {typ}: only Z and N are supported here")
+        # Q (in units of pi) must be commensurate with the superlattice: Q.S even for
+        # every superlattice vector S (the reference's check, src_qcm/lattice_model.cpp:1186-1190)
+        for S in self.S:
+            q = float(np.dot(Q, S))
+            if abs(q / 2.0 - np.floor(q / 2.0 + 1e-6)) > 1e-5:
+                raise ValueError(f"density-wave vector for {name} is incommensurate with the superlattice")
         el = {}
         for i, r in enumerate(self.sites):
             z = np.cos(np.pi * float(np.dot(Q, r)))

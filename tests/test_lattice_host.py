@@ -84,3 +84,13 @@ def test_tilted_superlattice_2x5_matches_reference(qed, oracle):
                              oracle.lattice_cluster_hopping(0, sd))) < 1e-14
         for k in [(0.0, 0.0), (0.3, 0.7), tuple(rng.uniform(0, 1, 2))]:
             assert np.max(np.abs(I.V(k, sd) - oracle.lattice_V(0, 0.4j, k, sd))) < 1e-13, (sd, k)
+
+
+def test_incommensurate_density_wave_is_rejected_like_the_reference(qed, oracle):
+    """A Neel vector incommensurate with a 2x3 tiling: both lattice layers refuse it."""
+    from pyqcm_b200 import lattice as LT
+    prob = W.square_lattice_vca(2, 3, U=8.0, M1=0.1)
+    with pytest.raises(oracle.OracleError, match="incommensurate"):
+        oracle.load_lattice(prob, 0)
+    with pytest.raises(ValueError, match="incommensurate"):
+        LT.LatticeModel(prob)

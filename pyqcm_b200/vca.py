@@ -5,9 +5,11 @@ solved by this package's GPU ED.
 The search is the reference's Newton-Raphson method (pyqcm/vca.py:239-430):
 every iteration fits a quadratic form through 1 + 2n + n(n-1)/2 points around
 the current x (the n +/- step pairs and n(n-1)/2 off-diagonal points at
-0.707 step), moves by dx = -H^{-1} g, then resets each step to |dx_i| (at most
-twice the initial step, at least twice the accuracy); it stops when every
-|dx_i| <= accur_i or |g| < gtol. Here the points of one iteration are solved
+0.707 step), moves by dx = -H^{-1} g, then resets each step to |dx_i|, at least
+twice the accuracy (the reference also compares with twice the initial step,
+but its "initial step" names the same array as the step, so that bound never
+applies; it does not here either); it stops when every |dx_i| <= accur_i or
+|g| < gtol. Here the points of one iteration are solved
 as one batch (their ground states and Green functions concurrently on the GPU,
 then their Omega on the GPU grid).
 """
@@ -143,8 +145,7 @@ def newton_raphson(func, start, step, accur, gtol: float = 1e-4, max_iteration: 
     Returns (x, Omega at the last fit point, gradient, Hessian, iterations)."""
     fit = nr_quadratic_fit if stencil == "reference" else central_fit
     x = np.array(start, dtype=np.float64)
-    step0 = np.array(step, dtype=np.float64)
-    step = step0.copy()
+    step = np.array(step, dtype=np.float64)
     accur = np.asarray(accur, dtype=np.float64)
     for it in range(1, max_iteration + 1):
         val, grad, hess = fit(func, x, step)
@@ -152,9 +153,7 @@ def newton_raphson(func, start, step, accur, gtol: float = 1e-4, max_iteration: 
             return x, val, grad, hess, it
         dx = -np.linalg.solve(hess, grad)
         x = x + dx
-        step = np.abs(dx)
-        step = np.where(step > step0, 2.0 * step0, step)
-        step = np.where(step < 2.0 * accur, 2.0 * accur, step)
+        step = np.maximum(np.abs(dx), 2.0 * accur)
         if np.all(np.abs(dx) <= accur):
             return x, val, grad, hess, it
     raise RuntimeError(f"VCA Newton-Raphson: no convergence after {max_iteration} iterations")

@@ -1,0 +1,38 @@
+"""The VCA Newton-Raphson restatement (pyqcm_b200.vca) against the reference's own
+functions run on an analytic function (golden values from
+tests/golden/make_vca_golden.py): the stencil fit and the whole search with the
+reference's stencil; and the central stencil reaching the same stationary point."""
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+G = json.load(open(os.path.join(HERE, "golden", "vca_nr.json")))
+A = np.array(G["A"])
+X0 = np.array(G["X0"])
+
+
+def f1(x):
+    d = np.asarray(x) - X0
+    return 0.5 * d @ A @ d + 0.1 * np.sum(np.sin(3 * x)) + 0.05 * x[0] ** 2 * x[1]
+
+
+def fb(X):
+    return np.array([f1(x) for x in np.atleast_2d(X)])
+
+
+def test_reference_stencil_fit_matches_the_reference():
+    from pyqcm_b200 import vca
+    val, grad, hess = vca.nr_quadratic_fit(fb, np.array(G["fit_x"]), np.array(G["fit_step"]))
+    assert abs(val - G["fit_val"]) < 1e-12
+    assert np.max(np.abs(grad - np.array(G["fit_grad"]))) < 1e-10
+    assert np.max(np.abs(hess - np.array(G["fit_hess"]))) < 1e-8
+
+
+def test_newton_raphson_matches_the_reference():
+    from pyqcm_b200 import vca
+    x, *_ = vca.newton_raphson(fb, G["nr_start"], G["nr_step"], G["nr_accur"], stencil="reference")
+    assert np.max(np.abs(x - np.array(G["nr_x"]))) < 1e-9, (x, G["nr_x"])
+    xc, *_ = vca.newton_raphson(fb, G["nr_start"], G["nr_step"], G["nr_accur"])  # central stencil
+    assert np.max(np.abs(xc - np.array(G["nr_x"]))) < 1e-5, (xc, G["nr_x"])

@@ -1,6 +1,7 @@
 """Generates tests/golden/vca_nr.json: the reference's own Newton-Raphson VCA step
 functions (_NR_Hessian, _newton_raphson_step, _newton_raphson of pyqcm/vca.py) run
-on an analytic test function, as golden values for pyqcm_b200.vca.
+on an analytic test function, and its regular_frequency_grid(2, 32, 32)
+(pyqcm/__init__.py), as golden values for pyqcm_b200.vca and workloads.
 
 The functions are taken out of the reference's module source with `ast` (pyqcm
 itself cannot be imported here: its compiled extension is not built) and run
@@ -19,6 +20,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF = "/root/reference/pyqcm/vca.py"
+REF_INIT = "/root/reference/pyqcm/__init__.py"  # regular_frequency_grid
 WANT = ("_evalF", "_NR_Hessian", "_newton_raphson_step", "_vca_accuracy_warning", "_newton_raphson")
 
 A = np.array([[1.3, 0.4], [0.4, -0.7]])
@@ -42,8 +44,17 @@ def load():
     return ns
 
 
+def load_grid():
+    tree = ast.parse(open(REF_INIT).read())
+    funcs = [n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name == "regular_frequency_grid"]
+    ns = {"np": np}
+    exec(compile(ast.Module(body=funcs, type_ignores=[]), REF_INIT, "exec"), ns)
+    return ns["regular_frequency_grid"]
+
+
 def main():
     ns = load()
+    gw, gp = load_grid()(2.0, 32, 32)
     x = np.array([0.3, -0.1])
     step = np.array([0.02, 0.03])
     val, grad, hess = ns["_NR_Hessian"](f, x.copy(), step.copy())
@@ -52,7 +63,7 @@ def main():
     out = {"A": A.tolist(), "X0": X0.tolist(), "fit_x": x.tolist(), "fit_step": step.tolist(),
            "fit_val": float(val), "fit_grad": np.asarray(grad).tolist(), "fit_hess": np.asarray(hess).tolist(),
            "nr_start": [0.3, -0.1], "nr_step": [0.02, 0.02], "nr_accur": [1e-6, 1e-6],
-           "nr_x": np.asarray(xs).tolist()}
+           "nr_x": np.asarray(xs).tolist(), "grid_w": np.asarray(gw).tolist(), "grid_p": np.asarray(gp).tolist()}
     with open(os.path.join(HERE, "vca_nr.json"), "w") as fh:
         json.dump(out, fh, indent=1)
     print(out)

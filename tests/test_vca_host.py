@@ -36,3 +36,10 @@ def test_newton_raphson_matches_the_reference():
     assert np.max(np.abs(x - np.array(G["nr_x"]))) < 1e-9, (x, G["nr_x"])
     xc, *_ = vca.newton_raphson(fb, G["nr_start"], G["nr_step"], G["nr_accur"])  # central stencil
     assert np.max(np.abs(xc - np.array(G["nr_x"]))) < 1e-5, (xc, G["nr_x"])
+
+
+def test_frequency_grid_matches_the_reference():
+    from pyqcm_b200 import workloads as W
+    w, p = W.regular_frequency_grid(2.0, 32, 32)
+    assert np.max(np.abs(w - np.array(G["grid_w"]))) < 1e-14 * np.max(w)
+    assert np.max(np.abs(p - np.array(G["grid_p"]))) < 1e-14 * np.max(p)

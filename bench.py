@@ -289,6 +289,7 @@ def run_ours(args, world, rank, local):
             t0 = time.perf_counter()
             Hr.bench(1)
             dt = time.perf_counter() - t0
+            del Hr  # released before the VCA line resets the oracle's model registry
             cpu = {"value": 16.0 * D / dt / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": "one full H.v application of the 4x4 sector by the reference's "
                              "Hamiltonian_Factorized::mult_add (no threading in the reference's H.v)"}

@@ -159,6 +159,52 @@ def newton_raphson(func, start, step, accur, gtol: float = 1e-4, max_iteration: 
     raise RuntimeError(f"VCA Newton-Raphson: no convergence after {max_iteration} iterations")
 
 
+def quasi_newton(func, start, step, accur, gtol: float = 1e-4, bfgs: bool = False, max_iteration: int = 30):
+    """The reference's quasi-Newton search (_quasi_newton / _quasi_newton_step,
+    pyqcm/vca.py:92-236), as it runs: each iteration evaluates the 2n + 1 points
+    x, x +/- step_i e_i (one batch), takes the central-difference gradient, and
+    moves by dx = -H g. H is diag(step_i^2 / second difference) at the first
+    iteration; afterwards the symmetric-rank-1 (or BFGS) update with y = g - g_prev
+    is applied to the identity, because the reference's step function starts
+    from a fresh identity each call instead of the previous inverse Hessian. The
+    gradient test comes after the move; steps are reset as in newton_raphson.
+    Returns (x, gradient, inverse-Hessian estimate, iterations)."""
+    x = np.array(start, dtype=np.float64)
+    step = np.array(step, dtype=np.float64)
+    accur = np.asarray(accur, dtype=np.float64)
+    n = len(x)
+    g = np.zeros(n)
+    dx = np.zeros(n)
+    for it in range(max_iteration):
+        xp = np.tile(x, (2 * n + 1, 1))
+        for i in range(n):
+            xp[2 * i + 1, i] += step[i]
+            xp[2 * i + 2, i] -= step[i]
+        F = func(xp)
+        g0 = g.copy()
+        g = np.array([(F[2 * i + 1] - F[2 * i + 2]) / (2 * step[i]) for i in range(n)])
+        ih = np.eye(n)
+        if it == 0:
+            for i in range(n):
+                ih[i, i] = step[i] * step[i] / (F[2 * i + 1] + F[2 * i + 2] - 2 * F[0])
+        else:
+            y = g - g0
+            if bfgs:
+                z1 = 1.0 / (1.0e-14 + np.dot(y, dx))
+                X = np.eye(n) - z1 * np.outer(y, dx)
+                ih = X.T @ ih @ X + z1 * np.outer(dx, dx)
+            else:
+                dx = dx - ih @ y
+                z1 = 1.0 / (1.0e-14 + np.dot(y, dx))
+                ih = ih + z1 * np.outer(dx, dx)
+        dx = -ih @ g
+        x = x + dx
+        if np.linalg.norm(g) < gtol or np.all(np.abs(dx) <= accur):
+            return x, g, ih, it + 1
+        step = np.maximum(np.abs(dx), 2.0 * accur)
+    raise RuntimeError(f"VCA quasi-Newton: no convergence after {max_iteration} iterations")
+
+
 # ------------------------------------------------------------ surrogate path --
 
 def vca_values(x):

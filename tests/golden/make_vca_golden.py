@@ -21,7 +21,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF = "/root/reference/pyqcm/vca.py"
 REF_INIT = "/root/reference/pyqcm/__init__.py"  # regular_frequency_grid
-WANT = ("_evalF", "_NR_Hessian", "_newton_raphson_step", "_vca_accuracy_warning", "_newton_raphson")
+WANT = ("_evalF", "_NR_Hessian", "_newton_raphson_step", "_vca_accuracy_warning", "_newton_raphson",
+        "_QN_values", "_quasi_newton_step", "_quasi_newton")
 
 A = np.array([[1.3, 0.4], [0.4, -0.7]])
 X0 = np.array([0.12, -0.05])
@@ -30,6 +31,14 @@ X0 = np.array([0.12, -0.05])
 def f(x):
     d = np.asarray(x) - X0
     return 0.5 * d @ A @ d + 0.1 * np.sum(np.sin(3 * x)) + 0.05 * x[0] ** 2 * x[1]
+
+
+B = np.array([[1.3, 0.4], [0.4, 0.9]])  # positive definite: a minimum for the quasi-Newton runs
+
+
+def fq(x):
+    d = np.asarray(x) - X0
+    return 0.5 * d @ B @ d + 0.1 * np.sum(np.sin(3 * x))
 
 
 def load():
@@ -60,7 +69,12 @@ def main():
     val, grad, hess = ns["_NR_Hessian"](f, x.copy(), step.copy())
     xs, gs, hs = ns["_newton_raphson"](func=f, start=np.array([0.3, -0.1]), step=np.array([0.02, 0.02]),
                                       accur=np.array([1e-6, 1e-6]), max_iteration=30)
-    out = {"A": A.tolist(), "X0": X0.tolist(), "fit_x": x.tolist(), "fit_step": step.tolist(),
+    qn = {}
+    for bfgs in (False, True):
+        xq, gq, hq = ns["_quasi_newton"](func=fq, start=np.array([0.3, -0.1]), step=np.array([0.02, 0.02]),
+                                        accur=np.array([1e-6, 1e-6]), bfgs=bfgs, max_iteration=60)
+        qn["bfgs" if bfgs else "sr1"] = np.asarray(xq).tolist()
+    out = {"qn_x": qn, "B": B.tolist(), "A": A.tolist(), "X0": X0.tolist(), "fit_x": x.tolist(), "fit_step": step.tolist(),
            "fit_val": float(val), "fit_grad": np.asarray(grad).tolist(), "fit_hess": np.asarray(hess).tolist(),
            "nr_start": [0.3, -0.1], "nr_step": [0.02, 0.02], "nr_accur": [1e-6, 1e-6],
            "nr_x": np.asarray(xs).tolist(), "grid_w": np.asarray(gw).tolist(), "grid_p": np.asarray(gp).tolist()}

@@ -43,3 +43,19 @@ def test_frequency_grid_matches_the_reference():
     w, p = W.regular_frequency_grid(2.0, 32, 32)
     assert np.max(np.abs(w - np.array(G["grid_w"]))) < 1e-14 * np.max(w)
     assert np.max(np.abs(p - np.array(G["grid_p"]))) < 1e-14 * np.max(p)
+
+
+def test_quasi_newton_matches_the_reference():
+    from pyqcm_b200 import vca
+    B = np.array(G["B"])
+
+    def fq(X):
+        out = []
+        for x in np.atleast_2d(X):
+            d = x - X0
+            out.append(0.5 * d @ B @ d + 0.1 * np.sum(np.sin(3 * x)))
+        return np.array(out)
+
+    for key, bfgs in (("sr1", False), ("bfgs", True)):
+        x, *_ = vca.quasi_newton(fq, [0.3, -0.1], [0.02, 0.02], [1e-6, 1e-6], bfgs=bfgs, max_iteration=60)
+        assert np.max(np.abs(x - np.array(G["qn_x"][key]))) < 1e-9, (key, x, G["qn_x"][key])

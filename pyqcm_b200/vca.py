@@ -205,6 +205,68 @@ def quasi_newton(func, start, step, accur, gtol: float = 1e-4, bfgs: bool = Fals
     raise RuntimeError(f"VCA quasi-Newton: no convergence after {max_iteration} iterations")
 
 
+class VCAError(RuntimeError):
+    """Failure of the VCA search (pyqcm.SolverError in the reference)."""
+
+
+class VCA:
+    """A VCA computation; the constructor runs it (pyqcm.vca.VCA, pyqcm/vca.py:520-800,
+    methods 'NR', 'SYMR1', 'BFGS2').
+
+    model: a lattice.LatticeModel; varia: names of the variational parameters (or
+    var2sef: point -> parameter values); start, steps, accur, max: per variable
+    (scalars are broadcast); accur_grad: gradient tolerance; freqs, weights, nk: the
+    fixed (frequency, k) grid of the Potthoff functional. stencil: 'reference' (the
+    reference's 1 + 2n + n(n-1)/2 point fit, default) or 'central' (3^n points, see
+    newton_raphson). func: a batched Omega (points -> values) to use instead of the
+    GPU evaluator. After the run: x, omega (at x), gradient, hessian, iterations,
+    omega_evaluations."""
+
+    def __init__(self, model=None, var2sef=None, varia=None, start=None, steps=0.01, accur=1e-4, max=100,
+                 accur_grad=1e-6, max_iter=30, method="NR", freqs=None, weights=None, nk=None, fixed=None,
+                 threads: int = 0, stencil: str = "reference", func=None):
+        varia = [varia] if isinstance(varia, str) else list(varia or [])
+        start = np.atleast_1d(np.asarray(start, dtype=np.float64))
+        nvar = len(start)
+        steps, accur, maxv = (np.broadcast_to(np.asarray(v, dtype=np.float64), (nvar,)).copy()
+                              for v in (steps, accur, max))
+        if func is None:
+            to_values = var2sef if var2sef is not None else (lambda x: {k: float(v) for k, v in zip(varia, x)})
+            func = OmegaEvaluator(model, varia, freqs, weights, nk, fixed=fixed, threads=threads,
+                                  to_values=to_values)
+        self.omega_evaluations = 0
+
+        def batch(P):
+            P = np.atleast_2d(P)
+            bad = np.abs(P) > maxv
+            if np.any(bad):
+                i = int(np.argwhere(bad)[0][1])
+                name = varia[i] if i < len(varia) else str(i)
+                raise VCAError(f"Failure of the VCA method: parameter {name} is out of bounds!")
+            self.omega_evaluations += len(P)
+            return np.asarray(func(P), dtype=np.float64)
+
+        try:
+            if method == "NR":
+                x, _, g, H, it = newton_raphson(batch, start, steps, accur, gtol=accur_grad, max_iteration=max_iter,
+                                                stencil=stencil)
+            elif method in ("SYMR1", "BFGS2"):
+                x, g, iH, it = quasi_newton(batch, start, steps, accur, gtol=accur_grad, bfgs=(method == "BFGS2"),
+                                            max_iteration=max_iter)
+                H = np.linalg.inv(iH)
+            else:
+                raise ValueError(f"method {method} unknown in VCA")
+        except RuntimeError as e:
+            if isinstance(e, VCAError):
+                raise
+            raise VCAError("Failure of the VCA method") from e
+        self.x = x
+        self.gradient = g
+        self.hessian = H
+        self.iterations = it
+        self.omega = float(batch(np.array([x]))[0])  # final, converged value
+
+
 # ------------------------------------------------------------ surrogate path --
 
 def vca_values(x):

@@ -59,3 +59,24 @@ def test_quasi_newton_matches_the_reference():
     for key, bfgs in (("sr1", False), ("bfgs", True)):
         x, *_ = vca.quasi_newton(fq, [0.3, -0.1], [0.02, 0.02], [1e-6, 1e-6], bfgs=bfgs, max_iteration=60)
         assert np.max(np.abs(x - np.array(G["qn_x"][key]))) < 1e-9, (key, x, G["qn_x"][key])
+
+
+def test_vca_class_methods_and_bounds():
+    """pyqcm.vca.VCA's interface on a batched analytic Omega: the three Newton-type
+    methods reach the stationary point; a point beyond `max` fails the search."""
+    import pytest
+    from pyqcm_b200 import vca
+    B = np.array(G["B"])
+
+    def fq(X):
+        return np.array([0.5 * (x - X0) @ B @ (x - X0) + 0.1 * np.sum(np.sin(3 * x)) for x in np.atleast_2d(X)])
+
+    xs = []
+    for method in ("NR", "SYMR1", "BFGS2"):
+        V = vca.VCA(varia=["a", "b"], start=[0.3, -0.1], steps=0.02, accur=1e-6, method=method, func=fq,
+                    max_iter=60)
+        assert V.omega_evaluations > 0 and V.hessian.shape == (2, 2)
+        xs.append(V.x)
+    assert np.max(np.abs(np.array(xs) - xs[0])) < 1e-4
+    with pytest.raises(vca.VCAError, match="out of bounds"):
+        vca.VCA(varia=["a", "b"], start=[0.3, -0.1], steps=0.02, accur=1e-6, max=0.2, func=fq)

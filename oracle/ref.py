@@ -51,6 +51,7 @@ def lib():
             "ref_set_char": [C.c_char_p, C.c_char],
             "ref_set_bool": [C.c_char_p, C.c_int],
             "ref_new_model": [C.c_char_p, C.c_int, C.c_int],
+            "ref_new_model_gen": [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int],
             "ref_new_operator": [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, ip, ip, dp],
             "ref_new_instance": [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, C.c_char_p, C.c_int, C.c_char],
             "ref_erase_instance": [C.c_int],
@@ -142,8 +143,14 @@ def set_param(name: str, value):
         raise TypeError(value)
 
 
-def new_model(name, n_sites, n_bath):
-    _check(lib().ref_new_model(name.encode(), n_sites, n_bath))
+def new_model(name, n_sites, n_bath, generators=None, bath_irrep=False):
+    """generators: pyqcm's form (1-based sites; see ref_new_model_gen)."""
+    if not generators:
+        _check(lib().ref_new_model(name.encode(), n_sites, n_bath))
+        return
+    flat = [int(v) for row in generators for v in row]
+    arr = (C.c_int * len(flat))(*flat)
+    _check(lib().ref_new_model_gen(name.encode(), n_sites, n_bath, len(generators), arr, int(bath_irrep)))
 
 
 def new_operator(model, op, typ, elements):
@@ -171,7 +178,8 @@ def load_problem(prob, label: int, model_name: str | None = None, fmt: str = "F"
     (src_ed/model_instance.cpp:52 with Hamiltonian_Factorized); use fmt='S'
     for GF_method 'F'."""
     mname = model_name or prob.name
-    new_model(mname, prob.n_sites, prob.n_bath)
+    new_model(mname, prob.n_sites, prob.n_bath, getattr(prob, "generators", None),
+              getattr(prob, "bath_irrep", False))
     for op, (typ, el) in prob.operators.items():
         new_operator(mname, op, typ, el)
     new_instance(mname, prob.params, prob.sectors, label, fmt)

@@ -101,6 +101,24 @@ int ref_new_model(const char *name, int n_sites, int n_bath) {
   return guarded([&] { ED::new_model(name, n_sites, n_bath, {}, false); });
 }
 
+// A cluster model with symmetry generators, given as pyqcm takes them (n_gen rows
+// of n_sites + n_bath entries, 1-based sites; bath entries 1-based orbitals, or
+// irrep phases when bath_irrep is set), converted to ED::new_model's 0-based form
+// as the reference's Python binding does (src_python/qcm_ED_wrap.hpp:145-163).
+int ref_new_model_gen(const char *name, int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep) {
+  return guarded([&] {
+    const int n_orb = n_sites + n_bath;
+    std::vector<std::vector<int>> g(n_gen, std::vector<int>(n_orb));
+    for (int j = 0; j < n_gen; ++j)
+      for (int i = 0; i < n_orb; ++i) {
+        int v = gen[j * n_orb + i];
+        if (i < n_sites || !bath_irrep) v -= 1;
+        g[j][i] = v;
+      }
+    ED::new_model(name, n_sites, n_bath, g, bath_irrep != 0);
+  });
+}
+
 int ref_new_operator(const char *model_name, const char *op, const char *type, int n, const int *r,
                      const int *c, const double *v) {
   return guarded([&] {

@@ -31,6 +31,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libqed_b200.so")
 
 QED_OK = 0
+QED_ERR_UNSUPPORTED = 6
 _CODES = {1: "argument", 2: "lanczos", 3: "qmatrix", 4: "cuda", 5: "memory", 6: "unsupported",
           7: "no-device", 8: "internal"}
 
@@ -186,6 +187,9 @@ def load_problem(prob, label: int = 0, model_name: str | None = None, fmt: str |
     Lanczos in every sector; 'S', 'E', 'O', 'N': sectors below max_dim_full are
     diagonalised densely, as in the reference). The format is latched by the
     model's first instance."""
+    if getattr(prob, "generators", None):
+        raise QEDError(QED_ERR_UNSUPPORTED, "symmetry generators (g > 1) are not supported: the "
+                       "spin-factorized Hamiltonian requires the trivial point group")
     if fmt is not None:
         set_global_parameter("Hamiltonian_format", fmt)
     mname = model_name or prob.name

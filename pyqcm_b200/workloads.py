@@ -30,6 +30,8 @@ class ClusterProblem:
     operators: dict = field(default_factory=dict)   # name -> (type, [(r, c, v), ...])
     params: dict = field(default_factory=dict)      # name -> value
     sectors: str = "R0"
+    generators: list | None = None   # pyqcm's symmetry generators (1-based sites)
+    bath_irrep: bool = False
 
     @property
     def n_orb(self) -> int:

@@ -71,3 +71,14 @@ def test_unknown_label_and_options(qed):
     qed.set_global_parameter("accur_lanczos", 1e-12)
     assert qed.get_global_double("accur_lanczos") == 1e-12
     qed.set_global_parameter("kgrid_side", 32)  # lattice-layer option is accepted
+
+
+def test_generators_are_refused_loudly():
+    """A cluster model with symmetry generators (g > 1) is outside the
+    spin-factorized solver: loading one raises the unsupported status instead of
+    silently solving the unsymmetrised Hamiltonian."""
+    import pyqcm_b200 as qed
+    from tests.helpers import c2v_golden, c2v_problem
+    with pytest.raises(qed.QEDError) as err:
+        qed.load_problem(c2v_problem(c2v_golden(), True), 1, model_name="c2v_refused")
+    assert err.value.code == qed.QED_ERR_UNSUPPORTED

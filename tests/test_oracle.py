@@ -145,3 +145,21 @@ def test_golden_fixtures_reproduce(oracle, fresh):
         n = int(g["dims"][i])
         assert abs(e - g["E0"][i]) <= 1e-10 * abs(e)
         assert np.max(np.abs(G - g["G"][i][:, :n, :n])) < 1e-8
+
+
+def test_c2v_record_pins_the_oracle(oracle, fresh):
+    """The reference's own diagonalization record (tests/test_diagonalization/
+    S_format.ref: 2x2 plaquette + 8 bath orbitals with C2v generators, solved in the
+    symmetry-adapted basis, CSR format): the compiled oracle reproduces its ground-state
+    energy (6 significant digits in the record) and each irrep's Green function built
+    from the record's 14-digit poles, at off-axis frequencies, to 1e-7."""
+    from tests.helpers import C2V_Z, c2v_golden, c2v_irrep_gf, c2v_problem, project_irreps
+    gold = c2v_golden()
+    suffix, label = fresh()
+    oracle.set_param("GF_method", "L")
+    oracle.load_problem(c2v_problem(gold, True), label, model_name="c2v" + suffix, fmt="S")
+    E, sec = oracle.ground_state(label)
+    assert abs(E - gold["gs"]["energy"]) < 5.1e-5, E
+    assert sec == gold["gs"]["sector"]
+    G = oracle.green_function(label, C2V_Z)
+    assert np.max(np.abs(project_irreps(G) - c2v_irrep_gf(gold, C2V_Z))) < 1e-7

@@ -30,6 +30,8 @@
 #ifndef QED_B200_H
 #define QED_B200_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -283,6 +285,31 @@ int qed_halfbasis_rank(int L, int N, long n, const unsigned *strings, unsigned *
  * src_ed/ED_basis.cpp:79-110), computed on the GPU: target index (or -1) and
  * fermion phase bit per source state. */
 int qed_destroy_table(int L, int n_up, int n_dn, int a, long *target, int *phase);
+
+/* ---- Cluster point group -----------------------------------------------------
+ * The Abelian point group of a cluster model (symmetry_group,
+ * src_ed/symmetry_group.hpp:38-92), built from generators given as
+ * ED::new_model (src_ed/qcm_ED.hpp:34) takes them: n_gen rows of n_sites + n_bath
+ * 0-based entries, site entries a permutation, bath entries orbital labels or,
+ * with bath_irrep, phases in units of 2 pi / g. Host logic (no device work);
+ * the kernels evaluate the same per-state maps. Errors carry the reference's
+ * messages (invalid or non-commuting generators). */
+
+/* symmetry_group::build (src_ed/symmetry_group.cpp:184-345): the group order g,
+ * the character phases phi (g x g, units of 2 pi / g), the symmetric site
+ * orbitals S (n_sites x n_sites row-major, real and imaginary parts; row k is
+ * the k-th orbital, irreps in order) and the number of them in each irrep
+ * (site_irrep_dim, g entries). Output pointers may be NULL; phi and
+ * site_irrep_dim need room for 16 x 16 and 16 entries when g is not known. */
+int qed_symmetry_group(int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep, int *g, int *phi,
+                       double *S_re, double *S_im, int *site_irrep_dim);
+
+/* symmetry_group::Representative (src_ed/symmetry_group.cpp:231-262) of n basis
+ * states (spin up in bits 0-31, spin down in bits 32-63) in irrep `irrep`: the
+ * orbit's smallest state, the phase (units of pi / g) and the orbit length (0:
+ * the projected state vanishes; rep and phase are then meaningless). */
+int qed_symmetry_representatives(int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep, int irrep,
+                                 long n, const uint64_t *states, uint64_t *rep, int *phase, int *length);
 
 /* ---- VCA surrogate network ---------------------------------------------------
  * No counterpart in the reference (its VCA, pyqcm/vca.py, evaluates the Potthoff

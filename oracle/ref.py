@@ -52,6 +52,10 @@ def lib():
             "ref_set_bool": [C.c_char_p, C.c_int],
             "ref_new_model": [C.c_char_p, C.c_int, C.c_int],
             "ref_new_model_gen": [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int],
+            "ref_symmetry_group": [C.c_int, C.c_int, C.c_int, ip, C.c_int, ip, ip, dp, dp, ip],
+            "ref_representatives": [C.c_int, C.c_int, C.c_int, ip, C.c_int, C.c_int, C.c_long,
+                                    C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), ip, ip],
+            "ref_mixed_basis": [C.c_int, C.c_int, C.c_int, ip, C.c_int, C.c_char_p, C.POINTER(C.c_uint64), lp],
             "ref_new_operator": [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, ip, ip, dp],
             "ref_new_instance": [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), dp, C.c_char_p, C.c_int, C.c_char],
             "ref_erase_instance": [C.c_int],
@@ -523,3 +527,53 @@ def cdmft_distance(label, p, clus=0):
     d = C.c_double()
     _check(lib().ref_qcm_cdmft_distance(label, len(v), _dp(v), clus, C.byref(d)))
     return d.value
+
+
+def _gen0(n_sites, n_bath, generators, bath_irrep):
+    """pyqcm's 1-based generators -> ED::new_model's 0-based rows (flat int array)."""
+    n_orb = n_sites + n_bath
+    rows = [list(map(int, g)) for g in (generators or [])]
+    for g in rows:
+        for i in range(n_orb):
+            if i < n_sites or not bath_irrep:
+                g[i] -= 1
+    flat = [v for g in rows for v in g]
+    return len(rows), (C.c_int * max(len(flat), 1))(*flat)
+
+
+def symmetry_group(n_sites, n_bath, generators, bath_irrep=False):
+    ng, arr = _gen0(n_sites, n_bath, generators, bath_irrep)
+    g = C.c_int()
+    phi = (C.c_int * 256)()
+    sre = np.zeros(n_sites * n_sites)
+    sim = np.zeros(n_sites * n_sites)
+    dims = (C.c_int * 16)()
+    _check(lib().ref_symmetry_group(n_sites, n_bath, ng, arr, int(bool(bath_irrep)), C.byref(g), phi, _dp(sre),
+                                    _dp(sim), dims))
+    n = g.value
+    return {"g": n, "phi": np.array(phi[:n * n]).reshape(n, n), "S": (sre + 1j * sim).reshape(n_sites, n_sites),
+            "site_irrep_dim": np.array(dims[:n])}
+
+
+def representatives(n_sites, n_bath, generators, bath_irrep, irrep, states):
+    ng, arr = _gen0(n_sites, n_bath, generators, bath_irrep)
+    st = np.ascontiguousarray(states, dtype=np.uint64)
+    rep = np.zeros(len(st), dtype=np.uint64)
+    ph = np.zeros(len(st), dtype=np.int32)
+    ln = np.zeros(len(st), dtype=np.int32)
+    u64 = C.POINTER(C.c_uint64)
+    ip = C.POINTER(C.c_int)
+    _check(lib().ref_representatives(n_sites, n_bath, ng, arr, int(bool(bath_irrep)), irrep, len(st),
+                                     st.ctypes.data_as(u64), rep.ctypes.data_as(u64), ph.ctypes.data_as(ip),
+                                     ln.ctypes.data_as(ip)))
+    return rep, ph, ln
+
+
+def mixed_basis(n_sites, n_bath, generators, bath_irrep, sector):
+    ng, arr = _gen0(n_sites, n_bath, generators, bath_irrep)
+    d = C.c_long()
+    _check(lib().ref_mixed_basis(n_sites, n_bath, ng, arr, int(bool(bath_irrep)), sector.encode(), None, C.byref(d)))
+    out = np.zeros(d.value, dtype=np.uint64)
+    _check(lib().ref_mixed_basis(n_sites, n_bath, ng, arr, int(bool(bath_irrep)), sector.encode(),
+                                 out.ctypes.data_as(C.POINTER(C.c_uint64)), C.byref(d)))
+    return out

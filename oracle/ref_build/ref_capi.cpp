@@ -21,6 +21,8 @@
 
 #include "qcm_ED.hpp"
 #include "model_instance.hpp"
+#include "ED_basis.hpp"
+#include "symmetry_group.hpp"
 #include "global_parameter.hpp"
 #include "QCM.hpp"
 #include "lattice_model.hpp"
@@ -99,6 +101,59 @@ int ref_set_bool(const char *name, int v) {
 
 int ref_new_model(const char *name, int n_sites, int n_bath) {
   return guarded([&] { ED::new_model(name, n_sites, n_bath, {}, false); });
+}
+
+// The reference's symmetry_group for 0-based generators (as ED::new_model
+// takes them): order, character phases, symmetric orbitals, orbitals per irrep.
+static std::vector<std::vector<int>> gen_rows(int n_orb, int n_gen, const int *gen) {
+  std::vector<std::vector<int>> g(n_gen, std::vector<int>(n_orb));
+  for (int j = 0; j < n_gen; ++j)
+    for (int i = 0; i < n_orb; ++i) g[j][i] = gen[j * n_orb + i];
+  return g;
+}
+
+int ref_symmetry_group(int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep, int *g, int *phi,
+                       double *S_re, double *S_im, int *dims) {
+  return guarded([&] {
+    symmetry_group G(n_sites + n_bath, n_sites, gen_rows(n_sites + n_bath, n_gen, gen), bath_irrep != 0);
+    *g = G.g;
+    for (int a = 0; a < G.g; ++a)
+      for (int b = 0; b < G.g; ++b) phi[a * G.g + b] = G.phi(a, b);
+    for (int k = 0; k < n_sites; ++k)
+      for (int i = 0; i < n_sites; ++i) {
+        S_re[k * n_sites + i] = G.S(k, i).real();
+        S_im[k * n_sites + i] = G.S(k, i).imag();
+      }
+    for (int r = 0; r < G.g; ++r) dims[r] = G.site_irrep_dim[r];
+  });
+}
+
+// symmetry_group::Representative of n states in irrep `irrep`.
+int ref_representatives(int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep, int irrep, long n,
+                        const uint64_t *states, uint64_t *rep, int *phase, int *length) {
+  return guarded([&] {
+    symmetry_group G(n_sites + n_bath, n_sites, gen_rows(n_sites + n_bath, n_gen, gen), bath_irrep != 0);
+    for (long i = 0; i < n; ++i) {
+      rep_map m = G.Representative(binary_state(states[i]), irrep);
+      rep[i] = m.b.b;
+      phase[i] = m.phase;
+      length[i] = m.length;
+    }
+  });
+}
+
+// ED_mixed_basis of a sector string ("R1:N6:S0") under the group: the sorted
+// representative states. With out == nullptr only *dim is set.
+int ref_mixed_basis(int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep, const char *sec, uint64_t *out,
+                    long *dim) {
+  return guarded([&] {
+    auto G = std::make_shared<symmetry_group>(n_sites + n_bath, n_sites, gen_rows(n_sites + n_bath, n_gen, gen),
+                                              bath_irrep != 0);
+    ED_mixed_basis B(sector(std::string(sec)), G);
+    *dim = (long)B.dim;
+    if (out)
+      for (size_t i = 0; i < B.dim; ++i) out[i] = B.binlist[i].b;
+  });
 }
 
 // A cluster model with symmetry generators, given as pyqcm takes them (n_gen rows

@@ -106,6 +106,9 @@ def lib():
         "qed_halfbasis": [C.c_int, C.c_int, up, lp],
         "qed_halfbasis_rank": [C.c_int, C.c_int, C.c_long, up, up],
         "qed_destroy_table": [C.c_int, C.c_int, C.c_int, C.c_int, lp, ip],
+        "qed_symmetry_group": [C.c_int, C.c_int, C.c_int, ip, C.c_int, ip, ip, dp, dp, ip],
+        "qed_symmetry_representatives": [C.c_int, C.c_int, C.c_int, ip, C.c_int, C.c_int, C.c_long,
+                                         C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), ip, ip],
         "qed_sef_integrand_grid": [C.c_int, C.c_int, C.c_int, dp, C.c_int, ip, ip, ip, dp, C.c_int, dp,
                                    C.c_int, C.c_int, C.c_int, dp],
         "qed_cpt_projected_green_function": [C.c_int, C.c_int, C.c_int, dp, C.c_int, ip, ip, ip, dp, C.c_int,
@@ -536,6 +539,57 @@ def halfbasis_rank(L: int, N: int, strings):
     _check(lib().qed_halfbasis_rank(L, N, len(s), s.ctypes.data_as(C.POINTER(C.c_uint)),
                                     r.ctypes.data_as(C.POINTER(C.c_uint))))
     return r
+
+
+def _generators_abi(n_sites, n_bath, generators, bath_irrep):
+    """pyqcm's generators (1-based sites; bath entries 1-based orbitals, or irrep
+    phases with bath_irrep) -> ED::new_model's 0-based rows, as the reference's
+    Python binding converts them (src_python/qcm_ED_wrap.hpp:145-163)."""
+    n_orb = n_sites + n_bath
+    rows = [list(map(int, g)) for g in (generators or [])]
+    for j, g in enumerate(rows):
+        if len(g) != n_orb:
+            raise QEDError(1, f"generator {j + 1} should have {n_orb} elements")
+        for i in range(n_orb):
+            if i < n_sites or not bath_irrep:
+                g[i] -= 1
+    flat = np.ascontiguousarray(np.array(rows, dtype=np.int32).reshape(-1))
+    return len(rows), flat
+
+
+def symmetry_group(n_sites: int, n_bath: int = 0, generators=None, bath_irrep: bool = False):
+    """The cluster point group of pyqcm's generators: dict with the order g, the
+    character phases phi (g x g, units of 2 pi / g), the symmetric site orbitals S
+    (rows, irreps in order) and site_irrep_dim."""
+    ng, flat = _generators_abi(n_sites, n_bath, generators, bath_irrep)
+    g = C.c_int()
+    phi = np.zeros(256, dtype=np.int32)
+    sre = np.zeros(n_sites * n_sites)
+    sim = np.zeros(n_sites * n_sites)
+    dims = np.zeros(16, dtype=np.int32)
+    ip = C.POINTER(C.c_int)
+    _check(lib().qed_symmetry_group(n_sites, n_bath, ng, flat.ctypes.data_as(ip), int(bool(bath_irrep)),
+                                    C.byref(g), phi.ctypes.data_as(ip), _dp(sre), _dp(sim),
+                                    dims.ctypes.data_as(ip)))
+    n = g.value
+    return {"g": n, "phi": phi[:n * n].reshape(n, n).copy(),
+            "S": (sre + 1j * sim).reshape(n_sites, n_sites), "site_irrep_dim": dims[:n].copy()}
+
+
+def symmetry_representatives(n_sites: int, n_bath: int, generators, bath_irrep: bool, irrep: int, states):
+    """symmetry_group::Representative of each 64-bit state (spin up in the low
+    word): (representative, phase in units of pi/g, orbit length; 0 = null)."""
+    ng, flat = _generators_abi(n_sites, n_bath, generators, bath_irrep)
+    st = np.ascontiguousarray(states, dtype=np.uint64)
+    rep = np.zeros(len(st), dtype=np.uint64)
+    ph = np.zeros(len(st), dtype=np.int32)
+    ln = np.zeros(len(st), dtype=np.int32)
+    ip = C.POINTER(C.c_int)
+    up = C.POINTER(C.c_uint64)
+    _check(lib().qed_symmetry_representatives(n_sites, n_bath, ng, flat.ctypes.data_as(ip), int(bool(bath_irrep)),
+                                              irrep, len(st), st.ctypes.data_as(up), rep.ctypes.data_as(up),
+                                              ph.ctypes.data_as(ip), ln.ctypes.data_as(ip)))
+    return rep, ph, ln
 
 
 def destroy_table(L: int, n_up: int, n_dn: int, a: int):

@@ -14,6 +14,7 @@
 #include "common.hpp"
 #include "instance.hpp"
 #include "options.hpp"
+#include "symmetry.hpp"
 #include "qed_b200.h"
 #include "worker_pool.hpp"
 
@@ -1098,6 +1099,50 @@ int qed_destroy_table(int L, int n_up, int n_dn, int a, long *target, int *phase
       long s = (long)std::llround(std::fabs(hy[I])) - 1;
       target[s] = (long)I;
       phase[s] = hy[I] < 0 ? 1 : 0;
+    }
+  });
+}
+
+
+// ---- point group (symmetry.hpp / symmetry.cuh) ------------------------------
+
+static SymmetryGroup group_from_abi(int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep) {
+  if (n_gen < 0 || (n_gen > 0 && !gen)) fail(QED_ERR_ARGUMENT, "bad generators");
+  const int N = n_sites + n_bath;
+  std::vector<std::vector<int>> g(n_gen, std::vector<int>(N));
+  for (int j = 0; j < n_gen; ++j)
+    for (int i = 0; i < N; ++i) g[j][i] = gen[(size_t)j * N + i];
+  return build_symmetry_group(n_sites, n_bath, g, bath_irrep != 0);
+}
+
+int qed_symmetry_group(int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep, int *g, int *phi,
+                       double *S_re, double *S_im, int *site_irrep_dim) {
+  return guarded([&] {
+    const SymmetryGroup G = group_from_abi(n_sites, n_bath, n_gen, gen, bath_irrep);
+    const int n = G.g();
+    if (g) *g = n;
+    if (phi)
+      for (int a = 0; a < n; ++a)
+        for (int b = 0; b < n; ++b) phi[a * n + b] = G.tab.phi[a][b];
+    for (size_t k = 0; k < G.S.size(); ++k) {
+      if (S_re) S_re[k] = G.S[k].real();
+      if (S_im) S_im[k] = G.S[k].imag();
+    }
+    if (site_irrep_dim)
+      for (int r = 0; r < n; ++r) site_irrep_dim[r] = G.site_irrep_dim[r];
+  });
+}
+
+int qed_symmetry_representatives(int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep, int irrep,
+                                 long n, const uint64_t *states, uint64_t *rep, int *phase, int *length) {
+  return guarded([&] {
+    const SymmetryGroup G = group_from_abi(n_sites, n_bath, n_gen, gen, bath_irrep);
+    if (irrep < 0 || irrep >= G.g()) fail(QED_ERR_ARGUMENT, "irrep out of range");
+    for (long i = 0; i < n; ++i) {
+      const RepMap m = sym_representative(G.tab, states[i], irrep);
+      rep[i] = m.rep;
+      phase[i] = m.phase;
+      length[i] = m.length;
     }
   });
 }

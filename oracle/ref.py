@@ -113,6 +113,8 @@ def lib():
             f.restype = C.c_int
         L.ref_hv_create.argtypes = [C.c_int, C.c_char_p, lp]
         L.ref_hv_create.restype = C.c_void_p
+        L.ref_hv_create_csr.argtypes = [C.c_int, C.c_char_p, lp]
+        L.ref_hv_create_csr.restype = C.c_void_p
         L.ref_hv_destroy.argtypes = [C.c_void_p]
         L.ref_hv_destroy.restype = None
         if L.ref_init() != 0:
@@ -383,11 +385,14 @@ def destroy_table(L, n_up, n_dn, a):
 
 
 class RefHamiltonian:
-    """y += H x through the reference's factorized Hamiltonian, for one sector."""
+    """y += H x through the reference's factorized Hamiltonian, for one sector
+    (csr=True: its CSR Hamiltonian, in the symmetry-adapted basis of a model with
+    generators)."""
 
-    def __init__(self, label, sector: str):
+    def __init__(self, label, sector: str, csr: bool = False):
         d = C.c_long()
-        self.h = lib().ref_hv_create(label, sector.encode(), C.byref(d))
+        fn = lib().ref_hv_create_csr if csr else lib().ref_hv_create
+        self.h = fn(label, sector.encode(), C.byref(d))
         if not self.h:
             _check(1)
         self.dim = d.value

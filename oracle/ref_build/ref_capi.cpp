@@ -477,6 +477,22 @@ void *ref_hv_create(int label, const char *sec, long *dim) {
   return rc ? nullptr : h;
 }
 
+// The reference's CSR Hamiltonian (src_ed/Hamiltonian/Hamiltonian_CSR.hpp) of a
+// sector of a model that is not factorized (one with symmetry generators): the
+// symmetry-adapted (mixed) basis, for H.v parity in that basis.
+void *ref_hv_create_csr(int label, const char *sec, long *dim) {
+  void *h = nullptr;
+  int rc = guarded([&] {
+    auto &I = *model_instances.at((size_t)label);
+    if (I.the_model->is_factorized) throw qcm_error("ref_hv_create_csr: model is factorized");
+    auto *hh = new hv_handle;
+    hh->H.reset(new Hamiltonian_CSR<double>(I.the_model, I.value, sector(sec)));
+    *dim = (long)hh->H->dim;
+    h = hh;
+  });
+  return rc ? nullptr : h;
+}
+
 int ref_hv_apply(void *h, const double *x, double *y) {
   return guarded([&] {
     auto *hh = (hv_handle *)h;

@@ -112,3 +112,56 @@ def test_bad_generators_raise_the_reference_messages(oracle, gens, msg):
         qed.symmetry_group(3, 0, gens, False)
     with pytest.raises(oracle.OracleError, match=msg):
         oracle.symmetry_group(3, 0, gens, False)
+
+
+def _port_gens(gens, n_sites, bath_irrep):
+    return [[v - 1 if (i < n_sites or not bath_irrep) else v for i, v in enumerate(g)] for g in gens]
+
+
+@pytest.mark.parametrize("name", ["c2v_8b_record", "plaquette_c4", "chain4_bath_irrep", "dimer_bath_swap"])
+def test_symmetry_port_matches_the_reference(oracle, name):
+    """The numpy restatement (oracle/port_sym.py) of the group and of the
+    representative map against the compiled reference."""
+    from oracle import port_sym
+    ns, nb, gens, bi = _group(name)
+    G = port_sym.group(ns, nb, _port_gens(gens, ns, bi), bi)
+    ref = oracle.symmetry_group(ns, nb, gens, bi)
+    assert G["g"] == ref["g"] and np.array_equal(G["phi"], ref["phi"])
+    n_orb = ns + nb
+    states = _sector_states(n_orb, n_orb // 2, (n_orb + 1) // 2)
+    states = np.random.default_rng(3).choice(states, min(len(states), 3000), replace=False)
+    for r in range(G["g"]):
+        rrep, rph, rln = oracle.representatives(ns, nb, gens, bi, r, states)
+        for b, a, p, n in zip(states, rrep, rph, rln):
+            rep, ph, ln = port_sym.representative(G, int(b), r)
+            assert ln == n and (n == 0 or (rep == a and ph == p))
+
+
+@pytest.mark.parametrize("case,sectors", [
+    ("sq2x3_c2v_hubbard", ["R0:N6:S0", "R1:N6:S0", "R3:N5:S1"]),
+    ("c2v_8b_record", ["R0:N3:S1", "R2:N3:S1"]),
+])
+def test_mixed_basis_hamiltonian_port_matches_reference_csr(oracle, fresh, case, sectors):
+    """H x in the symmetry-adapted basis: the numpy restatement (one-body elements
+    reaching orbit representatives with sign, character phase and
+    sqrt(len_I / len_J)) against the reference's own CSR Hamiltonian, to 1e-13."""
+    from oracle import port_sym
+    from pyqcm_b200 import workloads as W
+    from tests.helpers import c2v_golden, c2v_problem
+    if case == "c2v_8b_record":
+        prob = c2v_problem(c2v_golden(), True)
+    else:
+        prob = W.hubbard_cluster(3, 2, tp=0.3, U=6.0, mu=2.5)
+        prob.generators = [[3, 2, 1, 6, 5, 4], [4, 5, 6, 1, 2, 3]]
+    suffix, label = fresh()
+    oracle.load_problem(prob, label, model_name="sym" + suffix, fmt="S")
+    G = port_sym.group(prob.n_sites, prob.n_bath, _port_gens(prob.generators, prob.n_sites, prob.bath_irrep),
+                       prob.bath_irrep)
+    for sec in sectors:
+        H, basis = port_sym.mixed_hamiltonian(prob, G, sec)
+        R = oracle.RefHamiltonian(label, sec, csr=True)
+        assert R.dim == H.shape[0]
+        x = np.random.default_rng(11).standard_normal(R.dim)
+        y = np.zeros(R.dim)
+        R.mult_add(x, y)
+        assert np.max(np.abs(y - H @ x)) <= 1e-13 * max(1.0, np.max(np.abs(y))), sec

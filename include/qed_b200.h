@@ -295,6 +295,31 @@ int qed_destroy_table(int L, int n_up, int n_dn, int a, long *target, int *phase
  * the kernels evaluate the same per-state maps. Errors carry the reference's
  * messages (invalid or non-commuting generators). */
 
+/* ED::new_model with symmetry generators (src_ed/qcm_ED.hpp:34; the reference's
+ * Python binding converts pyqcm's 1-based generators to this 0-based form,
+ * src_python/qcm_ED_wrap.hpp:145-163). The group is checked and kept with the
+ * model; sector strings of its instances may name irreps R0..R(g-1). Ground
+ * states and Green functions of such instances return QED_ERR_UNSUPPORTED (they
+ * are solved in the spin-factorized basis, g = 1); their sectors' Hamiltonians
+ * are available through qed_mixed_hamiltonian_*. */
+int qed_new_model_generators(const char *name, int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep);
+
+/* Hamiltonian<double> of one sector in the symmetry-adapted basis
+ * (Hamiltonian_CSR over ED_mixed_basis: src_ed/Hamiltonian/Hamiltonian_CSR.hpp,
+ * src_ed/ED_basis.cpp:185-385, src_ed/Operators/HS_one_body_operator.hpp:11-39),
+ * built and kept on the device. dim is the basis dimension. */
+typedef struct qed_mixed_hamiltonian qed_mixed_hamiltonian;
+int qed_mixed_hamiltonian_create(int label, const char *sector, qed_mixed_hamiltonian **h, long *dim);
+/* the basis: sorted representative states (spin up in bits 0-31) */
+int qed_mixed_hamiltonian_states(qed_mixed_hamiltonian *h, uint64_t *states);
+/* y += H x on host vectors of dim doubles (Hamiltonian::mult_add) */
+int qed_mixed_hamiltonian_mult_add(qed_mixed_hamiltonian *h, const double *x, double *y);
+/* y = H x on device vectors, enqueued on `stream` (a cudaStream_t; NULL: default) */
+int qed_mixed_hamiltonian_apply_device(qed_mixed_hamiltonian *h, const double *x, double *y, void *stream);
+/* number of stored off-diagonal entries */
+int qed_mixed_hamiltonian_nnz(qed_mixed_hamiltonian *h, long *nnz);
+int qed_mixed_hamiltonian_destroy(qed_mixed_hamiltonian *h);
+
 /* symmetry_group::build (src_ed/symmetry_group.cpp:184-345): the group order g,
  * the character phases phi (g x g, units of 2 pi / g), the symmetric site
  * orbitals S (n_sites x n_sites row-major, real and imaginary parts; row k is

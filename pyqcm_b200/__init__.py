@@ -106,6 +106,13 @@ def lib():
         "qed_halfbasis": [C.c_int, C.c_int, up, lp],
         "qed_halfbasis_rank": [C.c_int, C.c_int, C.c_long, up, up],
         "qed_destroy_table": [C.c_int, C.c_int, C.c_int, C.c_int, lp, ip],
+        "qed_new_model_generators": [C.c_char_p, C.c_int, C.c_int, C.c_int, ip, C.c_int],
+        "qed_mixed_hamiltonian_create": [C.c_int, C.c_char_p, C.POINTER(C.c_void_p), lp],
+        "qed_mixed_hamiltonian_states": [C.c_void_p, C.POINTER(C.c_uint64)],
+        "qed_mixed_hamiltonian_mult_add": [C.c_void_p, dp, dp],
+        "qed_mixed_hamiltonian_apply_device": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+        "qed_mixed_hamiltonian_nnz": [C.c_void_p, lp],
+        "qed_mixed_hamiltonian_destroy": [C.c_void_p],
         "qed_symmetry_group": [C.c_int, C.c_int, C.c_int, ip, C.c_int, ip, ip, dp, dp, ip],
         "qed_symmetry_representatives": [C.c_int, C.c_int, C.c_int, ip, C.c_int, C.c_int, C.c_long,
                                          C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), ip, ip],
@@ -162,8 +169,16 @@ def get_global_double(name: str) -> float:
 
 # ---- models and instances ---------------------------------------------------
 
-def new_model(name: str, n_sites: int, n_bath: int = 0):
-    _check(lib().qed_new_model(name.encode(), n_sites, n_bath))
+def new_model(name: str, n_sites: int, n_bath: int = 0, generators=None, bath_irrep: bool = False):
+    """ED::new_model. generators: pyqcm's symmetry generators (1-based sites); a
+    model with a nontrivial group has its sector Hamiltonians in the
+    symmetry-adapted basis (MixedHamiltonian) but no ground-state solve yet."""
+    if not generators:
+        _check(lib().qed_new_model(name.encode(), n_sites, n_bath))
+        return
+    ng, flat = _generators_abi(n_sites, n_bath, generators, bath_irrep)
+    _check(lib().qed_new_model_generators(name.encode(), n_sites, n_bath, ng,
+                                          flat.ctypes.data_as(C.POINTER(C.c_int)), int(bool(bath_irrep))))
 
 
 def new_operator(model: str, op: str, typ: str, elements):
@@ -190,13 +205,11 @@ def load_problem(prob, label: int = 0, model_name: str | None = None, fmt: str |
     Lanczos in every sector; 'S', 'E', 'O', 'N': sectors below max_dim_full are
     diagonalised densely, as in the reference). The format is latched by the
     model's first instance."""
-    if getattr(prob, "generators", None):
-        raise QEDError(QED_ERR_UNSUPPORTED, "symmetry generators (g > 1) are not supported: the "
-                       "spin-factorized Hamiltonian requires the trivial point group")
     if fmt is not None:
         set_global_parameter("Hamiltonian_format", fmt)
     mname = model_name or prob.name
-    new_model(mname, prob.n_sites, prob.n_bath)
+    new_model(mname, prob.n_sites, prob.n_bath, getattr(prob, "generators", None),
+              getattr(prob, "bath_irrep", False))
     for op, (typ, el) in prob.operators.items():
         new_operator(mname, op, typ, el)
     new_model_instance(mname, prob.params, prob.sectors, label)
@@ -479,6 +492,40 @@ def ground_state_vector(label: int = 0):
 
 
 # ---- plugin point and basis -------------------------------------------------
+
+class MixedHamiltonian:
+    """Device Hamiltonian of one sector of a model with point-group generators, in
+    the symmetry-adapted basis (the reference's CSR format over ED_mixed_basis)."""
+
+    def __init__(self, label: int, sector: str):
+        h = C.c_void_p()
+        d = C.c_long()
+        _check(lib().qed_mixed_hamiltonian_create(label, sector.encode(), C.byref(h), C.byref(d)))
+        self.h = h
+        self.dim = d.value
+
+    def states(self):
+        out = np.zeros(self.dim, dtype=np.uint64)
+        _check(lib().qed_mixed_hamiltonian_states(self.h, out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return out
+
+    @property
+    def nnz(self) -> int:
+        n = C.c_long()
+        _check(lib().qed_mixed_hamiltonian_nnz(self.h, C.byref(n)))
+        return n.value
+
+    def mult_add(self, x, y):
+        """y += H x (host float64 arrays)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        assert y.dtype == np.float64 and y.flags.c_contiguous and len(y) == self.dim
+        _check(lib().qed_mixed_hamiltonian_mult_add(self.h, _dp(x), _dp(y)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.qed_mixed_hamiltonian_destroy(self.h)
+            self.h = None
+
 
 class Hamiltonian:
     """Device Hamiltonian of one sector (Hamiltonian<double> plugin point)."""

@@ -15,6 +15,7 @@
 #include "instance.hpp"
 #include "options.hpp"
 #include "symmetry.hpp"
+#include "mixed.hpp"
 #include "qed_b200.h"
 #include "worker_pool.hpp"
 
@@ -24,6 +25,11 @@ using namespace qed;
 // pass starting as soon as its copy lands; H x comes back in the same blocks and
 // the host adds each block into y while the next one is in flight.
 constexpr int kMultAddChunks = 8;
+
+struct qed_mixed_hamiltonian {
+  std::unique_ptr<MixedHamiltonian> H;
+  std::mutex m;
+};
 
 struct qed_hamiltonian {
   std::unique_ptr<SectorOp> H;
@@ -350,6 +356,23 @@ int qed_new_model(const char *name, int n_sites, int n_bath) {
   });
 }
 
+int qed_new_model_generators(const char *name, int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep) {
+  return guarded([&] {
+    // ED::new_model with generators (src_ed/qcm_ED.cpp:46-60, symmetry_group ctor)
+    std::vector<std::vector<int>> g(n_gen < 0 ? 0 : n_gen, std::vector<int>(n_sites + n_bath));
+    if (n_gen > 0 && !gen) fail(QED_ERR_ARGUMENT, "bad generators");
+    for (int j = 0; j < n_gen; ++j)
+      for (int i = 0; i < n_sites + n_bath; ++i) g[j][i] = gen[(size_t)j * (n_sites + n_bath) + i];
+    auto grp = std::make_shared<const SymmetryGroup>(build_symmetry_group(n_sites, n_bath, g, bath_irrep != 0));
+    const int rc = qed_new_model(name, n_sites, n_bath);
+    if (rc != QED_OK) fail(rc, t_err);
+    std::lock_guard<std::mutex> l(g_reg);
+    auto &m = g_models.at(name);
+    std::lock_guard<std::mutex> lm(m->mtx);
+    if (!m->group && m->term.empty() && grp->g() > 1) m->group = grp;
+  });
+}
+
 int qed_new_operator(const char *model, const char *name, const char *type, int n, const int *r,
                      const int *c, const double *v) {
   return guarded([&] {
@@ -419,6 +442,7 @@ int qed_mixing(int label, int *mixing) {
 int qed_ground_state_solve(int label, double *energy, char *sectors, int len) {
   return guarded([&] {
     auto I = instance(label);
+    I->require_trivial_group();
     std::lock_guard<std::mutex> li(I->mtx);
     auto r = I->low_energy_states(ws());
     *energy = r.first;
@@ -458,6 +482,7 @@ int qed_Green_function_solve_batch(const int *labels, int n, int threads) {
 int qed_Green_function_solve(int label) {
   return guarded([&] {
     auto I = instance(label);
+    I->require_trivial_group();
     std::lock_guard<std::mutex> li(I->mtx);
     I->green_solve(ws());
   });
@@ -1144,6 +1169,81 @@ int qed_symmetry_representatives(int n_sites, int n_bath, int n_gen, const int *
       phase[i] = m.phase;
       length[i] = m.length;
     }
+  });
+}
+
+// ---- Hamiltonian in the symmetry-adapted basis (mixed.hpp) -------------------
+
+int qed_mixed_hamiltonian_create(int label, const char *sector, qed_mixed_hamiltonian **h, long *dim) {
+  return guarded([&] {
+    auto I = instance(label);
+    if (!I->model->group) fail(QED_ERR_ARGUMENT, "model " + I->model->name + " has no point-group generators");
+    const Sector S(sector);
+    if (!sector_is_valid(S, I->model->n_orb, I->model->group->g()) || S.N >= Sector::odd || S.S >= Sector::odd)
+      fail(QED_ERR_ARGUMENT, std::string("sector ") + sector + " is not valid");
+    const MixedTerms t = mixed_terms(*I->model, I->value);
+    Workspace &w = ws();
+    auto *hh = new qed_mixed_hamiltonian;
+    try {
+      hh->H.reset(new MixedHamiltonian(*I->model->group, t, S.irrep, S.Nup(), S.Ndw(), w.stream));
+    } catch (...) {
+      delete hh;
+      throw;
+    }
+    *dim = (long)hh->H->D;
+    *h = hh;
+  });
+}
+
+int qed_mixed_hamiltonian_states(qed_mixed_hamiltonian *h, uint64_t *states) {
+  return guarded([&] {
+    if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
+    std::lock_guard<std::mutex> hl(h->m);
+    Workspace &w = ws();
+    h->H->states.download(states, h->H->D, w.stream);
+    w.sync();
+  });
+}
+
+int qed_mixed_hamiltonian_mult_add(qed_mixed_hamiltonian *h, const double *x, double *y) {
+  return guarded([&] {
+    if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
+    std::lock_guard<std::mutex> hl(h->m);
+    const size_t D = h->H->D;
+    if (!D) return;
+    Workspace &w = ws();
+    DevBuf<double> dx(D), dy(D);
+    dx.upload(x, D, w.stream);
+    h->H->apply(dx.p, dy.p, w.stream);
+    std::vector<double> hy(D);
+    dy.download(hy.data(), D, w.stream);
+    w.sync();
+    for (size_t i = 0; i < D; ++i) y[i] += hy[i];
+  });
+}
+
+int qed_mixed_hamiltonian_apply_device(qed_mixed_hamiltonian *h, const double *x, double *y, void *stream) {
+  return guarded([&] {
+    if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
+    h->H->apply(x, y, (cudaStream_t)stream);
+  });
+}
+
+int qed_mixed_hamiltonian_nnz(qed_mixed_hamiltonian *h, long *nnz) {
+  return guarded([&] {
+    if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
+    *nnz = (long)h->H->nnz;
+  });
+}
+
+int qed_mixed_hamiltonian_destroy(qed_mixed_hamiltonian *h) {
+  return guarded([&] {
+    if (!h) return;
+    {
+      std::lock_guard<std::mutex> hl(h->m);
+      if (h->H && h->H->D) ws().sync();
+    }
+    delete h;
   });
 }
 

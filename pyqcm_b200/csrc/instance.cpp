@@ -1,5 +1,6 @@
 // Model instance (see instance.hpp).
 #include "instance.hpp"
+#include "symmetry.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -24,8 +25,8 @@ double max_gap() {
 }
 }  // namespace
 
-// symmetry_group::sector_is_valid for the trivial group (src_ed/symmetry_group.cpp:515-532)
-bool sector_is_valid(const Sector &s, int n_orb) {
+// symmetry_group::sector_is_valid (src_ed/symmetry_group.cpp:515-532): irrep below the group order
+bool sector_is_valid(const Sector &s, int n_orb, int g) {
   if (s.N < Sector::odd) {
     if (s.N < 0 || s.N > 2 * n_orb) return false;
     if (s.S < Sector::odd) {
@@ -34,7 +35,7 @@ bool sector_is_valid(const Sector &s, int n_orb) {
     }
   }
   if (s.S < Sector::odd && (s.S > n_orb || s.S < -n_orb)) return false;
-  return s.irrep == 0;
+  return s.irrep >= 0 && s.irrep < g;
 }
 
 // symmetry_group::shift_sector (src_ed/symmetry_group.cpp:540-558)
@@ -96,7 +97,8 @@ Instance::Instance(int lab, std::shared_ptr<Model> m, std::map<std::string, doub
   while (std::getline(ss, item, '/')) {
     if (item.empty()) continue;
     Sector S(item);
-    if (!sector_is_valid(S, model->n_orb)) fail(QED_ERR_ARGUMENT, "sector " + item + " is not valid");
+    if (!sector_is_valid(S, model->n_orb, model->group ? model->group->g() : 1))
+      fail(QED_ERR_ARGUMENT, "sector " + item + " is not valid");
     if (S.S && mix == mixing::normal) mix = mixing::up_down;
     if (S.S >= Sector::odd)
       fail(QED_ERR_ARGUMENT, "sector string " + S.name() +
@@ -451,6 +453,7 @@ size_t Instance::sector_dim(const Sector &s) const {
 // (src_ed/Hamiltonian/Hamiltonian_Dense.hpp:110-125) below max_dim_full in the
 // non-factorized formats, the Lanczos eigenvalue pass otherwise.
 void Instance::solve_sector(const Sector &s, SectorSolve &out, Workspace &ws, DeferredSectors *defer) {
+  require_trivial_group();
   out.sec = s;
   try {
     auto Hp = std::make_unique<SectorOp>(terms, s, ws, &tables);
@@ -587,8 +590,18 @@ void Instance::finish_gs(Workspace &ws) {
 }
 
 // low_energy_states (src_ed/model_instance.hpp:245-347)
+void Instance::require_trivial_group() const {
+  if (model->group && model->group->g() > 1)
+    fail(QED_ERR_UNSUPPORTED, "model " + model->name + " has point-group generators (g = " +
+                                  std::to_string(model->group->g()) +
+                                  "): its sectors have the symmetry-adapted Hamiltonian "
+                                  "(qed_mixed_hamiltonian_*), but ground states and Green functions "
+                                  "are solved only in the spin-factorized basis (g = 1)");
+}
+
 std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
   if (gs_solved) return {GS_energy, gs_string()};
+  require_trivial_group();
   if (!is_correlated) {
     one_body_solve(ws);
     return {GS_energy, gs_string()};

@@ -98,6 +98,8 @@ struct Instance {
   Instance(int label, std::shared_ptr<Model> m, std::map<std::string, double> value,
            const std::string &sectors);
 
+  // fails (unsupported) for a model with point-group generators
+  void require_trivial_group() const;
   std::pair<double, std::string> low_energy_states(Workspace &ws);
   void green_solve(Workspace &ws);
 
@@ -159,7 +161,7 @@ struct Instance {
                   double coef, bool accumulate, Workspace &ws);
 };
 
-bool sector_is_valid(const Sector &s, int n_orb);
+bool sector_is_valid(const Sector &s, int n_orb, int g = 1);
 Sector shift_sector(const Sector &s, int pm, int spin);
 
 }  // namespace qed

@@ -1,0 +1,62 @@
+// Hamiltonian of one sector in the symmetry-adapted (mixed) basis of a cluster
+// with point-group generators: the reference's CSR format
+// (src_ed/Hamiltonian/Hamiltonian_CSR.hpp over ED_mixed_basis) built on the
+// device and kept resident in HBM.
+//
+// Build, all on the device: every state of the factorized (N_up, N_dn) sector
+// is marked when it is its orbit's representative with a nonzero projection
+// (sym_representative); a scan over the marks, in the factorized order (down
+// string major), gives the sorted representative list and a dense map from
+// factorized index to basis index. Each basis row J then applies every
+// off-diagonal one-body element to its state, finds the representative K of the
+// image and its basis index through the map (combinatorial ranks of the two
+// strings), and stores (K, phase x coefficient x fermion sign x
+// sqrt(len_J / len_K)): the reference's element of
+// src_ed/Operators/HS_one_body_operator.hpp:17-37 read along the row, as H is
+// symmetric. Rows are counted first, then filled. The diagonal (one-body
+// diagonal and interaction elements, mask rule of
+// src_ed/Operators/HS_interaction_operator.hpp:44-53) is its own vector.
+//
+// H x is then a CSR product: eight lanes per row, HBM-bound on the column and
+// value arrays (12 bytes per entry), x gathered through L2.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+#include "model.hpp"
+#include "symmetry.hpp"
+
+namespace qed {
+
+// Elements of H = sum over operators of value x operator, split as the mixed
+// basis uses them: off-diagonal one-body (r != c, both orders, merged by (r, c))
+// and diagonal masks (a one-body diagonal is one bit; an interaction element
+// (r, c) is mask(r) + mask(c)).
+struct MixedTerms {
+  std::vector<int> r, c;
+  std::vector<double> v;
+  std::vector<uint64_t> dmask;
+  std::vector<double> dval;
+};
+MixedTerms mixed_terms(const Model &m, const std::map<std::string, double> &value);
+
+struct MixedHamiltonian {
+  size_t D = 0;          // basis dimension
+  size_t nnz = 0;        // off-diagonal entries
+  DevBuf<uint64_t> states;   // sorted representatives (spin up in the low word)
+  DevBuf<uint8_t> len;       // orbit lengths
+  DevBuf<uint64_t> row_ptr;  // D + 1
+  DevBuf<uint32_t> col;
+  DevBuf<double> val;
+  DevBuf<double> dg;         // diagonal
+
+  MixedHamiltonian(const SymmetryGroup &G, const MixedTerms &t, int irrep, int n_up, int n_dn, cudaStream_t s);
+  // y = H x on device vectors of D doubles, on stream s
+  void apply(const double *x, double *y, cudaStream_t s) const;
+};
+
+}  // namespace qed

@@ -58,8 +58,12 @@ struct Operator {
   std::vector<Element> elements;  // after the reference's normalisation
 };
 
+struct SymmetryGroup;
+
 struct Model {
   std::string name;
+  // point group of the generators given at creation; null for none (g = 1)
+  std::shared_ptr<const SymmetryGroup> group;
   int n_sites = 0, n_bath = 0, n_orb = 0;
   bool is_closed = false;
   int mix = -1;  // mixing fixed by the first instance (src_ed/model_instance_base.cpp:71-78)

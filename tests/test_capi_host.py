@@ -73,12 +73,19 @@ def test_unknown_label_and_options(qed):
     qed.set_global_parameter("kgrid_side", 32)  # lattice-layer option is accepted
 
 
-def test_generators_are_refused_loudly():
-    """A cluster model with symmetry generators (g > 1) is outside the
-    spin-factorized solver: loading one raises the unsupported status instead of
-    silently solving the unsymmetrised Hamiltonian."""
+def test_models_with_generators_load_and_refuse_the_factorized_solve():
+    """A cluster model with symmetry generators (g > 1) loads with its group
+    (sector strings may name irreps below g); its ground state and Green function
+    are refused with the unsupported status instead of being solved silently on
+    the unsymmetrised basis."""
     import pyqcm_b200 as qed
     from tests.helpers import c2v_golden, c2v_problem
-    with pytest.raises(qed.QEDError) as err:
-        qed.load_problem(c2v_problem(c2v_golden(), True), 1, model_name="c2v_refused")
-    assert err.value.code == qed.QED_ERR_UNSUPPORTED
+    prob = c2v_problem(c2v_golden(), True)
+    qed.load_problem(prob, 4101, model_name="c2v_host")
+    for fn in (qed.ground_state_solve, qed.Green_function_solve):
+        with pytest.raises(qed.QEDError) as err:
+            fn(4101)
+        assert err.value.code == qed.QED_ERR_UNSUPPORTED
+    qed.new_model_instance("c2v_host", prob.params, "R3:N11:S1", 4102)
+    with pytest.raises(qed.QEDError, match="not valid"):
+        qed.new_model_instance("c2v_host", prob.params, "R4:N12:S0", 4103)

@@ -316,6 +316,9 @@ int qed_mixed_hamiltonian_states(qed_mixed_hamiltonian *h, uint64_t *states);
 int qed_mixed_hamiltonian_mult_add(qed_mixed_hamiltonian *h, const double *x, double *y);
 /* y = H x on device vectors, enqueued on `stream` (a cudaStream_t; NULL: default) */
 int qed_mixed_hamiltonian_apply_device(qed_mixed_hamiltonian *h, const double *x, double *y, void *stream);
+/* lowest eigenvalue of the sector by Lanczos (LanczosEigenvalue,
+ * src_ed/Hamiltonian/Lanczos.hpp:41-97; accur_lanczos, max_iter_lanczos, seed) */
+int qed_mixed_hamiltonian_ground_state(qed_mixed_hamiltonian *h, double *energy, int *iterations);
 /* number of stored off-diagonal entries */
 int qed_mixed_hamiltonian_nnz(qed_mixed_hamiltonian *h, long *nnz);
 int qed_mixed_hamiltonian_destroy(qed_mixed_hamiltonian *h);

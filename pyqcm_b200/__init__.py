@@ -111,6 +111,7 @@ def lib():
         "qed_mixed_hamiltonian_states": [C.c_void_p, C.POINTER(C.c_uint64)],
         "qed_mixed_hamiltonian_mult_add": [C.c_void_p, dp, dp],
         "qed_mixed_hamiltonian_apply_device": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+        "qed_mixed_hamiltonian_ground_state": [C.c_void_p, dp, ip],
         "qed_mixed_hamiltonian_nnz": [C.c_void_p, lp],
         "qed_mixed_hamiltonian_destroy": [C.c_void_p],
         "qed_symmetry_group": [C.c_int, C.c_int, C.c_int, ip, C.c_int, ip, ip, dp, dp, ip],
@@ -520,6 +521,13 @@ class MixedHamiltonian:
         x = np.ascontiguousarray(x, dtype=np.float64)
         assert y.dtype == np.float64 and y.flags.c_contiguous and len(y) == self.dim
         _check(lib().qed_mixed_hamiltonian_mult_add(self.h, _dp(x), _dp(y)))
+
+    def ground_state_energy(self):
+        """(lowest eigenvalue, Lanczos iterations) of the sector."""
+        e = C.c_double()
+        it = C.c_int()
+        _check(lib().qed_mixed_hamiltonian_ground_state(self.h, C.byref(e), C.byref(it)))
+        return e.value, it.value
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

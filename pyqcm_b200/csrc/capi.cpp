@@ -1229,6 +1229,16 @@ int qed_mixed_hamiltonian_apply_device(qed_mixed_hamiltonian *h, const double *x
   });
 }
 
+int qed_mixed_hamiltonian_ground_state(qed_mixed_hamiltonian *h, double *energy, int *iterations) {
+  return guarded([&] {
+    if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
+    std::lock_guard<std::mutex> hl(h->m);
+    const LanczosResult r = lanczos_energy_mixed(*h->H, ws(), (uint64_t)opt_int("seed"));
+    *energy = r.energy;
+    if (iterations) *iterations = r.iterations;
+  });
+}
+
 int qed_mixed_hamiltonian_nnz(qed_mixed_hamiltonian *h, long *nnz) {
   return guarded([&] {
     if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");

@@ -204,6 +204,52 @@ __global__ void k_mixed_spmv(const uint64_t *__restrict__ row_ptr, const uint32_
   }
 }
 
+// One ground-state Lanczos step on the mixed basis: w = H v - beta v_prev with
+// the per-block partial sums of <v, w> at partials[block * ld] (the layout the
+// factorized path's reductions use), rows as in k_mixed_spmv.
+__global__ void __launch_bounds__(256) k_mixed_lanczos_w(const uint64_t *__restrict__ row_ptr,
+                                                         const uint32_t *__restrict__ col,
+                                                         const double *__restrict__ val,
+                                                         const double *__restrict__ dg,
+                                                         const double *__restrict__ v,
+                                                         const double *__restrict__ vprev,
+                                                         const double *__restrict__ beta_dev,
+                                                         double *__restrict__ w, uint64_t D,
+                                                         double *__restrict__ partials, int ld) {
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t n_warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 7;
+  const int group = (threadIdx.x & 31) >> 3;
+  const double beta = *beta_dev;
+  double acc = 0.0;
+  for (uint64_t J0 = warp * 4; J0 < D; J0 += n_warps * 4) {
+    const uint64_t J = J0 + group;
+    double s = 0.0;
+    if (J < D) {
+      const uint64_t a = row_ptr[J], e = row_ptr[J + 1];
+      for (uint64_t k = a + lane; k < e; k += 8) s += val[k] * __ldg(v + col[k]);
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 4);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    if (J < D && lane == 0) {
+      const double vj = v[J];
+      const double wj = dg[J] * vj + s - beta * vprev[J];
+      w[J] = wj;
+      acc += vj * wj;
+    }
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ double red[8];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
+    partials[(size_t)blockIdx.x * ld] = t;
+  }
+}
+
 unsigned grid_for(uint64_t n, int threads) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
@@ -301,6 +347,15 @@ MixedHamiltonian::MixedHamiltonian(const SymmetryGroup &G, const MixedTerms &t, 
   k_mixed_diag<<<grid_for(D, 256), 256, 0, s>>>(states.p, D, dm.p, dv.p, (int)t.dmask.size(), dg.p);
   QED_LAUNCH();
   QED_CUDA(cudaStreamSynchronize(s));
+}
+
+int MixedHamiltonian::lanczos_w(const double *v, const double *vprev, const double *beta_dev, double *w,
+                                double *partials, int ld, int max_blocks, cudaStream_t s) const {
+  unsigned nb = grid_for(D * 8, 256);
+  if (nb > (unsigned)max_blocks) nb = (unsigned)max_blocks;
+  k_mixed_lanczos_w<<<nb, 256, 0, s>>>(row_ptr.p, col.p, val.p, dg.p, v, vprev, beta_dev, w, D, partials, ld);
+  QED_LAUNCH();
+  return (int)nb;
 }
 
 void MixedHamiltonian::apply(const double *x, double *y, cudaStream_t s) const {

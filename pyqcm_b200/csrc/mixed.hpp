@@ -57,6 +57,10 @@ struct MixedHamiltonian {
   MixedHamiltonian(const SymmetryGroup &G, const MixedTerms &t, int irrep, int n_up, int n_dn, cudaStream_t s);
   // y = H x on device vectors of D doubles, on stream s
   void apply(const double *x, double *y, cudaStream_t s) const;
+  // w = H v - (*beta_dev) vprev, with per-block partials of <v, w> at
+  // partials[block * ld]; returns the number of blocks (at most max_blocks)
+  int lanczos_w(const double *v, const double *vprev, const double *beta_dev, double *w, double *partials, int ld,
+                int max_blocks, cudaStream_t s) const;
 };
 
 }  // namespace qed

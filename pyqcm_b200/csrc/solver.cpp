@@ -1,5 +1,6 @@
 // Device sector Hamiltonian and Krylov drivers (see solver.hpp).
 #include "solver.hpp"
+#include "mixed.hpp"
 
 #include <algorithm>
 #include <functional>
@@ -555,6 +556,81 @@ LanczosResult lanczos_ground_state(const SectorOp &H, Workspace &ws, DevBuf<doub
                                    uint64_t seed) {
   LanczosResult res = lanczos_energy(H, ws, seed);
   lanczos_eigenvector(H, ws, res, seed, psi);
+  return res;
+}
+
+// Ground-state energy of one sector in the symmetry-adapted basis: the recurrence,
+// chunking and Ritz-residual stop of lanczos_energy, with the mixed-basis CSR
+// product (w = H v_j - beta_{j-1} v_{j-1} and the <v_j, w> partials in one kernel).
+LanczosResult lanczos_energy_mixed(const MixedHamiltonian &H, Workspace &ws, uint64_t seed) {
+  PhaseScope ps(kPhGsLanczos);
+  LanczosResult res;
+  const size_t D = H.D;
+  if (D == 0) fail(QED_ERR_ARGUMENT, "empty sector");
+  const double accur = opt_double("accur_lanczos");
+  const long max_iter = opt_int("max_iter_lanczos");
+  cudaStream_t s = ws.stream;
+  constexpr int kChunk = 16;
+  DevBuf<double> A(D), B(D), C(D);
+  start_vector(D, seed, B.p, ws);
+  QED_CUDA(cudaMemsetAsync(A.p, 0, D * sizeof(double), s));
+  const size_t cap = (size_t)std::max<long>(max_iter, 1) + 2 * kChunk;
+  DevBuf<double> sc(3 + 2 * cap);
+  DevBuf<int> jd(1);
+  QED_CUDA(cudaMemsetAsync(sc.p, 0, 3 * sizeof(double), s));
+  QED_CUDA(cudaMemsetAsync(jd.p, 0, sizeof(int), s));
+  LanczosScalars ls;
+  ls.alpha_cur = sc.p;
+  ls.b2_cur = sc.p + 1;
+  ls.beta_prev = sc.p + 2;
+  ls.alpha_hist = sc.p + 3;
+  ls.beta_hist = sc.p + 3 + cap;
+  ls.j = jd.p;
+  double *pa = A.p, *pb = B.p, *pc = C.p;
+  std::vector<double> &alpha = res.alpha, &beta = res.beta;
+  double lambda0 = 0.0;
+  RitzTracker tracker;
+  size_t launched = 0;
+  int chunk = (int)std::min<size_t>(std::max<size_t>(D, 2), 8);
+  bool stop = false;
+  while (!stop) {
+    if (launched + chunk > cap) fail(QED_ERR_INTERNAL, "Lanczos history overflow");
+    for (int k = 0; k < chunk; ++k) {
+      int nb = H.lanczos_w(pb, pa, ls.beta_prev, pc, ws.red.partials, Reducer::kMaxRed, ws.red.max_blocks, s);
+      launch_finalize(ws.red.partials, nb, 1, ls.alpha_cur, s);  // alpha_j = <v_j, w>
+      nb = launch_axpy_dev(D, pc, pb, ls.alpha_cur, ws.red, s);  // w -= alpha_j v_j
+      launch_finalize(ws.red.partials, nb, 1, ls.b2_cur, s);      // |w|^2
+      launch_lanczos_advance(D, pc, ls, s);                       // v_{j+1} = w / beta_j
+      double *t = pa;
+      pa = pb;
+      pb = pc;
+      pc = t;
+    }
+    QED_CUDA(cudaMemcpyAsync(ws.host, ls.alpha_hist + launched, chunk * sizeof(double), cudaMemcpyDeviceToHost, s));
+    QED_CUDA(cudaMemcpyAsync(ws.host + kChunk, ls.beta_hist + launched, chunk * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+    ws.sync();
+    launched += chunk;
+    for (int k = 0; k < chunk && !stop; ++k) {
+      const double a = ws.host[k], b = ws.host[kChunk + k];
+      alpha.push_back(a);
+      beta.push_back(b);
+      double last = 1.0;
+      tridiag_lowest_track((int)alpha.size(), alpha.data(), beta.data(), tracker, &lambda0, &last);
+      double ritz = std::fabs(last * b);
+      if (std::fabs(ritz - accur) < kQlBand * accur) {
+        if (!tridiag_lowest_last((int)alpha.size(), alpha.data(), beta.data(), &lambda0, &last))
+          fail(QED_ERR_LANCZOS, "tridiagonal eigensolver did not converge");
+        ritz = std::fabs(last * b);
+      }
+      if ((long)alpha.size() > max_iter)
+        fail(QED_ERR_LANCZOS, "Lanczos procedure exceeded " + std::to_string(max_iter) + " iterations");
+      if (!(ritz > accur)) stop = true;
+    }
+    chunk = kChunk;
+  }
+  res.energy = lambda0;
+  res.iterations = (int)alpha.size();
   return res;
 }
 

@@ -102,6 +102,10 @@ void lanczos_eigenvector(const SectorOp &H, Workspace &ws, const LanczosResult &
 LanczosResult lanczos_ground_state(const SectorOp &H, Workspace &ws, DevBuf<double> &psi,
                                    uint64_t seed);
 
+// Ground-state energy of a sector in the symmetry-adapted basis (mixed.hpp).
+struct MixedHamiltonian;
+LanczosResult lanczos_energy_mixed(const MixedHamiltonian &H, Workspace &ws, uint64_t seed);
+
 // Full diagonalisation of a small sector (Hamiltonian_Dense::states and
 // ::build_Q_matrix, src_ed/Hamiltonian/Hamiltonian_Dense.hpp:110-180): the dense
 // matrix is assembled on the device from the sector tables, the D x D symmetric

@@ -39,3 +39,38 @@ def test_mixed_hamiltonian_matches_reference_csr(qed, oracle, fresh, case, secto
         R.mult_add(x, yr)
         assert np.max(np.abs(y - yr)) <= 1e-13 * max(1.0, np.max(np.abs(yr))), sec
         del H, R
+
+
+def test_mixed_basis_ground_state_matches_reference_record(qed, oracle, fresh):
+    """Lanczos on the device in the symmetry-adapted basis of the reference's C2v
+    record: the record's ground-state energy (6 digits) and the compiled
+    reference's own ground state of that sector (CSR format) to 1e-10."""
+    gold = c2v_golden()
+    prob = c2v_problem(gold, True)
+    suffix, label = fresh()
+    name = "mixgs" + suffix
+    qed.load_problem(prob, label, model_name=name)
+    oracle.set_param("GF_method", "L")
+    oracle.load_problem(prob, label, model_name=name, fmt="S")
+    e_ref, _ = oracle.ground_state(label)
+    H = qed.MixedHamiltonian(label, gold["sectors"])
+    e, it = H.ground_state_energy()
+    assert abs(e - gold["gs"]["energy"]) < 5.1e-5, e
+    assert abs(e - e_ref) <= 1e-10 * abs(e_ref), (e, e_ref, it)
+
+
+def test_mixed_basis_lowest_levels_per_irrep(qed, fresh):
+    """The lowest level of every irrep of a 2x3 Hubbard cluster with C2v
+    generators against dense diagonalisation of the numpy restatement's
+    mixed-basis matrix (oracle/port_sym.py)."""
+    from oracle import port_sym
+    prob = _sq2x3_c2v()
+    suffix, label = fresh()
+    qed.load_problem(prob, label, model_name="mixirr" + suffix)
+    G = port_sym.group(6, 0, [[v - 1 for v in g] for g in prob.generators], False)
+    for r in range(4):
+        sec = f"R{r}:N6:S0"
+        Hp, _ = port_sym.mixed_hamiltonian(prob, G, sec)
+        e_dense = np.linalg.eigvalsh(Hp.toarray())[0]
+        e, _ = qed.MixedHamiltonian(label, sec).ground_state_energy()
+        assert abs(e - e_dense) < 1e-10, (sec, e, e_dense)

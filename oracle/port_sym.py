@@ -10,6 +10,13 @@ and the product on small cases; written for readability, not speed.
   mixed_basis         src_ed/ED_basis.cpp:185-385 (unmixed N, S sectors)
   mixed_hamiltonian   src_ed/Operators/HS_one_body_operator.hpp:17-37 and
                       src_ed/Operators/HS_interaction_operator.hpp:32-54 on that basis
+  symmetric_orbitals  src_ed/symmetry_group.cpp:282-318 (real characters)
+  destroy_matrix      Destroy (src_ed/ED_basis.cpp:62-78) and the destruction
+                      operator of a symmetric orbital
+                      (src_ed/Operators/destruction_operator.cpp:12-32)
+  shift_irrep         symmetry_group::shift_sector (src_ed/symmetry_group.cpp:540-558)
+  irrep_green_function the Lehmann Green function of one symmetric orbital by dense
+                      diagonalisation (small sectors only)
 
 States are 64-bit ints, spin up in bits 0..31, spin down in bits 32..63.
 Phases are integers in units of pi / g.
@@ -64,7 +71,7 @@ def group(n_sites, n_bath, gens0, bath_irrep):
         for b in range(g):
             da, db = digits(a), digits(b)
             phi[a, b] = sum(da[k] * db[k] * g // orders[k] for k in range(len(orders))) % g
-    return dict(N=N, L=L, g=g, elems=elems, phi=phi)
+    return dict(N=N, L=L, g=g, elems=elems, phi=phi, orders=orders)
 
 
 def _apply_half(G, e, b):
@@ -181,3 +188,104 @@ def mixed_hamiltonian(prob, G, sector):
                         diag[I] += val * v
     H = sp.coo_matrix((vals, (rows, cols)), shape=(D, D)).tocsr() + sp.diags(diag)
     return H.tocsr(), np.array(basis, dtype=np.uint64)
+
+
+def tensor(G, r1, r2):
+    """Irrep product: digit-wise sum of the mixed-radix labels (Index(r1, r2))."""
+    out, mult = 0, 1
+    for n in G["orders"]:
+        out += ((r1 % n + r2 % n) % n) * mult
+        r1 //= n
+        r2 //= n
+        mult *= n
+    return out
+
+
+def conjugate(G, r):
+    out, mult = 0, 1
+    for n in G["orders"]:
+        out += ((-(r % n)) % n) * mult
+        r //= n
+        mult *= n
+    return out
+
+
+def shift_irrep(G, r, pm, r_orb):
+    return tensor(G, r, r_orb) if pm == 1 else tensor(G, r, conjugate(G, r_orb))
+
+
+def symmetric_orbitals(G, n_sites):
+    """Rows of S (real characters) and the irrep of each row, irreps in order."""
+    g = G["g"]
+    rows, irreps = [], []
+    for r in range(g):
+        covered = [False] * n_sites
+        for site in range(n_sites):
+            if covered[site]:
+                continue
+            covered[site] = True
+            orb = np.zeros(n_sites)
+            for e in range(g):
+                t = G["elems"][e][site]
+                covered[t] = True
+                orb[t] += np.cos(2 * np.pi * G["phi"][r, e] / g)
+            nrm = np.linalg.norm(orb)
+            if nrm < 1e-12:
+                continue
+            rows.append(orb / nrm)
+            irreps.append(r)
+    return np.array(rows), irreps
+
+
+def destroy_matrix(G, s_row, spin, basis_src, r_src, basis_tgt, r_tgt):
+    """c of the symmetric orbital with site coefficients s_row (spin 0 up, 1 down),
+    from the basis of irrep r_src to that of r_tgt, as a dense (D_tgt, D_src) array."""
+    n, g = G["N"], G["g"]
+    index = {b: i for i, b in enumerate(basis_tgt)}
+    T = np.zeros((len(basis_tgt), len(basis_src)))
+    for I, b in enumerate(basis_src):
+        len_i = representative(G, b, r_src)[2]
+        for site, coef in enumerate(s_row):
+            if coef == 0.0:
+                continue
+            a = site + spin * n
+            mask = 1 << (a - n + 32) if a >= n else 1 << a
+            if not b & mask:
+                continue
+            rep, ph, ln = representative(G, b ^ mask, r_tgt)
+            if ln == 0 or rep not in index:
+                continue
+            if bin(b & (mask - 1)).count("1") & 1:
+                ph += g
+            ph %= 2 * g
+            T[index[rep], I] += (1.0 if ph == 0 else -1.0) * coef * np.sqrt(len_i / ln)
+    return T
+
+
+def irrep_green_function(prob, G, gs_sector, s_row, r_orb, z, spin=0):
+    """G(z) of one symmetric orbital (row s_row of S, irrep r_orb) in the
+    nondegenerate ground state of sector gs_sector, by dense diagonalisation of the
+    ground-state and the two target sectors (creation and destruction)."""
+    r0, N, S = (int(t[1:]) for t in gs_sector.split(":"))
+    H0, B0 = mixed_hamiltonian(prob, G, gs_sector)
+    e0, v0 = np.linalg.eigh(H0.toarray())
+    E0, psi = e0[0], v0[:, 0]
+    z = np.asarray(z, dtype=complex)
+    out = np.zeros(len(z), dtype=complex)
+    ds = -1 if spin else 1
+    for pm in (1, -1):
+        rt = shift_irrep(G, r0, pm, r_orb)
+        sec = f"R{rt}:N{N + pm}:S{S + pm * ds}"
+        Ht, Bt = mixed_hamiltonian(prob, G, sec)
+        if Ht.shape[0] == 0:
+            continue
+        et, vt = np.linalg.eigh(Ht.toarray())
+        if pm == 1:
+            phi = destroy_matrix(G, s_row, spin, Bt, rt, B0, r0).T @ psi   # c+ psi
+            w = (vt.T @ phi) ** 2
+            out += (w[None, :] / (z[:, None] - (et[None, :] - E0))).sum(axis=1)
+        else:
+            phi = destroy_matrix(G, s_row, spin, B0, r0, Bt, rt) @ psi     # c psi
+            w = (vt.T @ phi) ** 2
+            out += (w[None, :] / (z[:, None] + (et[None, :] - E0))).sum(axis=1)
+    return out, E0

@@ -192,3 +192,19 @@ def test_irrep_green_functions_port_matches_reference(oracle, fresh):
         gp, e0 = port_sym.irrep_green_function(prob, G, prob.sectors, row, rho, z)
         assert abs(e0 - e_ref) < 1e-10
         assert np.max(np.abs(gp - np.einsum("a,zab,b->z", row, Gs, row))) < 1e-10
+
+
+def test_trivial_group_and_model_generators_errors(oracle):
+    """No generators: the trivial group (g = 1, one orbital per site in irrep 0), as
+    the reference builds it. A model created with invalid generators fails with the
+    reference's message, through ED::new_model on both sides."""
+    import pyqcm_b200 as qed
+    mine = qed.symmetry_group(3, 1, None, False)
+    ref = oracle.symmetry_group(3, 1, None, False)
+    assert mine["g"] == ref["g"] == 1
+    assert np.array_equal(mine["site_irrep_dim"], ref["site_irrep_dim"])
+    assert np.max(np.abs(mine["S"] - ref["S"])) < 1e-15
+    with pytest.raises(qed.QEDError, match="is not valid"):
+        qed.new_model("badgen_host", 3, 0, [[1, 1, 2]], False)
+    with pytest.raises(oracle.OracleError, match="is not valid"):
+        oracle.new_model("badgen_host", 3, 0, [[1, 1, 2]], False)

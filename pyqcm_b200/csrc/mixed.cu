@@ -251,8 +251,12 @@ __global__ void __launch_bounds__(256) k_mixed_lanczos_w(const uint64_t *__restr
 }
 
 unsigned grid_for(uint64_t n, int threads) {
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  static const int sms = [] {
+    int dev = 0, v = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v;
+  }();
   const uint64_t want = (n + threads - 1) / threads;
   const uint64_t cap = (uint64_t)sms * 16;
   return (unsigned)(want < 1 ? 1 : (want > cap ? cap : want));

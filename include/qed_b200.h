@@ -319,6 +319,10 @@ int qed_mixed_hamiltonian_apply_device(qed_mixed_hamiltonian *h, const double *x
 /* lowest eigenvalue of the sector by Lanczos (LanczosEigenvalue,
  * src_ed/Hamiltonian/Lanczos.hpp:41-97; accur_lanczos, max_iter_lanczos, seed) */
 int qed_mixed_hamiltonian_ground_state(qed_mixed_hamiltonian *h, double *energy, int *iterations);
+/* the ground-state energy and vector (dim doubles, in the basis order of
+ * qed_mixed_hamiltonian_states) by the two Lanczos passes (LanczosEigenvalue and
+ * LanczosEigenvector, src_ed/Hamiltonian/Lanczos.hpp:41-143) */
+int qed_mixed_hamiltonian_ground_state_vector(qed_mixed_hamiltonian *h, double *energy, double *psi);
 /* number of stored off-diagonal entries */
 int qed_mixed_hamiltonian_nnz(qed_mixed_hamiltonian *h, long *nnz);
 int qed_mixed_hamiltonian_destroy(qed_mixed_hamiltonian *h);

@@ -112,6 +112,7 @@ def lib():
         "qed_mixed_hamiltonian_mult_add": [C.c_void_p, dp, dp],
         "qed_mixed_hamiltonian_apply_device": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
         "qed_mixed_hamiltonian_ground_state": [C.c_void_p, dp, ip],
+        "qed_mixed_hamiltonian_ground_state_vector": [C.c_void_p, dp, dp],
         "qed_mixed_hamiltonian_nnz": [C.c_void_p, lp],
         "qed_mixed_hamiltonian_destroy": [C.c_void_p],
         "qed_symmetry_group": [C.c_int, C.c_int, C.c_int, ip, C.c_int, ip, ip, dp, dp, ip],
@@ -528,6 +529,13 @@ class MixedHamiltonian:
         it = C.c_int()
         _check(lib().qed_mixed_hamiltonian_ground_state(self.h, C.byref(e), C.byref(it)))
         return e.value, it.value
+
+    def ground_state(self):
+        """(lowest eigenvalue, its eigenvector in the order of states())."""
+        e = C.c_double()
+        psi = np.zeros(self.dim)
+        _check(lib().qed_mixed_hamiltonian_ground_state_vector(self.h, C.byref(e), _dp(psi)))
+        return e.value, psi
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

@@ -1239,6 +1239,21 @@ int qed_mixed_hamiltonian_ground_state(qed_mixed_hamiltonian *h, double *energy,
   });
 }
 
+int qed_mixed_hamiltonian_ground_state_vector(qed_mixed_hamiltonian *h, double *energy, double *psi) {
+  return guarded([&] {
+    if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");
+    std::lock_guard<std::mutex> hl(h->m);
+    Workspace &w = ws();
+    const uint64_t seed = (uint64_t)opt_int("seed");
+    const LanczosResult r = lanczos_energy_mixed(*h->H, w, seed);
+    DevBuf<double> v;
+    lanczos_eigenvector_mixed(*h->H, w, r, seed, v);
+    v.download(psi, h->H->D, w.stream);
+    w.sync();
+    *energy = r.energy;
+  });
+}
+
 int qed_mixed_hamiltonian_nnz(qed_mixed_hamiltonian *h, long *nnz) {
   return guarded([&] {
     if (!h) fail(QED_ERR_ARGUMENT, "null Hamiltonian");

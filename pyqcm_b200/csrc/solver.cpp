@@ -634,6 +634,36 @@ LanczosResult lanczos_energy_mixed(const MixedHamiltonian &H, Workspace &ws, uin
   return res;
 }
 
+// The ground-state vector of a mixed-basis sector: the replay of
+// lanczos_eigenvector (LanczosEigenvector, src_ed/Hamiltonian/Lanczos.hpp:109-143)
+// with the CSR product.
+void lanczos_eigenvector_mixed(const MixedHamiltonian &H, Workspace &ws, const LanczosResult &res, uint64_t seed,
+                               DevBuf<double> &psi) {
+  PhaseScope ps(kPhGsVector);
+  const size_t D = H.D;
+  cudaStream_t s = ws.stream;
+  const std::vector<double> &alpha = res.alpha, &beta = res.beta;
+  const int M = (int)alpha.size();
+  std::vector<double> d(alpha), e(beta), Z;
+  e.resize(M > 0 ? M - 1 : 0);
+  if (!tridiag_eig(M, d, e, &Z)) fail(QED_ERR_LANCZOS, "tridiagonal eigensolver did not converge");
+  psi.alloc(D);
+  DevBuf<double> A(D), B(D), C(D);
+  start_vector(D, seed, B.p, ws);
+  launch_axpby(D, 0.0, psi.p, Z[0], B.p, 0, ws.red, s);
+  double *pa = A.p, *pb = B.p, *pc = C.p;
+  for (int j = 1; j < M; ++j) {
+    H.apply(pb, pc, s);                                         // H v_{j-1}
+    launch_axpby(D, 1.0, pc, -alpha[j - 1], pb, 0, ws.red, s);  // - alpha_{j-1} v_{j-1}
+    if (j >= 2) launch_axpby(D, 1.0, pc, -beta[j - 2], pa, 0, ws.red, s);  // - beta_{j-2} v_{j-2}
+    launch_scale(D, pc, 1.0 / beta[j - 1], s);
+    launch_axpby(D, 1.0, psi.p, Z[j], pc, 0, ws.red, s);
+    std::swap(pa, pb);
+    std::swap(pb, pc);
+  }
+  ws.sync();
+}
+
 // ------------------------------------------------------ full diagonalisation --
 
 void dense_eigensystem(const SectorOp &H, Workspace &ws, std::vector<double> &w,

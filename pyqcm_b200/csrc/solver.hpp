@@ -105,6 +105,8 @@ LanczosResult lanczos_ground_state(const SectorOp &H, Workspace &ws, DevBuf<doub
 // Ground-state energy of a sector in the symmetry-adapted basis (mixed.hpp).
 struct MixedHamiltonian;
 LanczosResult lanczos_energy_mixed(const MixedHamiltonian &H, Workspace &ws, uint64_t seed);
+void lanczos_eigenvector_mixed(const MixedHamiltonian &H, Workspace &ws, const LanczosResult &res, uint64_t seed,
+                               DevBuf<double> &psi);
 
 // Full diagonalisation of a small sector (Hamiltonian_Dense::states and
 // ::build_Q_matrix, src_ed/Hamiltonian/Hamiltonian_Dense.hpp:110-180): the dense

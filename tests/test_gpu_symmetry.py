@@ -62,7 +62,8 @@ def test_mixed_basis_ground_state_matches_reference_record(qed, oracle, fresh):
 def test_mixed_basis_lowest_levels_per_irrep(qed, fresh):
     """The lowest level of every irrep of a 2x3 Hubbard cluster with C2v
     generators against dense diagonalisation of the numpy restatement's
-    mixed-basis matrix (oracle/port_sym.py)."""
+    mixed-basis matrix (oracle/port_sym.py); the ground-state vector (second
+    Lanczos pass) is a unit eigenvector of that matrix."""
     from oracle import port_sym
     prob = _sq2x3_c2v()
     suffix, label = fresh()
@@ -72,5 +73,10 @@ def test_mixed_basis_lowest_levels_per_irrep(qed, fresh):
         sec = f"R{r}:N6:S0"
         Hp, _ = port_sym.mixed_hamiltonian(prob, G, sec)
         e_dense = np.linalg.eigvalsh(Hp.toarray())[0]
-        e, _ = qed.MixedHamiltonian(label, sec).ground_state_energy()
+        H = qed.MixedHamiltonian(label, sec)
+        e, _ = H.ground_state_energy()
         assert abs(e - e_dense) < 1e-10, (sec, e, e_dense)
+        e2, psi = H.ground_state()
+        assert abs(e2 - e) < 1e-12
+        assert abs(np.linalg.norm(psi) - 1.0) < 1e-9
+        assert np.linalg.norm(Hp @ psi - e * psi) < 1e-6, sec  # eigenvector of the restated matrix

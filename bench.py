@@ -188,6 +188,10 @@ def run_reference(args, world, rank):
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "steps_requested": args.steps, "warmup_requested": args.warmup,
+            "steps_capped": (f"ran {steps} timed step(s) and {warm} warm-up step(s) of the {args.steps} + "
+                             f"{args.warmup} requested: one H.v of the reference on one core takes "
+                             f"{dt:.1f} s") if (steps, warm) != (args.steps, args.warmup) else None,
             "config": {"workload": WORKLOAD, "inputs": "larger than L2 (1.33 GB vectors)",
                        "reference": "Hamiltonian_Factorized::mult_add compiled from the reference sources (oracle/_ref)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",

@@ -1017,6 +1017,11 @@ int qed_hamiltonian_apply_dots_device_noalloc(qed_hamiltonian *h, const double *
                                               double *dots, void *stream) {
   return guarded([&] {
     if (!h || !x || !y || !dots) fail(QED_ERR_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> hl(h->m);
+    // The Hamiltonian's tables live on the library's device: make it current in
+    // this thread (cudaSetDevice allocates nothing), so that the scratch address
+    // is looked up, and the kernels run, on that device.
+    QED_CUDA(cudaSetDevice(g_device.load()));
     cudaStream_t s = (cudaStream_t)stream;
     if (!h->H->D) {
       QED_CUDA(cudaMemsetAsync(dots, 0, 3 * sizeof(double), s));
@@ -1178,6 +1183,13 @@ int qed_mixed_hamiltonian_create(int label, const char *sector, qed_mixed_hamilt
   return guarded([&] {
     auto I = instance(label);
     if (!I->model->group) fail(QED_ERR_ARGUMENT, "model " + I->model->name + " has no point-group generators");
+    // A generator of order above 2 gives the group complex characters; the
+    // reference then works in a complex Hilbert space (src_ed/qcm_ED.cpp:153)
+    // with phases such as i in the matrix elements. This product is real only.
+    if (I->model->group->has_complex_irrep)
+      fail(QED_ERR_UNSUPPORTED, "model " + I->model->name +
+                                    ": point group with complex characters (a generator of order above 2) needs "
+                                    "a complex Hilbert space, which this solver does not provide");
     const Sector S(sector);
     if (!sector_is_valid(S, I->model->n_orb, I->model->group->g()) || S.N >= Sector::odd || S.S >= Sector::odd)
       fail(QED_ERR_ARGUMENT, std::string("sector ") + sector + " is not valid");

@@ -643,8 +643,17 @@ void lanczos_eigenvector_mixed(const MixedHamiltonian &H, Workspace &ws, const L
   const size_t D = H.D;
   cudaStream_t s = ws.stream;
   const std::vector<double> &alpha = res.alpha, &beta = res.beta;
-  const int M = (int)alpha.size();
-  std::vector<double> d(alpha), e(beta), Z;
+  // The replay divides by beta_{j-1} for j < M. The energy recurrence stops at
+  // the first step whose beta vanishes (its Ritz residual is then 0), so only the
+  // last beta can be zero; cut the replay at the first beta that is not
+  // positive anyway (an exhausted Krylov space of a 1- or 2-state irrep).
+  int M = (int)alpha.size();
+  for (int j = 1; j < M; ++j)
+    if (!(beta[j - 1] > 0.0)) {
+      M = j;
+      break;
+    }
+  std::vector<double> d(alpha.begin(), alpha.begin() + M), e(beta), Z;
   e.resize(M > 0 ? M - 1 : 0);
   if (!tridiag_eig(M, d, e, &Z)) fail(QED_ERR_LANCZOS, "tridiagonal eigensolver did not converge");
   psi.alloc(D);

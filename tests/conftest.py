@@ -33,9 +33,10 @@ def pytest_collection_modifyitems(config, items):
 @pytest.fixture(scope="session")
 def oracle():
     """The reference's own ED library, compiled as the CPU oracle."""
-    from oracle import ref
-    if not ref.available() and os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle", "ref_build")], check=True)
+    from oracle import ref, refpath
+    if not ref.available() and refpath.reference_root() is not None:
+        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle", "ref_build")] + refpath.make_args(),
+                       check=True)
     if not ref.available():
         pytest.skip("oracle library not built")
     ref.lib()

@@ -22,9 +22,13 @@ this cluster's ED instance, so they are not written.
 import ast
 import json
 import os
+import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/tests/test_diagonalization/S_format.ref"
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+from oracle.refpath import reference_file  # noqa: E402
+
+REF = reference_file("tests/test_diagonalization/S_format.ref")
 
 
 def _call_args(line):

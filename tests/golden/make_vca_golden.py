@@ -13,14 +13,18 @@ pyqcm.get_global_parameter('accur_SEF') = 1e-8, prints silenced).
 import ast
 import json
 import os
+import sys
 import types
 import warnings
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/pyqcm/vca.py"
-REF_INIT = "/root/reference/pyqcm/__init__.py"  # regular_frequency_grid
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+from oracle.refpath import reference_file  # noqa: E402
+
+REF = reference_file("pyqcm/vca.py")
+REF_INIT = reference_file("pyqcm/__init__.py")  # regular_frequency_grid
 WANT = ("_evalF", "_NR_Hessian", "_newton_raphson_step", "_vca_accuracy_warning", "_newton_raphson",
         "_QN_values", "_quasi_newton_step", "_quasi_newton")
 

@@ -89,3 +89,21 @@ def test_models_with_generators_load_and_refuse_the_factorized_solve():
     qed.new_model_instance("c2v_host", prob.params, "R3:N11:S1", 4102)
     with pytest.raises(qed.QEDError, match="not valid"):
         qed.new_model_instance("c2v_host", prob.params, "R4:N12:S0", 4103)
+
+
+def test_complex_character_groups_are_refused_by_the_mixed_hamiltonian():
+    """A generator of order 4 (C4 on a plaquette) gives the group complex
+    characters, for which the reference switches to a complex Hilbert space; the
+    real symmetry-adapted Hamiltonian refuses such models with the unsupported
+    status (before any device work) instead of returning real-phase products."""
+    import pyqcm_b200 as qed
+    qed.new_model("c4_plaquette_host", 4, 0, [[2, 4, 1, 3]])
+    hop = [(0, 1, -1.0), (1, 3, -1.0), (3, 2, -1.0), (0, 2, -1.0)]
+    hop += [(a + 4, b + 4, v) for a, b, v in hop]
+    qed.new_operator("c4_plaquette_host", "t", "one-body", hop)
+    qed.new_operator("c4_plaquette_host", "U", "interaction", [(i, i + 4, 1.0) for i in range(4)])
+    qed.new_model_instance("c4_plaquette_host", {"t": 1.0, "U": 4.0}, "R1:N4:S0", 4201)
+    with pytest.raises(qed.QEDError) as err:
+        qed.MixedHamiltonian(4201, "R1:N4:S0")
+    assert err.value.code == qed.QED_ERR_UNSUPPORTED
+    assert "complex" in str(err.value)

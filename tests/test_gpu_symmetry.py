@@ -80,3 +80,17 @@ def test_mixed_basis_lowest_levels_per_irrep(qed, fresh):
         assert abs(e2 - e) < 1e-12
         assert abs(np.linalg.norm(psi) - 1.0) < 1e-9
         assert np.linalg.norm(Hp @ psi - e * psi) < 1e-6, sec  # eigenvector of the restated matrix
+    # one-electron irreps hold one or two states: the Krylov space is exhausted
+    # after one or two steps (a zero beta ends the recurrence and the replay)
+    for r in range(4):
+        sec = f"R{r}:N1:S1"
+        Hp, _ = port_sym.mixed_hamiltonian(prob, G, sec)
+        if Hp.shape[0] == 0:
+            continue
+        assert Hp.shape[0] <= 2, (sec, Hp.shape)
+        e_dense = np.linalg.eigvalsh(Hp.toarray())[0]
+        H = qed.MixedHamiltonian(label, sec)
+        e2, psi = H.ground_state()
+        assert abs(e2 - e_dense) < 1e-10, (sec, e2, e_dense)
+        assert abs(np.linalg.norm(psi) - 1.0) < 1e-9
+        assert np.linalg.norm(Hp @ psi - e2 * psi) < 1e-8, sec

@@ -24,7 +24,7 @@ def test_surrogate_guided_vca_reaches_the_ed_stationary_point(qed):
     f_ed = lambda P: ev(np.c_[np.full(len(P), U), P])
     acc = [2e-5, 2e-5]
     n0 = ev.n_evals
-    x_ed, *_ = vca.newton_raphson(f_ed, [0.15, 0.0], [0.02, 0.02], acc)
+    x_ed, _, g_ed, _, _ = vca.newton_raphson(f_ed, [0.15, 0.0], [0.02, 0.02], acc, certify=1e-6)
     n_ed = ev.n_evals - n0
     box = [[7.0, 9.0], [0.0, 0.4], [-0.5, 0.5]]
     X = vca.training_points(512, box, seed=1)
@@ -33,8 +33,10 @@ def test_surrogate_guided_vca_reaches_the_ed_stationary_point(qed):
     sur.fit(X, y, epochs=400)
     x0 = sur.propose(U, [0.2, 0.0], [0.02, 0.02])
     n0 = ev.n_evals
-    x_s, *_ = vca.newton_raphson(f_ed, x0, [0.005, 0.005], acc)
+    x_s, _, g_s, _, _ = vca.newton_raphson(f_ed, x0, [0.005, 0.005], acc, certify=1e-6)
     n_s = ev.n_evals - n0
+    # both end points are certified stationary: |grad Omega| < 1e-6 from a 1e-4 central stencil
+    assert np.linalg.norm(g_ed) < 1e-6 and np.linalg.norm(g_s) < 1e-6, (g_ed, g_s)
     assert n_s < n_ed, (n_s, n_ed)  # what the trained surrogate saves: ED evaluations
     om = ev(np.c_[[U, U], np.vstack([x_ed, x_s])])
     assert abs(om[0] - om[1]) < 1e-8, (x_ed, x_s, om)
@@ -64,8 +66,8 @@ def test_vca_stationary_point_matches_reference(qed, oracle):
 
     f_gpu = lambda P: ev(np.c_[np.full(len(P), U), P])
     acc = [2e-5, 2e-5]
-    x_ref, *_ = vca.newton_raphson(f_ref, [0.15, 0.0], [0.02, 0.02], acc)
-    x_gpu, *_ = vca.newton_raphson(f_gpu, [0.15, 0.0], [0.02, 0.02], acc)
+    x_ref, *_ = vca.newton_raphson(f_ref, [0.15, 0.0], [0.02, 0.02], acc, certify=1e-6)
+    x_gpu, *_ = vca.newton_raphson(f_gpu, [0.15, 0.0], [0.02, 0.02], acc, certify=1e-6)
     assert np.max(np.abs(x_ref - x_gpu)) < 1e-4, (x_ref, x_gpu)
     om_ref = f_ref(np.array([x_ref]))[0]
     om_gpu = f_gpu(np.array([x_gpu]))[0]

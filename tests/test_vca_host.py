@@ -80,3 +80,25 @@ def test_vca_class_methods_and_bounds():
     assert np.max(np.abs(np.array(xs) - xs[0])) < 1e-4
     with pytest.raises(vca.VCAError, match="out of bounds"):
         vca.VCA(varia=["a", "b"], start=[0.3, -0.1], steps=0.02, accur=1e-6, max=0.2, func=fq)
+
+
+def test_certified_stationary_point():
+    """A functional with strong cubic terms and a flat direction: the reference's
+    gradient exit (gtol 1e-4, read off the large-step fit) stops away from the
+    stationary point; with certify the search continues on a 1e-4 central stencil
+    until |grad| < 1e-6, and ends within 1e-5 of the exact stationary point."""
+    from pyqcm_b200 import vca
+    from scipy.optimize import fsolve
+
+    def f(x):
+        return 0.285 * x[0] ** 2 - 0.0075 * x[1] ** 2 + 0.8 * x[0] ** 3 + 0.02 * x[0] * x[1] - 0.1 * x[0]
+
+    fb2 = lambda X: np.array([f(x) for x in np.atleast_2d(X)])
+    grad = lambda x: np.array([0.57 * x[0] + 2.4 * x[0] ** 2 + 0.02 * x[1] - 0.1, -0.015 * x[1] + 0.02 * x[0]])
+    xs = fsolve(grad, [0.15, 0.0], xtol=1e-14)
+    assert np.linalg.norm(grad(xs)) < 1e-12
+    x, *_ = vca.newton_raphson(fb2, [0.3, 0.1], [0.05, 0.05], [2e-5, 2e-5], gtol=1e-3)
+    xc, _, g, _, _ = vca.newton_raphson(fb2, [0.3, 0.1], [0.05, 0.05], [2e-5, 2e-5], gtol=1e-3, certify=1e-6)
+    assert np.linalg.norm(grad(x)) > 1e-6  # the uncertified exit is not stationary to 1e-6
+    assert np.linalg.norm(g) < 1e-6 and np.linalg.norm(grad(xc)) < 2e-6
+    assert np.max(np.abs(xc - xs)) < 1e-4, (xc, xs)

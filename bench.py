@@ -248,7 +248,8 @@ def run_ours(args, world, rank, local):
     if args.profile:
         if rank == 0:
             print(json.dumps({"profile": True, "dim": D, "ms_per_hv": ms,
-                              "GBps_16D": 16.0 * D / (ms * 1e-3) / 1e9}), flush=True)
+                              "GBps_16D": 16.0 * D / (ms * 1e-3) / 1e9,
+                              "hv_tuning": qed.hv_tuning_report()}), flush=True)
         return
     # end to end through the C ABI with host buffers (y += H x, copies inside)
     xh = torch.empty(D, dtype=torch.float64, pin_memory=True).numpy()
@@ -317,6 +318,7 @@ def run_ours(args, world, rank, local):
                 "path": "qed_hamiltonian_mult_add (y += H x) on pinned host buffers: x up and H x down in row "
                         "blocks overlapped with the row pass, y += H x on host threads"},
         "gpu_launches": 2 * args.steps,
+        "hv_tuning": qed.hv_tuning_report(),
         "clocks": clk,
         "cpu_baseline": cpu,
     }

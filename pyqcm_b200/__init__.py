@@ -61,6 +61,7 @@ def lib():
     up = C.POINTER(C.c_uint)
     sig = {
         "qed_last_error": [C.c_char_p, C.c_int],
+        "qed_hv_tuning_report": [C.c_char_p, C.c_int],
         "qed_init": [C.c_int],
         "qed_set_global_int": [C.c_char_p, C.c_long],
         "qed_set_global_double": [C.c_char_p, C.c_double],
@@ -663,3 +664,13 @@ def destroy_table(L: int, n_up: int, n_dn: int, a: int):
     _check(lib().qed_destroy_table(L, n_up, n_dn, a, tgt.ctypes.data_as(C.POINTER(C.c_long)),
                                    ph.ctypes.data_as(C.POINTER(C.c_int))))
     return tgt, ph
+
+
+def hv_tuning_report():
+    """Launch shapes chosen by the H.v autotuner so far (list of dicts: dim_up,
+    dim_dn, choice, ms per candidate)."""
+    import json
+    n = lib().qed_hv_tuning_report(None, 0)
+    buf = C.create_string_buffer(n + 1)
+    lib().qed_hv_tuning_report(buf, n + 1)
+    return json.loads(buf.value.decode() or "[]")

@@ -2,6 +2,7 @@
 #include "bank_order.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <functional>
 
 namespace qed {
@@ -78,6 +79,86 @@ bool order_for_banks(std::vector<uint32_t> &ell, std::vector<uint8_t> &cnt, uint
       for (int l = 0; l < nl; ++l) ell[(size_t)k * dim + u0 + l] = out[g][(size_t)k * G + l];
     for (int l = 0; l < nl; ++l) cnt[u0 + l] = (uint8_t)steps[g];
   }
+  return true;
+}
+
+}  // namespace qed
+
+namespace qed {
+
+bool pack_hops16(const std::vector<uint32_t> &ell, const std::vector<uint8_t> &cnt, uint32_t dim,
+                 const std::vector<double> &vals, int zero_slot, PackedHops &out) {
+  constexpr int G = 8;
+  if (dim == 0 || dim + G > (1u << 14)) return false;
+  std::vector<double> mags;  // magnitude classes of the value slots in use
+  for (uint32_t i = 0; i < dim; ++i)
+    for (int k = 0; k < cnt[i]; ++k) {
+      const int slot = (int)(ell[(size_t)k * dim + i] & 255u);
+      if (slot == zero_slot) continue;
+      const double m = std::fabs(vals[slot]);
+      if (m != 0.0 && std::find(mags.begin(), mags.end(), m) == mags.end()) mags.push_back(m);
+    }
+  if (mags.size() > 2) return false;
+  std::sort(mags.begin(), mags.end(), [](double a, double b) { return a > b; });
+  while (mags.size() < 2) mags.push_back(0.0);
+  // per class: an ELL sub-table (target << 8 | sign) ordered for banks
+  const uint32_t zbase = dim % G;  // bank group of zero slot dim + j is (zbase + j) % G
+  auto zero_entry = [&](uint32_t group) -> uint16_t { return (uint16_t)(dim + (group + G - zbase) % G); };
+  std::vector<uint8_t> words[2];
+  for (int c = 0; c < 2; ++c) {
+    std::vector<std::vector<uint32_t>> lists(dim);
+    int w = 0;
+    for (uint32_t i = 0; i < dim; ++i) {
+      for (int k = 0; k < cnt[i]; ++k) {
+        const uint32_t e = ell[(size_t)k * dim + i];
+        const int slot = (int)(e & 255u);
+        if (slot == zero_slot) continue;
+        const double v = vals[slot];
+        if (v == 0.0 || std::fabs(v) != mags[c]) continue;
+        lists[i].push_back(((e >> 8) << 8) | (v < 0 ? 1u : 0u));
+      }
+      w = std::max<int>(w, (int)lists[i].size());
+    }
+    std::vector<uint32_t> sub((size_t)std::max(w, 1) * dim, 0u);
+    std::vector<uint8_t> sc(dim);
+    for (uint32_t i = 0; i < dim; ++i) {
+      sc[i] = (uint8_t)lists[i].size();
+      for (size_t k = 0; k < lists[i].size(); ++k) sub[k * dim + i] = lists[i][k];
+    }
+    // bank ordering; its padding entries carry "slot" 2 (neither sign)
+    int w2 = w;
+    if (w > 0 && !order_for_banks(sub, sc, dim, w2, 2)) return false;
+    if (w == 0) w2 = 0;
+    words[c].assign(dim, 0);
+    int wmax = 0;
+    for (uint32_t i = 0; i < dim; ++i) {
+      const int nw = (sc[i] + 3) / 4;
+      if (nw > 15) return false;
+      words[c][i] = (uint8_t)nw;
+      wmax = std::max(wmax, nw);
+    }
+    out.width[c] = wmax;
+    out.pk[c].assign((size_t)4 * wmax * dim, 0);
+    for (uint32_t i = 0; i < dim; ++i) {
+      const uint32_t lane = i % G;
+      for (int k = 0; k < 4 * words[c][i]; ++k) {
+        uint16_t e;
+        if (k < sc[i]) {
+          const uint32_t v = sub[(size_t)k * dim + i];
+          const uint32_t tgt = v >> 8, tag = v & 255u;
+          if (tag == 2) e = zero_entry(tgt % G);  // bank padding keeps its bank group
+          else e = (uint16_t)(tgt | (tag ? 0x8000u : 0u));
+        } else {
+          e = zero_entry(lane);  // rounding to whole words: the lane's own bank group
+        }
+        out.pk[c][((size_t)(k / 4) * dim + i) * 4 + (k % 4)] = e;
+      }
+    }
+  }
+  out.cnt.assign(dim, 0);
+  for (uint32_t i = 0; i < dim; ++i) out.cnt[i] = (uint8_t)(words[0][i] | (words[1][i] << 4));
+  out.mag[0] = mags[0];
+  out.mag[1] = mags[1];
   return true;
 }
 

@@ -23,3 +23,31 @@ namespace qed {
 bool order_for_banks(std::vector<uint32_t> &ell, std::vector<uint8_t> &cnt, uint32_t dim, int &width, int zero_slot);
 
 }  // namespace qed
+
+namespace qed {
+
+// Packed hop table for the staged-row H.v kernels (k_hv_rows16, k_hv_cols16).
+// Every hop of a string is one 16-bit entry: target (bits 0-13) | sign
+// (bit 15); its value is (sign ? -1 : 1) * mag[class]. The hops of each
+// magnitude class form their own list, packed four entries per 8-byte word:
+// word (k, i) of class c at pk[c][(k * dim + i) * 4 .. + 4). Per group of eight
+// strings each class list is bank-ordered (order_for_banks) and padded to a
+// multiple of four entries; every string then carries its group's word counts
+// cnt[i] = words of class 0 | words of class 1 << 4. Padding entries point at
+// one of eight zero slots dim .. dim + 7 placed in the bank group the padded
+// lane needs, so they add 0 * 0.
+struct PackedHops {
+  std::vector<uint16_t> pk[2];  // per class: 4 * width[c] * dim entries
+  std::vector<uint8_t> cnt;     // per string: class-0 words | class-1 words << 4
+  double mag[2] = {0.0, 0.0};
+  int width[2] = {0, 0};        // words per string of each class table
+};
+
+// Packs an ELL table (entry k of string i at ell[k * dim + i] = target << 8 |
+// value slot, cnt[i] hops; vals: the value of each slot, zero_slot unused here).
+// Returns false when the table does not fit the format: dim + 8 > 2^14, more
+// than two distinct magnitudes, or more than 15 words of one class per string.
+bool pack_hops16(const std::vector<uint32_t> &ell, const std::vector<uint8_t> &cnt, uint32_t dim,
+                 const std::vector<double> &vals, int zero_slot, PackedHops &out);
+
+}  // namespace qed

@@ -323,6 +323,15 @@ int qed_last_error(char *buf, int len) {
   return (int)t_err.size();
 }
 
+int qed_hv_tuning_report(char *buf, int len) {
+  const std::string r = hv_tuning_report();
+  if (buf && len > 0) {
+    std::strncpy(buf, r.c_str(), (size_t)len - 1);
+    buf[len - 1] = 0;
+  }
+  return (int)r.size();
+}
+
 int qed_init(int device) {
   return guarded([&] {
     if (g_device_fixed && device != g_device) fail(QED_ERR_ARGUMENT, "qed_init: device already selected");
@@ -979,8 +988,7 @@ int qed_hamiltonian_apply_device(qed_hamiltonian *h, const double *x, double *y,
     cudaStream_t s = (cudaStream_t)stream;
     if (!h->H->D) return;
     SubList none;
-    launch_hv_rows(h->H->op, x, 1.0, y, none, s);
-    launch_hv_cols(h->H->op, x, 1.0, y, 0, w.red, s);
+    launch_hv(h->H->op, x, 1.0, y, none, 0, w.red, s);
   });
 }
 
@@ -1004,8 +1012,7 @@ int qed_hamiltonian_apply_dots_device(qed_hamiltonian *h, const double *x, doubl
     r.partials = h->partials.p;
     r.max_blocks = kHvColsMaxBlocks;
     SubList none;
-    launch_hv_rows(h->H->op, x, 1.0, y, none, s);
-    int nb = launch_hv_cols(h->H->op, x, 1.0, y, 7, r, s);
+    int nb = launch_hv(h->H->op, x, 1.0, y, none, 7, r, s);
     launch_finalize(r.partials, nb, 3, dots, s);
   });
 }

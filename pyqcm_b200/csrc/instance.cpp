@@ -254,8 +254,7 @@ std::vector<Instance::SusQ> Instance::susceptibility_qmatrices(const std::string
       std::vector<DevBuf<double>> b(1);
       b[0].alloc(H.D);
       SubList none;
-      launch_hv_rows(O.op, st->psi.p, 1.0, b[0].p, none, ws.stream);  // b = O psi
-      launch_hv_cols(O.op, st->psi.p, 1.0, b[0].p, 0, ws.red, ws.stream);
+      launch_hv(O.op, st->psi.p, 1.0, b[0].p, none, 0, ws.red, ws.stream);  // b = O psi
       SusQ q;
       q.st = st.get();
       int M = 0;
@@ -572,8 +571,7 @@ void Instance::finish_gs(Workspace &ws) {
       if (O.D == 0) continue;
       DevBuf<double> y(O.D);
       SubList none;
-      launch_hv_rows(O.op, st->psi.p, 1.0, y.p, none, ws.stream);
-      const int nb = launch_hv_cols(O.op, st->psi.p, 1.0, y.p, 3, ws.red, ws.stream);
+      const int nb = launch_hv(O.op, st->psi.p, 1.0, y.p, none, 3, ws.red, ws.stream);
       const double *r = ws.sums(nb, 2);
       ave += st->weight * r[0];
       var += st->weight * r[1];

@@ -4,10 +4,13 @@
 // row-major (index up + dim_up * dn), the factorized basis order of the
 // reference (src_ed/ED_basis.cpp:142-165). Up-spin hops act along rows,
 // down-spin hops along columns. All arithmetic is FP64.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cstdint>
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -510,6 +513,322 @@ __global__ void __launch_bounds__(kThreads) k_hv_cols2(HvOperator op, const doub
     }
   }
   if (red_mask) block_reduce_store<3>(red, partials, 3);
+}
+
+// ------------------------------------------- staged-row H.v (packed hops) ----
+//
+// Both spins' hops gather from shared memory. The row pass stages two dn-rows
+// of x (one double2 per up string) and applies the diagonal and the up hops;
+// the column pass stages two columns of x (one double2 per dn string, all dn
+// rows, brought in by TMA) and adds the down hops into y, which it reads and
+// writes by TMA in chunks of rows. Hop entries are the 16-bit packed, bank-
+// ordered tables of SpinTable::pk: target | sign << 14 | class << 15.
+
+// Set by a kernel whose bounded wait on a TMA transaction gave up; the host
+// reads it (check_device_waits) and reports the failure.
+__device__ int g_wait_timeout = 0;
+
+// One packed word (four hops of one magnitude class) gathered from the staged
+// pairs at shared byte address base `sb`: p += sum_q (+-1) * st[target_q]. The
+// target becomes a byte offset with one shift and one mask, the sign a +-1.0
+// operand of the FMA (its high word from one LOP3).
+__device__ __forceinline__ void hop_word(uint2 w, const char *sb, double2 &p) {
+  const uint32_t o[4] = {(w.x << 4) & 0x3FFF0u, (w.x >> 12) & 0x3FFF0u, (w.y << 4) & 0x3FFF0u,
+                         (w.y >> 12) & 0x3FFF0u};
+  const uint32_t sh[4] = {((w.x << 16) & 0x80000000u) | 0x3FF00000u, (w.x & 0x80000000u) | 0x3FF00000u,
+                          ((w.y << 16) & 0x80000000u) | 0x3FF00000u, (w.y & 0x80000000u) | 0x3FF00000u};
+  double2 t[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) t[q] = *reinterpret_cast<const double2 *>(sb + o[q]);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const double sg = __hiloint2double((int)sh[q], 0);
+    p.x = fma(sg, t[q].x, p.x);
+    p.y = fma(sg, t[q].y, p.y);
+  }
+}
+
+// Hop words of one string, loaded ahead of its gathers: up to A0 / A1 words of
+// each class in one batch of independent loads (the counts come one string
+// earlier), so that a string costs one L2 round trip. The accumulation order
+// does not depend on A0 / A1 (words alternate between two class-0 partial sums
+// by their index), so every variant gives the same bits.
+template <int A0, int A1> struct HopRow {
+  uint2 a[A0], b[A1];
+  uint32_t cw;
+};
+
+template <int A0, int A1>
+__device__ __forceinline__ void load_row(const SpinTable &t, uint32_t stride, uint32_t i, uint32_t cw,
+                                         HopRow<A0, A1> &h) {
+  const uint32_t n0 = cw & 15u, n1 = cw >> 4;
+  h.cw = cw;
+#pragma unroll
+  for (int k = 0; k < A0; ++k)
+    if (k < (int)n0) h.a[k] = __ldg(t.pk[0] + (size_t)k * stride + i);
+#pragma unroll
+  for (int k = 0; k < A1; ++k)
+    if (k < (int)n1) h.b[k] = __ldg(t.pk[1] + (size_t)k * stride + i);
+}
+
+// (a0, a1) += the hops of string i (both classes, magnitudes applied).
+template <int A0, int A1>
+__device__ __forceinline__ void apply_row(const HopRow<A0, A1> &h, const SpinTable &t, uint32_t stride, uint32_t i,
+                                          const char *sb, double &a0, double &a1) {
+  const int n0 = (int)(h.cw & 15u), n1 = (int)(h.cw >> 4);
+  double2 p0 = make_double2(0.0, 0.0), p1 = make_double2(0.0, 0.0), q = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int k = 0; k < A0; ++k)
+    if (k < n0) hop_word(h.a[k], sb, (k & 1) ? p1 : p0);
+  for (int k = A0; k < n0; ++k) {
+    const uint2 w = __ldg(t.pk[0] + (size_t)k * stride + i);
+    if (k & 1) hop_word(w, sb, p1);
+    else hop_word(w, sb, p0);
+  }
+#pragma unroll
+  for (int k = 0; k < A1; ++k)
+    if (k < n1) hop_word(h.b[k], sb, q);
+  for (int k = A1; k < n1; ++k) hop_word(__ldg(t.pk[1] + (size_t)k * stride + i), sb, q);
+  a0 = fma(t.mag[0], p0.x + p1.x, fma(t.mag[1], q.x, a0));
+  a1 = fma(t.mag[0], p0.y + p1.y, fma(t.mag[1], q.y, a1));
+}
+
+// Row pass: y = (diag + up hops) (xs x) - sub, two dn rows per CTA step (du even).
+// Each thread walks its strings with the next string's hop words and basis data
+// in flight while the current string gathers (and the counts one string further).
+// RMW: y holds xs * (dn hops) x already (k_hv_cols16w) and is read back (also
+// one string ahead); the reductions of the column pass (red_mask) are then
+// taken here on the final y.
+template <int THREADS, int A0, int A1, bool RMW>
+__global__ void __launch_bounds__(THREADS, 1) k_hv_rows16(HvOperator op, const double *__restrict__ x, double xs,
+                                                          double *y, SubList sub, int red_mask, double *partials) {
+  if (op.skip && *op.skip) return;
+  double red[3] = {0.0, 0.0, 0.0};
+  extern __shared__ __align__(128) double2 st2[];
+  const uint32_t du = op.up.dim, dd = op.dn.dim, hdu = du >> 1, T = THREADS;
+  const char *sb = reinterpret_cast<const char *>(st2);
+  if (threadIdx.x < 8) st2[du + threadIdx.x] = make_double2(0.0, 0.0);  // padding targets
+  for (uint32_t d0 = 2 * blockIdx.x; d0 < dd; d0 += 2 * gridDim.x) {
+    const bool two = d0 + 1 < dd;
+    const double2 *r0 = reinterpret_cast<const double2 *>(x + (size_t)d0 * du);
+    const double2 *r1 = reinterpret_cast<const double2 *>(x + (size_t)(d0 + (two ? 1 : 0)) * du);
+    const size_t row0 = (size_t)d0 * du;
+    HopRow<A0, A1> cur;
+    uint32_t ub = 0, cw1 = 0;
+    double dup = 0.0, yo0 = 0.0, yo1 = 0.0;
+    const uint32_t u0 = threadIdx.x;  // the first string's loads overlap the staging
+    if (u0 < du) {
+      load_row(op.up, du, u0, op.up.cntw[u0], cur);
+      ub = op.up.bits[u0];
+      dup = op.up.diag[u0];
+      if (RMW) {
+        yo0 = y[row0 + u0];
+        if (two) yo1 = y[row0 + du + u0];
+      }
+    }
+    if (u0 + T < du) cw1 = op.up.cntw[u0 + T];
+    __syncthreads();  // every thread is done with the previous pair
+    for (uint32_t q = threadIdx.x; q < hdu; q += T) {
+      const double2 a = r0[q];
+      const double2 b = two ? r1[q] : make_double2(0.0, 0.0);
+      st2[2 * q] = make_double2(a.x, b.x);
+      st2[2 * q + 1] = make_double2(a.y, b.y);
+    }
+    __syncthreads();
+    const uint32_t b0 = op.dn.bits[d0], b1 = two ? op.dn.bits[d0 + 1] : 0u;
+    const double e0 = op.dn.diag[d0], e1 = two ? op.dn.diag[d0 + 1] : 0.0;
+    for (uint32_t u = u0; u < du; u += T) {
+      const uint32_t un = u + T;
+      HopRow<A0, A1> nxt;
+      uint32_t ubn = 0, cw2 = 0;
+      double dupn = 0.0, yn0 = 0.0, yn1 = 0.0;
+      if (un < du) {
+        load_row(op.up, du, un, cw1, nxt);
+        ubn = op.up.bits[un];
+        dupn = op.up.diag[un];
+        if (RMW) {
+          yn0 = y[row0 + un];
+          if (two) yn1 = y[row0 + du + un];
+        }
+        if (un + T < du) cw2 = op.up.cntw[un + T];
+      }
+      const double2 xu = st2[u];
+      double a0 = (dup + e0 + inter_term(op.inter, ub, b0)) * xu.x;
+      double a1 = (dup + e1 + inter_term(op.inter, ub, b1)) * xu.y;
+      apply_row(cur, op.up, du, u, sb, a0, a1);
+      const size_t I0 = row0 + u;
+      a0 *= xs;
+      a1 *= xs;
+      for (int s = 0; s < sub.n; ++s) {
+        const double cs = sub.cdev ? sub.cdev[s] : sub.c[s];
+        a0 -= cs * sub.z[s][I0];
+        if (two) a1 -= cs * sub.z[s][I0 + du];
+      }
+      if (RMW) {
+        a0 += yo0;
+        a1 += yo1;
+        if (red_mask) {
+          red[0] += xs * (xu.x * a0 + (two ? xu.y * a1 : 0.0));
+          red[1] += a0 * a0 + (two ? a1 * a1 : 0.0);
+          red[2] += xs * xs * (xu.x * xu.x + xu.y * xu.y);
+        }
+      }
+      y[I0] = a0;
+      if (two) y[I0 + du] = a1;
+      cur = nxt;
+      ub = ubn;
+      dup = dupn;
+      cw1 = cw2;
+      yo0 = yn0;
+      yo1 = yn1;
+    }
+  }
+  if (RMW && red_mask) block_reduce_store<3>(red, partials, 3);
+}
+
+// ---- TMA and mbarrier helpers (1-CTA clusters; no multicast) ----
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the phase of parity `parity` of bar to complete; gives up after
+// about two seconds, records the timeout and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((it & 255u) == 0) {
+      const uint64_t t = global_ns();
+      if (it == 0) t0 = t;
+      else if (t - t0 > 2000000000ull) {
+        atomicExch(&g_wait_timeout, 1);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, int c0, int c1, const void *src) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
+               ::"l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(src))
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+constexpr int kSliceRows = 32;  // rows of one warp's TMA store
+constexpr int kTmaBoxRows = 256;
+
+// Column pass, write form: y = xs * (dn hops) x. Work item = one column pair
+// (u0, u0 + 1): its x values for all dn rows are TMA-loaded into shared memory
+// (box 2 x 256, zero-filled past dd, which also clears the padding targets
+// dd .. dd + 7, or they are cleared once below). Each warp then takes slices of
+// 32 rows, one row per lane, and sends each slice out with its own TMA store
+// (box 2 x 32) from its 512-byte staging slot; no CTA barrier inside a column
+// pair. The lanes load the hop words of their next row while gathering.
+template <int THREADS, int A0, int A1>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_hv_cols16w(const __grid_constant__ CUtensorMap tmx, const __grid_constant__ CUtensorMap tmy, HvOperator op,
+                 double xs) {
+  if (op.skip && *op.skip) return;
+  extern __shared__ __align__(1024) unsigned char sm_raw[];
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const uint32_t nbox = (dd + kTmaBoxRows - 1) / kTmaBoxRows;
+  const uint32_t nst = nbox * kTmaBoxRows + 8;
+  constexpr uint32_t nwarps = THREADS / 32;
+  double2 *st2 = reinterpret_cast<double2 *>(sm_raw);
+  double2 *ob = st2 + nst;  // one slot per thread: a warp's slots are its slice buffer
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(ob + THREADS);
+  double2 *buf = ob + warp * kSliceRows;
+  const char *sb = reinterpret_cast<const char *>(st2);
+  const uint32_t npairs = du >> 1;
+  const uint32_t nslice = (dd + kSliceRows - 1) / kSliceRows;
+  const uint32_t step = nwarps * kSliceRows;
+  if (threadIdx.x < 8) st2[nbox * kTmaBoxRows + threadIdx.x] = make_double2(0.0, 0.0);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  uint32_t px = 0;
+  for (uint32_t pp = blockIdx.x; pp < npairs; pp += gridDim.x) {
+    const int u0 = (int)(2 * pp);
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(&bar[0], nbox * kTmaBoxRows * 16);
+      for (uint32_t b = 0; b < nbox; ++b)
+        tma_load_2d(st2 + b * kTmaBoxRows, &tmx, u0, (int)(b * kTmaBoxRows), &bar[0]);
+    }
+    // the first row's hop words (the table does not depend on x) while x arrives
+    uint32_t d = warp * kSliceRows + lane;
+    HopRow<A0, A1> cur;
+    uint32_t cw1 = 0;
+    if (d < dd) load_row(op.dn, dd, d, op.dn.cntw[d], cur);
+    if (d + step < dd) cw1 = op.dn.cntw[d + step];
+    // every thread takes the same branch, also when the wait gave up
+    if (!__syncthreads_and(mbar_wait(&bar[0], px))) break;
+    px ^= 1u;
+    for (uint32_t sl = warp; sl < nslice; sl += nwarps, d += step) {
+      HopRow<A0, A1> nxt;
+      uint32_t cw2 = 0;
+      if (d + step < dd) {
+        load_row(op.dn, dd, d + step, cw1, nxt);
+        if (d + 2 * step < dd) cw2 = op.dn.cntw[d + 2 * step];
+      }
+      double a0 = 0.0, a1 = 0.0;
+      if (d < dd) apply_row(cur, op.dn, dd, d, sb, a0, a1);
+      if (lane == 0) bulk_wait_read_all();  // the warp's previous store has read the slot
+      __syncwarp();
+      buf[lane] = make_double2(xs * a0, xs * a1);
+      fence_proxy_async_smem();  // the lane's write is visible to the TMA store
+      __syncwarp();
+      if (lane == 0) {
+        tma_store_2d(&tmy, u0, (int)(sl * kSliceRows), buf);  // rows past dd are clipped
+        bulk_commit();
+      }
+      cur = nxt;
+      cw1 = cw2;
+    }
+    __syncthreads();  // every warp is done with st2 before the next pair's loads
+  }
+  if (lane == 0) bulk_wait_all();  // stores complete while the staging slots are still ours
 }
 
 // --------------------------------------------------------- vector kernels ----
@@ -1448,16 +1767,91 @@ int hv_variant() {
   return v;
 }
 
+namespace {
+
+constexpr size_t kSmemOptin = 227 * 1024;  // per-CTA dynamic shared memory limit (sm_100)
+constexpr size_t kStagedMaxThreads = 1024;  // the largest launch shape of the staged kernels
+
+bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+// Shared memory of k_hv_rows16 / k_hv_cols16 for this operator (0: not applicable).
+size_t rows16_smem(const HvOperator &op) {
+  const uint32_t du = op.up.dim;
+  if (!op.up.cntw || du % 2 || du < 512 || op.dn.dim < 2) return 0;
+  const size_t b = (size_t)(du + 8) * sizeof(double2);
+  return b <= kRowSmem2Max ? b : 0;
+}
+
+size_t cols16_smem(const HvOperator &op) {
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  if (!op.dn.cntw || du % 2 || du < 2 || dd < 512) return 0;
+  const size_t nst = (size_t)(dd + kTmaBoxRows - 1) / kTmaBoxRows * kTmaBoxRows + 8;
+  const size_t b = nst * sizeof(double2) + kStagedMaxThreads * sizeof(double2) + 2 * sizeof(uint64_t);
+  return b <= kSmemOptin - 1024 ? b : 0;
+}
+
+bool staged_disabled() { return (hv_variant() & 4) != 0; }
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    QED_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !p) fail(QED_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// TMA map of a dd x du row-major FP64 matrix with a box of 2 columns x box_rows
+// rows (16 bytes wide: du even keeps the row stride and every box start, at an
+// even column, on 16-byte boundaries); reads past the last row fill zeros.
+CUtensorMap column_pair_map(const double *base, uint32_t du, uint32_t dd, uint32_t box_rows) {
+  CUtensorMap m;
+  cuuint64_t dims[2] = {du, dd};
+  cuuint64_t strides[1] = {(cuuint64_t)du * sizeof(double)};
+  cuuint32_t box[2] = {2, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(base), dims,
+                                    strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(QED_ERR_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+  return m;
+}
+
+}  // namespace
+
 int hv_cols_grid(const HvOperator &op) {
   const uint32_t du = op.up.dim, dd = op.dn.dim;
   const uint32_t W = ((du % 2 == 0) ? 2 : 1) * kThreads;
   const size_t nitems = (size_t)((du + W - 1) / W) * ((dd + kColsR - 1) / kColsR);
-  return (int)std::max<size_t>(1, std::min<size_t>(nitems, (size_t)device_sms() * 8));
+  const int g = (int)std::max<size_t>(1, std::min<size_t>(nitems, (size_t)device_sms() * 8));
+  // the staged pass runs one CTA per column pair, at most one per SM
+  const int g16 = (int)std::max<size_t>(1, std::min<size_t>(du / 2, (size_t)device_sms()));
+  return std::max(g, g16);
+}
+
+void check_device_waits() {
+  int flag = 0;
+  QED_CUDA(cudaMemcpyFromSymbol(&flag, g_wait_timeout, sizeof(int)));
+  if (flag) fail(QED_ERR_CUDA, "a kernel's wait on its TMA transfers gave up after 2 s (results are invalid)");
 }
 
 void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,
                     const SubList &sub, cudaStream_t s) {
   const uint32_t du = op.up.dim, dd = op.dn.dim;
+  if (const size_t sm16 = staged_disabled() ? 0 : rows16_smem(op); sm16 && aligned16(x)) {
+    static const bool attr16 = [] {
+      QED_CUDA(cudaFuncSetAttribute(k_hv_rows16<512, 6, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kRowSmem2Max));
+      return true;
+    }();
+    (void)attr16;
+    const int grid = (int)std::min<size_t>((dd + 1) / 2, (size_t)device_sms());
+    k_hv_rows16<512, 6, 4, false><<<grid, 512, sm16, s>>>(op, x, xs, y, sub, 0, nullptr);
+    QED_LAUNCH();
+    return;
+  }
   const size_t smem = (size_t)du * sizeof(double);
   int threads = du >= 512 ? 512 : (du >= 256 ? 256 : 128);
   const size_t smem2 = 2 * smem;  // two rows interleaved
@@ -1508,6 +1902,140 @@ int launch_hv_cols(const HvOperator &op, const double *x, double xs, double *y, 
     k_hv_cols2<1, false><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
   QED_LAUNCH();
   return grid;
+}
+
+// ---- staged H.v launch shapes and their autotuner ----
+//
+// The staged kernels come in launch shapes (threads per CTA, hop words loaded
+// ahead per class) that give the same bits; which is fastest depends on the
+// sector. The first staged H.v of each (dim_up, dim_dn) runs every shape a few
+// times on the call's own vectors (y is fully rewritten by every run), times it
+// with CUDA events and keeps the fastest for that shape.
+namespace {
+
+using RowsFn = void (*)(HvOperator, const double *, double, double *, SubList, int, double *);
+using ColsFn = void (*)(CUtensorMap, CUtensorMap, HvOperator, double);
+
+struct StagedShape {
+  int threads;
+  RowsFn rows;
+  ColsFn cols;
+  const char *name;
+};
+
+const StagedShape kShapes[] = {
+    {512, k_hv_rows16<512, 6, 4, true>, k_hv_cols16w<512, 6, 4>, "512t/6+4"},
+    {768, k_hv_rows16<768, 4, 2, true>, k_hv_cols16w<768, 4, 2>, "768t/4+2"},
+    {1024, k_hv_rows16<1024, 2, 1, true>, k_hv_cols16w<1024, 2, 1>, "1024t/2+1"},
+    {384, k_hv_rows16<384, 8, 5, true>, k_hv_cols16w<384, 8, 5>, "384t/8+5"},
+};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+
+struct TuneRecord {
+  int choice = 0;
+  float ms[kNumShapes] = {};
+};
+std::mutex g_tune_mtx;
+std::map<std::pair<uint32_t, uint32_t>, TuneRecord> g_tune;
+
+void set_shape_attributes() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    for (const auto &v : kShapes) {
+      QED_CUDA(cudaFuncSetAttribute(v.rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRowSmem2Max));
+      QED_CUDA(cudaFuncSetAttribute(v.cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kSmemOptin - 1024)));
+    }
+  });
+}
+
+int launch_staged(int v, const HvOperator &op, const double *x, double xs, double *y, const SubList &sub,
+                  int red_mask, Reducer &r, size_t smr, size_t smc, cudaStream_t s) {
+  const StagedShape &sh = kShapes[v];
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const int gc = (int)std::min<size_t>(du / 2, (size_t)device_sms());
+  const CUtensorMap mx = column_pair_map(x, du, dd, kTmaBoxRows);
+  const CUtensorMap my = column_pair_map(y, du, dd, kSliceRows);
+  sh.cols<<<gc, sh.threads, smc, s>>>(mx, my, op, xs);
+  QED_LAUNCH();
+  int gr = (int)std::min<size_t>((dd + 1) / 2, (size_t)device_sms());
+  if (red_mask && gr > r.max_blocks) gr = r.max_blocks;
+  sh.rows<<<gr, sh.threads, smr, s>>>(op, x, xs, y, sub, red_mask, r.partials);
+  QED_LAUNCH();
+  return gr;
+}
+
+int staged_shape(const HvOperator &op, const double *x, double *y, Reducer &r, size_t smr, size_t smc,
+                 cudaStream_t s, bool may_tune) {
+  const std::pair<uint32_t, uint32_t> key{op.up.dim, op.dn.dim};
+  {
+    std::lock_guard<std::mutex> l(g_tune_mtx);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second.choice;
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  QED_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (!may_tune || cs != cudaStreamCaptureStatusNone) return 0;
+  TuneRecord rec;
+  cudaEvent_t e0, e1;
+  QED_CUDA(cudaEventCreate(&e0));
+  QED_CUDA(cudaEventCreate(&e1));
+  SubList none;
+  float best = 0.0f;
+  for (int v = 0; v < kNumShapes; ++v) {
+    launch_staged(v, op, x, 1.0, y, none, 0, r, smr, smc, s);  // warm-up
+    QED_CUDA(cudaEventRecord(e0, s));
+    for (int k = 0; k < 3; ++k) launch_staged(v, op, x, 1.0, y, none, 0, r, smr, smc, s);
+    QED_CUDA(cudaEventRecord(e1, s));
+    QED_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    QED_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    rec.ms[v] = ms / 3.0f;
+    if (v == 0 || rec.ms[v] < best) {
+      best = rec.ms[v];
+      rec.choice = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> l(g_tune_mtx);
+  return g_tune.emplace(key, rec).first->second.choice;
+}
+
+int launch_hv_impl(const HvOperator &op, const double *x, double xs, double *y, const SubList &sub, int red_mask,
+                   Reducer &r, cudaStream_t s, bool may_tune) {
+  const size_t smr = staged_disabled() ? 0 : rows16_smem(op);
+  const size_t smc = smr ? cols16_smem(op) : 0;
+  bool staged = smr && smc && aligned16(x) && aligned16(y);
+  for (int k = 0; k < sub.n && staged; ++k)
+    if (sub.z[k] == y) staged = false;  // the column pass would overwrite a term of the row pass
+  if (!staged) {
+    launch_hv_rows(op, x, xs, y, sub, s);
+    return launch_hv_cols(op, x, xs, y, red_mask, r, s);
+  }
+  set_shape_attributes();
+  const int v = staged_shape(op, x, y, r, smr, smc, s, may_tune);
+  return launch_staged(v, op, x, xs, y, sub, red_mask, r, smr, smc, s);
+}
+
+}  // namespace
+
+int launch_hv(const HvOperator &op, const double *x, double xs, double *y, const SubList &sub, int red_mask,
+              Reducer &r, cudaStream_t s) {
+  return launch_hv_impl(op, x, xs, y, sub, red_mask, r, s, true);
+}
+
+std::string hv_tuning_report() {
+  std::lock_guard<std::mutex> l(g_tune_mtx);
+  std::string out = "[";
+  for (const auto &kv : g_tune) {
+    if (out.size() > 1) out += ", ";
+    out += "{\"dim_up\": " + std::to_string(kv.first.first) + ", \"dim_dn\": " + std::to_string(kv.first.second) +
+           ", \"choice\": \"" + kShapes[kv.second.choice].name + "\", \"ms\": {";
+    for (int v = 0; v < kNumShapes; ++v)
+      out += std::string(v ? ", " : "") + "\"" + kShapes[v].name + "\": " + std::to_string(kv.second.ms[v]);
+    out += "}}";
+  }
+  return out + "]";
 }
 
 int launch_dots(size_t D, double *x, double xs, int write_x, const VecList &ys, Reducer &r,
@@ -1778,10 +2306,10 @@ void launch_hv_dots_noalloc(const HvOperator &op, const double *x, double *y, do
   r.partials = noalloc_partials_address();
   r.max_blocks = kHvColsMaxBlocks;
   SubList none;
-  launch_hv_rows(op, x, 1.0, y, none, s);
-  int nb = launch_hv_cols(op, x, 1.0, y, 7, r, s);
-  // Every block of this launch overwrites its own row, and the sum reads only
-  // those rows, so nothing has to be cleared between calls.
+  // no tuning here (it would create events): a shape tuned earlier, else the first
+  const int nb = launch_hv_impl(op, x, 1.0, y, none, 7, r, s, false);
+  // Every block of the reducing launch overwrites its own row, and the sum reads
+  // only those rows, so nothing has to be cleared between calls.
   launch_finalize(r.partials, nb, 3, dots, s);
 }
 

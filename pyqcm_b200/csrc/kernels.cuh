@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
 
 namespace qed {
 
@@ -24,6 +25,14 @@ struct SpinTable {
   const double *diag = nullptr;
   uint32_t dim = 0;
   int nvals = 0;
+  // Packed form of the same hops for the staged-row kernels (null when the
+  // table does not fit it; see PackedHops in bank_order.hpp): one list per
+  // magnitude class, four 16-bit entries (target | sign << 15) per word, word
+  // (k, i) of class c at pk[c][k * dim + i]; cntw[i] = class-0 words | class-1
+  // words << 4; the value of an entry is +-mag[c].
+  const uint2 *pk[2] = {nullptr, nullptr};
+  const uint8_t *cntw = nullptr;
+  double mag[2] = {0.0, 0.0};
 };
 
 // Inter-spin density-density terms sum_{r,s} v[r][s] dn_r up_s.
@@ -172,6 +181,17 @@ void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,
 int launch_hv_cols(const HvOperator &op, const double *x, double xs, double *y, int red_mask,
                     Reducer &r, cudaStream_t s);
 
+// Whole H.v with the column pass's reductions: y = xs H x - sum_k sub.c[k]
+// sub.z[k], reductions of the final y as launch_hv_cols; returns the block count
+// of the reducing launch. Takes the staged-row kernels when the tables are
+// packed (down pass first, writing y; then the row pass adding to it), else the
+// row pass and the column pass above.
+int launch_hv(const HvOperator &op, const double *x, double xs, double *y, const SubList &sub, int red_mask,
+              Reducer &r, cudaStream_t s);
+// JSON list of the staged H.v launch shapes chosen so far, with the timings
+// that chose them (one entry per (dim_up, dim_dn)).
+std::string hv_tuning_report();
+
 // ---- vector kernels -------------------------------------------------------
 struct VecList {
   int n = 0;
@@ -207,6 +227,9 @@ void finalize_sums(Reducer &r, int nblocks, int nred, cudaStream_t s);
 // Adds per-block partials (stride Reducer::kMaxRed) of `nred` slots into the
 // device array out[0..nred), on stream s; nothing is copied to the host.
 void launch_finalize(const double *partials, int nblocks, int nred, double *out, cudaStream_t s);
+// Raises Error(QED_ERR_CUDA) if a kernel's bounded wait on its TMA transfers has
+// given up since the library was loaded (the flag is sticky).
+void check_device_waits();
 // Number of per-block partial-sum rows a reducing H.v column pass can use.
 constexpr int kHvColsMaxBlocks = 8 * 148;
 

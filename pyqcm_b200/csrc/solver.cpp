@@ -54,7 +54,10 @@ const double *Workspace::sums(int nblocks, int nred) {
   return host;
 }
 
-void Workspace::sync() { QED_CUDA(cudaStreamSynchronize(stream)); }
+void Workspace::sync() {
+  QED_CUDA(cudaStreamSynchronize(stream));
+  check_device_waits();
+}
 
 double *Workspace::pinned(size_t n) {
   if (n > pin_n) {
@@ -73,6 +76,9 @@ double *Workspace::pinned(size_t n) {
 namespace {
 
 constexpr double kSmall = 1.0e-12;  // SMALL_VALUE (src_util/vector_num.hpp:23)
+// Spin tables of at least this many strings also get the packed copy that the
+// staged-row H.v kernels read (smaller sectors never take those kernels).
+constexpr uint64_t kPackMinDim = 512;
 
 void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
                 const std::vector<double> &vsame, Workspace &ws, bool bank_order) {
@@ -124,7 +130,8 @@ void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
     launch_build_hops(L, N, h.dim, h.bits.p, (int)pd.size(), dpd.p, dps.p, dsl.p, h.cnt.p, h.ell.p,
                       width, ws.stream);
     ws.sync();  // the pair arrays are freed on scope exit
-    if (bank_order && dim >= 64 && vals.size() < 256) {
+    const bool want_pack = dim >= kPackMinDim && dim + 8 <= (1u << 14);
+    if ((bank_order || want_pack) && dim >= 64 && vals.size() < 256) {
       std::vector<uint32_t> he((size_t)width * dim);
       std::vector<uint8_t> hc(dim);
       h.ell.download(he.data(), he.size(), ws.stream);
@@ -132,14 +139,29 @@ void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
       ws.sync();
       const int zero_slot = (int)vals.size();
       int w2 = width;
+      std::vector<double> vz(vals);
+      vz.push_back(0.0);
       if (order_for_banks(he, hc, (uint32_t)dim, w2, zero_slot)) {
-        vals.push_back(0.0);
-        h.nvals = (int)vals.size();
-        h.vals.upload(vals, ws.stream);
-        h.width = w2;
-        h.ell.alloc((size_t)w2 * dim);
-        h.ell.upload(he, ws.stream);
-        h.cnt.upload(hc, ws.stream);
+        // the staged-row kernels read the packed copy of the ordered table
+        PackedHops ph;
+        if (want_pack && pack_hops16(he, hc, (uint32_t)dim, vz, zero_slot, ph)) {
+          for (int c = 0; c < 2; ++c) {
+            if (ph.pk[c].empty()) ph.pk[c].assign(4, 0);  // a valid pointer for an empty class
+            h.pk[c].upload(ph.pk[c], ws.stream);
+          }
+          h.cntw.upload(ph.cnt, ws.stream);
+          h.mag[0] = ph.mag[0];
+          h.mag[1] = ph.mag[1];
+        }
+        if (bank_order) {  // the ELL itself is reordered for the up spin only
+          vals = vz;
+          h.nvals = (int)vals.size();
+          h.vals.upload(vals, ws.stream);
+          h.width = w2;
+          h.ell.alloc((size_t)w2 * dim);
+          h.ell.upload(he, ws.stream);
+          h.cnt.upload(hc, ws.stream);
+        }
         ws.sync();
       }
     }
@@ -167,6 +189,13 @@ SpinTable view(const HalfTables &h) {
   s.diag = h.diag.p;
   s.dim = h.dim;
   s.nvals = h.nvals;
+  if (h.cntw.n) {
+    for (int c = 0; c < 2; ++c) {
+      s.pk[c] = reinterpret_cast<const uint2 *>(h.pk[c].p);
+      s.mag[c] = h.mag[c];
+    }
+    s.cntw = h.cntw.p;
+  }
   return s;
 }
 
@@ -236,8 +265,7 @@ SectorOp::SectorOp(const SpinData &t, const Sector &s, Workspace &ws, HalfCache 
 void SectorOp::apply(const double *x, double *y, Workspace &ws) const {
   if (!D) return;
   SubList none;
-  launch_hv_rows(op, x, 1.0, y, none, ws.stream);
-  launch_hv_cols(op, x, 1.0, y, 0, ws.red, ws.stream);
+  launch_hv(op, x, 1.0, y, none, 0, ws.red, ws.stream);
 }
 
 // ------------------------------------------------------ Lanczos (ground state) --
@@ -474,8 +502,7 @@ LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed) {
     if (launched + chunk > cap) fail(QED_ERR_INTERNAL, "Lanczos history overflow");
     for (int k = 0; k < chunk; ++k) {
       sub.z[0] = pa;
-      launch_hv_rows(H.op, pb, 1.0, pc, sub, s);
-      int nb = launch_hv_cols(H.op, pb, 1.0, pc, 1, ws.red, s);
+      int nb = launch_hv(H.op, pb, 1.0, pc, sub, 1, ws.red, s);
       launch_finalize(ws.red.partials, nb, 1, ls.alpha_cur, s);      // alpha_j = <v_j, w>
       nb = launch_axpy_dev(D, pc, pb, ls.alpha_cur, ws.red, s);      // w -= alpha_j v_j
       launch_finalize(ws.red.partials, nb, 1, ls.b2_cur, s);          // |w|^2
@@ -542,8 +569,7 @@ void lanczos_eigenvector(const SectorOp &H, Workspace &ws, const LanczosResult &
       sub.c[1] = beta[j - 2];
       sub.z[1] = pa;
     }
-    launch_hv_rows(H.op, pb, 1.0, pc, sub, s);
-    launch_hv_cols(H.op, pb, 1.0, pc, 0, ws.red, s);
+    launch_hv(H.op, pb, 1.0, pc, sub, 0, ws.red, s);
     launch_scale(D, pc, 1.0 / beta[j - 1], s);
     launch_axpby(D, 1.0, psi.p, Z[j], pc, 0, ws.red, s);
     std::swap(pa, pb);
@@ -705,8 +731,7 @@ void lanczos_green(const SectorOp &H, Workspace &ws, double *psi, double *q,
     sub.n = 1;
     sub.c[0] = -1.0;
     sub.z[0] = q;
-    launch_hv_rows(H.op, psi, 1.0, q, sub, s);
-    int nb = launch_hv_cols(H.op, psi, 1.0, q, 1, ws.red, s);
+    int nb = launch_hv(H.op, psi, 1.0, q, sub, 1, ws.red, s);
     const double z = ws.sums(nb, 1)[0];
     a.push_back(z);
     nb = launch_axpby(D, 1.0, q, -z, psi, 1, ws.red, s);
@@ -1109,8 +1134,7 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
         SubList sub;
         sub.cdev = rec;
         for (int k = jj - pc; k < jj; ++k) sub.z[sub.n++] = pool.p(v[k]);
-        launch_hv_rows(op, vj, 1.0, w, sub, s);
-        nb = launch_hv_cols(op, vj, 1.0, w, 1, ws.red, s);
+        nb = launch_hv(op, vj, 1.0, w, sub, 1, ws.red, s);
         launch_finalize(ws.red.partials, nb, 1, rec + pc, s);  // (10): T(j, j) = <v_j, w>
         launch_axpy_dev(D, w, vj, rec + pc, ws.red, s, dflag.p);
       }
@@ -1204,8 +1228,7 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
       sub.c[sub.n] = T(k, j);
       sub.z[sub.n++] = pool.p(v[k]);
     }
-    launch_hv_rows(H.op, pool.p(v[j]), 1.0, w, sub, s);
-    nb = launch_hv_cols(H.op, pool.p(v[j]), 1.0, w, nd == 0 ? 1 : 0, ws.red, s);
+    nb = launch_hv(H.op, pool.p(v[j]), 1.0, w, sub, nd == 0 ? 1 : 0, ws.red, s);
     double wjj;
     if (nd == 0) {
       wjj = ws.sums(nb, 1)[0];

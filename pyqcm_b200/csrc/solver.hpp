@@ -45,6 +45,10 @@ struct HalfTables {
   DevBuf<uint32_t> ell;
   DevBuf<double> vals, diag;
   int nvals = 0, width = 0;
+  // packed, bank-ordered copy of the hops (empty when the table does not fit it)
+  DevBuf<uint16_t> pk[2];
+  DevBuf<uint8_t> cntw;
+  double mag[2] = {0.0, 0.0};
 };
 
 // Per-instance cache of the spin tables: a sector (N_up, N_dn) uses the up

@@ -1087,259 +1087,6 @@ __global__ void k_scale(size_t D, double *y, double a) {
 // of two, p <= P <= 16) threads serve one basis state, thread c its column c,
 // so every gather of the block H.v reads the p values of one state at once.
 
-__global__ void k_interleave(size_t D, int p, BlockSrc src, double *x) {
-  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < D * p; t += (size_t)gridDim.x * blockDim.x)
-    x[t] = src.v[t % p][t / p];
-}
-
-// Up-spin hops, diagonal and the X2 M2 term of a block H.v, rows pass: `parts`
-// CTAs share one dn-row (each a quarter of its up strings by default), so the
-// rows in flight (grid / parts: 74 on a B200 with two CTAs per SM) keep their
-// gather targets (du * p * 8 bytes each, 1.65 MB for the 4x4 sector at p = 16)
-// resident in L2; each hop gathers the p values of one state (one 128-byte line
-// for p = 16); one hop-table read serves p vectors; four hops are in flight per
-// thread. On the 4x4 Green function (p = 16): 8 parts x 1 CTA per SM 20.0-20.7 s,
-// 16 x 2 19.6 s, 4 x 2 18.6-19.2 s, 2 x 2 19.9 s, 4 x 3 19.9 s.
-constexpr int kRowParts = 4;
-constexpr int kUpCtasPerSm = 2;
-constexpr int kUpThreads = 1024;
-template <int P>
-__global__ void __launch_bounds__(kUpThreads, 2) k_block_up(HvOperator op, int p, const double *__restrict__ X,
-                                                    double *__restrict__ Y, const double *__restrict__ X2,
-                                                    const double *__restrict__ M2, double s2, int parts) {
-  __shared__ double uvals[256], m2[P * P];
-  for (int i = threadIdx.x; i < op.up.nvals; i += blockDim.x) uvals[i] = op.up.vals[i];
-  if (X2)
-    for (int i = threadIdx.x; i < p * p; i += blockDim.x) m2[i] = M2[i];
-  __syncthreads();
-  const uint32_t du = op.up.dim, dd = op.dn.dim;
-  const int c = threadIdx.x % P, g = threadIdx.x / P, G = blockDim.x / P;
-  if (c >= p) return;  // no barrier below
-  const int part = blockIdx.x % parts;
-  const uint32_t uchunk = (du + parts - 1) / parts;
-  const uint32_t ub = part * uchunk, ue = min(du, ub + uchunk);
-  for (uint32_t d = blockIdx.x / parts; d < dd; d += gridDim.x / parts) {
-    const size_t rowb = (size_t)d * du;
-    const double ddg = op.dn.diag[d];
-    const uint32_t dnb = op.dn.bits[d];
-    for (uint32_t u = ub + g; u < ue; u += G) {
-      const size_t I = rowb + u;
-      double acc = (op.up.diag[u] + ddg + inter_term(op.inter, op.up.bits[u], dnb)) * X[I * p + c];
-      const int cu = op.up.cnt[u];
-      // four hops in flight: table entries first, then the four gathers
-      double a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      int k = 0;
-      for (; k + 4 <= cu; k += 4) {
-        const uint32_t e0 = __ldg(op.up.ell + (size_t)k * du + u);
-        const uint32_t e1 = __ldg(op.up.ell + (size_t)(k + 1) * du + u);
-        const uint32_t e2 = __ldg(op.up.ell + (size_t)(k + 2) * du + u);
-        const uint32_t e3 = __ldg(op.up.ell + (size_t)(k + 3) * du + u);
-        const double x0 = X[(rowb + (e0 >> 8)) * p + c], x1 = X[(rowb + (e1 >> 8)) * p + c];
-        const double x2 = X[(rowb + (e2 >> 8)) * p + c], x3 = X[(rowb + (e3 >> 8)) * p + c];
-        acc += uvals[e0 & 255u] * x0;
-        a1 += uvals[e1 & 255u] * x1;
-        a2 += uvals[e2 & 255u] * x2;
-        a3 += uvals[e3 & 255u] * x3;
-      }
-      for (; k < cu; ++k) {
-        const uint32_t e = __ldg(op.up.ell + (size_t)k * du + u);
-        acc += uvals[e & 255u] * X[(rowb + (e >> 8)) * p + c];
-      }
-      acc += (a1 + a2) + a3;
-      if (X2) {
-        double t = 0.0;
-        for (int i = 0; i < p; ++i) t += X2[I * p + i] * m2[i * p + c];
-        acc += s2 * t;
-      }
-      Y[I * p + c] = acc;
-    }
-  }
-}
-
-// The same rows pass when one dn-row of X (du * p doubles) fits in shared
-// memory: a CTA stages its row with coalesced loads and gathers the hops from
-// shared memory. Thread t of the row handles entry (u, c) = (t / p, t % p), so
-// the p threads of a state share its table entries (one broadcast load).
-constexpr size_t kBlockRowSmemMax = 200 * 1024;
-__global__ void __launch_bounds__(1024) k_block_up_smem(HvOperator op, int p, const double *__restrict__ X,
-                                                        double *__restrict__ Y, const double *__restrict__ X2,
-                                                        const double *__restrict__ M2, double s2) {
-  extern __shared__ double xs[];  // [du * p]
-  __shared__ double uvals[256], m2[256];
-  for (int i = threadIdx.x; i < op.up.nvals; i += blockDim.x) uvals[i] = op.up.vals[i];
-  if (X2)
-    for (int i = threadIdx.x; i < p * p; i += blockDim.x) m2[i] = M2[i];
-  const uint32_t du = op.up.dim, dd = op.dn.dim;
-  const uint32_t n = du * (uint32_t)p;  // entries of one row (du * p * 8 bytes fit in shared memory)
-  for (uint32_t d = blockIdx.x; d < dd; d += gridDim.x) {
-    const size_t rowb = (size_t)d * du;
-    const double *xr = X + rowb * p;
-    __syncthreads();  // the previous row's gathers are done
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) xs[i] = xr[i];
-    __syncthreads();
-    const double ddg = op.dn.diag[d];
-    const uint32_t dnb = op.dn.bits[d];
-    for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
-      const uint32_t u = t / p, c = t - u * p;
-      double acc = (op.up.diag[u] + ddg + inter_term(op.inter, op.up.bits[u], dnb)) * xs[t];
-      const int cu = op.up.cnt[u];
-      double a1 = 0.0;
-      int k = 0;
-      for (; k + 2 <= cu; k += 2) {
-        const uint32_t e0 = __ldg(op.up.ell + (size_t)k * du + u);
-        const uint32_t e1 = __ldg(op.up.ell + (size_t)(k + 1) * du + u);
-        acc += uvals[e0 & 255u] * xs[(e0 >> 8) * p + c];
-        a1 += uvals[e1 & 255u] * xs[(e1 >> 8) * p + c];
-      }
-      if (k < cu) {
-        const uint32_t e = __ldg(op.up.ell + (size_t)k * du + u);
-        acc += uvals[e & 255u] * xs[(e >> 8) * p + c];
-      }
-      acc += a1;
-      if (X2) {
-        const double *x2 = X2 + (rowb + u) * p;
-        double s = 0.0;
-        for (int i = 0; i < p; ++i) s += x2[i] * m2[i * p + c];
-        acc += s2 * s;
-      }
-      Y[rowb * p + t] = acc;
-    }
-  }
-}
-
-// Down-spin hops of a block H.v, Y += (dn hops) X: work items (chunk of
-// kThreads / P up strings, dn-row d) in chunk-major order, so the chunk's
-// columns of X for all rows (dd * chunk * p * 8 bytes) stay in L2 while its
-// rows are processed; every hop reads one contiguous segment.
-template <int P>
-__global__ void __launch_bounds__(kThreads) k_block_dn(HvOperator op, int p, const double *__restrict__ X,
-                                                        double *__restrict__ Y) {
-  __shared__ double dvals[256];
-  __shared__ double hv[256];      // the row's hop values
-  __shared__ size_t hoff[256];    // and source-row offsets (e >> 8) * du
-  for (int i = threadIdx.x; i < op.dn.nvals; i += blockDim.x) dvals[i] = op.dn.vals[i];
-  const uint32_t du = op.up.dim, dd = op.dn.dim;
-  constexpr int C = kThreads / P;
-  const int c = threadIdx.x % P, g = threadIdx.x / P;
-  const uint32_t nch = (du + C - 1) / C;
-  const size_t items = (size_t)nch * dd;
-  for (size_t it = blockIdx.x; it < items; it += gridDim.x) {
-    const uint32_t ch = (uint32_t)(it / dd), d = (uint32_t)(it % dd);
-    const int cd = op.dn.cnt[d];
-    __syncthreads();  // dvals ready; previous item's hop list consumed
-    for (int k = threadIdx.x; k < cd; k += blockDim.x) {
-      const uint32_t e = __ldg(op.dn.ell + (size_t)k * dd + d);
-      hv[k] = dvals[e & 255u];
-      hoff[k] = (size_t)(e >> 8) * du;
-    }
-    __syncthreads();
-    const uint32_t u = ch * C + g;
-    if (u < du && c < p) {
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      int k = 0;
-      for (; k + 4 <= cd; k += 4) {
-        const double x0 = X[(hoff[k] + u) * p + c], x1 = X[(hoff[k + 1] + u) * p + c];
-        const double x2 = X[(hoff[k + 2] + u) * p + c], x3 = X[(hoff[k + 3] + u) * p + c];
-        a0 += hv[k] * x0;
-        a1 += hv[k + 1] * x1;
-        a2 += hv[k + 2] * x2;
-        a3 += hv[k + 3] * x3;
-      }
-      for (; k < cd; ++k) a0 += hv[k] * X[(hoff[k] + u) * p + c];
-      Y[((size_t)d * du + u) * p + c] += (a0 + a1) + (a2 + a3);
-    }
-  }
-}
-
-// Block partial sums of X^T Y: partials[b * ld + i * p + c] = sum over this
-// block's states of X[I][i] Y[I][c] (fixed order).
-template <int P>
-__device__ __forceinline__ void block_gram_store(const double (&acc)[P], int p, double *partials, int ld) {
-  __shared__ double sm[kThreads * (P + 1)];
-  constexpr int G = kThreads / P;
-  const int c = threadIdx.x % P, g = threadIdx.x / P;
-#pragma unroll
-  for (int i = 0; i < P; ++i) sm[(g * P + c) * (P + 1) + i] = acc[i];
-  __syncthreads();
-  for (int t = threadIdx.x; t < p * p; t += blockDim.x) {
-    const int i = t / p, cc = t % p;
-    double s = 0.0;
-    for (int gg = 0; gg < G; ++gg) s += sm[(gg * P + cc) * (P + 1) + i];
-    partials[(size_t)blockIdx.x * ld + t] = s;
-  }
-}
-
-template <int P>
-__global__ void __launch_bounds__(kThreads) k_block_gram(size_t D, int p, const double *__restrict__ X,
-                                                          const double *__restrict__ Y, double *partials, int ld) {
-  constexpr int G = kThreads / P;
-  const int c = threadIdx.x % P, g = threadIdx.x / P;
-  double acc[P];
-#pragma unroll
-  for (int i = 0; i < P; ++i) acc[i] = 0.0;
-  if (c < p)
-    for (size_t I = (size_t)blockIdx.x * G + g; I < D; I += (size_t)gridDim.x * G) {
-      const double y = Y[I * p + c];
-      if (p == P && P >= 2) {  // the state's row of X as 16-byte loads
-        const double2 *x2 = reinterpret_cast<const double2 *>(X + I * p);
-#pragma unroll
-        for (int i = 0; i < P / 2; ++i) {
-          const double2 v = x2[i];
-          acc[2 * i] += v.x * y;
-          acc[2 * i + 1] += v.y * y;
-        }
-      } else {
-#pragma unroll
-        for (int i = 0; i < P; ++i)
-          if (i < p) acc[i] += X[I * p + i] * y;
-      }
-    }
-  block_gram_store<P>(acc, p, partials, ld);
-}
-
-// Y = a Y + s1 X1 M1 (M1 p x p row-major, device; Y != X1); optionally the
-// block partials of Y^T Y of the result (gram != 0).
-template <int P>
-__global__ void __launch_bounds__(kThreads) k_block_muladd(size_t D, int p, double a, double *Y, double s1,
-                                                            const double *__restrict__ X1,
-                                                            const double *__restrict__ M1, int gram,
-                                                            double *partials, int ld) {
-  __shared__ double m1[P * P];
-  for (int i = threadIdx.x; i < p * p; i += blockDim.x) m1[i] = M1[i];
-  __syncthreads();
-  constexpr int G = kThreads / P;
-  const int c = threadIdx.x % P, g = threadIdx.x / P;
-  const unsigned gmask = (P == 32) ? 0xffffffffu : (((1u << P) - 1u) << ((threadIdx.x & 31) / P * P));
-  double acc[P];
-#pragma unroll
-  for (int i = 0; i < P; ++i) acc[i] = 0.0;
-  for (size_t I0 = (size_t)blockIdx.x * G; I0 < D; I0 += (size_t)gridDim.x * G) {
-    const size_t I = I0 + g;
-    double v = 0.0;
-    if (I < D && c < p) {
-      double t = 0.0;
-      if (p == P && P >= 2) {  // the state's row of X1 as 16-byte loads
-        const double2 *x2 = reinterpret_cast<const double2 *>(X1 + I * p);
-#pragma unroll
-        for (int i = 0; i < P / 2; ++i) {
-          const double2 xv = x2[i];
-          t += xv.x * m1[2 * i * p + c];
-          t += xv.y * m1[(2 * i + 1) * p + c];
-        }
-      } else {
-        for (int i = 0; i < p; ++i) t += X1[I * p + i] * m1[i * p + c];
-      }
-      v = (a != 0.0 ? a * Y[I * p + c] : 0.0) + s1 * t;
-      Y[I * p + c] = v;
-    }
-    if (gram) {  // the group's p results are in its lanes: acc[i] += v_i * v_c
-#pragma unroll
-      for (int i = 0; i < P; ++i) acc[i] += __shfl_sync(gmask, v, i, P) * v;
-    }
-  }
-  if (gram) block_gram_store<P>(acc, p, partials, ld);
-}
-
 // out[slot] = sum over blocks of partials[b * ld + slot], slot < n, fixed order.
 __global__ void k_finalize_ld(const double *partials, int nblocks, int ld, double *out) {
   __shared__ double sm[kThreads];
@@ -2099,86 +1846,7 @@ void launch_lanczos_jobs(const LanczosJob *jobs, int njobs, cudaStream_t s) {
 }
 
 namespace {
-int block_pow2(int p) {
-  int P = 1;
-  while (P < p) P <<= 1;
-  return P;
-}
-int block_grid(size_t D, int P, int max_blocks) {
-  const size_t G = kThreads / P;
-  size_t g = (D + G - 1) / G;
-  const size_t cap = (size_t)device_sms() * 8;
-  if (g > cap) g = cap;
-  if (g > (size_t)max_blocks) g = (size_t)max_blocks;
-  return (int)std::max<size_t>(g, 1);
-}
 }  // namespace
-
-void launch_interleave(size_t D, int p, const BlockSrc &src, double *x, cudaStream_t s) {
-  k_interleave<<<grid_for(D * p, device_sms(), 8), kThreads, 0, s>>>(D, p, src, x);
-  QED_LAUNCH();
-}
-
-#define QED_BLOCK_DISPATCH(P, CALL)                                       \
-  switch (P) {                                                            \
-    case 1: { constexpr int PP = 1; CALL; } break;                        \
-    case 2: { constexpr int PP = 2; CALL; } break;                        \
-    case 4: { constexpr int PP = 4; CALL; } break;                        \
-    case 8: { constexpr int PP = 8; CALL; } break;                        \
-    case 16: { constexpr int PP = 16; CALL; } break;                      \
-    default: fail(QED_ERR_UNSUPPORTED, "block of more than 16 vectors");  \
-  }
-
-void launch_block_hv(const HvOperator &op, int p, const double *X, double *Y, const double *X2, const double *M2,
-                     double s2, cudaStream_t s) {
-  const int P = block_pow2(p);
-  const int sms = device_sms();
-  const size_t row_bytes = (size_t)op.up.dim * p * sizeof(double);
-  if (row_bytes <= kBlockRowSmemMax && op.dn.dim > 0) {
-    static const bool attr = [] {
-      QED_CUDA(cudaFuncSetAttribute(k_block_up_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)kBlockRowSmemMax));
-      return true;
-    }();
-    (void)attr;
-    const uint32_t n = op.up.dim * (uint32_t)p;
-    const int threads = n >= 1024 ? 1024 : (int)((n + 31) / 32 * 32);
-    const int by_threads = std::max(1, 2048 / threads);
-    const int by_smem = std::max<int>(1, (int)((228 * 1024) / (row_bytes + 4 * 1024)));
-    const int grid = (int)std::min<size_t>(op.dn.dim, (size_t)sms * std::min(by_threads, by_smem));
-    k_block_up_smem<<<grid, threads, row_bytes, s>>>(op, p, X, Y, X2, M2, s2);
-  } else {
-    static const std::pair<int, int> cfg = [] {  // (CTAs per dn-row, CTAs per SM); QED_BLOCKUP="parts,mult"
-      int parts = kRowParts, mult = kUpCtasPerSm;
-      if (const char *e = getenv("QED_BLOCKUP")) sscanf(e, "%d,%d", &parts, &mult);
-      return std::make_pair(std::max(1, parts), std::max(1, mult));
-    }();
-    const int parts = cfg.first;
-    const int up_grid = std::max(parts, (sms * cfg.second / parts) * parts);
-    QED_BLOCK_DISPATCH(P, (k_block_up<PP><<<up_grid, kUpThreads, 0, s>>>(op, p, X, Y, X2, M2, s2, parts)));
-  }
-  QED_LAUNCH();
-  QED_BLOCK_DISPATCH(P, (k_block_dn<PP><<<sms * 8, kThreads, 0, s>>>(op, p, X, Y)));
-  QED_LAUNCH();
-}
-
-int launch_block_gram(size_t D, int p, const double *X, const double *Y, double *partials, int ld, int max_blocks,
-                      cudaStream_t s) {
-  const int P = block_pow2(p);
-  const int grid = block_grid(D, P, max_blocks);
-  QED_BLOCK_DISPATCH(P, (k_block_gram<PP><<<grid, kThreads, 0, s>>>(D, p, X, Y, partials, ld)));
-  QED_LAUNCH();
-  return grid;
-}
-
-int launch_block_muladd(size_t D, int p, double a, double *Y, double s1, const double *X1, const double *M1,
-                        int gram, double *partials, int ld, int max_blocks, cudaStream_t s) {
-  const int P = block_pow2(p);
-  const int grid = block_grid(D, P, max_blocks);
-  QED_BLOCK_DISPATCH(P, (k_block_muladd<PP><<<grid, kThreads, 0, s>>>(D, p, a, Y, s1, X1, M1, gram, partials, ld)));
-  QED_LAUNCH();
-  return grid;
-}
 
 void launch_finalize_ld(const double *partials, int nblocks, int ld, int n, double *out, cudaStream_t s) {
   k_finalize_ld<<<n, kThreads, 0, s>>>(partials, nblocks, ld, out);

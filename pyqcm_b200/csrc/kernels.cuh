@@ -134,24 +134,19 @@ struct LanczosJob {
 void launch_lanczos_start_jobs(const LanczosJob *jobs, int njobs, cudaStream_t s);
 void launch_lanczos_jobs(const LanczosJob *jobs, int njobs, cudaStream_t s);
 
-// ---- blocks of p vectors (interleaved: element (I, c) at I * p + c) --------
-// These serve the block form of the band-Lanczos recurrence, where one table
-// read of the H.v serves p right-hand sides.
-struct BlockSrc {
-  const double *v[32];
+// ---- blocks of p separate vectors (block.cu) ---------------------------------
+struct BlockIn {
+  const double *v[16] = {};
 };
-// x = the p vectors src.v[0..p) interleaved
-void launch_interleave(size_t D, int p, const BlockSrc &src, double *x, cudaStream_t s);
-// Y = H X + s2 X2 M2 (X2, M2 optional; M2 p x p row-major in device memory):
-// a row pass (diagonal, up hops, X2 term) and a chunk-major down-hop pass
-void launch_block_hv(const HvOperator &op, int p, const double *X, double *Y, const double *X2, const double *M2,
-                     double s2, cudaStream_t s);
-// per-block partials of X^T Y (p x p row-major) at partials[b * ld]; returns the block count
-int launch_block_gram(size_t D, int p, const double *X, const double *Y, double *partials, int ld, int max_blocks,
-                      cudaStream_t s);
-// Y = a Y + s1 X1 M1 (Y and X1 distinct); if gram, also the partials of Y^T Y
-int launch_block_muladd(size_t D, int p, double a, double *Y, double s1, const double *X1, const double *M1,
-                        int gram, double *partials, int ld, int max_blocks, cudaStream_t s);
+struct BlockOut {
+  double *v[16] = {};
+};
+// Y = a Y + s1 X1 M1 (M1 p x p row-major, device; skipped when X1.v[0] is null;
+// Y is not read when a == 0); gram 1: per-CTA partials of Y^T Y of the result,
+// gram 2: of L^T Y; partials[b * p * p + i * p + c]. Returns the CTA count.
+int launch_bl_update(size_t D, int p, double a, const BlockOut &Y, double s1, const BlockIn &X1, const double *M1,
+                     int gram, const BlockIn &L, double *partials, int max_blocks, cudaStream_t s);
+
 // out[0..n) = fixed-order sums of partials with row stride ld
 void launch_finalize_ld(const double *partials, int nblocks, int ld, int n, double *out, cudaStream_t s);
 // log |det(V(k) G(iw) - 1)| on the (w, k) grid, V(k) = V0 + sum_e v_e exp(2 pi i k.R_e)

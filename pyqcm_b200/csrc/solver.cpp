@@ -839,17 +839,30 @@ bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<
   auto upload = [&](double *dst, const std::vector<double> &h) {
     QED_CUDA(cudaMemcpyAsync(dst, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s));
   };
+  // Blocks are p separate vectors (column-major D x p buffers, or the start
+  // vectors themselves); their H.v is p single-vector H.v launches.
+  const BlockIn none;
+  auto block = [&](double *base) {
+    BlockOut o;
+    for (int c = 0; c < p; ++c) o.v[c] = base + (size_t)c * D;
+    return o;
+  };
+  auto in = [&](const BlockOut &o) {
+    BlockIn i;
+    for (int c = 0; c < p; ++c) i.v[c] = o.v[c];
+    return i;
+  };
   // Cholesky QR, twice: X (its gram already in hG) -> tmp -> out; B = R2 R1
-  auto cholqr2 = [&](const double *X, double *tmp, double *out, std::vector<double> &B) {
+  auto cholqr2 = [&](const BlockIn &X, const BlockOut &tmp, const BlockOut &out, std::vector<double> &B) {
     if (!cholesky_upper(p, hG.data(), R1, R1i)) return false;
     for (int i = 0; i < p; ++i)
       if (R1[i * p + i] < kPivotMin) return false;
     upload(dM, R1i);
-    int nb = launch_block_muladd(D, p, 0.0, tmp, 1.0, X, dM, 1, part.p, pp, max_blocks, s);
+    int nb = launch_bl_update(D, p, 0.0, tmp, 1.0, X, dM, 1, none, part.p, max_blocks, s);
     gram_to_host(nb);
     if (!cholesky_upper(p, hG.data(), R2, R2i)) return false;
     upload(dM, R2i);
-    launch_block_muladd(D, p, 0.0, out, 1.0, tmp, dM, 0, part.p, pp, max_blocks, s);
+    launch_bl_update(D, p, 0.0, out, 1.0, in(tmp), dM, 0, none, part.p, max_blocks, s);
     B.assign(pp, 0.0);
     for (int i = 0; i < p; ++i)
       for (int j = i; j < p; ++j) {
@@ -861,16 +874,15 @@ bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<
   };
   const size_t bl = D * (size_t)p;
   DevBuf<double> b0(bl), b1(bl), b2(bl);
-  double *Vprev = b0.p, *Vk = b1.p, *W = b2.p;
+  BlockOut Vprev = block(b0.p), Vk = block(b1.p), W = block(b2.p);
   // V_0 = QR(phi) and P = phi^T V_0
-  BlockSrc src;
-  for (int i = 0; i < p; ++i) src.v[i] = phi[i].p;
-  launch_interleave(D, p, src, W, s);  // W holds X0 = phi
+  BlockOut X0;
+  for (int i = 0; i < p; ++i) X0.v[i] = phi[i].p;
   std::vector<double> B;
-  int nb = launch_block_gram(D, p, W, W, part.p, pp, max_blocks, s);
+  int nb = launch_bl_update(D, p, 1.0, X0, 0.0, none, nullptr, 1, none, part.p, max_blocks, s);  // phi^T phi
   gram_to_host(nb);
-  if (!cholqr2(W, Vprev, Vk, B)) return false;
-  nb = launch_block_gram(D, p, W, Vk, part.p, pp, max_blocks, s);  // P(k, i) = <phi_k, v_i>
+  if (!cholqr2(in(X0), Vprev, Vk, B)) return false;
+  nb = launch_bl_update(D, p, 1.0, Vk, 0.0, none, nullptr, 2, in(X0), part.p, max_blocks, s);  // P(k, i) = <phi_k, v_i>
   gram_to_host(nb);
   const std::vector<double> P(hG);  // row-major [k][i]
   std::vector<double> t((size_t)M0 * M0, 0.0);
@@ -897,29 +909,31 @@ bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<
       cudaEventDestroy(e[1]);
     }
   } ev_guard{ev};
+  SubList nosub;
   auto enqueue = [&](int k) {
-    // W = H V_k - V_{k-1} B_k^T
-    if (k > 0)
-      launch_block_hv(H.op, p, Vk, W, Vprev, dBt, -1.0, s);
-    else
-      launch_block_hv(H.op, p, Vk, W, nullptr, nullptr, 0.0, s);
-    // A_k = V_k^T W ; W -= V_k A_k (with the gram of the result for the QR)
+    // W = H V_k - V_{k-1} B_k^T, then A_k = V_k^T W
+    for (int c = 0; c < p; ++c) launch_hv(H.op, Vk.v[c], 1.0, W.v[c], nosub, 0, ws.red, s);
     double *rk = drec.p + (size_t)ldr * k;
-    int nbk = launch_block_gram(D, p, Vk, W, part.p, pp, max_blocks, s);
+    int nbk;
+    if (k > 0)
+      nbk = launch_bl_update(D, p, 1.0, W, -1.0, in(Vprev), dBt, 2, in(Vk), part.p, max_blocks, s);
+    else
+      nbk = launch_bl_update(D, p, 1.0, W, 0.0, none, nullptr, 2, in(Vk), part.p, max_blocks, s);
     launch_finalize_ld(part.p, nbk, pp, pp, rk, s);
-    nbk = launch_block_muladd(D, p, 1.0, W, -1.0, Vk, rk, 1, part.p, pp, max_blocks, s);
+    // W -= V_k A_k (with the gram of the result for the QR)
+    nbk = launch_bl_update(D, p, 1.0, W, -1.0, in(Vk), rk, 1, none, part.p, max_blocks, s);
     if ((k + 1) * p < M0) {
       // W = V_{k+1} B_{k+1}, Cholesky QR twice, through V_{k-1}'s buffer
       launch_finalize_ld(part.p, nbk, pp, pp, dG, s);
       launch_block_chol(p, dG, kPivotMin, dR1, dR1i, nullptr, nullptr, nullptr, rk + 2 * pp, s);
-      nbk = launch_block_muladd(D, p, 0.0, Vprev, 1.0, W, dR1i, 1, part.p, pp, max_blocks, s);
+      nbk = launch_bl_update(D, p, 0.0, Vprev, 1.0, in(W), dR1i, 1, none, part.p, max_blocks, s);
       launch_finalize_ld(part.p, nbk, pp, pp, dG, s);
       launch_block_chol(p, dG, 0.0, dR2, dR2i, dR1, rk + pp, dBt, rk + 2 * pp, s);
-      launch_block_muladd(D, p, 0.0, W, 1.0, Vprev, dR2i, 0, part.p, pp, max_blocks, s);
+      launch_bl_update(D, p, 0.0, W, 1.0, in(Vprev), dR2i, 0, none, part.p, max_blocks, s);
     }
     QED_CUDA(cudaMemcpyAsync(hrec + (size_t)ldr * (k & 1), rk, ldr * sizeof(double), cudaMemcpyDeviceToHost, s));
     QED_CUDA(cudaEventRecord(ev[k & 1], s));
-    double *nv = W;  // V_{k+1}
+    const BlockOut nv = W;  // V_{k+1}
     W = Vprev;
     Vprev = Vk;
     Vk = nv;

@@ -9,6 +9,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -831,6 +832,63 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (lane == 0) bulk_wait_all();  // stores complete while the staging slots are still ours
 }
 
+// ---- block H.v on separate vectors (sectors without packed tables) ----
+//
+// A block of p <= 16 vectors (pointer arrays) through the ELL tables: one
+// thread per state applies every hop to all p vectors, so each table entry is
+// read once per state for the whole block. Row pass: Y_c = (diag + up hops) X_c;
+// column pass: Y_c += (dn hops) X_c. Small sectors are launch-bound, where one
+// launch per pass for the whole block is what counts.
+template <int P>
+__global__ void __launch_bounds__(kThreads) k_blhv_rows(HvOperator op, int p, BlockIn X, BlockOut Y) {
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const size_t D = (size_t)du * dd;
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t u = (uint32_t)(I % du), d = (uint32_t)(I / du);
+    const double dg = op.up.diag[u] + op.dn.diag[d] + inter_term(op.inter, op.up.bits[u], op.dn.bits[d]);
+    const size_t row = (size_t)d * du;
+    double acc[P];
+#pragma unroll
+    for (int c = 0; c < P; ++c) acc[c] = c < p ? dg * X.v[c][I] : 0.0;
+    const int cu = op.up.cnt[u];
+    for (int k = 0; k < cu; ++k) {
+      const uint32_t e = __ldg(op.up.ell + (size_t)k * du + u);
+      const double v = op.up.vals[e & 255u];
+      const size_t J = row + (e >> 8);
+#pragma unroll
+      for (int c = 0; c < P; ++c)
+        if (c < p) acc[c] += v * X.v[c][J];
+    }
+#pragma unroll
+    for (int c = 0; c < P; ++c)
+      if (c < p) Y.v[c][I] = acc[c];
+  }
+}
+
+template <int P>
+__global__ void __launch_bounds__(kThreads) k_blhv_cols(HvOperator op, int p, BlockIn X, BlockOut Y) {
+  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const size_t D = (size_t)du * dd;
+  for (size_t I = blockIdx.x * (size_t)blockDim.x + threadIdx.x; I < D; I += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t u = (uint32_t)(I % du), d = (uint32_t)(I / du);
+    double acc[P];
+#pragma unroll
+    for (int c = 0; c < P; ++c) acc[c] = 0.0;
+    const int cd = op.dn.cnt[d];
+    for (int k = 0; k < cd; ++k) {
+      const uint32_t e = __ldg(op.dn.ell + (size_t)k * dd + d);
+      const double v = op.dn.vals[e & 255u];
+      const size_t J = (size_t)(e >> 8) * du + u;
+#pragma unroll
+      for (int c = 0; c < P; ++c)
+        if (c < p) acc[c] += v * X.v[c][J];
+    }
+#pragma unroll
+    for (int c = 0; c < P; ++c)
+      if (c < p) Y.v[c][I] += acc[c];
+  }
+}
+
 // --------------------------------------------------------- vector kernels ----
 
 template <int G>
@@ -1578,9 +1636,15 @@ int hv_cols_grid(const HvOperator &op) {
   return std::max(g, g16);
 }
 
-void check_device_waits() {
-  int flag = 0;
-  QED_CUDA(cudaMemcpyFromSymbol(&flag, g_wait_timeout, sizeof(int)));
+std::atomic<bool> g_staged_used{false};  // set by the first staged H.v launch
+
+bool staged_kernels_used() { return g_staged_used.load(std::memory_order_relaxed); }
+
+void read_wait_flag_async(int *host_flag, cudaStream_t s) {
+  QED_CUDA(cudaMemcpyFromSymbolAsync(host_flag, g_wait_timeout, sizeof(int), 0, cudaMemcpyDeviceToHost, s));
+}
+
+void check_wait_flag(int flag) {
   if (flag) fail(QED_ERR_CUDA, "a kernel's wait on its TMA transfers gave up after 2 s (results are invalid)");
 }
 
@@ -1760,6 +1824,7 @@ int launch_hv_impl(const HvOperator &op, const double *x, double xs, double *y, 
     return launch_hv_cols(op, x, xs, y, red_mask, r, s);
   }
   set_shape_attributes();
+  g_staged_used.store(true, std::memory_order_relaxed);
   const int v = staged_shape(op, x, y, r, smr, smc, s, may_tune);
   return launch_staged(v, op, x, xs, y, sub, red_mask, r, smr, smc, s);
 }
@@ -1783,6 +1848,34 @@ std::string hv_tuning_report() {
     out += "}}";
   }
   return out + "]";
+}
+
+void launch_block_hv(const HvOperator &op, int p, const BlockIn &X, const BlockOut &Y, Reducer &r, cudaStream_t s) {
+  if (p < 1 || p > 16) fail(QED_ERR_ARGUMENT, "block H.v: block size outside [1, 16]");
+  const size_t D = (size_t)op.up.dim * op.dn.dim;
+  if (!D) return;
+  bool staged = !staged_disabled() && rows16_smem(op) && cols16_smem(op);
+  for (int c = 0; c < p && staged; ++c) staged = aligned16(X.v[c]) && aligned16(Y.v[c]);
+  if (staged) {  // large sectors: the staged single-vector kernels, one vector at a time
+    SubList none;
+    for (int c = 0; c < p; ++c) launch_hv(op, X.v[c], 1.0, Y.v[c], none, 0, r, s);
+    return;
+  }
+  const int grid = grid_for(D, device_sms(), 8);
+  if (p <= 4) {
+    k_blhv_rows<4><<<grid, kThreads, 0, s>>>(op, p, X, Y);
+    QED_LAUNCH();
+    k_blhv_cols<4><<<grid, kThreads, 0, s>>>(op, p, X, Y);
+  } else if (p <= 8) {
+    k_blhv_rows<8><<<grid, kThreads, 0, s>>>(op, p, X, Y);
+    QED_LAUNCH();
+    k_blhv_cols<8><<<grid, kThreads, 0, s>>>(op, p, X, Y);
+  } else {
+    k_blhv_rows<16><<<grid, kThreads, 0, s>>>(op, p, X, Y);
+    QED_LAUNCH();
+    k_blhv_cols<16><<<grid, kThreads, 0, s>>>(op, p, X, Y);
+  }
+  QED_LAUNCH();
 }
 
 int launch_dots(size_t D, double *x, double xs, int write_x, const VecList &ys, Reducer &r,

@@ -146,6 +146,10 @@ struct BlockOut {
 // gram 2: of L^T Y; partials[b * p * p + i * p + c]. Returns the CTA count.
 int launch_bl_update(size_t D, int p, double a, const BlockOut &Y, double s1, const BlockIn &X1, const double *M1,
                      int gram, const BlockIn &L, double *partials, int max_blocks, cudaStream_t s);
+// Y_c = H X_c for the p vectors of a block: the staged single-vector H.v per
+// vector when the sector has packed tables, else one row and one column launch
+// for the whole block (ELL tables, every entry read once per state for all p).
+void launch_block_hv(const HvOperator &op, int p, const BlockIn &X, const BlockOut &Y, Reducer &r, cudaStream_t s);
 
 // out[0..n) = fixed-order sums of partials with row stride ld
 void launch_finalize_ld(const double *partials, int nblocks, int ld, int n, double *out, cudaStream_t s);
@@ -222,9 +226,13 @@ void finalize_sums(Reducer &r, int nblocks, int nred, cudaStream_t s);
 // Adds per-block partials (stride Reducer::kMaxRed) of `nred` slots into the
 // device array out[0..nred), on stream s; nothing is copied to the host.
 void launch_finalize(const double *partials, int nblocks, int nred, double *out, cudaStream_t s);
-// Raises Error(QED_ERR_CUDA) if a kernel's bounded wait on its TMA transfers has
-// given up since the library was loaded (the flag is sticky).
-void check_device_waits();
+// The staged H.v kernels' bounded waits on their TMA transfers set a sticky
+// device flag when they give up. staged_kernels_used(): any staged launch so
+// far; read_wait_flag_async enqueues a copy of the flag to (pinned) host
+// memory on s; check_wait_flag raises Error(QED_ERR_CUDA) if it was set.
+bool staged_kernels_used();
+void read_wait_flag_async(int *host_flag, cudaStream_t s);
+void check_wait_flag(int flag);
 // Number of per-block partial-sum rows a reducing H.v column pass can use.
 constexpr int kHvColsMaxBlocks = 8 * 148;
 

@@ -31,6 +31,8 @@ Workspace::Workspace() {
   partials.alloc((size_t)red.max_blocks * Reducer::kMaxRed);
   out.alloc(Reducer::kMaxRed);
   QED_CUDA(cudaMallocHost(&host, Reducer::kMaxRed * sizeof(double)));
+  QED_CUDA(cudaMallocHost(&wait_flag, sizeof(int)));
+  *wait_flag = 0;
   red.partials = partials.p;
   red.out = out.p;
   red.host = host;
@@ -44,6 +46,7 @@ Workspace::~Workspace() {
   if (stream) cudaStreamSynchronize(stream);
   if (host) cudaFreeHost(host);
   if (pin) cudaFreeHost(pin);
+  if (wait_flag) cudaFreeHost(wait_flag);
   if (tls_stream == stream) tls_stream = nullptr;
   if (stream) cudaStreamDestroy(stream);
 }
@@ -55,8 +58,11 @@ const double *Workspace::sums(int nblocks, int nred) {
 }
 
 void Workspace::sync() {
+  // the wait flag of the staged kernels rides along with the stream's work
+  const bool check = staged_kernels_used();
+  if (check) read_wait_flag_async(wait_flag, stream);
   QED_CUDA(cudaStreamSynchronize(stream));
-  check_device_waits();
+  if (check) check_wait_flag(*wait_flag);
 }
 
 double *Workspace::pinned(size_t n) {
@@ -909,10 +915,9 @@ bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<
       cudaEventDestroy(e[1]);
     }
   } ev_guard{ev};
-  SubList nosub;
   auto enqueue = [&](int k) {
     // W = H V_k - V_{k-1} B_k^T, then A_k = V_k^T W
-    for (int c = 0; c < p; ++c) launch_hv(H.op, Vk.v[c], 1.0, W.v[c], nosub, 0, ws.red, s);
+    launch_block_hv(H.op, p, in(Vk), W, ws.red, s);
     double *rk = drec.p + (size_t)ldr * k;
     int nbk;
     if (k > 0)

@@ -25,6 +25,7 @@ struct Workspace {
   DevBuf<double> partials, out;
   double *host = nullptr;
   double *pin = nullptr;  // pinned host staging, grown on demand
+  int *wait_flag = nullptr;  // pinned copy of the staged kernels' wait-timeout flag
   size_t pin_n = 0;
   Workspace();
   ~Workspace();

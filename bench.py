@@ -162,6 +162,43 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+class UtilSampler:
+    """Mean GPU utilization (nvidia-smi utilization.gpu, the fraction of time a
+    kernel was running) sampled every 100 ms while a step runs."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=utilization.gpu", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "100"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        vals = []
+        with open(self.file.name) as f:
+            for line in f:
+                try:
+                    vals.append(float(line.strip()))
+                except ValueError:
+                    pass
+        os.unlink(self.file.name)
+        return {"mean_pct": statistics.mean(vals), "samples": len(vals)} if vals else None
+
+
 def cpu_baseline_sample():
     """The reference's mult_add on the same sector, one application, one core."""
     from oracle import ref
@@ -199,6 +236,7 @@ def run_reference(args, world, rank):
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if world == 1 and not args.no_secondary:
         line["secondary"] = secondary_lines("reference")
+        line.update(secondary_summary(line["secondary"]))
     print(json.dumps(line), flush=True)
 
 
@@ -326,6 +364,7 @@ def run_ours(args, world, rank, local):
         line["solve"] = solve
     if world == 1 and not args.no_secondary:
         line["secondary"] = secondary_lines("ours")
+        line.update(secondary_summary(line["secondary"]))
     print(json.dumps(line), flush=True)
 
 
@@ -405,10 +444,16 @@ def batch_line(workload, batch, threads, steps, warmup, impl, world=1, rank=0, l
             qed.erase_model_instance(l)
         return dt, G
 
-    for w in range(max(0, min(warmup, 1))):
-        one_step(200000 + 10000 * w)
+    if warmup > 0:  # the code paths and allocations of every geometry, on a smaller batch
+        full = probs
+        probs = full[:min(len(full), 64)]
+        one_step(200000)
+        probs = full
     steps = max(1, min(steps, 3))
+    busy = UtilSampler(local)
+    busy.start()
     times = [one_step(300000 + 10000 * k)[0] for k in range(steps)]
+    gpu_busy = busy.stop()
     dt = sum(times) / steps
     dt = max_over_ranks([dt], world, device=f"cuda:{local}")[0]
     if rank != 0:
@@ -418,13 +463,14 @@ def batch_line(workload, batch, threads, steps, warmup, impl, world=1, rank=0, l
             "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": wl, "instances_per_step": batch,
                                             "host_threads": threads or os.cpu_count()},
+            "gpu_busy": gpu_busy,
             "e2e": {"value": batch / dt, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 16 * batch,
                     "path": "qed_ground_state_solve_batch + qed_Green_function_solve_batch + G(z) read back"}}
 
 
-SECONDARY = (("batch", 64), ("baths", 16))
-VCA_SECONDARY_POINTS = 1024
+SECONDARY = (("batch", 1024), ("baths", 256))  # the stated sizes: 1024 random clusters, 256 bath points
+VCA_SECONDARY_POINTS = 4096
 
 
 def secondary_lines(impl):
@@ -432,11 +478,29 @@ def secondary_lines(impl):
     beside the H.v line of the default run."""
     out = []
     for wl, n in SECONDARY:
-        line = batch_line(wl, n, 0, 2, 1, impl)
+        line = batch_line(wl, n, 0, 1, 1, impl)
         if line:
             out.append(line)
     if impl == "ours":
         out.append(vca_line(VCA_SECONDARY_POINTS, 400, 0))
+    return out
+
+
+def secondary_summary(lines):
+    """Headline figures of the batched and VCA lines, as top-level keys."""
+    out = {}
+    for ln in lines:
+        wl = ln.get("config", {}).get("workload", "")
+        if ln.get("metric") == "ED solves/s":
+            key = "batched_random_clusters" if wl == BATCH_WORKLOADS["batch"] else "batched_bath_points"
+            out[key] = {"solves_per_s": ln["value"], "instances": ln["config"].get("instances_per_step"),
+                        "gpu_busy_pct": (ln.get("gpu_busy") or {}).get("mean_pct"),
+                        "cpu_pool": ln.get("cpu_baseline")}
+        elif ln.get("metric", "").startswith("VCA"):
+            out["vca"] = {k: ln.get(k) for k in ("value", "ed_only_seconds", "speedup", "surrogate_total_seconds",
+                                                  "speedup_including_training", "breakeven_searches",
+                                                  "max_omega_abs_diff", "max_grad_norm")}
+            out["vca"]["training_points"] = ln["config"]["training_points"]
     return out
 
 
@@ -496,18 +560,19 @@ def vca_line(n_points, epochs, threads, Us=(5.0, 7.0, 9.0), local=0):
     losses = sur.fit(X, y, epochs=epochs, batch=256, lr=1e-3, seed=0)
     t_train = time.perf_counter() - t0
     acc = [2e-5, 2e-5]
+    cert = 1e-6  # both searches end on |grad Omega| < 1e-6 from a 1e-4 central stencil
     runs = []
     for U in Us:
         f_ed = lambda P, U=U: ev(np.c_[np.full(len(P), U), P])
         n0 = ev.n_evals
         t0 = time.perf_counter()
-        x_ed, _, _, _, it_ed = vca.newton_raphson(f_ed, [0.2, 0.0], [0.02, 0.02], acc)
+        x_ed, _, g_ed, _, it_ed = vca.newton_raphson(f_ed, [0.2, 0.0], [0.02, 0.02], acc, certify=cert)
         t_ed = time.perf_counter() - t0
         n_ed = ev.n_evals - n0
         n0 = ev.n_evals
         t0 = time.perf_counter()
         x0 = sur.propose(U, [0.2, 0.0], [0.02, 0.02])
-        x_s, _, _, _, it_s = vca.newton_raphson(f_ed, x0, [0.005, 0.005], acc)
+        x_s, _, g_s, _, it_s = vca.newton_raphson(f_ed, x0, [0.005, 0.005], acc, certify=cert)
         t_s = time.perf_counter() - t0
         n_s = ev.n_evals - n0
         x_poly = sur.propose(U, [0.2, 0.0], [0.02, 0.02], use_net=False)
@@ -515,6 +580,8 @@ def vca_line(n_points, epochs, threads, Us=(5.0, 7.0, 9.0), local=0):
         runs.append({"U": U, "ed_only_s": t_ed, "surrogate_s": t_s, "ed_only_iterations": it_ed,
                      "surrogate_iterations": it_s, "ed_only_omega_evals": n_ed, "surrogate_omega_evals": n_s,
                      "x_ed_only": [float(v) for v in x_ed], "x_surrogate": [float(v) for v in x_s],
+                     "grad_norm_ed_only": float(np.linalg.norm(g_ed)),
+                     "grad_norm_surrogate": float(np.linalg.norm(g_s)),
                      "x_proposed": [float(v) for v in x0],
                      "x_proposed_polynomial_only": [float(v) for v in x_poly], "omega": float(om[0]),
                      "omega_abs_diff": float(abs(om[0] - om[1]))})
@@ -523,13 +590,23 @@ def vca_line(n_points, epochs, threads, Us=(5.0, 7.0, 9.0), local=0):
     om_here = float(ev(np.array([VCA_REF_POINT]))[0])
     t_ref, om_ref = vca_reference_sample()
     n_ed = sum(r["ed_only_omega_evals"] for r in runs)
+    # what the surrogate costs in full, and after how many searches it pays for itself
+    t_fixed = t_data + t_train
+    gain = (t_ed - t_sur) / len(Us)
+    breakeven = (t_fixed / gain) if gain > 0 else None
     return {"metric": "VCA wall time, surrogate-guided (same stationary point as ED-only within 1e-8)",
             "value": t_sur, "unit": "s", "n_gpus": 1, "steps": len(Us), "warmup": 0,
             "ms_per_step": 1e3 * t_sur / len(Us), "higher_is_better": False, "scaling": "replicas",
             "vs_baseline": None, "dtype": "f64 (ED, Omega); bf16 x bf16 -> f32 (surrogate)",
             "data": "synthetic", "config": {"workload": VCA_WORKLOAD, "U": list(Us),
-                                            "training_points": n_points, "epochs": epochs},
+                                            "training_points": n_points, "epochs": epochs,
+                                            "stop": "certified |grad Omega| < 1e-6 (central stencil, step 1e-4)"},
             "ed_only_seconds": t_ed, "speedup": t_ed / t_sur if t_sur > 0 else None,
+            "surrogate_total_seconds": t_fixed + t_sur,
+            "surrogate_total_what": "training data (ED Omega at every training point) + training + the searches",
+            "speedup_including_training": t_ed / (t_fixed + t_sur),
+            "breakeven_searches": breakeven,
+            "max_grad_norm": max(max(r["grad_norm_ed_only"], r["grad_norm_surrogate"]) for r in runs),
             "cpu_baseline": {"value": t_ref * n_ed, "unit": "s", "cores": 1, "kind": "reference",
                              "sample": f"one Potthoff-functional evaluation by the reference's compiled lattice "
                                        f"layer at (U, M', dmu) = {VCA_REF_POINT} took {t_ref:.2f} s on one host "

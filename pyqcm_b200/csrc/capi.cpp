@@ -451,7 +451,7 @@ int qed_mixing(int label, int *mixing) {
 int qed_ground_state_solve(int label, double *energy, char *sectors, int len) {
   return guarded([&] {
     auto I = instance(label);
-    I->require_trivial_group();
+    I->require_supported_group();
     std::lock_guard<std::mutex> li(I->mtx);
     auto r = I->low_energy_states(ws());
     *energy = r.first;
@@ -491,7 +491,7 @@ int qed_Green_function_solve_batch(const int *labels, int n, int threads) {
 int qed_Green_function_solve(int label) {
   return guarded([&] {
     auto I = instance(label);
-    I->require_trivial_group();
+    I->require_supported_group();
     std::lock_guard<std::mutex> li(I->mtx);
     I->green_solve(ws());
   });

@@ -445,15 +445,33 @@ void Instance::one_body_solve(Workspace &ws) {
 size_t Instance::sector_dim(const Sector &s) const {
   const int L = model->n_orb, nu = s.Nup(), nd = s.Ndw();
   if (nu < 0 || nu > L || nd < 0 || nd > L) return 0;
-  return (size_t)binom(L, nu) * (size_t)binom(L, nd);
+  const size_t d = (size_t)binom(L, nu) * (size_t)binom(L, nd);
+  return has_group() ? d / (size_t)model->group->g() + 1 : d;  // a point group: about d / g per irrep
 }
 
 // Eigenvalue pass of one sector: Hamiltonian_Dense::states
 // (src_ed/Hamiltonian/Hamiltonian_Dense.hpp:110-125) below max_dim_full in the
 // non-factorized formats, the Lanczos eigenvalue pass otherwise.
 void Instance::solve_sector(const Sector &s, SectorSolve &out, Workspace &ws, DeferredSectors *defer) {
-  require_trivial_group();
+  require_supported_group();
   out.sec = s;
+  if (has_group()) {  // the symmetry-adapted basis: dense below max_dim_full, else Lanczos on the CSR product
+    try {
+      auto H = mixed_sector(s, ws);
+      out.dim = H->D;
+      if (H->D == 0) return;
+      if ((long)H->D < opt_int("max_dim_full")) {
+        out.dense = true;
+        std::vector<double> A = H->dense(ws.stream);
+        if (!sym_eig((int)H->D, A, out.w, &out.U)) fail(QED_ERR_INTERNAL, "dense eigensolver did not converge");
+      } else {
+        out.lanczos = lanczos_energy_mixed(*H, ws, (uint64_t)opt_int("seed"));
+      }
+    } catch (const Error &e) {
+      fail(e.code, std::string(e.what()) + where(s));
+    }
+    return;
+  }
   try {
     auto Hp = std::make_unique<SectorOp>(terms, s, ws, &tables);
     SectorOp &H = *Hp;
@@ -544,8 +562,13 @@ void Instance::state_vector(State &st, Workspace &ws) {
       st.hpsi = std::vector<double>();
       return;
     }
-    SectorOp H(terms, st.sec, ws, &tables);
-    lanczos_eigenvector(H, ws, st.lanczos, (uint64_t)opt_int("seed"), st.psi);
+    if (has_group()) {
+      auto H = mixed_sector(st.sec, ws);
+      lanczos_eigenvector_mixed(*H, ws, st.lanczos, (uint64_t)opt_int("seed"), st.psi);
+    } else {
+      SectorOp H(terms, st.sec, ws, &tables);
+      lanczos_eigenvector(H, ws, st.lanczos, (uint64_t)opt_int("seed"), st.psi);
+    }
   } catch (const Error &e) {
     fail(e.code, std::string(e.what()) + where(st.sec));
   }
@@ -567,10 +590,21 @@ void Instance::finish_gs(Workspace &ws) {
     const SpinData t = collect_terms(*model, {{v.first, 1.0}});
     double ave = 0.0, var = 0.0;
     for (auto &st : states) {
+      SubList none;
+      if (has_group()) {  // the operator in the state's symmetry-adapted basis
+        MixedHamiltonian O(*model->group, mixed_terms(*model, {{v.first, 1.0}}), st->sec.irrep, st->sec.Nup(),
+                           st->sec.Ndw(), ws.stream);
+        if (O.D == 0) continue;
+        DevBuf<double> y(O.D);
+        const int nb = O.apply_full(st->psi.p, 1.0, y.p, none, 3, ws.red, ws.stream);
+        const double *r = ws.sums(nb, 2);
+        ave += st->weight * r[0];
+        var += st->weight * r[1];
+        continue;
+      }
       SectorOp O(t, st->sec, ws, &op_tables[v.first]);
       if (O.D == 0) continue;
       DevBuf<double> y(O.D);
-      SubList none;
       const int nb = launch_hv(O.op, st->psi.p, 1.0, y.p, none, 3, ws.red, ws.stream);
       const double *r = ws.sums(nb, 2);
       ave += st->weight * r[0];
@@ -588,18 +622,26 @@ void Instance::finish_gs(Workspace &ws) {
 }
 
 // low_energy_states (src_ed/model_instance.hpp:245-347)
-void Instance::require_trivial_group() const {
-  if (model->group && model->group->g() > 1)
-    fail(QED_ERR_UNSUPPORTED, "model " + model->name + " has point-group generators (g = " +
-                                  std::to_string(model->group->g()) +
-                                  "): its sectors have the symmetry-adapted Hamiltonian "
-                                  "(qed_mixed_hamiltonian_*), but ground states and Green functions "
-                                  "are solved only in the spin-factorized basis (g = 1)");
+void Instance::require_supported_group() const {
+  if (!has_group()) return;
+  if (model->group->has_complex_irrep)
+    fail(QED_ERR_UNSUPPORTED, "model " + model->name +
+                                  ": point group with complex characters (a generator of order above 2) needs "
+                                  "a complex Hilbert space, which this solver does not provide");
+  if (use_cf)
+    fail(QED_ERR_UNSUPPORTED, "model " + model->name +
+                                  ": continued-fraction Green functions (GF_method 'F') of models with a point "
+                                  "group are not in this solver; use the Lehmann form ('L')");
+}
+
+std::unique_ptr<MixedHamiltonian> Instance::mixed_sector(const Sector &s, Workspace &ws) const {
+  return std::make_unique<MixedHamiltonian>(*model->group, mixed_terms(*model, value), s.irrep, s.Nup(), s.Ndw(),
+                                            ws.stream);
 }
 
 std::pair<double, std::string> Instance::low_energy_states(Workspace &ws) {
   if (gs_solved) return {GS_energy, gs_string()};
-  require_trivial_group();
+  require_supported_group();
   if (!is_correlated) {
     one_body_solve(ws);
     return {GS_energy, gs_string()};
@@ -699,6 +741,10 @@ static void streamline(std::vector<double> &e, std::vector<double> &V, int L) {
 // band Lanczos (or the full eigensystem of a small non-factorized sector),
 // energy shift and sign, streamline.
 void Instance::qmatrix_part(State &st, bool spin_down, int s, QPart &out, Workspace &ws) {
+  if (has_group()) {
+    qmatrix_part_mixed(st, spin_down, s, out, ws);
+    return;
+  }
   const int p = model->n_sites;
   const int pm = 2 * s - 1;
   const int spin = spin_down ? 1 : 0;
@@ -755,6 +801,10 @@ void Instance::qmatrix_part(State &st, bool spin_down, int s, QPart &out, Worksp
 // The rest of build_qmatrix (src_ed/model_instance.hpp:711-817): append the two
 // halves, check_norm, times sqrt(weight), upload for G(z).
 void Instance::qmatrix_combine(State &st, bool spin_down, QPart (&parts)[2], Workspace &ws) {
+  if (has_group()) {
+    qmatrix_combine_mixed(st, spin_down, parts, ws);
+    return;
+  }
   const int p = model->n_sites;
   QMat &q = st.q[spin_down ? 1 : 0];
   q.L = p;
@@ -777,6 +827,142 @@ void Instance::qmatrix_combine(State &st, bool spin_down, QPart (&parts)[2], Wor
   }
   if (ztot > opt_double("accur_Q_matrix"))
     fail(QED_ERR_QMATRIX, "Q-matrix does not satisfy unitary condition by " + std::to_string(ztot));
+  const double sw = std::sqrt(st.weight);
+  for (auto &x : q.V) x *= sw;
+  q.de.upload(q.e, ws.stream);
+  q.dV.upload(q.V, ws.stream);
+  ws.sync();
+}
+
+// build_qmatrix for a model with a point group (src_ed/model_instance.hpp:711-817):
+// for each irrep r of the symmetric orbitals, the target sector (irrep
+// r0 x r for electrons, r0 x conj(r) for holes, shift_sector
+// src_ed/symmetry_group.cpp:540-558), the start vectors c^{pm} of the n_r
+// orbitals of r on the state (mixed_cdag), band Lanczos on the target's
+// symmetry-adapted Hamiltonian (or its full eigensystem below max_dim_full),
+// energy shift and sign, streamline in the irrep's orbital basis.
+void Instance::qmatrix_part_mixed(State &st, bool spin_down, int s, QPart &out, Workspace &ws) {
+  const SymmetryGroup &G = *model->group;
+  const int pm = 2 * s - 1;
+  const int spin = spin_down ? 1 : 0;
+  const int ns = model->n_sites;
+  out.e.clear();
+  out.V.clear();
+  out.segs.clear();
+  std::unique_ptr<MixedHamiltonian> Hs;  // the state's own sector, for its basis map
+  int off = 0;
+  for (int r = 0; r < G.g(); ++r) {
+    const int nr = G.site_irrep_dim[r];
+    const int r_off = off;
+    off += nr;
+    if (nr == 0) continue;
+    Sector tsec = shift_sector(st.sec, pm, spin);
+    const int conj_r = sym_conjugate(G, r);
+    tsec.irrep = sym_tensor(G, st.sec.irrep, pm == 1 ? r : conj_r);
+    if (!sector_is_valid(tsec, model->n_orb, G.g())) continue;
+    auto Ht = mixed_sector(tsec, ws);
+    if (Ht->D == 0) continue;
+    if (!Hs) Hs = mixed_sector(st.sec, ws);
+    std::vector<DevBuf<double>> phi;
+    phi.reserve(nr);
+    {
+      PhaseScope ps_cdag(kPhCdag);
+      std::vector<double> coef(ns);
+      for (int i = 0; i < nr; ++i) {
+        for (int a = 0; a < ns; ++a) coef[a] = G.S[(size_t)(r_off + i) * ns + a].real();
+        phi.emplace_back(Ht->D);
+        mixed_cdag(*Hs, *Ht, pm, spin, ns, coef.data(), st.psi.p, phi.back().p, ws.stream);
+      }
+      ws.sync();
+    }
+    std::vector<double> ev, Q;
+    int M = 0;
+    bool ok;
+    if ((long)Ht->D < opt_int("max_dim_full")) {
+      // Hamiltonian_Dense::build_Q_matrix: all D poles, Q(k, i) = <phi_i, u_k>
+      std::vector<double> A = Ht->dense(ws.stream), U, ph(Ht->D);
+      if (!sym_eig((int)Ht->D, A, ev, &U)) fail(QED_ERR_INTERNAL, "dense eigensolver did not converge");
+      M = (int)Ht->D;
+      Q.assign((size_t)M * nr, 0.0);
+      for (int i = 0; i < nr; ++i) {
+        phi[i].download(ph.data(), Ht->D, ws.stream);
+        ws.sync();
+        for (int k = 0; k < M; ++k) {
+          const double *uk = U.data() + (size_t)k * Ht->D;
+          double acc = 0.0;
+          for (size_t j = 0; j < Ht->D; ++j) acc += ph[j] * uk[j];
+          Q[(size_t)k * nr + i] = acc;
+        }
+      }
+      ok = true;
+    } else {
+      ok = band_lanczos_qmatrix(KrylovOp(*Ht), ws, phi, ev, Q, M);
+    }
+    if (!ok || M == 0) continue;
+    QPart::Seg seg;
+    seg.r = r;
+    seg.e = std::move(ev);
+    seg.V = std::move(Q);
+    for (auto &x : seg.e) x -= st.energy;
+    if (pm == -1)
+      for (auto &x : seg.e) x = -x;
+    streamline(seg.e, seg.V, nr);
+    out.segs.push_back(std::move(seg));
+  }
+}
+
+// The rest of build_qmatrix with a point group: per irrep, hole then electron
+// poles, check_norm in the irrep's orbital basis, then the consolidated
+// Q-matrix in the site basis (Q_matrix_set::consolidated_qmatrix,
+// src_ed/Q_matrix_set.hpp:144-163, to_site_basis src_ed/symmetry_group.cpp:487-505:
+// site a gets sum over the irrep's orbitals alpha of S(alpha, a) V(alpha)),
+// irreps in order, times sqrt(weight).
+void Instance::qmatrix_combine_mixed(State &st, bool spin_down, QPart (&parts)[2], Workspace &ws) {
+  const SymmetryGroup &G = *model->group;
+  const int ns = model->n_sites;
+  QMat &q = st.q[spin_down ? 1 : 0];
+  q.L = ns;
+  q.e.clear();
+  q.V.clear();
+  int off = 0;
+  for (int r = 0; r < G.g(); ++r) {
+    const int nr = G.site_irrep_dim[r];
+    const int r_off = off;
+    off += nr;
+    if (nr == 0) continue;
+    std::vector<double> e, V;
+    for (int s = 0; s < 2; ++s)
+      for (const auto &sg : parts[s].segs)
+        if (sg.r == r) {
+          e.insert(e.end(), sg.e.begin(), sg.e.end());
+          V.insert(V.end(), sg.V.begin(), sg.V.end());
+        }
+    const int M = (int)e.size();
+    // check_norm (src_ed/Q_matrix.hpp:236-260) of the irrep's block
+    double ztot = 0.0;
+    for (int i = 0; i < nr; ++i) {
+      double z = 0.0;
+      for (int k = 0; k < M; ++k) z += V[(size_t)k * nr + i] * V[(size_t)k * nr + i];
+      ztot += (z - 1.0) * (z - 1.0);
+      for (int j = 0; j < i; ++j) {
+        double zz = 0.0;
+        for (int k = 0; k < M; ++k) zz += V[(size_t)k * nr + i] * V[(size_t)k * nr + j];
+        ztot += 2.0 * zz * zz;
+      }
+    }
+    if (ztot > opt_double("accur_Q_matrix"))
+      fail(QED_ERR_QMATRIX, "Q-matrix does not satisfy unitary condition by " + std::to_string(ztot) +
+                                " (irrep " + std::to_string(r) + ")" + where(st.sec));
+    for (int k = 0; k < M; ++k) {
+      q.e.push_back(e[k]);
+      for (int a = 0; a < ns; ++a) {
+        double y = 0.0;
+        for (int al = 0; al < nr; ++al) y += V[(size_t)k * nr + al] * G.S[(size_t)(r_off + al) * ns + a].real();
+        q.V.push_back(y);
+      }
+    }
+  }
+  q.M = (int)q.e.size();
   const double sw = std::sqrt(st.weight);
   for (auto &x : q.V) x *= sw;
   q.de.upload(q.e, ws.stream);

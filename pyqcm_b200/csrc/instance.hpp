@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "model.hpp"
+#include "mixed.hpp"
 #include "solver.hpp"
 
 namespace qed {
@@ -67,6 +68,13 @@ struct DeferredSectors {
 // Hole (s = 0) or electron (s = 1) part of the Q-matrix of one state and spin.
 struct QPart {
   std::vector<double> e, V;
+  // models with a point group: one segment per irrep of the symmetric orbitals,
+  // V in that irrep's orbital basis (n_r rows), in irrep order
+  struct Seg {
+    int r = 0;
+    std::vector<double> e, V;
+  };
+  std::vector<Seg> segs;
 };
 
 struct Instance {
@@ -98,8 +106,10 @@ struct Instance {
   Instance(int label, std::shared_ptr<Model> m, std::map<std::string, double> value,
            const std::string &sectors);
 
-  // fails (unsupported) for a model with point-group generators
-  void require_trivial_group() const;
+  // fails (unsupported) for what the symmetry-adapted path does not cover:
+  // complex characters, continued-fraction Green functions, susceptibilities
+  void require_supported_group() const;
+  bool has_group() const { return model->group && model->group->g() > 1; }
   std::pair<double, std::string> low_energy_states(Workspace &ws);
   void green_solve(Workspace &ws);
 
@@ -159,6 +169,10 @@ struct Instance {
   // fills phi = c^{pm}_{orb, spin} |psi> on the target sector of H
   void apply_cdag(const State &st, int pm, int spin, int orb, const SectorOp &H, double *y,
                   double coef, bool accumulate, Workspace &ws);
+  // the symmetry-adapted Hamiltonian of a sector (models with a point group)
+  std::unique_ptr<MixedHamiltonian> mixed_sector(const Sector &s, Workspace &ws) const;
+  void qmatrix_part_mixed(State &st, bool spin_down, int s, QPart &out, Workspace &ws);
+  void qmatrix_combine_mixed(State &st, bool spin_down, QPart (&parts)[2], Workspace &ws);
 };
 
 bool sector_is_valid(const Sector &s, int n_orb, int g = 1);

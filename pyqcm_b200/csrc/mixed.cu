@@ -250,6 +250,134 @@ __global__ void __launch_bounds__(256) k_mixed_lanczos_w(const uint64_t *__restr
   }
 }
 
+// y = xs H x - sum_k c_k z_k with the reductions of the factorized column pass
+// (block partials at partials[block * Reducer::kMaxRed + i]); rows as in
+// k_mixed_spmv. *skip != 0: the whole call does nothing.
+__global__ void __launch_bounds__(256) k_mixed_full(const uint64_t *__restrict__ row_ptr,
+                                                    const uint32_t *__restrict__ col,
+                                                    const double *__restrict__ val, const double *__restrict__ dg,
+                                                    const double *__restrict__ x, double xs, double *y, uint64_t D,
+                                                    SubList sub, int red_mask, double *partials, const int *skip) {
+  if (skip && *skip) return;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t n_warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 7;
+  const int group = (threadIdx.x & 31) >> 3;
+  double red[3] = {0.0, 0.0, 0.0};
+  for (uint64_t J0 = warp * 4; J0 < D; J0 += n_warps * 4) {
+    const uint64_t J = J0 + group;
+    double s = 0.0;
+    if (J < D) {
+      const uint64_t a = row_ptr[J], e = row_ptr[J + 1];
+      for (uint64_t k = a + lane; k < e; k += 8) s += val[k] * __ldg(x + col[k]);
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 4);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    if (J < D && lane == 0) {
+      const double xj = x[J];
+      double yj = xs * (dg[J] * xj + s);
+      for (int k = 0; k < sub.n; ++k) yj -= (sub.cdev ? sub.cdev[k] : sub.c[k]) * sub.z[k][J];
+      y[J] = yj;
+      red[0] += xs * xj * yj;
+      red[1] += yj * yj;
+      red[2] += xs * xs * xj * xj;
+    }
+  }
+  if (!red_mask) return;
+  __shared__ double sm[3][8];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    double v = red[i];
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sm[i][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sm[threadIdx.x][k];
+    partials[(size_t)blockIdx.x * Reducer::kMaxRed + threadIdx.x] = t;
+  }
+}
+
+struct OrbCoef {
+  double c[kMaxSymOrb];
+};
+
+// basis index of state b in a sector: through the colex ranks of its two words
+__device__ __forceinline__ int32_t mixed_index(const int32_t *fmap, uint32_t du, uint64_t b) {
+  return fmap[(uint64_t)colex_rank((uint32_t)b) + (uint64_t)du * colex_rank((uint32_t)(b >> 32))];
+}
+
+// phi[J] = (c+ psi)[J]: the target state J carries the created particle; each
+// occupied orbital a of the orbital's support, emptied, gives a source state
+// whose representative (in the source irrep) holds the amplitude.
+__global__ void k_mixed_create(SymGroup G, int r_src, int r_tgt, int spin, int n_sites, OrbCoef cf,
+                               const uint64_t *__restrict__ tstates, const uint8_t *__restrict__ tlen, uint64_t Dt,
+                               const int32_t *__restrict__ sfmap, uint32_t sdu, const uint8_t *__restrict__ slen,
+                               const double *__restrict__ psi, double *__restrict__ phi) {
+  const int N = G.N;
+  for (uint64_t J = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; J < Dt; J += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t b = tstates[J];
+    const double lj = (double)tlen[J];
+    double acc = 0.0;
+    for (int a = 0; a < n_sites; ++a) {
+      if (cf.c[a] == 0.0) continue;
+      const uint64_t m = orb_mask(a + spin * N, N);
+      if (!(b & m)) continue;
+      const RepMap rm = sym_representative(G, b ^ m, r_src);
+      if (rm.length == 0) continue;
+      const int32_t I = mixed_index(sfmap, sdu, rm.rep);
+      if (I < 0) continue;
+      int ph = rm.phase + ((__popcll(b & (m - 1)) & 1) ? G.g : 0);
+      ph %= 2 * G.g;
+      acc += (ph == 0 ? 1.0 : -1.0) * cf.c[a] * sqrt(lj / (double)rm.length) * psi[I];
+    }
+    phi[J] = acc;
+  }
+}
+
+// phi[J] = (c psi)[J]: every source state b' whose orbital a, emptied, lands in
+// J's orbit is b' = h(J) + a for a group element h (each distinct image h(J)
+// once) and an orbital a that h(J) leaves empty; b' contributes when it is its
+// own representative in the source irrep.
+__global__ void k_mixed_destroy(SymGroup G, int r_src, int r_tgt, int spin, int n_sites, OrbCoef cf,
+                                const uint64_t *__restrict__ tstates, uint64_t Dt, const int32_t *__restrict__ sfmap,
+                                uint32_t sdu, const uint8_t *__restrict__ slen, const double *__restrict__ psi,
+                                double *__restrict__ phi) {
+  const int N = G.N;
+  for (uint64_t J = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; J < Dt; J += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t bj = tstates[J];
+    uint64_t seen[kMaxGroup];
+    int nseen = 0;
+    double acc = 0.0;
+    for (int h = 0; h < G.g; ++h) {
+      int q;
+      const uint64_t sh = sym_apply(G, h, 0, bj, q);
+      bool dup = false;
+      for (int k = 0; k < nseen; ++k) dup |= seen[k] == sh;
+      if (dup) continue;
+      seen[nseen++] = sh;
+      for (int a = 0; a < n_sites; ++a) {
+        if (cf.c[a] == 0.0) continue;
+        const uint64_t m = orb_mask(a + spin * N, N);
+        if (sh & m) continue;
+        const uint64_t bs = sh | m;  // the source state
+        const RepMap rs = sym_representative(G, bs, r_src);
+        if (rs.length == 0 || rs.rep != bs) continue;
+        const int32_t I = mixed_index(sfmap, sdu, bs);
+        if (I < 0) continue;
+        const RepMap rt = sym_representative(G, sh, r_tgt);  // rep bj; its phase and length
+        if (rt.length == 0) continue;
+        int ph = rt.phase + ((__popcll(bs & (m - 1)) & 1) ? G.g : 0);
+        ph %= 2 * G.g;
+        acc += (ph == 0 ? 1.0 : -1.0) * cf.c[a] * sqrt((double)slen[I] / (double)rt.length) * psi[I];
+      }
+    }
+    phi[J] = acc;
+  }
+}
+
 unsigned grid_for(uint64_t n, int threads) {
   static const int sms = [] {
     int dev = 0, v = 148;
@@ -284,6 +412,12 @@ MixedHamiltonian::MixedHamiltonian(const SymmetryGroup &G, const MixedTerms &t, 
   const uint64_t du = binom(N, n_up), dd = binom(N, n_dn), nf = du * dd;
   if (du > 0xffffffffull || dd > 0xffffffffull || nf > 0x7fffffffull)
     fail(QED_ERR_UNSUPPORTED, "sector too large for the mixed-basis index map");
+  this->irrep = irrep;
+  this->n_up = n_up;
+  this->n_dn = n_dn;
+  this->du = (uint32_t)du;
+  this->dd = (uint32_t)dd;
+  group = G.tab;
   DevBuf<uint32_t> us(du), ds(dd);
   launch_unrank(N, n_up, (uint32_t)du, us.p, s);
   launch_unrank(N, n_dn, (uint32_t)dd, ds.p, s);
@@ -308,7 +442,7 @@ MixedHamiltonian::MixedHamiltonian(const SymmetryGroup &G, const MixedTerms &t, 
   dtoff.upload(toff, s);
   states.alloc(D);
   len.alloc(D);
-  DevBuf<int32_t> fmap(nf);
+  fmap.alloc(nf);
   k_mixed_scatter<<<(unsigned)ntiles, kMarkThreads, 0, s>>>(lenf.p, nf, dtoff.p, us.p, (uint32_t)du, ds.p, fmap.p,
                                                             states.p, len.p);
   QED_LAUNCH();
@@ -365,6 +499,51 @@ int MixedHamiltonian::lanczos_w(const double *v, const double *vprev, const doub
 void MixedHamiltonian::apply(const double *x, double *y, cudaStream_t s) const {
   if (!D) return;
   k_mixed_spmv<<<grid_for(D * 8, 256), 256, 0, s>>>(row_ptr.p, col.p, val.p, dg.p, x, y, D);
+  QED_LAUNCH();
+}
+
+int MixedHamiltonian::apply_full(const double *x, double xs, double *y, const SubList &sub, int red_mask,
+                                 Reducer &r, cudaStream_t s, const int *skip) const {
+  if (!D) return 0;
+  unsigned nb = grid_for(D * 8, 256);
+  if (red_mask && nb > (unsigned)r.max_blocks) nb = (unsigned)r.max_blocks;
+  k_mixed_full<<<nb, 256, 0, s>>>(row_ptr.p, col.p, val.p, dg.p, x, xs, y, D, sub, red_mask, r.partials, skip);
+  QED_LAUNCH();
+  return (int)nb;
+}
+
+std::vector<double> MixedHamiltonian::dense(cudaStream_t s) const {
+  std::vector<uint64_t> rp(D + 1);
+  std::vector<uint32_t> c(nnz);
+  std::vector<double> v(nnz), d(D), out(D * D, 0.0);
+  row_ptr.download(rp.data(), D + 1, s);
+  if (nnz) {
+    col.download(c.data(), nnz, s);
+    val.download(v.data(), nnz, s);
+  }
+  dg.download(d.data(), D, s);
+  QED_CUDA(cudaStreamSynchronize(s));
+  for (size_t J = 0; J < D; ++J) {
+    out[J + D * J] += d[J];
+    for (uint64_t k = rp[J]; k < rp[J + 1]; ++k) out[J + D * c[k]] += v[k];
+  }
+  return out;
+}
+
+void mixed_cdag(const MixedHamiltonian &src, const MixedHamiltonian &tgt, int pm, int spin, int n_sites,
+                const double *coef, const double *psi, double *phi, cudaStream_t s) {
+  if (!tgt.D) return;
+  if (n_sites > kMaxSymOrb) fail(QED_ERR_UNSUPPORTED, "more than 32 sites");
+  OrbCoef cf{};
+  for (int a = 0; a < n_sites; ++a) cf.c[a] = coef[a];
+  if (pm == 1)
+    k_mixed_create<<<grid_for(tgt.D, 128), 128, 0, s>>>(src.group, src.irrep, tgt.irrep, spin, n_sites, cf,
+                                                        tgt.states.p, tgt.len.p, tgt.D, src.fmap.p, src.du, src.len.p,
+                                                        psi, phi);
+  else
+    k_mixed_destroy<<<grid_for(tgt.D, 128), 128, 0, s>>>(src.group, src.irrep, tgt.irrep, spin, n_sites, cf,
+                                                         tgt.states.p, tgt.D, src.fmap.p, src.du, src.len.p, psi,
+                                                         phi);
   QED_LAUNCH();
 }
 

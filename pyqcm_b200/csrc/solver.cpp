@@ -268,6 +268,25 @@ SectorOp::SectorOp(const SpinData &t, const Sector &s, Workspace &ws, HalfCache 
   ws.sync();
 }
 
+KrylovOp::KrylovOp(const MixedHamiltonian &h) : D(h.D), mixed(&h) {}
+
+int KrylovOp::apply(const double *x, double xs, double *y, const SubList &sub, int red_mask, Reducer &r,
+                    cudaStream_t s, const int *skip) const {
+  if (mixed) return mixed->apply_full(x, xs, y, sub, red_mask, r, s, skip);
+  HvOperator op = fact->op;
+  op.skip = skip;
+  return launch_hv(op, x, xs, y, sub, red_mask, r, s);
+}
+
+void KrylovOp::apply_block(int p, const BlockIn &X, const BlockOut &Y, Reducer &r, cudaStream_t s) const {
+  if (fact) {
+    launch_block_hv(fact->op, p, X, Y, r, s);
+    return;
+  }
+  SubList none;
+  for (int c = 0; c < p; ++c) mixed->apply_full(X.v[c], 1.0, Y.v[c], none, 0, r, s);
+}
+
 void SectorOp::apply(const double *x, double *y, Workspace &ws) const {
   if (!D) return;
   SubList none;
@@ -721,7 +740,7 @@ void dense_eigensystem(const SectorOp &H, Workspace &ws, std::vector<double> &w,
 
 // ------------------------------------------------------------ LanczosGreen --
 
-void lanczos_green(const SectorOp &H, Workspace &ws, double *psi, double *q,
+void lanczos_green(const KrylovOp &H, Workspace &ws, double *psi, double *q,
                    std::vector<double> &a, std::vector<double> &b) {
   const size_t D = H.D;
   const double accur = opt_double("accur_continued_fraction");
@@ -737,7 +756,7 @@ void lanczos_green(const SectorOp &H, Workspace &ws, double *psi, double *q,
     sub.n = 1;
     sub.c[0] = -1.0;
     sub.z[0] = q;
-    int nb = launch_hv(H.op, psi, 1.0, q, sub, 1, ws.red, s);
+    int nb = H.apply(psi, 1.0, q, sub, 1, ws.red, s);
     const double z = ws.sums(nb, 1)[0];
     a.push_back(z);
     nb = launch_axpby(D, 1.0, q, -z, psi, 1, ws.red, s);
@@ -815,7 +834,7 @@ bool cholesky_upper(int p, const double *G, std::vector<double> &R, std::vector<
 // the same. Returns false, leaving phi intact, when a QR pivot falls below 1e-4
 // (a deflation the band algorithm must handle), for p > 16 and for p = 1; the
 // caller then runs the band recurrence.
-bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
+bool block_lanczos_qmatrix(const KrylovOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
                            std::vector<double> &evals, std::vector<double> &Q, int &Mout) {
   const size_t D = H.D;
   const int p = (int)phi.size();
@@ -917,7 +936,7 @@ bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<
   } ev_guard{ev};
   auto enqueue = [&](int k) {
     // W = H V_k - V_{k-1} B_k^T, then A_k = V_k^T W
-    launch_block_hv(H.op, p, in(Vk), W, ws.red, s);
+    H.apply_block(p, in(Vk), W, ws.red, s);
     double *rk = drec.p + (size_t)ldr * k;
     int nbk;
     if (k > 0)
@@ -1017,7 +1036,7 @@ bool block_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<
 
 }  // namespace
 
-bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
+bool band_lanczos_qmatrix(const KrylovOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
                           std::vector<double> &evals, std::vector<double> &Q, int &Mout) {
   const size_t D = H.D;
   const int p = (int)phi.size();
@@ -1119,8 +1138,6 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
       if (chk <= je) je = chk;
       const std::vector<int> free0 = pool.free_list, v0 = v;
       QED_CUDA(cudaMemsetAsync(dflag.p, 0, sizeof(int), s));
-      HvOperator op = H.op;
-      op.skip = dflag.p;
       auto slots = [&](int jj) {  // steady-state window move of step jj
         pool.put(v[jj - pc - 1]);
         v[jj - pc - 1] = -1;
@@ -1153,7 +1170,7 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
         SubList sub;
         sub.cdev = rec;
         for (int k = jj - pc; k < jj; ++k) sub.z[sub.n++] = pool.p(v[k]);
-        nb = launch_hv(op, vj, 1.0, w, sub, 1, ws.red, s);
+        nb = H.apply(vj, 1.0, w, sub, 1, ws.red, s, dflag.p);
         launch_finalize(ws.red.partials, nb, 1, rec + pc, s);  // (10): T(j, j) = <v_j, w>
         launch_axpy_dev(D, w, vj, rec + pc, ws.red, s, dflag.p);
       }
@@ -1247,7 +1264,7 @@ bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<d
       sub.c[sub.n] = T(k, j);
       sub.z[sub.n++] = pool.p(v[k]);
     }
-    nb = launch_hv(H.op, pool.p(v[j]), 1.0, w, sub, nd == 0 ? 1 : 0, ws.red, s);
+    nb = H.apply(pool.p(v[j]), 1.0, w, sub, nd == 0 ? 1 : 0, ws.red, s);
     double wjj;
     if (nd == 0) {
       wjj = ws.sums(nb, 1)[0];

@@ -121,9 +121,24 @@ void lanczos_eigenvector_mixed(const MixedHamiltonian &H, Workspace &ws, const L
 void dense_eigensystem(const SectorOp &H, Workspace &ws, std::vector<double> &w,
                        std::vector<double> &U);
 
+// The H.v the Krylov drivers below apply: the spin-factorized sector operator
+// or the symmetry-adapted (mixed-basis) CSR Hamiltonian. Built implicitly from
+// either. apply: y = xs H x - sum_k sub.c[k] sub.z[k] with the reductions of
+// launch_hv (nothing when *skip != 0); apply_block: Y_c = H X_c for p vectors.
+struct KrylovOp {
+  size_t D = 0;
+  const SectorOp *fact = nullptr;
+  const MixedHamiltonian *mixed = nullptr;
+  KrylovOp(const SectorOp &h) : D(h.D), fact(&h) {}
+  KrylovOp(const MixedHamiltonian &h);
+  int apply(const double *x, double xs, double *y, const SubList &sub, int red_mask, Reducer &r, cudaStream_t s,
+            const int *skip = nullptr) const;
+  void apply_block(int p, const BlockIn &X, const BlockOut &Y, Reducer &r, cudaStream_t s) const;
+};
+
 // LanczosGreen (src_ed/Hamiltonian/Lanczos.hpp:156-183) from a normalised start
 // vector psi (overwritten). Returns the (a, b) coefficients.
-void lanczos_green(const SectorOp &H, Workspace &ws, double *psi, double *q,
+void lanczos_green(const KrylovOp &H, Workspace &ws, double *psi, double *q,
                    std::vector<double> &a, std::vector<double> &b);
 
 // Band Lanczos (src_ed/Hamiltonian/Lanczos.hpp:214-395) followed by the
@@ -131,7 +146,7 @@ void lanczos_green(const SectorOp &H, Workspace &ws, double *psi, double *q,
 // phi: p device start vectors of length H.D (consumed). Outputs the eigenvalues
 // and the Q-matrix residues Q = P U (p x M, column-major), as
 // Hamiltonian::build_Q_matrix does (src_ed/Hamiltonian/Hamiltonian_base.hpp:229-254).
-bool band_lanczos_qmatrix(const SectorOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
+bool band_lanczos_qmatrix(const KrylovOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
                           std::vector<double> &evals, std::vector<double> &Q, int &M);
 
 }  // namespace qed

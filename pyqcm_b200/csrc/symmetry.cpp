@@ -184,4 +184,25 @@ SymmetryGroup build_symmetry_group(int n_sites, int n_bath, const std::vector<st
   return G;
 }
 
+int sym_tensor(const SymmetryGroup &G, int r1, int r2) {
+  int out = 0, mult = 1;
+  for (int n : G.orders) {
+    out += ((r1 % n + r2 % n) % n) * mult;
+    r1 /= n;
+    r2 /= n;
+    mult *= n;
+  }
+  return out;
+}
+
+int sym_conjugate(const SymmetryGroup &G, int r) {
+  int out = 0, mult = 1;
+  for (int n : G.orders) {
+    out += ((n - r % n) % n) * mult;
+    r /= n;
+    mult *= n;
+  }
+  return out;
+}
+
 }  // namespace qed

@@ -34,4 +34,10 @@ struct SymmetryGroup {
 SymmetryGroup build_symmetry_group(int n_sites, int n_bath, const std::vector<std::vector<int>> &gen,
                                    bool bath_irrep);
 
+// Irrep labels are mixed-radix numbers over the generators' orders: the product
+// of two irreps adds the digits, the conjugate negates them, each modulo its
+// order (symmetry_group::tensor and conjugate, src_ed/symmetry_group.cpp:343-356).
+int sym_tensor(const SymmetryGroup &G, int r1, int r2);
+int sym_conjugate(const SymmetryGroup &G, int r);
+
 }  // namespace qed

@@ -73,19 +73,25 @@ def test_unknown_label_and_options(qed):
     qed.set_global_parameter("kgrid_side", 32)  # lattice-layer option is accepted
 
 
-def test_models_with_generators_load_and_refuse_the_factorized_solve():
+def test_models_with_generators_load_and_refuse_what_is_not_covered():
     """A cluster model with symmetry generators (g > 1) loads with its group
-    (sector strings may name irreps below g); its ground state and Green function
-    are refused with the unsupported status instead of being solved silently on
-    the unsymmetrised basis."""
+    (sector strings may name irreps below g) and is solved in the
+    symmetry-adapted basis; what that path does not cover is refused with the
+    unsupported status before any device work: continued-fraction Green
+    functions (GF_method 'F') and, below, groups with complex characters."""
     import pyqcm_b200 as qed
     from tests.helpers import c2v_golden, c2v_problem
     prob = c2v_problem(c2v_golden(), True)
-    qed.load_problem(prob, 4101, model_name="c2v_host")
-    for fn in (qed.ground_state_solve, qed.Green_function_solve):
-        with pytest.raises(qed.QEDError) as err:
-            fn(4101)
-        assert err.value.code == qed.QED_ERR_UNSUPPORTED
+    qed.set_global_parameter("GF_method", "F")
+    try:
+        qed.load_problem(prob, 4101, model_name="c2v_host")
+        for fn in (qed.ground_state_solve, qed.Green_function_solve):
+            with pytest.raises(qed.QEDError) as err:
+                fn(4101)
+            assert err.value.code == qed.QED_ERR_UNSUPPORTED
+            assert "continued-fraction" in str(err.value)
+    finally:
+        qed.set_global_parameter("GF_method", "L")
     qed.new_model_instance("c2v_host", prob.params, "R3:N11:S1", 4102)
     with pytest.raises(qed.QEDError, match="not valid"):
         qed.new_model_instance("c2v_host", prob.params, "R4:N12:S0", 4103)
@@ -105,5 +111,9 @@ def test_complex_character_groups_are_refused_by_the_mixed_hamiltonian():
     qed.new_model_instance("c4_plaquette_host", {"t": 1.0, "U": 4.0}, "R1:N4:S0", 4201)
     with pytest.raises(qed.QEDError) as err:
         qed.MixedHamiltonian(4201, "R1:N4:S0")
+    assert err.value.code == qed.QED_ERR_UNSUPPORTED
+    assert "complex" in str(err.value)
+    with pytest.raises(qed.QEDError) as err:
+        qed.ground_state_solve(4201)
     assert err.value.code == qed.QED_ERR_UNSUPPORTED
     assert "complex" in str(err.value)

@@ -94,3 +94,61 @@ def test_mixed_basis_lowest_levels_per_irrep(qed, fresh):
         assert abs(e2 - e_dense) < 1e-10, (sec, e2, e_dense)
         assert abs(np.linalg.norm(psi) - 1.0) < 1e-9
         assert np.linalg.norm(Hp @ psi - e2 * psi) < 1e-8, sec
+
+
+def _solve_both(qed, oracle, prob, label, name, fmt="S"):
+    qed.set_global_parameter("GF_method", "L")
+    oracle.set_param("GF_method", "L")
+    qed.load_problem(prob, label, model_name=name, fmt=fmt)
+    oracle.load_problem(prob, label, model_name=name, fmt=fmt)
+    return qed.ground_state_solve(label), oracle.ground_state(label)
+
+
+def test_record_green_function_in_the_symmetry_adapted_basis(qed, oracle, fresh):
+    """The reference's C2v record (2x2 plaquette + 8 bath orbitals, generators,
+    bath irreps) solved through the ED entries in the symmetry-adapted basis:
+    ground state and sector against the record (6 digits) and the compiled
+    reference's own solve of the same model (1e-10); G(z) in the site basis,
+    built from the per-irrep band-Lanczos Q-matrices, against the reference's
+    (1e-8) and, projected on each irrep's symmetric orbital, against the record's
+    14-digit poles (1e-7, the oracle's own pin); the averages of every operator
+    against the reference's (1e-9)."""
+    from tests.helpers import C2V_Z, c2v_irrep_gf, project_irreps
+    gold = c2v_golden()
+    prob = c2v_problem(gold, True)
+    suffix, label = fresh()
+    (e, sec), (e_ref, sec_ref) = _solve_both(qed, oracle, prob, label, "mixgf" + suffix)
+    assert sec == sec_ref == gold["gs"]["sector"]
+    assert abs(e - gold["gs"]["energy"]) < 5.1e-5, e
+    assert abs(e - e_ref) <= 1e-10 * abs(e_ref), (e, e_ref)
+    G = qed.Green_function(C2V_Z, label=label)
+    G_ref = oracle.green_function(label, C2V_Z)
+    assert np.max(np.abs(G - G_ref)) < 1e-8
+    assert np.max(np.abs(project_irreps(G) - c2v_irrep_gf(gold, C2V_Z))) < 1e-7
+    z = W.matsubara(64)
+    assert np.max(np.abs(qed.Green_function(z, label=label) - oracle.green_function(label, z))) < 1e-8
+    ave = {n: (a, v) for n, a, v in qed.cluster_averages(label)}
+    for n, a, v in oracle.cluster_averages(label):
+        assert abs(ave[n][0] - a) < 1e-9 * max(1.0, abs(a)), (n, ave[n], a)
+        assert abs(ave[n][1] - v) < 1e-8 * max(1.0, abs(v)), (n, ave[n], v)
+
+
+@pytest.mark.parametrize("sectors", ["R0:N6:S0/R1:N6:S0/R2:N6:S0/R3:N6:S0", "R0:N5:S1/R1:N5:S1/R2:N5:S1/R3:N5:S1"])
+def test_cluster_with_generators_matches_reference(qed, oracle, fresh, sectors):
+    """A 2x3 Hubbard cluster with t' and C2v generators: the lowest state over
+    the four irreps of the half-filled (or one-hole) sectors, G(i w_n) on 64
+    Matsubara frequencies and the Potthoff functional against the compiled
+    reference's symmetry-adapted solve. The hole and electron targets are small
+    enough that some go through full diagonalisation (below max_dim_full)."""
+    prob = _sq2x3_c2v()
+    prob.sectors = sectors
+    suffix, label = fresh()
+    (e, sec), (e_ref, sec_ref) = _solve_both(qed, oracle, prob, label, "mix23" + suffix)
+    assert sec == sec_ref, (sec, sec_ref)
+    assert abs(e - e_ref) <= 1e-10 * abs(e_ref), (e, e_ref)
+    z = W.matsubara(64)
+    assert np.max(np.abs(qed.Green_function(z, label=label) - oracle.green_function(label, z))) < 1e-8
+    if "S1" in sectors:
+        Gd = qed.Green_function(z, spin_down=True, label=label)
+        assert np.max(np.abs(Gd - oracle.green_function(label, z, spin_down=True))) < 1e-8
+    assert abs(qed.Potthoff_functional(label) - oracle.potthoff(label)) < 1e-9

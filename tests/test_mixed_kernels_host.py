@@ -137,3 +137,74 @@ def test_mixed_kernels_on_the_host_match_the_restatement(emulator, case, sector)
     Hp, basis = port_sym.mixed_hamiltonian(prob, G, sector)
     assert np.array_equal(states, basis)
     assert np.max(np.abs(A - Hp.toarray())) < 1e-13
+
+
+@pytest.fixture(scope="module")
+def cdag_emulator(tmp_path_factory):
+    if not shutil.which("g++"):
+        pytest.skip("g++ not available")
+    src = open(os.path.join(CSRC, "mixed.cu")).read()
+    k = src.index("struct OffTerms {")
+    parts = [src[k:src.index("};", k) + 2],
+             _grab(src, "__device__ __forceinline__ uint32_t colex_rank"),
+             _grab(src, "__device__ __forceinline__ uint64_t orb_mask"),
+             _grab(src, "__global__ void k_mixed_mark"),
+             src[src.index("struct OrbCoef {"):src.index("};", src.index("struct OrbCoef {")) + 2],
+             _grab(src, "__device__ __forceinline__ int32_t mixed_index"),
+             _grab(src, "__global__ void k_mixed_create"),
+             _grab(src, "__global__ void k_mixed_destroy")]
+    d = tmp_path_factory.mktemp("mixed_cdag_emu")
+    (d / "kernels_host.hpp").write_text(SHIM + "\n\n".join(parts) + "\n}\n")
+    exe = d / "emu"
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", str(d), "-I", CSRC, "-I", os.path.join(ROOT, "include"),
+                    "-I", cuda_inc, os.path.join(HERE, "mixed_cdag_main.cpp"), os.path.join(CSRC, "symmetry.cpp"),
+                    "-o", str(exe)], check=True, capture_output=True)
+    return str(exe)
+
+
+@pytest.mark.parametrize("case,sector", [("record", "R0:N4:S0"), ("record", "R2:N5:S1"), ("sq2x3", "R0:N6:S0"),
+                                         ("sq2x3", "R3:N5:S-1")])
+def test_mixed_cdag_kernels_on_the_host_match_the_restatement(cdag_emulator, case, sector):
+    """c and c+ of every symmetric orbital, both spins, on a random vector of the
+    sector: the device gathers (creation over target states, destruction over
+    the orbits of the target states) against the restatement's destruction
+    matrices (oracle/port_sym.destroy_matrix, pinned to the reference)."""
+    prob = {"sq2x3": _sq2x3, "record": lambda: c2v_problem(c2v_golden(), True)}[case]()
+    r0, N, S = (int(t[1:]) for t in sector.split(":"))
+    gens0 = [[v - 1 if (i < prob.n_sites or not prob.bath_irrep) else v for i, v in enumerate(g)]
+             for g in prob.generators]
+    G = port_sym.group(prob.n_sites, prob.n_bath, gens0, prob.bath_irrep)
+    _, B0 = port_sym.mixed_hamiltonian(prob, G, sector)
+    psi = np.random.default_rng(r0 + 7 * N).standard_normal(len(B0))
+    rows, irr = port_sym.symmetric_orbitals(G, prob.n_sites)
+    checked = 0
+    for k, (s_row, r_orb) in enumerate(zip(rows, irr)):
+        for spin in (0, 1):
+            for pm in (1, -1):
+                rt = port_sym.shift_irrep(G, r0, pm, r_orb)
+                ds = -1 if spin else 1
+                tsec = f"R{rt}:N{N + pm}:S{S + pm * ds}"
+                _, Bt = port_sym.mixed_hamiltonian(prob, G, tsec)
+                if len(Bt) == 0:
+                    continue
+                if pm == 1:
+                    ref = port_sym.destroy_matrix(G, s_row, spin, Bt, rt, B0, r0).T @ psi
+                else:
+                    ref = port_sym.destroy_matrix(G, s_row, spin, B0, r0, Bt, rt) @ psi
+                nu, nd = (N + S) // 2, (N - S) // 2
+                lines = [f"{prob.n_sites} {prob.n_bath} {int(prob.bath_irrep)} {len(gens0)}"]
+                lines += [" ".join(map(str, g)) for g in gens0]
+                lines.append(f"{r0} {nu} {nd} {rt} {pm} {spin}")
+                lines.append(" ".join(repr(float(c)) for c in s_row))
+                lines.append(" ".join(repr(float(x)) for x in psi))
+                out = subprocess.run([cdag_emulator], input="\n".join(lines), capture_output=True, text=True,
+                                     check=True).stdout.split("\n")
+                ds_, dt_ = (int(t) for t in out[0].split())
+                assert ds_ == len(B0) and dt_ == len(Bt)
+                st = np.array([int(s.split()[0]) for s in out[1:1 + dt_]], dtype=np.uint64)
+                phi = np.array([float(s.split()[1]) for s in out[1:1 + dt_]])
+                assert np.array_equal(st, Bt)
+                assert np.max(np.abs(phi - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref))), (k, spin, pm)
+                checked += 1
+    assert checked >= 4

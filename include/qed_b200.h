@@ -43,7 +43,7 @@ extern "C" {
 #define QED_ERR_QMATRIX 3       /* Q-matrix norm check (src_ed/Q_matrix.hpp:255-259)         */
 #define QED_ERR_CUDA 4          /* CUDA runtime error                                       */
 #define QED_ERR_MEMORY 5        /* device memory budget exceeded                            */
-#define QED_ERR_UNSUPPORTED 6   /* model outside this solver's scope (e.g. g > 1, anomalous) */
+#define QED_ERR_UNSUPPORTED 6   /* model outside this solver's scope (e.g. anomalous, complex) */
 #define QED_ERR_NO_DEVICE 7     /* no CUDA device / extension not usable                    */
 #define QED_ERR_INTERNAL 8
 
@@ -67,9 +67,8 @@ int qed_set_global_char(const char *name, char value);
 int qed_set_global_bool(const char *name, int value);
 int qed_get_global_double(const char *name, double *value);
 
-/* ED::new_model (src_ed/qcm_ED.hpp:33). Only the trivial point group (no
- * generators) is supported: the spin-factorized Hamiltonian requires g = 1
- * (src_ed/model_instance_base.cpp:85-97). */
+/* ED::new_model (src_ed/qcm_ED.hpp:33) without generators (trivial point group,
+ * the spin-factorized basis; models with generators: qed_new_model_generators). */
 int qed_new_model(const char *name, int n_sites, int n_bath);
 
 /* ED::new_operator (src_ed/qcm_ED.hpp:56), real elements. type is "one-body"
@@ -303,10 +302,14 @@ int qed_destroy_table(int L, int n_up, int n_dn, int a, long *target, int *phase
 /* ED::new_model with symmetry generators (src_ed/qcm_ED.hpp:34; the reference's
  * Python binding converts pyqcm's 1-based generators to this 0-based form,
  * src_python/qcm_ED_wrap.hpp:145-163). The group is checked and kept with the
- * model; sector strings of its instances may name irreps R0..R(g-1). Ground
- * states and Green functions of such instances return QED_ERR_UNSUPPORTED (they
- * are solved in the spin-factorized basis, g = 1); their sectors' Hamiltonians
- * are available through qed_mixed_hamiltonian_*. */
+ * model; sector strings of its instances may name irreps R0..R(g-1). Their
+ * ground states and Green functions are solved in the symmetry-adapted basis:
+ * per-irrep sector solves, per-irrep band-Lanczos Q-matrices of the symmetric
+ * orbitals, consolidated in the site basis as Q_matrix_set::consolidated_qmatrix
+ * (src_ed/Q_matrix_set.hpp:144-163) does. QED_ERR_UNSUPPORTED for groups with
+ * complex characters (a generator of order above 2) and for continued-fraction
+ * Green functions (GF_method 'F') of such models. The sectors' Hamiltonians are
+ * also available through qed_mixed_hamiltonian_*. */
 int qed_new_model_generators(const char *name, int n_sites, int n_bath, int n_gen, const int *gen, int bath_irrep);
 
 /* Hamiltonian<double> of one sector in the symmetry-adapted basis

@@ -104,12 +104,13 @@ def peaks():
         return 6650.0, "fallback"
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one H.v, i.e. one
-# k_hv_rows2 + one k_hv_cols2 launch, per basis state: ncu --set full on the
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one H.v, one
+# k_hv_cols16w launch (writes y = dn hops x) and one k_hv_rows16 launch (adds the
+# up hops and the diagonal, reads y back), per basis state: ncu --set full on the
 # 4x4 N_up = N_dn = 6 sector (64,128,064 states, vectors larger than L2) read
-# 0.982 + 1.569 GB. Both passes stream the vectors once, so the traffic scales
-# with the number of states.
-TRAFFIC_BYTES_PER_STATE = (0.514027e9 + 0.467779e9 + 1.080543e9 + 0.487590e9) / 64128064
+# 0.983 + 1.511 GB (profiles/hv_staged_sq4x4_N12_ncu_full.md). Both passes stream
+# the vectors once, so the traffic scales with the number of states.
+TRAFFIC_BYTES_PER_STATE = (0.514972e9 + 0.467877e9 + 1.029826e9 + 0.481437e9) / 64128064
 
 
 def ncu_traffic(D):
@@ -350,7 +351,7 @@ def run_ours(args, world, rank, local):
                    "parallelism": f"replicas x{world}", "bytes_per_step": alg},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": src,
-                     "unit_of_work": "one H.v (row pass + column pass kernels), 16 B per basis state"},
+                     "unit_of_work": "one H.v (column pass k_hv_cols16w + row pass k_hv_rows16), 16 B per basis state"},
         "e2e": {"value": aggregate_value(alg, e2e_s * 1e3, world), "unit": UNIT, "h2d_bytes_per_step": 8 * D,
                 "d2h_bytes_per_step": 8 * D,
                 "path": "qed_hamiltonian_mult_add (y += H x) on pinned host buffers: x up and H x down in row "

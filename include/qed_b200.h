@@ -50,8 +50,9 @@ extern "C" {
 /* Copies the last error message of the calling thread; returns its length. */
 int qed_last_error(char *buf, int len);
 /* No counterpart in the reference: the launch shapes the H.v autotuner picked so
- * far, one JSON object per sector shape (dim_up, dim_dn) with the shape chosen
- * and the time of every candidate (ms per H.v). Writes at most len - 1 bytes
+ * far, one JSON object per sector shape (dim_up, dim_dn) with the shape chosen,
+ * whether every candidate wrote the same bits of H x (bit_identical) and the time
+ * of every candidate (ms per H.v). Writes at most len - 1 bytes
  * and a terminating 0; returns the full length. */
 int qed_hv_tuning_report(char *buf, int len);
 

@@ -668,7 +668,8 @@ def destroy_table(L: int, n_up: int, n_dn: int, a: int):
 
 def hv_tuning_report():
     """Launch shapes chosen by the H.v autotuner so far (list of dicts: dim_up,
-    dim_dn, choice, ms per candidate)."""
+    dim_dn, choice, bit_identical -- every candidate wrote the same bits of
+    H x --, ms per candidate)."""
     import json
     n = lib().qed_hv_tuning_report(None, 0)
     buf = C.create_string_buffer(n + 1)

@@ -1745,7 +1745,24 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 struct TuneRecord {
   int choice = 0;
   float ms[kNumShapes] = {};
+  bool identical = true;  // every shape wrote the same bits of y
 };
+
+// Order-independent fingerprint of the bits of y: the sum over i of
+// splitmix64(bits(y_i) ^ golden-ratio * i) mod 2^64 (Vigna's splitmix64
+// finaliser); two vectors that differ in any bit or position give different
+// sums except with probability about 2^-64.
+__global__ void k_bits_fingerprint(const double *__restrict__ y, size_t n, unsigned long long *h) {
+  unsigned long long acc = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long z = (unsigned long long)__double_as_longlong(y[i]) ^ (i * 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    acc += z ^ (z >> 31);
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(h, acc);
+}
 std::mutex g_tune_mtx;
 std::map<std::pair<uint32_t, uint32_t>, TuneRecord> g_tune;
 
@@ -1790,6 +1807,10 @@ int staged_shape(const HvOperator &op, const double *x, double *y, Reducer &r, s
   cudaEvent_t e0, e1;
   QED_CUDA(cudaEventCreate(&e0));
   QED_CUDA(cudaEventCreate(&e1));
+  unsigned long long *fp = nullptr;  // one fingerprint of y per shape
+  QED_CUDA(cudaMallocAsync((void **)&fp, kNumShapes * sizeof(unsigned long long), s));
+  QED_CUDA(cudaMemsetAsync(fp, 0, kNumShapes * sizeof(unsigned long long), s));
+  const size_t D = (size_t)op.up.dim * op.dn.dim;
   SubList none;
   float best = 0.0f;
   for (int v = 0; v < kNumShapes; ++v) {
@@ -1797,6 +1818,8 @@ int staged_shape(const HvOperator &op, const double *x, double *y, Reducer &r, s
     QED_CUDA(cudaEventRecord(e0, s));
     for (int k = 0; k < 3; ++k) launch_staged(v, op, x, 1.0, y, none, 0, r, smr, smc, s);
     QED_CUDA(cudaEventRecord(e1, s));
+    k_bits_fingerprint<<<2 * device_sms(), 256, 0, s>>>(y, D, fp + v);
+    QED_LAUNCH();
     QED_CUDA(cudaEventSynchronize(e1));
     float ms = 0.0f;
     QED_CUDA(cudaEventElapsedTime(&ms, e0, e1));
@@ -1806,6 +1829,11 @@ int staged_shape(const HvOperator &op, const double *x, double *y, Reducer &r, s
       rec.choice = v;
     }
   }
+  unsigned long long h[kNumShapes];
+  QED_CUDA(cudaMemcpyAsync(h, fp, sizeof(h), cudaMemcpyDeviceToHost, s));
+  QED_CUDA(cudaFreeAsync(fp, s));
+  QED_CUDA(cudaStreamSynchronize(s));
+  for (int v = 1; v < kNumShapes; ++v) rec.identical = rec.identical && h[v] == h[0];
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   std::lock_guard<std::mutex> l(g_tune_mtx);
@@ -1842,7 +1870,8 @@ std::string hv_tuning_report() {
   for (const auto &kv : g_tune) {
     if (out.size() > 1) out += ", ";
     out += "{\"dim_up\": " + std::to_string(kv.first.first) + ", \"dim_dn\": " + std::to_string(kv.first.second) +
-           ", \"choice\": \"" + kShapes[kv.second.choice].name + "\", \"ms\": {";
+           ", \"choice\": \"" + kShapes[kv.second.choice].name +
+           "\", \"bit_identical\": " + (kv.second.identical ? "true" : "false") + ", \"ms\": {";
     for (int v = 0; v < kNumShapes; ++v)
       out += std::string(v ? ", " : "") + "\"" + kShapes[v].name + "\": " + std::to_string(kv.second.ms[v]);
     out += "}}";

@@ -200,6 +200,9 @@ def test_apply_dots_device_staged_kernels(qed, oracle, fresh):
         assert abs(d[0] - x @ y_ref) < 1e-10 * abs(x @ y_ref)
         assert abs(d[1] - y_ref @ y_ref) < 1e-10 * (y_ref @ y_ref)
         assert abs(d[2] - x @ x) < 1e-12 * (x @ x)
+    # the autotuner timed every launch shape on this sector; they wrote the same bits
+    rec = [t for t in qed.hv_tuning_report() if (t["dim_up"], t["dim_dn"]) == (3432, 3432)]
+    assert rec and all(t["bit_identical"] for t in rec), rec
 
 
 def test_ground_state_staged_kernels(qed, oracle, fresh):

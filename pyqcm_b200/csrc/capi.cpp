@@ -298,6 +298,10 @@ int batch_green_functions(BatchSet &b, int threads) {
           tasks.push_back({cost * p, [I, sp, sd] { I->build_cf(*sp, sd != 0, ws()); }});
           continue;
         }
+        if (I->use_mcf) {
+          tasks.push_back({cost * p, [I, sp, sd] { I->build_mcf(*sp, sd != 0, ws()); }});
+          continue;
+        }
         jobs.emplace_back(new Job{I, sp, sd != 0, {}});
         Job *j = jobs.back().get();
         for (int s = 0; s < 2; ++s)
@@ -829,7 +833,8 @@ int qed_qmatrix(int label, int spin_down, int *M, int *L, double *e, double *v) 
   return guarded([&] {
     auto I = instance(label);
     std::lock_guard<std::mutex> li(I->mtx);
-    if (I->use_cf) fail(QED_ERR_ARGUMENT, "Green function format is not Lehmann! Cannot output the Q matrix.");
+    if (I->use_cf || I->use_mcf)
+      fail(QED_ERR_ARGUMENT, "Green function format is not Lehmann! Cannot output the Q matrix.");
     {
       I->green_solve(ws());
     }

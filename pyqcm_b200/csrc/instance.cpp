@@ -55,9 +55,15 @@ Instance::Instance(int lab, std::shared_ptr<Model> m, std::map<std::string, doub
                                model->name + " has no parameters!");
   char gf = opt_char("GF_method");
   if (gf == 'L' && opt_bool("continued_fraction")) gf = 'F';
-  if (gf == 'M' || (gf == 'L' && opt_bool("combine_mcf")))
-    fail(QED_ERR_UNSUPPORTED, "matrix continued fractions (GF_method 'M') are not in this solver");
+  if (gf == 'L' && opt_bool("combine_mcf"))
+    fail(QED_ERR_UNSUPPORTED, "Q-matrix to matrix-continued-fraction conversion (GF_method 'L' with combine_mcf) "
+                              "is not in this solver");
+  if (gf == 'M' && opt_bool("combine_mcf"))
+    fail(QED_ERR_UNSUPPORTED, "combining the electron and hole matrix continued fractions (combine_mcf) is not in "
+                              "this solver");
   use_cf = (gf == 'F');
+  use_mcf = (gf == 'M');
+  mcf_qr = opt_bool("block_Lanczos_QR");
   if (opt_char("Ground_state_method") != 'L')
     fail(QED_ERR_UNSUPPORTED, "only the Lanczos ground-state method ('L') is in this solver");
   if (opt_int("n_states") > 1)
@@ -628,10 +634,10 @@ void Instance::require_supported_group() const {
     fail(QED_ERR_UNSUPPORTED, "model " + model->name +
                                   ": point group with complex characters (a generator of order above 2) needs "
                                   "a complex Hilbert space, which this solver does not provide");
-  if (use_cf)
+  if (use_cf || use_mcf)
     fail(QED_ERR_UNSUPPORTED, "model " + model->name +
-                                  ": continued-fraction Green functions (GF_method 'F') of models with a point "
-                                  "group are not in this solver; use the Lehmann form ('L')");
+                                  ": continued-fraction Green functions (GF_method 'F' or 'M') of models with a "
+                                  "point group are not in this solver; use the Lehmann form ('L')");
 }
 
 std::unique_ptr<MixedHamiltonian> Instance::mixed_sector(const Sector &s, Workspace &ws) const {
@@ -1020,8 +1026,48 @@ void Instance::build_cf(State &st, bool spin_down, Workspace &ws) {
 }
 
 // Green_function_solve (src_ed/model_instance.hpp:517-555)
+void Instance::build_mcf(State &st, bool spin_down, Workspace &ws) {
+  PhaseScope ps(kPhCf);
+  const int n = model->n_sites;
+  if (n > kMcfMaxP) fail(QED_ERR_UNSUPPORTED, "matrix continued fractions of more than 16 cluster sites");
+  McfSet &m = st.mcf[spin_down ? 1 : 0];
+  m = McfSet();
+  const double accur_def = opt_double("accur_deflation");
+  for (int pm = -1; pm < 2; pm += 2) {
+    Sector tsec = shift_sector(st.sec, pm, spin_down ? 1 : 0);
+    if (!sector_is_valid(tsec, model->n_orb)) continue;
+    SectorOp H(terms, tsec, ws, &tables);
+    if (H.D == 0) continue;
+    // start block phi_i = c_i^{pm} |state>, then its QR phi = q W
+    DevBuf<double> phi(H.D * (size_t)n);
+    for (int i = 0; i < n; ++i) apply_cdag(st, pm, spin_down ? 1 : 0, i, H, phi.p + (size_t)i * H.D, 1.0, false, ws);
+    std::vector<double> R;
+    const int pa = mgs_qr(H.D, n, phi.p, accur_def, R, ws);
+    if (pa == 0) continue;
+    McfFloors f;
+    block_lanczos_mcf(KrylovOp(H), ws, phi.p, pa, mcf_qr, f);
+    if (f.M == 0) continue;
+    McfPart &part = pm == 1 ? m.e : m.h;
+    part.M = f.M;
+    part.p = pa;
+    part.q = n;
+    part.A = std::move(f.A);
+    part.B = std::move(f.B);
+    for (int j = 0; j < part.M; ++j)  // A_j - e0 (electron) or e0 - A_j (hole)
+      for (int r = 0; r < pa; ++r)
+        for (int c = 0; c < pa; ++c) {
+          double &a = part.A[(size_t)j * pa * pa + (size_t)r * pa + c];
+          a = pm == 1 ? a - (r == c ? st.energy : 0.0) : -a + (r == c ? st.energy : 0.0);
+        }
+    const double sw = std::sqrt(st.weight);
+    part.W.assign((size_t)pa * n, 0.0);
+    for (int r = 0; r < pa; ++r)
+      for (int c = 0; c < n; ++c) part.W[(size_t)r * n + c] = R[(size_t)r * n + c] * sw;
+  }
+}
+
 void Instance::check_gf_solvable() const {
-  if (opt_bool("merge_states") && states.size() > 1 && !use_cf)
+  if (opt_bool("merge_states") && states.size() > 1 && !use_cf && !use_mcf)
     fail(QED_ERR_UNSUPPORTED, "merge_states is not in this solver");
 }
 
@@ -1030,11 +1076,10 @@ void Instance::green_solve(Workspace &ws) {
   if (!gs_solved) low_energy_states(ws);
   check_gf_solvable();
   for (auto &x : states) {
-    if (use_cf) build_cf(*x, false, ws);
-    else build_qmatrix(*x, false, ws);
-    if (mix & mixing::up_down) {
-      if (use_cf) build_cf(*x, true, ws);
-      else build_qmatrix(*x, true, ws);
+    for (int sd = 0; sd < ((mix & mixing::up_down) ? 2 : 1); ++sd) {
+      if (use_cf) build_cf(*x, sd != 0, ws);
+      else if (use_mcf) build_mcf(*x, sd != 0, ws);
+      else build_qmatrix(*x, sd != 0, ws);
     }
   }
   finish_gf();
@@ -1062,7 +1107,15 @@ void Instance::green_average() {
     Mave[sd].assign((size_t)n * n, 0.0);
     if (sd == 1 && !(mix & mixing::up_down)) continue;
     for (auto &st : states) {
-      if (!use_cf) {
+      if (use_mcf) {  // mcf_set::integrated_Green_function (src_ed/mcf_set.hpp:140-152): (W_h^T W_h)^T
+        const McfPart &h = st->mcf[sd].h;
+        for (int a = 0; a < n && h.M; ++a)
+          for (int b = 0; b < n; ++b) {
+            double acc = 0.0;
+            for (int k = 0; k < h.p; ++k) acc += h.W[(size_t)k * n + a] * h.W[(size_t)k * n + b];
+            Mave[sd][a + (size_t)n * b] += acc;
+          }
+      } else if (!use_cf) {
         const QMat &q = st->q[sd];
         for (int i = 0; i < q.M; ++i) {
           if (q.e[i] >= 0.0) continue;
@@ -1096,6 +1149,42 @@ void Instance::green_function(const cplx *z, int nz, bool spin_down, cplx *out, 
   if (nz <= 0) return;
   DevBuf<double> dz(2 * (size_t)nz);
   dz.upload(reinterpret_cast<const double *>(z), 2 * (size_t)nz, ws.stream);
+  if (use_mcf) {  // mcf_set::Green_function (src_ed/mcf_set.hpp:113-131): G_e + G_h^T, every state
+    std::vector<McfDesc> desc;
+    std::vector<double> blob;
+    for (auto &st : states)
+      for (int part = 0; part < 2; ++part) {
+        const McfPart &f = part ? st->mcf[sd].h : st->mcf[sd].e;
+        if (!f.M) continue;
+        McfDesc d;
+        d.M = f.M;
+        d.p = f.p;
+        d.q = n;
+        d.transpose = part;
+        d.offA = (long long)blob.size();
+        blob.insert(blob.end(), f.A.begin(), f.A.end());
+        d.offB = (long long)blob.size();
+        blob.insert(blob.end(), f.B.begin(), f.B.end());
+        d.offW = (long long)blob.size();
+        blob.insert(blob.end(), f.W.begin(), f.W.end());
+        desc.push_back(d);
+      }
+    const int nf = (int)desc.size();
+    if (!nf) return;
+    DevBuf<McfDesc> ddesc(nf);
+    DevBuf<double> dblob(blob.size()), dF(2 * (size_t)nf * nz * nn);
+    ddesc.upload(desc, ws.stream);
+    dblob.upload(blob, ws.stream);
+    launch_mcf_eval(nf, ddesc.p, dblob.p, n, nz, dz.p, dF.p, ws.stream);
+    std::vector<cplx> F((size_t)nf * nz * nn);
+    dF.download(reinterpret_cast<double *>(F.data()), 2 * F.size(), ws.stream);
+    ws.sync();
+    // F[(f * nz + k) * nn + a * n + b] = G_f(z_k)(a, b); out[k * nn + b + a * n] = G(a, b)
+    for (int f = 0; f < nf; ++f)
+      for (int k = 0; k < nz; ++k)
+        for (size_t i = 0; i < nn; ++i) out[nn * k + i] += F[((size_t)f * nz + k) * nn + i];
+    return;
+  }
   if (!use_cf) {
     DevBuf<double> dG(2 * nn * nz);
     QED_CUDA(cudaMemsetAsync(dG.p, 0, dG.bytes(), ws.stream));
@@ -1161,7 +1250,7 @@ void Instance::green_function_device(const cplx *z, int nz, bool spin_down, doub
   const int sd = (spin_down && (mix & mixing::up_down)) ? 1 : 0;
   const size_t nn = (size_t)n * n;
   if (nz <= 0) return;
-  if (use_cf) {  // continued fractions: evaluated by green_function, then uploaded
+  if (use_cf || use_mcf) {  // continued fractions: evaluated by green_function, then uploaded
     std::vector<cplx> G(nn * nz);
     green_function(z, nz, spin_down, G.data(), ws);
     QED_CUDA(cudaMemcpyAsync(dG, G.data(), G.size() * sizeof(cplx), cudaMemcpyHostToDevice, ws.stream));

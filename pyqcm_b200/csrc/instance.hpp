@@ -34,6 +34,19 @@ struct CFSet {
   std::vector<std::vector<double>> ea, eb, ha, hb;  // index o1*n + o2
 };
 
+// One matrix continued fraction of a state and spin (the hole or the electron
+// part of mcf_set, src_ed/mcf_set.hpp:51-60): M floors of p x p blocks, A
+// shifted by the state's energy as matrix_continued_fraction's constructor
+// does (src_ed/matrix_continued_fraction.hpp:84-100), B the off-diagonal blocks,
+// W the p x q weight (row-major; sqrt(weight) folded in).
+struct McfPart {
+  int M = 0, p = 0, q = 0;
+  std::vector<double> A, B, W;
+};
+struct McfSet {
+  McfPart e, h;
+};
+
 struct State {
   Sector sec;
   double energy = 0.0, weight = 0.0;
@@ -43,6 +56,7 @@ struct State {
   std::vector<double> hpsi;  // dense: the eigenvector on the host until it is uploaded
   QMat q[2];   // [spin_down]
   CFSet cf[2];
+  McfSet mcf[2];
 };
 
 // Eigenvalue pass of one target sector: the unit of work that batched drivers
@@ -85,6 +99,8 @@ struct Instance {
   int mix = 0;
   bool is_correlated = false;
   bool use_cf = false;
+  bool use_mcf = false;  // GF_method 'M': matrix continued fractions (block Lanczos)
+  bool mcf_qr = false;   // block_Lanczos_QR: QR (true) or polar (false) off-diagonal blocks
   int dim_GF = 0;
   bool gs_solved = false, gf_solved = false, hopping_solved = false;
   double GS_energy = 0.0, E0 = 0.0, SEF_bath = 0.0, GF_density = 0.0;
@@ -131,6 +147,9 @@ struct Instance {
   void qmatrix_part(State &st, bool spin_down, int s, QPart &out, Workspace &ws);
   void qmatrix_combine(State &st, bool spin_down, QPart (&parts)[2], Workspace &ws);
   void build_cf(State &st, bool spin_down, Workspace &ws);
+  // build_mcf (src_ed/model_instance.hpp:847-946): per hole / electron part, the
+  // start block c_i^{-+}|state>, its QR (weight W), block Lanczos, the shifted floors
+  void build_mcf(State &st, bool spin_down, Workspace &ws);
   void finish_gf();
   // G(z) for nz frequencies: out[k*n*n + b + a*n] (column-major blocks)
   void green_function(const cplx *z, int nz, bool spin_down, cplx *out, Workspace &ws);

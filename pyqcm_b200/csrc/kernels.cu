@@ -849,6 +849,126 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (lane == 0) bulk_wait_all();  // stores complete while the staging slots are still ours
 }
 
+// ---- matrix continued fractions --------------------------------------------
+//
+// One CTA per (frequency, fraction): the backward recursion of the p x p complex
+// floors in shared memory, each floor inverted by Gauss-Jordan elimination with
+// partial pivoting on the augmented matrix [D | I].
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__global__ void __launch_bounds__(256) k_mcf_eval(const McfDesc *desc, const double *blob, int q, int nz,
+                                                  const double *z, double *out) {
+  const McfDesc d = desc[blockIdx.y];
+  const int k = blockIdx.x, p = d.p, pp = p * p, t = threadIdx.x, nt = blockDim.x;
+  const double zr = z[2 * k], zi = z[2 * k + 1];
+  __shared__ double2 F[kMcfMaxP * kMcfMaxP], T1[kMcfMaxP * kMcfMaxP];
+  __shared__ double2 Aug[kMcfMaxP][2 * kMcfMaxP];
+  __shared__ double2 fac[kMcfMaxP];
+  __shared__ int piv;
+  for (int i = t; i < pp; i += nt) F[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int j = d.M - 1; j >= 0; --j) {
+    const double *A = blob + d.offA + (size_t)j * pp, *B = blob + d.offB + (size_t)j * pp;
+    const bool tail = j < d.M - 1;  // B_{M-1} is the truncation residual, not used
+    if (tail) {
+      for (int i = t; i < pp; i += nt) {  // T1 = F B_j
+        const int r = i / p, c = i % p;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int a = 0; a < p; ++a) {
+          const double b = B[a * p + c];
+          acc.x += F[r * p + a].x * b;
+          acc.y += F[r * p + a].y * b;
+        }
+        T1[i] = acc;
+      }
+      __syncthreads();
+    }
+    for (int i = t; i < 2 * pp; i += nt) {  // Aug = [z - A_j - B_j^T T1 | I]
+      const int r = i / (2 * p), c = i % (2 * p);
+      double2 v;
+      if (c < p) {
+        double2 sg = make_double2(0.0, 0.0);
+        if (tail)
+          for (int a = 0; a < p; ++a) {
+            const double b = B[a * p + r];
+            sg.x += b * T1[a * p + c].x;
+            sg.y += b * T1[a * p + c].y;
+          }
+        v = make_double2((r == c ? zr : 0.0) - A[r * p + c] - sg.x, (r == c ? zi : 0.0) - sg.y);
+      } else {
+        v = make_double2(r == c - p ? 1.0 : 0.0, 0.0);
+      }
+      Aug[r][c] = v;
+    }
+    __syncthreads();
+    for (int c = 0; c < p; ++c) {
+      if (t == 0) {
+        int best = c;
+        double bm = Aug[c][c].x * Aug[c][c].x + Aug[c][c].y * Aug[c][c].y;
+        for (int r = c + 1; r < p; ++r) {
+          const double m = Aug[r][c].x * Aug[r][c].x + Aug[r][c].y * Aug[r][c].y;
+          if (m > bm) {
+            bm = m;
+            best = r;
+          }
+        }
+        piv = best;
+      }
+      __syncthreads();
+      const int pr = piv;
+      if (pr != c)
+        for (int i = t; i < 2 * p; i += nt) {
+          const double2 tmp = Aug[c][i];
+          Aug[c][i] = Aug[pr][i];
+          Aug[pr][i] = tmp;
+        }
+      __syncthreads();
+      const double2 pv = Aug[c][c];
+      const double den = pv.x * pv.x + pv.y * pv.y;
+      const double2 inv = make_double2(pv.x / den, -pv.y / den);
+      __syncthreads();  // every thread has read the pivot
+      for (int i = t; i < 2 * p; i += nt) Aug[c][i] = cmul(Aug[c][i], inv);
+      if (t < p) fac[t] = Aug[t][c];
+      __syncthreads();
+      for (int i = t; i < 2 * pp; i += nt) {
+        const int r = i / (2 * p), col = i % (2 * p);
+        if (r == c) continue;
+        const double2 m = cmul(fac[r], Aug[c][col]);
+        Aug[r][col].x -= m.x;
+        Aug[r][col].y -= m.y;
+      }
+      __syncthreads();
+    }
+    for (int i = t; i < pp; i += nt) F[i] = Aug[i / p][p + i % p];
+    __syncthreads();
+  }
+  // G = W^T F_0 W
+  const double *W = blob + d.offW;
+  double *o = out + ((size_t)blockIdx.y * nz + k) * (size_t)q * q * 2;
+  for (int i = t; i < q * q; i += nt) {
+    const int a = i / q, b = i % q;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int r = 0; r < p; ++r) {
+      const double wa = W[r * q + a];
+      if (wa == 0.0) continue;
+      double2 row = make_double2(0.0, 0.0);
+      for (int c = 0; c < p; ++c) {
+        const double wb = W[c * q + b];
+        row.x += F[r * p + c].x * wb;
+        row.y += F[r * p + c].y * wb;
+      }
+      acc.x += wa * row.x;
+      acc.y += wa * row.y;
+    }
+    const size_t idx = d.transpose ? (size_t)b * q + a : (size_t)a * q + b;
+    o[2 * idx] = acc.x;
+    o[2 * idx + 1] = acc.y;
+  }
+}
+
 // ---- block H.v on separate vectors (sectors without packed tables) ----
 //
 // A block of p <= 16 vectors (pointer arrays) through the ELL tables: one
@@ -2133,6 +2253,14 @@ void launch_cf_eval(int nf, const int *off, const int *len, const double *a, con
   if (nf <= 0 || nz <= 0) return;
   size_t n = (size_t)nf * nz;
   k_cf_eval<<<grid_for(n, device_sms(), 8), kThreads, 0, s>>>(nf, off, len, a, b, nz, z, F);
+  QED_LAUNCH();
+}
+
+void launch_mcf_eval(int nf, const McfDesc *desc, const double *blob, int q, int nz, const double *z, double *out,
+                     cudaStream_t s) {
+  if (nf <= 0 || nz <= 0) return;
+  if (q > 32) fail(QED_ERR_UNSUPPORTED, "matrix continued fractions of more than 32 orbitals");
+  k_mcf_eval<<<dim3(nz, nf), 256, 0, s>>>(desc, blob, q, nz, z, out);
   QED_LAUNCH();
 }
 

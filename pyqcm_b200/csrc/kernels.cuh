@@ -252,5 +252,18 @@ void launch_qmatrix_gf(int L, int M, const double *e, const double *V, int nz, c
 // fractions with offsets off[f] into a/b and lengths len[f].
 void launch_cf_eval(int nf, const int *off, const int *len, const double *a, const double *b,
                     int nz, const double *z, double *F, cudaStream_t s);
+// Matrix continued fractions (matrix_continued_fraction::evaluate,
+// src_ed/matrix_continued_fraction.hpp:137-187): for fraction f with M floors of
+// p x p blocks (A_j, B_j row-major at blob + offA / offB + j p^2) and weight W
+// (p x q row-major at blob + offW), G_f(z) = W^T F_0 W with F_M = 0 and
+// F_j = (z - A_j - B_j^T F_{j+1} B_j)^{-1}. out[((f * nz + k) * q + a) * q + b]
+// = G_f(z_k)(a, b), or G_f(z_k)(b, a) when transpose is set. p <= 16, q <= 32.
+struct McfDesc {
+  int M = 0, p = 0, q = 0, transpose = 0;
+  long long offA = 0, offB = 0, offW = 0;
+};
+constexpr int kMcfMaxP = 16;
+void launch_mcf_eval(int nf, const McfDesc *desc, const double *blob, int q, int nz, const double *z, double *out,
+                     cudaStream_t s);
 
 }  // namespace qed

@@ -1036,6 +1036,193 @@ bool block_lanczos_qmatrix(const KrylovOp &H, Workspace &ws, std::vector<DevBuf<
 
 }  // namespace
 
+int mgs_qr(size_t D, int p, double *X, double tol, std::vector<double> &R, Workspace &ws) {
+  R.assign((size_t)p * p, 0.0);
+  cudaStream_t s = ws.stream;
+  for (int l = 0; l < p; ++l) {
+    double *xl = X + (size_t)l * D;
+    for (int k = 0; k < l; ++k) {
+      VecList one;
+      one.n = 1;
+      one.v[0] = X + (size_t)k * D;
+      const int nb = launch_dots(D, xl, 1.0, 0, one, ws.red, s);
+      const double z = ws.sums(nb, 1)[0];
+      R[(size_t)k * p + l] = z;
+      launch_axpby(D, 1.0, xl, -z, X + (size_t)k * D, 0, ws.red, s);
+    }
+    VecList self;
+    self.n = 1;
+    self.v[0] = xl;
+    const int nb = launch_dots(D, xl, 1.0, 0, self, ws.red, s);
+    const double nrm = std::sqrt(ws.sums(nb, 1)[0]);
+    if (nrm < tol) return l;
+    R[(size_t)l * p + l] = nrm;
+    launch_scale(D, xl, 1.0 / nrm, s);
+  }
+  return p;
+}
+
+void block_lanczos_mcf(const KrylovOp &H, Workspace &ws, const double *Q0, int p, bool qr, McfFloors &out) {
+  out = McfFloors();
+  out.p = p;
+  const size_t D = H.D;
+  if (D == 0 || p < 1 || p > 16) fail(QED_ERR_ARGUMENT, "block Lanczos: block size outside [1, 16]");
+  cudaStream_t s = ws.stream;
+  const double accur_def = opt_double("accur_deflation");
+  double accur_bl = opt_double("accur_band_lanczos");
+  if (accur_bl < 0.0) accur_bl = 0.0;
+  int M0 = (int)(14 * p * std::log(1.0 * D));
+  if (M0 > opt_int("max_iter_BL")) M0 = (int)opt_int("max_iter_BL");
+  constexpr double kPivotMin = 1e-4;
+  const int pp = p * p;
+  const int max_blocks = 4096;
+  DevBuf<double> part((size_t)max_blocks * pp), dsmall(2 * (size_t)pp);
+  double *dG = dsmall.p, *dM = dsmall.p + pp;
+  std::vector<double> hG(pp);
+  auto gram_to_host = [&](int nb) {
+    launch_finalize_ld(part.p, nb, pp, pp, dG, s);
+    QED_CUDA(cudaMemcpyAsync(hG.data(), dG, pp * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ws.sync();
+  };
+  auto upload = [&](const std::vector<double> &h) {
+    QED_CUDA(cudaMemcpyAsync(dM, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  };
+  const BlockIn none;
+  auto block = [&](double *base) {
+    BlockOut o;
+    for (int c = 0; c < p; ++c) o.v[c] = base + (size_t)c * D;
+    return o;
+  };
+  auto in = [&](double *base) {
+    BlockIn i;
+    for (int c = 0; c < p; ++c) i.v[c] = base + (size_t)c * D;
+    return i;
+  };
+  const size_t bl = D * (size_t)p;
+  DevBuf<double> b0(bl), b1(bl), b2(bl), b3(bl);
+  double *Qprev = b0.p, *Qcur = b1.p, *Z = b2.p, *Tmp = b3.p;
+  QED_CUDA(cudaMemcpyAsync(Qcur, Q0, bl * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  std::vector<double> Aj(pp), Bj(pp), Bt(pp), R1, R1i, R2, R2i;
+  double ev_old = 1e12;
+  BandLowest lowest;
+  const int bw = qr ? p : 2 * p - 1;  // half-bandwidth of the projected matrix
+  // convergence test on the (j + 1) p leading rows (blockLanczos step 6)
+  auto converged = [&](int j) {
+    if (!((j + 1) >= 2 * p && (j + 1) % p == 0)) return false;
+    const int n = (j + 1) * p;
+    auto T = [&](int r, int c) -> double {  // r >= c, r - c <= bw
+      const int I = r / p, J = c / p;
+      if (I == J) return out.A[(size_t)I * pp + (r % p) * p + (c % p)];
+      if (I == J + 1) return out.B[(size_t)J * pp + (r % p) * p + (c % p)];
+      return 0.0;
+    };
+    std::vector<double> Bb((size_t)n * (bw + 1), 0.0);
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k <= std::min(i, bw); ++k) Bb[(size_t)i * (bw + 1) + k] = T(i, i - k);
+    double ev0 = 0.0;
+    if (!band_lowest(n, bw, Bb, lowest, &ev0)) {
+      std::vector<double> full((size_t)n * n, 0.0), evs;
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k <= std::min(i, bw); ++k) {
+          full[(size_t)i + (size_t)n * (i - k)] = Bb[(size_t)i * (bw + 1) + k];
+          full[(size_t)(i - k) + (size_t)n * i] = Bb[(size_t)i * (bw + 1) + k];
+        }
+      if (!band_eigenvalues(n, bw, full, evs)) fail(QED_ERR_INTERNAL, "projected eigensolver failed");
+      ev0 = evs[0];
+      lowest.valid = false;
+    }
+    const double delta = std::fabs(ev0 - ev_old);
+    ev_old = ev0;
+    return delta < accur_bl;
+  };
+  PhaseScope ps_loop(kPhBlockLoop);
+  for (int j = 0; j < M0; ++j) {
+    // Z = H Q_j - Q_{j-1} B_{j-1}^T, A_j = Q_j^T Z (upper triangle, mirrored)
+    H.apply_block(p, in(Qcur), block(Z), ws.red, s);
+    int nb;
+    if (j > 0) {
+      for (int r = 0; r < p; ++r)
+        for (int c = 0; c < p; ++c) Bt[(size_t)r * p + c] = Bj[(size_t)c * p + r];
+      upload(Bt);
+      nb = launch_bl_update(D, p, 1.0, block(Z), -1.0, in(Qprev), dM, 2, in(Qcur), part.p, max_blocks, s);
+    } else {
+      nb = launch_bl_update(D, p, 1.0, block(Z), 0.0, none, nullptr, 2, in(Qcur), part.p, max_blocks, s);
+    }
+    gram_to_host(nb);
+    for (int l = 0; l < p; ++l)
+      for (int k = 0; k <= l; ++k) Aj[(size_t)k * p + l] = Aj[(size_t)l * p + k] = hG[(size_t)k * p + l];
+    out.A.insert(out.A.end(), Aj.begin(), Aj.end());
+    // Z -= Q_j A_j, with the Gram matrix of the result
+    upload(Aj);
+    nb = launch_bl_update(D, p, 1.0, block(Z), -1.0, in(Qcur), dM, 1, none, part.p, max_blocks, s);
+    gram_to_host(nb);
+    bool singular = false;
+    double *Qnext = Qprev;  // Q_{j-1}'s buffer is free once Z has been formed
+    if (qr) {
+      bool chol = cholesky_upper(p, hG.data(), R1, R1i);
+      for (int i = 0; i < p && chol; ++i) chol = R1[(size_t)i * p + i] >= kPivotMin;
+      if (chol) {  // Cholesky QR twice: Z -> Tmp -> Q_{j+1}; B_j = R2 R1
+        upload(R1i);
+        nb = launch_bl_update(D, p, 0.0, block(Tmp), 1.0, in(Z), dM, 1, none, part.p, max_blocks, s);
+        gram_to_host(nb);
+        chol = cholesky_upper(p, hG.data(), R2, R2i);
+        if (chol) {
+          upload(R2i);
+          launch_bl_update(D, p, 0.0, block(Qnext), 1.0, in(Tmp), dM, 0, none, part.p, max_blocks, s);
+          std::fill(Bj.begin(), Bj.end(), 0.0);
+          for (int i = 0; i < p; ++i)
+            for (int c = i; c < p; ++c) {
+              double t = 0.0;
+              for (int k = i; k <= c; ++k) t += R2[(size_t)i * p + k] * R1[(size_t)k * p + c];
+              Bj[(size_t)i * p + c] = t;
+            }
+        }
+      }
+      if (!chol) {  // the reference's column-by-column QR, which may deflate
+        const int l = mgs_qr(D, p, Z, accur_def, Bj, ws);
+        if (l < p) {
+          singular = true;
+          QED_CUDA(cudaMemsetAsync(Z + (size_t)l * D, 0, (size_t)(p - l) * D * sizeof(double), s));
+        }
+        Qnext = Z;
+      }
+      out.B.insert(out.B.end(), Bj.begin(), Bj.end());
+      out.M = j + 1;
+      if (converged(j) || singular) break;
+    } else {
+      // polar factor: G = V diag(d) V^T, B_j = V d^(1/2) V^T, Q_{j+1} = Z V d^(-1/2) V^T
+      std::vector<double> d, V;
+      if (!sym_eig(p, hG, d, &V)) fail(QED_ERR_INTERNAL, "block Lanczos: Gram eigensolver failed");
+      for (int m = 0; m < p; ++m)
+        if (d[m] < accur_def * accur_def) singular = true;
+      std::vector<double> Binv(pp, 0.0);
+      for (int r = 0; r < p; ++r)
+        for (int c = 0; c < p; ++c) {
+          double b = 0.0, bi = 0.0;
+          for (int m = 0; m < p; ++m) {
+            const double vv = V[(size_t)r + (size_t)p * m] * V[(size_t)c + (size_t)p * m];
+            b += vv * std::sqrt(std::max(d[m], 0.0));
+            if (!singular) bi += vv / std::sqrt(d[m]);
+          }
+          Bj[(size_t)r * p + c] = b;
+          Binv[(size_t)r * p + c] = bi;
+        }
+      out.B.insert(out.B.end(), Bj.begin(), Bj.end());
+      out.M = j + 1;
+      if (singular) break;
+      upload(Binv);
+      launch_bl_update(D, p, 0.0, block(Qnext), 1.0, in(Z), dM, 0, none, part.p, max_blocks, s);
+      if (converged(j)) break;
+    }
+    // Q_{j-1} <- Q_j, Q_j <- Q_{j+1}
+    double *freed = Qprev;
+    Qprev = Qcur;
+    if (Qnext == Z) Z = freed;  // the MGS path left Q_{j+1} in Z's buffer
+    Qcur = Qnext;
+  }
+  ws.sync();
+}
+
 bool band_lanczos_qmatrix(const KrylovOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
                           std::vector<double> &evals, std::vector<double> &Q, int &Mout) {
   const size_t D = H.D;

@@ -149,4 +149,34 @@ void lanczos_green(const KrylovOp &H, Workspace &ws, double *psi, double *q,
 bool band_lanczos_qmatrix(const KrylovOp &H, Workspace &ws, std::vector<DevBuf<double>> &phi,
                           std::vector<double> &evals, std::vector<double> &Q, int &M);
 
+// Modified Gram-Schmidt QR, in place, of the p device vectors X + c * D
+// (c < p), as the reference orthonormalises a start block
+// (src_ed/model_instance.hpp:888-907): column l loses its projections on the
+// columns before it one at a time, then is normalised. Stops at the first
+// column whose norm falls below tol and returns its index (p if none); R
+// (p x p, row-major, upper triangular) holds the coefficients of the columns
+// before it, zeros elsewhere.
+int mgs_qr(size_t D, int p, double *X, double tol, std::vector<double> &R, Workspace &ws);
+
+// Floors of a block Lanczos run: M diagonal blocks A_j and off-diagonal blocks
+// B_j, p x p row-major each (B_{M-1} is the truncation residual).
+struct McfFloors {
+  int p = 0, M = 0;
+  std::vector<double> A, B;
+};
+
+// Block Lanczos for matrix continued fractions from the p orthonormal device
+// vectors Q0 + c * D (left unchanged): blockLanczos (qr = true: upper-triangular
+// B_j by QR of the residual block) or blockLanczosSVD (qr = false: Hermitian
+// B_j = G^(1/2) by the eigensystem of the residual's Gram matrix G), with the
+// reference's step count min(14 p ln D, max_iter_BL), its convergence test (the
+// lowest eigenvalue of the projected block tridiagonal matrix every p steps from
+// step 2p, accur_band_lanczos) and its deflation rules (a QR column or a Gram
+// eigenvalue below accur_deflation (squared) ends the run)
+// (src_ed/Hamiltonian/Lanczos.hpp:426-571, 597-768). The residual block's QR is
+// a Cholesky QR done twice on the device; a Cholesky pivot below 1e-4 sends that
+// step through mgs_qr, which then decides a deflation exactly as the reference's
+// column-by-column QR does.
+void block_lanczos_mcf(const KrylovOp &H, Workspace &ws, const double *Q0, int p, bool qr, McfFloors &out);
+
 }  // namespace qed

@@ -67,6 +67,39 @@ def test_errors_follow_reference_conventions(qed, fresh):
     assert e.value.code == 1
 
 
+def test_matrix_continued_fraction_options(qed, fresh):
+    """GF_method 'M' (matrix continued fractions from block Lanczos) is
+    accepted; combining the electron and hole fractions (combine_mcf, with 'M'
+    or 'L') is refused with the unsupported status when the instance is made,
+    as is 'M' for a model with generators once it is solved."""
+    suffix, label = fresh()
+    qed.new_model("mcf" + suffix, 4, 0)
+    qed.new_operator("mcf" + suffix, "t", "one-body", [(0, 1, 1.0), (4, 5, 1.0)])
+    qed.new_operator("mcf" + suffix, "U", "interaction", [(i, i + 4, 1.0) for i in range(4)])
+    try:
+        qed.set_global_parameter("GF_method", "M")
+        qed.new_model_instance("mcf" + suffix, {"t": -1.0, "U": 2.0}, "R0:N4:S0", label)
+        qed.set_global_parameter("combine_mcf", True)
+        for gf in ("M", "L"):
+            qed.set_global_parameter("GF_method", gf)
+            with pytest.raises(qed.QEDError) as e:
+                qed.new_model_instance("mcf" + suffix, {"t": -1.0, "U": 2.0}, "R0:N4:S0", label + 1)
+            assert e.value.code == qed.QED_ERR_UNSUPPORTED and "combine_mcf" in str(e.value)
+    finally:
+        qed.set_global_parameter("combine_mcf", False)
+        qed.set_global_parameter("GF_method", "L")
+    from tests.helpers import c2v_golden, c2v_problem
+    prob = c2v_problem(c2v_golden(), True)
+    qed.set_global_parameter("GF_method", "M")
+    try:
+        qed.load_problem(prob, label + 2, model_name="c2v_mcf" + suffix)
+        with pytest.raises(qed.QEDError) as e:
+            qed.ground_state_solve(label + 2)
+        assert e.value.code == qed.QED_ERR_UNSUPPORTED and "'M'" in str(e.value)
+    finally:
+        qed.set_global_parameter("GF_method", "L")
+
+
 def test_unknown_label_and_options(qed):
     qed.set_global_parameter("accur_lanczos", 1e-12)
     assert qed.get_global_double("accur_lanczos") == 1e-12

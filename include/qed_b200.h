@@ -107,6 +107,27 @@ int qed_ground_state_solve_batch(const int *labels, int n, int threads, double *
 /* Batched Green_function_solve over labels[0..n), same threading rules. */
 int qed_Green_function_solve_batch(const int *labels, int n, int threads);
 
+/* No counterpart in the reference (its batching is the OpenMP loop of the
+ * lattice layer): the batched solves as an asynchronous work queue. A batch of
+ * instances is handed to a background host thread, which runs
+ * qed_ground_state_solve_batch (what = QED_BATCH_GROUND_STATE) or
+ * qed_Green_function_solve_batch (QED_BATCH_GREEN_FUNCTION: ground states
+ * first where needed) on `threads` threads; the call returns at once with a
+ * ticket (> 0). While the batch runs, other calls on its instances wait for
+ * it (each instance is locked for the batch); results are then read through
+ * the per-instance entries (qed_ground_state_solve returns the solved state).
+ * Batches run concurrently with one another, each on its own streams. */
+#define QED_BATCH_GROUND_STATE 1
+#define QED_BATCH_GREEN_FUNCTION 2
+int qed_batch_submit(const int *labels, int n, int what, int threads, long long *ticket);
+/* *done = 0 while the batch runs (returns QED_OK); once it has finished,
+ * *done = 1, the ticket is released and the batch's status is returned (its
+ * first failure's message via qed_last_error). Unknown ticket: QED_ERR_ARGUMENT. */
+int qed_batch_poll(long long ticket, int *done);
+/* As qed_batch_poll, after waiting up to timeout_ms milliseconds for the
+ * batch to finish (timeout_ms < 0: without limit). */
+int qed_batch_wait(long long ticket, int timeout_ms, int *done);
+
 /* ED::Green_function_solve (src_ed/qcm_ED.hpp:122 -> src_ed/model_instance.hpp:517-555):
  * band-Lanczos Q-matrix (GF_method 'L') or continued fractions ('F'). */
 int qed_Green_function_solve(int label);

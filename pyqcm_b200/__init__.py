@@ -31,7 +31,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libqed_b200.so")
 
 QED_OK = 0
+QED_ERR_ARGUMENT = 1
 QED_ERR_UNSUPPORTED = 6
+QED_ERR_NO_DEVICE = 7
 _CODES = {1: "argument", 2: "lanczos", 3: "qmatrix", 4: "cuda", 5: "memory", 6: "unsupported",
           7: "no-device", 8: "internal"}
 
@@ -259,6 +261,44 @@ def Green_function_solve_batch(labels, threads: int = 0):
     L.qed_Green_function_solve_batch.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_int]
     L.qed_Green_function_solve_batch.restype = C.c_int
     _check(L.qed_Green_function_solve_batch(lab.ctypes.data_as(C.POINTER(C.c_int)), len(lab), threads))
+
+
+QED_BATCH_GROUND_STATE = 1
+QED_BATCH_GREEN_FUNCTION = 2
+
+
+def batch_submit(labels, what: int = QED_BATCH_GREEN_FUNCTION, threads: int = 0) -> int:
+    """Hands the ground states (what = QED_BATCH_GROUND_STATE) or Green functions
+    (QED_BATCH_GREEN_FUNCTION) of `labels` to a background thread and returns a
+    ticket at once (qed_batch_submit)."""
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    t = C.c_longlong()
+    L = lib()
+    L.qed_batch_submit.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int, C.POINTER(C.c_longlong)]
+    L.qed_batch_submit.restype = C.c_int
+    _check(L.qed_batch_submit(lab.ctypes.data_as(C.POINTER(C.c_int)), len(lab), what, threads, C.byref(t)))
+    return t.value
+
+
+def batch_poll(ticket: int) -> bool:
+    """True once the batch has finished (its failure, if any, is raised then and
+    the ticket released); False while it runs."""
+    d = C.c_int()
+    L = lib()
+    L.qed_batch_poll.argtypes = [C.c_longlong, C.POINTER(C.c_int)]
+    L.qed_batch_poll.restype = C.c_int
+    _check(L.qed_batch_poll(ticket, C.byref(d)))
+    return bool(d.value)
+
+
+def batch_wait(ticket: int, timeout: float | None = None) -> bool:
+    """Waits for the batch (at most `timeout` seconds if given); as batch_poll."""
+    d = C.c_int()
+    L = lib()
+    L.qed_batch_wait.argtypes = [C.c_longlong, C.c_int, C.POINTER(C.c_int)]
+    L.qed_batch_wait.restype = C.c_int
+    _check(L.qed_batch_wait(ticket, -1 if timeout is None else int(timeout * 1000), C.byref(d)))
+    return bool(d.value)
 
 
 def Green_function_dimension(label: int = 0) -> int:

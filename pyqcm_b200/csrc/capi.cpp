@@ -1,6 +1,7 @@
 // The C ABI of include/qed_b200.h: registries of models / instances / sector
 // Hamiltonians, and the error convention (status code + per-thread message).
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <condition_variable>
 #include <cstring>
@@ -491,6 +492,109 @@ int qed_Green_function_solve_batch(const int *labels, int n, int threads) {
   if (rc != QED_OK) return rc;
   return batch_green_functions(*b, threads);
 }
+
+}  // extern "C"
+
+namespace {
+
+// The asynchronous batch queue: one background thread per submitted batch.
+struct AsyncBatch {
+  std::thread th;
+  std::mutex m;
+  std::condition_variable cv;
+  bool done = false;
+  int status = QED_OK;
+  std::string msg;
+};
+
+struct AsyncBatches {
+  std::mutex m;
+  long long next = 1;
+  std::map<long long, std::shared_ptr<AsyncBatch>> jobs;
+  ~AsyncBatches() {  // batches still running at exit finish first
+    for (auto &j : jobs)
+      if (j.second->th.joinable()) j.second->th.join();
+  }
+};
+
+AsyncBatches &async_batches() {
+  static AsyncBatches b;
+  return b;
+}
+
+// *done and the batch's status once it has finished (the ticket is then released)
+int async_result(long long ticket, int timeout_ms, int *done) {
+  if (!done) {
+    t_err = "null argument";
+    return QED_ERR_ARGUMENT;
+  }
+  std::shared_ptr<AsyncBatch> job;
+  {
+    std::lock_guard<std::mutex> l(async_batches().m);
+    auto it = async_batches().jobs.find(ticket);
+    if (it == async_batches().jobs.end()) {
+      t_err = "unknown batch ticket " + std::to_string(ticket);
+      return QED_ERR_ARGUMENT;
+    }
+    job = it->second;
+  }
+  {
+    std::unique_lock<std::mutex> l(job->m);
+    if (timeout_ms < 0) job->cv.wait(l, [&] { return job->done; });
+    else if (timeout_ms > 0) job->cv.wait_for(l, std::chrono::milliseconds(timeout_ms), [&] { return job->done; });
+    *done = job->done ? 1 : 0;
+    if (!job->done) return QED_OK;
+  }
+  job->th.join();
+  {
+    std::lock_guard<std::mutex> l(async_batches().m);
+    async_batches().jobs.erase(ticket);
+  }
+  if (job->status != QED_OK) t_err = job->msg;
+  return job->status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qed_batch_submit(const int *labels, int n, int what, int threads, long long *ticket) {
+  if ((n > 0 && !labels) || !ticket) {
+    t_err = "null argument";
+    return QED_ERR_ARGUMENT;
+  }
+  if (what != QED_BATCH_GROUND_STATE && what != QED_BATCH_GREEN_FUNCTION) {
+    t_err = "qed_batch_submit: what must be QED_BATCH_GROUND_STATE or QED_BATCH_GREEN_FUNCTION";
+    return QED_ERR_ARGUMENT;
+  }
+  std::vector<int> lab(labels, labels + std::max(n, 0));
+  for (int x : lab)  // unknown labels fail here, before anything runs
+    if (int rc = guarded([&] { instance(x); }); rc != QED_OK) return rc;
+  auto job = std::make_shared<AsyncBatch>();
+  std::lock_guard<std::mutex> l(async_batches().m);
+  const long long t = async_batches().next++;
+  job->th = std::thread([job, lab, what, threads] {
+    int rc;
+    if (what == QED_BATCH_GROUND_STATE) {
+      std::vector<double> e(lab.size());
+      rc = qed_ground_state_solve_batch(lab.data(), (int)lab.size(), threads, e.data());
+    } else {
+      rc = qed_Green_function_solve_batch(lab.data(), (int)lab.size(), threads);
+    }
+    std::lock_guard<std::mutex> lj(job->m);
+    job->status = rc;
+    if (rc != QED_OK) job->msg = t_err;
+    job->done = true;
+    job->cv.notify_all();
+  });
+  async_batches().jobs[t] = job;
+  *ticket = t;
+  return QED_OK;
+}
+
+int qed_batch_poll(long long ticket, int *done) { return async_result(ticket, 0, done); }
+
+int qed_batch_wait(long long ticket, int timeout_ms, int *done) { return async_result(ticket, timeout_ms, done); }
 
 int qed_Green_function_solve(int label) {
   return guarded([&] {

@@ -100,6 +100,33 @@ def test_matrix_continued_fraction_options(qed, fresh):
         qed.set_global_parameter("GF_method", "L")
 
 
+def test_async_batch_queue_host_logic(qed, fresh):
+    """qed_batch_submit / poll / wait: unknown labels and a bad kind fail at
+    submission, unknown tickets at poll; a submitted batch finishes (here, with
+    no device, with the no-device status, which the wait returns once and then
+    releases the ticket)."""
+    suffix, label = fresh()
+    with pytest.raises(qed.QEDError) as e:
+        qed.batch_submit([987655], qed.QED_BATCH_GROUND_STATE)
+    assert e.value.code == qed.QED_ERR_ARGUMENT
+    qed.new_model("ab" + suffix, 4, 0)
+    qed.new_operator("ab" + suffix, "t", "one-body", [(0, 1, 1.0), (4, 5, 1.0), (1, 2, 1.0), (5, 6, 1.0)])
+    qed.new_operator("ab" + suffix, "U", "interaction", [(i, i + 4, 1.0) for i in range(4)])
+    qed.new_model_instance("ab" + suffix, {"t": -1.0, "U": 2.0}, "R0:N4:S0", label)
+    with pytest.raises(qed.QEDError) as e:
+        qed.batch_submit([label], 7)
+    assert e.value.code == qed.QED_ERR_ARGUMENT
+    t = qed.batch_submit([label], qed.QED_BATCH_GREEN_FUNCTION, threads=2)
+    assert t > 0
+    try:
+        assert qed.batch_wait(t, timeout=600)
+    except qed.QEDError as err:  # no GPU here: the batch's own status comes back
+        assert err.code == qed.QED_ERR_NO_DEVICE, err
+    with pytest.raises(qed.QEDError) as e:
+        qed.batch_poll(t)
+    assert e.value.code == qed.QED_ERR_ARGUMENT
+
+
 def test_unknown_label_and_options(qed):
     qed.set_global_parameter("accur_lanczos", 1e-12)
     assert qed.get_global_double("accur_lanczos") == 1e-12

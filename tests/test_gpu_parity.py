@@ -254,6 +254,47 @@ def test_batched_solves_match_reference(qed, oracle, fresh):
     assert np.sum(errs >= 1e-8) <= 1, errs
 
 
+def test_async_batch_queue(qed, oracle, fresh):
+    """The asynchronous work queue: two batches (ground states of one half,
+    Green functions of the other) submitted at once run on background threads
+    while this thread solves the same problems with the reference; polling
+    returns while they run, the results then match the reference (G of random
+    clusters to 1e-8 but one instance at the deflation threshold, as in the
+    blocking batched test) and the tickets are released."""
+    import time
+    probs = W.random_batch(10, seed=91, geoms=[(2, 2), (2, 3), (2, 4), (8, 1)])
+    labels = []
+    for p in probs:
+        suffix, label = fresh()
+        load_both(qed, oracle, p, suffix, label, fmt="F")
+        labels.append(label)
+    set_both(qed, oracle, GF_method="L")
+    t_gs = qed.batch_submit(labels[:5], qed.QED_BATCH_GROUND_STATE, threads=3)
+    t_gf = qed.batch_submit(labels[5:], qed.QED_BATCH_GREEN_FUNCTION, threads=3)
+    z = W.matsubara(64)
+    ref = [(oracle.ground_state(lab), oracle.green_function(lab, z)) for lab in labels]
+    polls = 0
+    pending = {t_gs, t_gf}
+    while pending:
+        for t in list(pending):
+            if qed.batch_poll(t):
+                pending.discard(t)
+        polls += 1
+        time.sleep(0.01)
+    assert polls >= 1
+    for t in (t_gs, t_gf):
+        with pytest.raises(qed.QEDError):
+            qed.batch_poll(t)
+    errs = []
+    for lab, ((e_ref, sec_ref), G2) in zip(labels, ref):
+        e, sec = qed.ground_state_solve(lab)
+        assert abs(e - e_ref) <= 1e-10 * max(1.0, abs(e_ref)) and sec == sec_ref, (lab, e, e_ref)
+        errs.append(np.max(np.abs(qed.Green_function(z, label=lab) - G2)))
+    errs = np.array(errs)
+    assert np.max(errs) < 5e-7, errs
+    assert np.sum(errs >= 1e-8) <= 1, errs
+
+
 # Non-factorized formats ('S' here): sectors below max_dim_full (256) are
 # diagonalised densely on both sides (Hamiltonian_Dense), which keeps every
 # degenerate ground state of a sector; larger sectors run Lanczos.

@@ -398,6 +398,12 @@ int qed_mlp_gradients(void *handle, int rows, const float *x, const float *t, fl
  * batches (a multiple of 16 rows); per epoch, the loss of its last batch */
 int qed_mlp_train(void *handle, int rows, const float *x, const float *t, int epochs, int batch, float lr,
                   unsigned long long seed, float *epoch_loss);
+/* The network's matrix product on its own: C[M][N] = A[M][K] B[N][K]^T with A, B
+ * given as BF16 bit patterns (host arrays, K contiguous) and C in FP32, computed
+ * by the tcgen05 kernel of the surrogate (fp32 accumulation in tensor memory).
+ * K and N multiples of 16. No counterpart in the reference; it lets a test check
+ * the tensor-core path on shapes the network does not use. */
+int qed_mlp_tensor_product(int M, int N, int K, const uint16_t *A, const uint16_t *B, float *C);
 
 #ifdef __cplusplus
 }

@@ -5,16 +5,15 @@
 // Arithmetic: weights and activations enter the matrix products in BF16 on
 // the tensor cores with FP32 accumulation; biases, pre-activations, gradients,
 // the loss and Adam's master weights and moments are FP32. Every matrix
-// product is one kernel of 16 x 16 x 16 BF16 tensor-core tiles (one warp per
-// 32 x 32 output tile); sizes are padded to multiples of 16 (the input width
-// to 16 with zero columns).
+// product is one tcgen05 kernel (128 x BN tiles accumulated in tensor memory,
+// operands staged in shared memory); sizes are padded to multiples of 16 (the
+// input width to 16 with zero columns).
 //
 // One training step (forward, backward, Adam) is a fixed sequence of kernels
 // on the network's stream; the steps of an epoch are captured once into a
 // CUDA graph and replayed, the epoch's shuffled data being gathered into the
 // same device buffers before each replay.
 #include <cuda_bf16.h>
-#include <mma.h>
 
 #include <algorithm>
 #include <cmath>
@@ -29,66 +28,254 @@
 #include "common.hpp"
 #include "qed_b200.h"
 
-using namespace nvcuda;
 typedef __nv_bfloat16 bf16;
 
 namespace qed {
 namespace {
 
-constexpr int kTile = 16;
-constexpr int kGemmWarps = 4;  // a CTA: 2 x 2 warps, 64 x 64 outputs
-
 inline int pad16(int x) { return (x + 15) / 16 * 16; }
 
-// C[M x N] (fp32, row-major, ldc) (+)= op(A) op(B), op(A) M x K, op(B) K x N.
-// TA: A stored K x M (A^T row-major), else M x K row-major. TB: B stored N x K,
-// else K x N row-major. M, N, K multiples of 16; leading dimensions multiples of 16.
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(kGemmWarps * 32) k_mlp_gemm(int M, int N, int K, const bf16 *__restrict__ A,
-                                                               int lda, const bf16 *__restrict__ B, int ldb,
-                                                               float *__restrict__ C, int ldc, int accumulate) {
-  using LA = typename std::conditional<TA, wmma::col_major, wmma::row_major>::type;
-  using LB = typename std::conditional<TB, wmma::col_major, wmma::row_major>::type;
-  const int warp = threadIdx.x / 32;
-  const int m0 = (blockIdx.y * 2 + warp / 2) * 32, n0 = (blockIdx.x * 2 + warp % 2) * 32;
-  if (m0 >= M || n0 >= N) return;
-  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[2][2];
-  for (int i = 0; i < 2; ++i)
-    for (int j = 0; j < 2; ++j) {
-      const int mi = m0 + 16 * i, nj = n0 + 16 * j;
-      if (accumulate && mi < M && nj < N)
-        wmma::load_matrix_sync(acc[i][j], C + (size_t)mi * ldc + nj, ldc, wmma::mem_row_major);
-      else
-        wmma::fill_fragment(acc[i][j], 0.0f);
-    }
-  for (int k0 = 0; k0 < K; k0 += kTile) {
-    wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, LA> a[2];
-    wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, LB> b[2];
-    for (int i = 0; i < 2; ++i) {
-      const int mi = m0 + 16 * i;
-      if (mi < M) wmma::load_matrix_sync(a[i], TA ? A + (size_t)k0 * lda + mi : A + (size_t)mi * lda + k0, lda);
-    }
-    for (int j = 0; j < 2; ++j) {
-      const int nj = n0 + 16 * j;
-      if (nj < N) wmma::load_matrix_sync(b[j], TB ? B + (size_t)nj * ldb + k0 : B + (size_t)k0 * ldb + nj, ldb);
-    }
-    for (int i = 0; i < 2; ++i)
-      for (int j = 0; j < 2; ++j)
-        if (m0 + 16 * i < M && n0 + 16 * j < N) wmma::mma_sync(acc[i][j], a[i], b[j], acc[i][j]);
-  }
-  for (int i = 0; i < 2; ++i)
-    for (int j = 0; j < 2; ++j) {
-      const int mi = m0 + 16 * i, nj = n0 + 16 * j;
-      if (mi < M && nj < N) wmma::store_matrix_sync(C + (size_t)mi * ldc + nj, acc[i][j], ldc, wmma::mem_row_major);
-    }
+// ---- matrix products on the 5th-generation tensor cores (tcgen05) ----------
+//
+// One CTA of 128 threads computes a 128 x BN tile of C = A B^T (A: M x K, B: N x K,
+// both bf16 with K contiguous) into a TMEM accumulator (fp32, 128 lanes x BN
+// columns). Per round of 64 K-elements the CTA stages the A and B tiles in
+// shared memory with cp.async in the canonical K-major layout without swizzle
+// (8 x 8 core matrices of 128 contiguous bytes, core matrices adjacent in K 128
+// bytes apart, 8-row groups 1024 bytes apart); one elected thread then issues
+// the round's four 128 x BN x 16 tcgen05.mma (kind::f16, bf16 inputs, fp32
+// accumulation) and commits them to an mbarrier, which every thread waits on
+// (bounded) before the tiles are overwritten. The epilogue reads the
+// accumulator back with tcgen05.ld (each warp its 32 lanes = 32 rows).
+
+constexpr int kUmmaM = 128;       // rows of a tile = TMEM lanes (cta_group::1)
+constexpr int kUmmaBK = 64;       // K elements staged per round
+constexpr int kUmmaMaxBN = 128;   // columns of a tile
+constexpr int kUmmaThreads = 128;
+constexpr uint32_t kUmmaSbo = kUmmaBK / 8 * 128;  // bytes between 8-row groups
+constexpr uint32_t kUmmaLbo = 128;                // bytes between K-adjacent core matrices
+constexpr size_t kUmmaTileBytes = (size_t)kUmmaM * kUmmaBK * 2;
+// Dynamic shared memory per CTA: both tiles, the barrier and the TMEM address,
+// rounded up so that at most three CTAs share an SM (3 x 128 TMEM columns <= 512).
+constexpr size_t kUmmaSmem = 72 * 1024;
+
+// Set when a bounded wait for the tensor core gave up; read by the host.
+__device__ int g_mlp_wait_timeout = 0;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor (sm_100 format): start address, leading and
+// stride byte offsets (all >> 4), descriptor version 1 at bit 46, no swizzle.
+__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((kUmmaLbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((kUmmaSbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
+// Instruction descriptor of kind::f16: fp32 D (bits 4-5 = 1), bf16 A and B
+// (bits 7-9 and 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+
+// Waits for phase `parity` of the mbarrier; gives up after about two seconds.
+__device__ __forceinline__ bool umma_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((it & 255u) == 0) {
+      uint64_t t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      if (it == 0) t0 = t;
+      else if (t - t0 > 2000000000ull) {
+        atomicExch(&g_mlp_wait_timeout, 1);
+        return false;
+      }
+    }
+  }
+}
+
+// Stages rows [r0, r0 + rows_tile) x K-elements [k0, k0 + kc) of a row-major
+// bf16 matrix (leading dimension ld) in the canonical layout; rows at or past
+// `rows_total` are zero-filled.
+__device__ __forceinline__ void umma_stage(uint32_t sdst, const bf16 *src, int ld, int r0, int rows_tile,
+                                           int rows_total, int k0, int kc) {
+  const int chunks = kc >> 3;  // 16-byte chunks per row
+  for (int c = threadIdx.x; c < rows_tile * chunks; c += kUmmaThreads) {
+    const int r = c / chunks, q = c - r * chunks;
+    const bool in = r0 + r < rows_total;
+    const bf16 *g = src + (size_t)(in ? r0 + r : 0) * ld + k0 + 8 * q;
+    cp_async16(sdst + (uint32_t)(r >> 3) * kUmmaSbo + (uint32_t)q * kUmmaLbo + (uint32_t)(r & 7) * 16, g,
+               in ? 16 : 0);
+  }
+}
+
+// C[M x N] (fp32 row-major, ldc) (+)= A[M x K] B[N x K]^T. A and B are bf16
+// row-major with K contiguous (lda, ldb multiples of 8, 16-byte aligned rows);
+// K a multiple of 16; bn (columns per tile) a multiple of 16 in [16, 128].
+__global__ void __launch_bounds__(kUmmaThreads) k_umma_gemm(int M, int N, int K, const bf16 *__restrict__ A, int lda,
+                                                            const bf16 *__restrict__ B, int ldb, float *__restrict__ C,
+                                                            int ldc, int accumulate, int bn) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const uint32_t sa = smem_u32(sm), sb = sa + (uint32_t)kUmmaTileBytes;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + 2 * kUmmaTileBytes);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  const int m0 = blockIdx.x * kUmmaM, n0 = blockIdx.y * bn;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t ncols = bn <= 32 ? 32u : bn <= 64 ? 64u : 128u;  // a power of two >= 32
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 32) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = umma_idesc_bf16(kUmmaM, bn);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int k0 = 0; k0 < K; k0 += kUmmaBK) {
+    const int kc = min(kUmmaBK, K - k0);
+    umma_stage(sa, A, lda, m0, kUmmaM, M, k0, kc);
+    umma_stage(sb, B, ldb, n0, bn, N, k0, kc);
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor core's reads
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int kk = 0; kk < kc / 16; ++kk) {
+        const uint64_t ad = umma_smem_desc(sa + 2u * kUmmaLbo * (uint32_t)kk);
+        const uint64_t bd = umma_smem_desc(sb + 2u * kUmmaLbo * (uint32_t)kk);
+        const uint32_t acc = (k0 > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(bar))
+                   : "memory");
+    }
+    ok = __syncthreads_and(umma_wait(bar, phase));  // the MMAs have read the tiles
+    phase ^= 1u;
+    if (!ok) break;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const int row = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < bn; c0 += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < M) {
+        float *crow = C + (size_t)row * ldc + n0 + c0;
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (n0 + c0 + j < N) crow[j] = (accumulate ? crow[j] : 0.0f) + __uint_as_float(v[j]);
+      }
+    }
+  } else {
+    umma_wait(bar, phase ^ 1u);  // a commit still in flight has had its bounded chance to land
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+}
+
+// out[c][r] = in[r][c] for an R x Cn bf16 matrix (leading dimensions ld_in, ld_out).
+__global__ void k_transpose_bf16(int R, int Cn, const bf16 *__restrict__ in, int ld_in, bf16 *__restrict__ out,
+                                 int ld_out) {
+  __shared__ bf16 t[32][34];
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int r = r0 + i, c = c0 + threadIdx.x;
+    t[i][threadIdx.x] = (r < R && c < Cn) ? in[(size_t)r * ld_in + c] : __float2bfloat16_rn(0.0f);
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int c = c0 + i, r = r0 + threadIdx.x;
+    if (c < Cn && r < R) out[(size_t)c * ld_out + r] = t[threadIdx.x][i];
+  }
+}
+
+void transpose(int R, int Cn, const bf16 *in, int ld_in, bf16 *out, int ld_out, cudaStream_t s) {
+  k_transpose_bf16<<<dim3((Cn + 31) / 32, (R + 31) / 32), dim3(32, 8), 0, s>>>(R, Cn, in, ld_in, out, ld_out);
+  QED_LAUNCH();
+}
+
+void umma_setup() {
+  static bool done = false;  // the attribute is per function, once per process is enough
+  if (!done) {
+    QED_CUDA(cudaFuncSetAttribute(k_umma_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUmmaSmem));
+    done = true;
+  }
+}
+
+// Fails the call if a product's bounded wait for the tensor core gave up since
+// the last check (the flag is cleared for the next call).
+void check_umma_wait(cudaStream_t s) {
+  int flag = 0;
+  QED_CUDA(cudaStreamSynchronize(s));
+  QED_CUDA(cudaMemcpyFromSymbol(&flag, g_mlp_wait_timeout, sizeof(int)));
+  if (flag) {
+    const int zero = 0;
+    cudaMemcpyToSymbol(g_mlp_wait_timeout, &zero, sizeof(int));
+    fail(QED_ERR_CUDA, "mlp: a tensor-core product timed out waiting for its MMAs");
+  }
+}
+
+// C[M x N] (+)= A B^T on the tensor cores, A: M x K, B: N x K (K contiguous).
+void gemm_tn(int M, int N, int K, const bf16 *A, int lda, const bf16 *B, int ldb, float *C, int ldc, bool acc,
+             cudaStream_t s) {
+  if (M <= 0 || N <= 0 || K <= 0 || K % 16 || N % 16 || lda % 8 || ldb % 8)
+    fail(QED_ERR_ARGUMENT, "mlp: tensor-core product needs K and N multiples of 16 and 16-byte rows");
+  const int bn = std::min(N, kUmmaMaxBN);
+  dim3 grid((M + kUmmaM - 1) / kUmmaM, (N + bn - 1) / bn);
+  k_umma_gemm<<<grid, kUmmaThreads, kUmmaSmem, s>>>(M, N, K, A, lda, B, ldb, C, ldc, acc ? 1 : 0, bn);
+  QED_LAUNCH();
+}
+
+// C[M x N] (fp32, row-major, ldc) (+)= op(A) op(B), op(A) M x K, op(B) K x N.
+// TA: A stored K x M, else M x K row-major. TB: B stored N x K, else K x N
+// row-major. Operands not already K-contiguous are transposed into the
+// scratch buffers ta / tb first (each at least M*K / N*K elements).
 template <bool TA, bool TB>
 void gemm(int M, int N, int K, const bf16 *A, int lda, const bf16 *B, int ldb, float *C, int ldc, bool acc,
-          cudaStream_t s) {
-  dim3 grid((N + 63) / 64, (M + 63) / 64);
-  k_mlp_gemm<TA, TB><<<grid, kGemmWarps * 32, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc, acc ? 1 : 0);
-  QED_LAUNCH();
+          bf16 *ta, bf16 *tb, cudaStream_t s) {
+  if (TA) {
+    transpose(K, M, A, lda, ta, K, s);
+    A = ta;
+    lda = K;
+  }
+  if (!TB) {
+    transpose(K, N, B, ldb, tb, K, s);
+    B = tb;
+    ldb = K;
+  }
+  gemm_tn(M, N, K, A, lda, B, ldb, C, ldc, acc, s);
 }
 
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
@@ -220,6 +407,7 @@ struct MLP {
   DevBuf<bf16> X, H[3], dZh[3];
   DevBuf<float> T, Z[3], dZ[3], y, dy, lt;
   DevBuf<float> tmp;
+  DevBuf<bf16> ta, tb;  // transposed operands of the backward products
   DevBuf<int> perm;
   DevBuf<float> data_x, data_t;
   int n_data = 0;
@@ -248,6 +436,7 @@ struct MLP {
     k_in = pad16(nin);
     W = width;
     QED_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    umma_setup();
     const size_t sizes[8] = {(size_t)W * k_in, (size_t)W, (size_t)W * W, (size_t)W, (size_t)W * W, (size_t)W,
                              (size_t)W, 16};
     off.resize(8);
@@ -322,6 +511,8 @@ struct MLP {
     dy.alloc(cap);
     lt.alloc(cap);
     tmp.alloc((size_t)cap * 16);
+    ta.alloc((size_t)W * std::max(cap, W));
+    tb.alloc((size_t)W * std::max(cap, W));
   }
 
   // forward on rows [0, rows) of X (bf16, padded); y = network output
@@ -329,7 +520,7 @@ struct MLP {
     const bf16 *in = X.p;
     int kin = k_in;
     for (int l = 0; l < 3; ++l) {
-      gemm<false, true>(rows, W, kin, in, kin, Ph(2 * l), kin, Z[l].p, W, false, s);
+      gemm_tn(rows, W, kin, in, kin, Ph(2 * l), kin, Z[l].p, W, false, s);
       k_bias_gelu<<<blocks_for((size_t)rows * W), 256, 0, s>>>(rows, W, Z[l].p, P(2 * l + 1), H[l].p);
       QED_LAUNCH();
       in = H[l].p;
@@ -353,11 +544,11 @@ struct MLP {
       const bf16 *prev = l > 0 ? H[l - 1].p : X.p;
       const int kin = l > 0 ? W : k_in;
       // dW_l [W][kin] = dZ_l^T prev ; db_l = column sums of dZ_l
-      gemm<true, false>(W, kin, rows, dZh[l].p, W, prev, kin, Gr(2 * l), kin, false, s);
+      gemm<true, false>(W, kin, rows, dZh[l].p, W, prev, kin, Gr(2 * l), kin, false, ta.p, tb.p, s);
       k_colsum<<<(W + 255) / 256, 256, 0, s>>>(rows, W, dZ[l].p, nullptr, Gr(2 * l + 1));
       QED_LAUNCH();
       if (l > 0) {  // dH_{l-1} = dZ_l W_l, then through GELU'
-        gemm<false, false>(rows, W, W, dZh[l].p, W, Ph(2 * l), W, dZ[l - 1].p, W, false, s);
+        gemm<false, false>(rows, W, W, dZh[l].p, W, Ph(2 * l), W, dZ[l - 1].p, W, false, ta.p, tb.p, s);
         k_gelu_back<<<blocks_for((size_t)rows * W), 256, 0, s>>>(rows, W, dZ[l - 1].p, Z[l - 1].p, dZh[l - 1].p);
         QED_LAUNCH();
       }
@@ -461,7 +652,7 @@ int qed_mlp_forward(void *handle, int rows, const float *x, float *y) {
     h.load_rows(rows, x, nullptr);
     h.forward(qed::pad16(rows));
     QED_CUDA(cudaMemcpyAsync(y, h.y.p, rows * sizeof(float), cudaMemcpyDeviceToHost, h.s));
-    QED_CUDA(cudaStreamSynchronize(h.s));
+    qed::check_umma_wait(h.s);
   });
 }
 
@@ -475,7 +666,7 @@ int qed_mlp_gradients(void *handle, int rows, const float *x, const float *t, fl
     std::vector<float> lt(rows);
     QED_CUDA(cudaMemcpyAsync(grads, h.g.p, h.n_par * sizeof(float), cudaMemcpyDeviceToHost, h.s));
     QED_CUDA(cudaMemcpyAsync(lt.data(), h.lt.p, rows * sizeof(float), cudaMemcpyDeviceToHost, h.s));
-    QED_CUDA(cudaStreamSynchronize(h.s));
+    qed::check_umma_wait(h.s);
     double L = 0.0;
     for (float v : lt) L += v;
     *loss = (float)L;
@@ -544,13 +735,40 @@ int qed_mlp_train(void *handle, int rows, const float *x, const float *t, int ep
       QED_CUDA(cudaGraphLaunch(h.exec, h.s));
       if (epoch_loss) {  // the loss terms of the last batch of the epoch
         QED_CUDA(cudaMemcpyAsync(lt.data(), h.lt.p, batch * sizeof(float), cudaMemcpyDeviceToHost, h.s));
-        QED_CUDA(cudaStreamSynchronize(h.s));
+        qed::check_umma_wait(h.s);
         double L = 0.0;
         for (int i = 0; i < batch; ++i) L += lt[i];
         epoch_loss[ep] = (float)L;
       }
     }
-    QED_CUDA(cudaStreamSynchronize(h.s));
+    qed::check_umma_wait(h.s);
+  });
+}
+
+int qed_mlp_tensor_product(int M, int N, int K, const uint16_t *A, const uint16_t *B, float *C) {
+  return mlp_guarded([&] {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) qed::fail(QED_ERR_NO_DEVICE, "mlp: no CUDA device available");
+    if (M <= 0 || N <= 0 || K <= 0 || K % 16 || N % 16)
+      qed::fail(QED_ERR_ARGUMENT, "mlp: tensor product needs positive M and K, N multiples of 16");
+    cudaStream_t s = nullptr;
+    QED_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct Guard {
+      cudaStream_t s;
+      ~Guard() {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+      }
+    } guard{s};
+    qed::umma_setup();
+    qed::DevBuf<bf16> a((size_t)M * K), b((size_t)N * K);
+    qed::DevBuf<float> c((size_t)M * N);
+    QED_CUDA(cudaStreamSynchronize(qed::alloc_stream()));  // the allocations are usable on s
+    a.upload(reinterpret_cast<const bf16 *>(A), (size_t)M * K, s);
+    b.upload(reinterpret_cast<const bf16 *>(B), (size_t)N * K, s);
+    qed::gemm_tn(M, N, K, a.p, K, b.p, K, c.p, N, false, s);
+    c.download(C, (size_t)M * N, s);
+    qed::check_umma_wait(s);
   });
 }
 

@@ -27,6 +27,7 @@ def _lib():
             "qed_mlp_forward": [vp, C.c_int, fp, fp],
             "qed_mlp_gradients": [vp, C.c_int, fp, fp, fp, fp],
             "qed_mlp_train": [vp, C.c_int, fp, fp, C.c_int, C.c_int, C.c_float, C.c_ulonglong, fp],
+            "qed_mlp_tensor_product": [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), fp],
         }
         for k, a in sig.items():
             getattr(L, k).argtypes = a
@@ -46,6 +47,30 @@ def _check(rc):
 
 def _fp(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def to_bf16_bits(a) -> np.ndarray:
+    """BF16 bit patterns of a float array (round to nearest even), as uint16."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+    r = ((u >> 16) & 1) + 0x7FFF
+    return ((u + r) >> 16).astype(np.uint16)
+
+
+def from_bf16_bits(b) -> np.ndarray:
+    return (np.asarray(b, dtype=np.uint32) << 16).view(np.float32)
+
+
+def tensor_product(a_bits, b_bits) -> np.ndarray:
+    """C = A B^T on the surrogate's tcgen05 kernel; A (M x K) and B (N x K) as BF16
+    bit patterns (uint16), C in FP32."""
+    a_bits = np.ascontiguousarray(a_bits, dtype=np.uint16)
+    b_bits = np.ascontiguousarray(b_bits, dtype=np.uint16)
+    M, K = a_bits.shape
+    N = b_bits.shape[0]
+    c = np.empty((M, N), dtype=np.float32)
+    u16 = C.POINTER(C.c_uint16)
+    _check(_lib().qed_mlp_tensor_product(M, N, K, a_bits.ctypes.data_as(u16), b_bits.ctypes.data_as(u16), _fp(c)))
+    return c
 
 
 class MLP:

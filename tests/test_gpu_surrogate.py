@@ -53,3 +53,22 @@ def test_training_fits_a_smooth_function():
     rmse = np.sqrt(np.mean((net(xt) - f(xt)) ** 2))
     assert losses[-1] < 0.01 * losses[0]
     assert rmse < 0.02, rmse
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (100, 16, 16), (300, 256, 272), (256, 48, 4096), (16, 144, 80)])
+def test_tensor_product_matches_exact_products(M, N, K):
+    """The tcgen05 product on shapes with partial tiles (M not a multiple of 128,
+    N not a multiple of the 128-column tile, K not a multiple of the 64-element
+    round) against the exact products of the same BF16 inputs summed in float64.
+    Products of two BF16 numbers are exact in FP32, so the only difference is the
+    FP32 accumulation: bounded by K * 2^-24 * sum |a b| per entry."""
+    from pyqcm_b200 import surrogate as S
+    rng = np.random.default_rng(M * 7 + N * 3 + K)
+    a = S.to_bf16_bits(rng.standard_normal((M, K)).astype(np.float32))
+    b = S.to_bf16_bits(rng.standard_normal((N, K)).astype(np.float32))
+    c = S.tensor_product(a, b)
+    A = S.from_bf16_bits(a).astype(np.float64)
+    B = S.from_bf16_bits(b).astype(np.float64)
+    want = A @ B.T
+    bound = K * 2.0 ** -23 * (np.abs(A) @ np.abs(B).T) + 1e-30
+    assert np.all(np.abs(c - want) <= bound), float(np.max(np.abs(c - want) / bound))

@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: warm-up and timed H.v only (no e2e, clocks or CPU baseline)")
     ap.add_argument("--sector", default=None, help="sector of the 4x4 cluster to use (default R0:N16:S0)")
-    ap.add_argument("--workload", default="hv", choices=["hv", "batch", "baths", "vca"],
+    ap.add_argument("--workload", default="hv", choices=["hv", "batch", "baths", "vca", "cdmft"],
                     help="hv: H.v on the 4x4 cluster (default); batch: independent random clusters, "
                          "every sector, ground state + Green function; baths: 2x2 + 8-bath points; "
                          "vca: 2x5-cluster VCA, surrogate-guided against ED-only")
@@ -484,6 +484,7 @@ def secondary_lines(impl):
             out.append(line)
     if impl == "ours":
         out.append(vca_line(VCA_SECONDARY_POINTS, 400, 0))
+        out.append(cdmft_line())
     return out
 
 
@@ -502,6 +503,10 @@ def secondary_summary(lines):
                                                   "speedup_including_training", "breakeven_searches",
                                                   "max_omega_abs_diff", "max_grad_norm")}
             out["vca"]["training_points"] = ln["config"]["training_points"]
+        elif ln.get("metric", "").startswith("CDMFT"):
+            out["cdmft_bath_surrogate"] = {k: ln.get(k) for k in ("value", "plain_solves", "plain_seconds",
+                                                                  "speedup", "surrogate_total_seconds",
+                                                                  "breakeven_runs", "max_gamma_abs_diff")}
     return out
 
 
@@ -620,6 +625,78 @@ def vca_line(n_points, epochs, threads, Us=(5.0, 7.0, 9.0), local=0):
             "runs": runs}
 
 
+CDMFT_WORKLOAD = ("CDMFT on the square lattice (t=1) tiled by 2x2 plaquettes with eight bath orbitals "
+                  "(two per site; dim 924^2 = 853776 at half filling, mu=U/2), 16 bath parameters, "
+                  "Legendre grid (1, 10, 5, 10, 5), host k-sum on 16x16 points, Broyden iterations, "
+                  "least-squares bath fits with the exact Jacobian, converged when the bath moves less "
+                  "than 1e-5 (per parameter, over two iterations)")
+
+
+def cdmft_line(n_train=15, Us=(7.1, 7.7, 8.3, 8.9, 9.4), local=0):
+    """Surrogate-proposed against model-bath starts of CDMFT on the bath-point cluster:
+    training data (CDMFT converged by continuation in U), training, then per U the
+    ED solves and wall time of both runs to the same hybridisation function."""
+    import pyqcm_b200 as qed
+    from pyqcm_b200 import cdmft, lattice as LT
+    from pyqcm_b200 import workloads as W
+    qed.init(local)
+    qed.set_global_parameter("GF_method", "L")
+    names = [f"eb{b}_1" for b in range(8)] + [f"tb{b}_1" for b in range(8)]
+    rng = np.random.default_rng(7)
+    prob = W.cdmft_2x2_bath(rng.uniform(-2, 2, 8), rng.uniform(0.3, 1, 8), U=8.0)
+    model = LT.LatticeModel(prob)
+    canon = lambda x: cdmft.canonical_bath(x, list(range(8)), list(range(8, 16)), [b // 2 for b in range(8)])
+    args = dict(method="trf", accur=1e-5, maxiter=60, side=16)
+    box = (6.5, 10.0)
+    train_U = np.linspace(box[0], box[1], n_train)
+    x0 = np.array([prob.params[n] for n in names])
+    t0 = time.perf_counter()
+    ok, baths, iters = cdmft.converge_baths(model, names, ["U"], train_U[:, None], x0, canonical=canon,
+                                            label=910000, **args)
+    t_data = time.perf_counter() - t0
+    sur = cdmft.BathSurrogate(["U"], [box], names, seed=1)
+    t0 = time.perf_counter()
+    losses = sur.fit(train_U[ok, None], baths, epochs=800, seed=2)
+    t_train = time.perf_counter() - t0
+    runs = []
+    for k, U in enumerate(Us):
+        vals = dict(prob.params, U=U)
+        t0 = time.perf_counter()
+        plain = cdmft.CDMFT(model, names, values=vals, label=920000 + 100 * k, **args)
+        t_plain = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        start = sur.propose([U])
+        guided = cdmft.CDMFT(model, names, values=vals, start=start, label=930000 + 100 * k, **args)
+        t_guided = time.perf_counter() - t0
+        bd = cdmft.BathDistance(model, names, vals)
+        dg = float(np.max(np.abs(bd.gamma(plain.x, plain.grid.wr) - bd.gamma(guided.x, guided.grid.wr))))
+        runs.append({"U": U, "plain_solves": plain.n_solves, "surrogate_solves": guided.n_solves,
+                     "plain_s": t_plain, "surrogate_s": t_guided, "gamma_abs_diff": dg,
+                     "E0_abs_diff": abs(plain.E0 - guided.E0),
+                     "proposal_to_converged": float(np.max(np.abs(canon(guided.x) - start)))})
+        plain.I.erase()
+        guided.I.erase()
+    t_p = sum(r["plain_s"] for r in runs)
+    t_g = sum(r["surrogate_s"] for r in runs)
+    gain = (t_p - t_g) / len(Us)
+    return {"metric": "CDMFT wall time, surrogate-proposed starting bath (same hybridisation as the plain run)",
+            "value": t_g, "unit": "s", "n_gpus": 1, "steps": len(Us), "warmup": 0,
+            "ms_per_step": 1e3 * t_g / len(Us), "higher_is_better": False, "scaling": "replicas",
+            "vs_baseline": None, "dtype": "f64 (ED, host, bath fits); bf16 x bf16 -> f32 (surrogate)",
+            "data": "synthetic", "config": {"workload": CDMFT_WORKLOAD, "U": list(Us), "training_U": list(train_U),
+                                            "model_bath_seed": 7},
+            "plain_seconds": t_p, "speedup": t_p / t_g if t_g > 0 else None,
+            "plain_solves": sum(r["plain_solves"] for r in runs),
+            "surrogate_solves": sum(r["surrogate_solves"] for r in runs),
+            "surrogate_total_seconds": t_data + t_train + t_g,
+            "surrogate_total_what": "training data (CDMFT converged at every training U) + training + the runs",
+            "breakeven_runs": (t_data + t_train) / gain if gain > 0 else None,
+            "max_gamma_abs_diff": max(r["gamma_abs_diff"] for r in runs),
+            "training": {"data_seconds": t_data, "points_converged": int(len(ok)), "iterations": iters.tolist(),
+                         "train_seconds": t_train, "first_loss": float(losses[0]), "last_loss": float(losses[-1])},
+            "runs": runs}
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -627,6 +704,9 @@ def main():
         if args.workload == "vca":
             if rank == 0:
                 print(json.dumps(vca_line(args.vca_points, args.vca_epochs, args.threads, local=local)), flush=True)
+        elif args.workload == "cdmft":
+            if rank == 0:
+                print(json.dumps(cdmft_line(local=local)), flush=True)
         elif args.workload != "hv":
             run_batch_workload(args, world, rank, local)
         elif args.impl == "reference":

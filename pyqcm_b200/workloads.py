@@ -228,22 +228,26 @@ def vca_2x5(U: float = 8.0, M1: float = 0.1, dmu: float = 0.0) -> LatticeProblem
 
 
 def cdmft_2x2_bath(eps, hyb, U: float = 8.0, t: float = 1.0) -> LatticeProblem:
-    """Square lattice (hopping -t) tiled by 2x2 plaquettes, each with 8 bath
-    orbitals (two per site): bath energies eb{b}_1 = eps[b], hybridisations
-    tb{b}_1 = hyb[b] with cluster site b // 2, half filling (mu = U/2, sector
-    R0:N12:S0). The cluster model is that of plaquette_bath."""
-    ns, nb = 4, 8
+    """Square lattice (hopping -t) tiled by 2x2 plaquettes, each with nb = len(eps)
+    bath orbitals (4 or 8: one or two per site): bath energies eb{b}_1 = eps[b],
+    hybridisations tb{b}_1 = hyb[b] with cluster site b // (nb / 4), half filling
+    (mu = U/2, sector R0:N{4 + nb}:S0). With eight bath orbitals the cluster model
+    is that of plaquette_bath."""
+    ns, nb = 4, len(eps)
+    if nb not in (4, 8) or len(hyb) != nb:
+        raise ValueError("cdmft_2x2_bath: 4 or 8 bath orbitals, one energy and one hybridisation each")
     L = ns + nb
+    per = nb // ns
     sites = [(x, y, 0) for y in range(2) for x in range(2)]
     cops = {}
     params = {"t": t, "U": U, "mu": U / 2}
     for b in range(nb):
         cops[f"eb{b}"] = ("one-body", _both_spins(L, [(ns + b, ns + b, 1.0)]))
-        cops[f"tb{b}"] = ("one-body", _both_spins(L, [(b // 2, ns + b, 1.0)]))
+        cops[f"tb{b}"] = ("one-body", _both_spins(L, [(b // per, ns + b, 1.0)]))
         params[f"eb{b}_1"] = float(eps[b])
         params[f"tb{b}_1"] = float(hyb[b])
-    return LatticeProblem("cdmft2x2", sites, [(2, 0, 0), (0, 2, 0)], hoppings=[("t", (1, 0, 0), -1.0),
-                          ("t", (0, 1, 0), -1.0)], interactions=["U"], sectors="R0:N12:S0", params=params,
+    return LatticeProblem(f"cdmft2x2b{nb}", sites, [(2, 0, 0), (0, 2, 0)], hoppings=[("t", (1, 0, 0), -1.0),
+                          ("t", (0, 1, 0), -1.0)], interactions=["U"], sectors=f"R0:N{ns + nb}:S0", params=params,
                           equiv=[("t_1", 1.0, "t"), ("U_1", 1.0, "U"), ("mu_1", 1.0, "mu")], n_bath=nb,
                           cluster_operators=cops)
 

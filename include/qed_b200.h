@@ -253,6 +253,40 @@ int qed_qmatrix(int label, int spin_down, int *M, int *L, double *e, double *v);
 int qed_cf_coefficients(int label, int spin_down, int o1, int o2, int pm, int *n, double *a,
                         double *b);
 
+/* ---- instance checkpoints ----------------------------------------------------
+ * The data of model_instance::write_hdf5 / read_hdf5 (src_ed/model_instance.hpp:1339-1421,
+ * state.hpp:52-115, Q_matrix.hpp:321-345, continued_fraction_set.cpp:136-176),
+ * behind ED::write_instance_hdf5 / ED::read_instance_hdf5 (src_ed/qcm_ED.cpp:373-403).
+ * The HDF5 file itself is written and read by the caller (pyqcm_b200/hdf5.py).
+ * gf_format: 0 Q-matrices ("bl"), 1 continued fractions ("cf"), 2 matrix
+ * continued fractions ("mcf", not supported here). Trivial point group only. */
+/* Solves the Green function if needed (as write_hdf5 does), then: state count,
+ * GS energy, GS sector string, GF format and mixing. */
+int qed_instance_states(int label, int *n_states, double *gs_energy, char *gs_sectors, int len, int *gf_format,
+                        int *mixing);
+/* Parameter values of the instance: names separated by '\n' in names (capacity
+ * names_size), values[cap]; *n the count. */
+int qed_instance_parameters(int label, int cap, int *n, char *names, int names_size, double *values);
+/* State i: sector string, energy, weight. */
+int qed_instance_state(int label, int i, char *sector, int len, double *energy, double *weight);
+/* Q-matrix of state i: L x M residues v (column-major, sqrt(weight) included) and
+ * poles e; with e == NULL only L and M. */
+int qed_instance_state_qmatrix(int label, int i, int spin_down, int cap, int *L, int *M, double *e, double *v);
+/* Continued fraction (o1, o2), o2 <= o1, electron (pm = +1) or hole (pm = -1) of
+ * state i: levels a[n], b[n]; with a == NULL only n. */
+int qed_instance_state_cf(int label, int i, int spin_down, int o1, int o2, int pm, int cap, int *n, double *a,
+                          double *b);
+/* Loading (read_hdf5): begin (drops the instance's states), one load_state per
+ * state (its index returned), its Q-matrices or continued fractions, then end:
+ * the instance is then solved, with Green_function_average and the density
+ * computed from the loaded data as the reference does after reading. */
+int qed_instance_load_begin(int label, double gs_energy, int gf_format, int mixing);
+int qed_instance_load_state(int label, const char *sector, double energy, double weight, int *index);
+int qed_instance_load_qmatrix(int label, int i, int spin_down, int L, int M, const double *e, const double *v);
+int qed_instance_load_cf(int label, int i, int spin_down, int o1, int o2, int pm, int n, const double *a,
+                         const double *b);
+int qed_instance_load_end(int label);
+
 /* Ground-state vector of the first kept state (factorized layout
  * psi[up_rank + dim_up * dn_rank], src_ed/ED_basis.cpp:142-165).
  * *dim receives the dimension; psi may be NULL to query it. */

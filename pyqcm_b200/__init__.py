@@ -99,6 +99,16 @@ def lib():
         "qed_susceptibility_poles": [C.c_int, C.c_char_p, C.c_int, ip, dp, dp],
         "qed_qmatrix": [C.c_int, C.c_int, ip, ip, dp, dp],
         "qed_cf_coefficients": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, ip, dp, dp],
+        "qed_instance_states": [C.c_int, ip, dp, C.c_char_p, C.c_int, ip, ip],
+        "qed_instance_parameters": [C.c_int, C.c_int, ip, C.c_char_p, C.c_int, dp],
+        "qed_instance_state": [C.c_int, C.c_int, C.c_char_p, C.c_int, dp, dp],
+        "qed_instance_state_qmatrix": [C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, dp, dp],
+        "qed_instance_state_cf": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, ip, dp, dp],
+        "qed_instance_load_begin": [C.c_int, C.c_double, C.c_int, C.c_int],
+        "qed_instance_load_state": [C.c_int, C.c_char_p, C.c_double, C.c_double, ip],
+        "qed_instance_load_qmatrix": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp, dp],
+        "qed_instance_load_cf": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp, dp],
+        "qed_instance_load_end": [C.c_int],
         "qed_ground_state_vector": [C.c_int, lp, dp],
         "qed_hamiltonian_create": [C.c_int, C.c_char_p, C.POINTER(C.c_void_p), lp],
         "qed_hamiltonian_mult_add": [C.c_void_p, dp, dp],
@@ -715,3 +725,128 @@ def hv_tuning_report():
     buf = C.create_string_buffer(n + 1)
     lib().qed_hv_tuning_report(buf, n + 1)
     return json.loads(buf.value.decode() or "[]")
+
+
+# ------------------------------------------------------------ instance checkpoints --
+
+_GF_FORMATS = ("bl", "cf", "mcf")
+
+
+def write_instance_to_hdf5(filename: str, group: str, label: int = 0):
+    """qcm.write_instance_to_hdf5 (src_python/qcm_ED_wrap.hpp:364-369 -> ED::write_instance_hdf5,
+    src_ed/qcm_ED.cpp:373-389): solves the instance's Green function if needed and
+    writes it to `group` of the HDF5 file (created if absent, the group replaced if
+    present) in the reference's layout: attributes GS_energy, GS_sectors, GF_format,
+    mixing, complex_HS, nstates; group params; one group state_i per state (sec,
+    energy, weight, gf_format; gf and, with spin asymmetry, gf_down holding a
+    Q-matrix set or a continued-fraction set). The file is written by
+    pyqcm_b200.hdf5 (no HDF5 library needed)."""
+    from . import hdf5
+    L = lib()
+    n, e0, fmt, mix = C.c_int(), C.c_double(), C.c_int(), C.c_int()
+    gs = C.create_string_buffer(4096)
+    _check(L.qed_instance_states(label, C.byref(n), C.byref(e0), gs, 4096, C.byref(fmt), C.byref(mix)))
+    cap, npar = 4096, C.c_int()
+    names = C.create_string_buffer(1 << 16)
+    vals = np.zeros(cap)
+    _check(L.qed_instance_parameters(label, cap, C.byref(npar), names, 1 << 16, _dp(vals)))
+    pnames = names.value.decode().split("\n")[:npar.value]
+    nsites = Green_function_dimension(label)
+    f = hdf5.File(filename, "a")
+    f.root.unlink(group)
+    g = f.root.create_group(group)
+    g.attrs.update({"GS_energy": e0.value, "GS_sectors": gs.value.decode(), "GF_format": _GF_FORMATS[fmt.value],
+                    "mixing": mix.value, "complex_HS": 0})
+    pg = g.create_group("params")
+    for k, v in zip(pnames, vals):
+        pg.attrs[k] = float(v)
+    g.attrs["nstates"] = n.value
+    for i in range(n.value):
+        sec = C.create_string_buffer(256)
+        en, w = C.c_double(), C.c_double()
+        _check(L.qed_instance_state(label, i, sec, 256, C.byref(en), C.byref(w)))
+        sg = g.create_group(f"state_{i}")
+        sg.attrs.update({"sec": sec.value.decode(), "energy": en.value, "weight": w.value,
+                         "gf_format": _GF_FORMATS[fmt.value]})
+        for sd in ((0, 1) if mix.value & 4 else (0,)):
+            gg = sg.create_group("gf_down" if sd else "gf")
+            if fmt.value == 0:  # Q_matrix_set::write_hdf5 (src_ed/Q_matrix_set.hpp:187-194), one block
+                Lr, M = C.c_int(), C.c_int()
+                _check(L.qed_instance_state_qmatrix(label, i, sd, 0, C.byref(Lr), C.byref(M), None, None))
+                e = np.zeros(M.value)
+                v = np.zeros(Lr.value * M.value)
+                _check(L.qed_instance_state_qmatrix(label, i, sd, M.value, C.byref(Lr), C.byref(M), _dp(e), _dp(v)))
+                gg.attrs["nblocks"] = 1
+                bg = gg.create_group("block_0")
+                bg.attrs.update({"L": Lr.value, "M": M.value})
+                bg.create_dataset("e", e)
+                vg = bg.create_group("v")
+                vg.attrs.update({"r": Lr.value, "c": M.value})
+                vg.create_dataset("data", v)
+            else:  # continued_fraction_set::write_hdf5 (src_ed/continued_fraction_set.cpp:136-153)
+                gg.attrs["is_complex"] = 0
+                for a in range(nsites):
+                    for b in range(a + 1):
+                        cg = gg.create_group(f"r0_a{a}_b{b}")
+                        for part, pm in (("e", 1), ("h", -1)):
+                            nl = C.c_int()
+                            _check(L.qed_instance_state_cf(label, i, sd, a, b, pm, 0, C.byref(nl), None, None))
+                            ca, cb = np.zeros(nl.value), np.zeros(nl.value)
+                            _check(L.qed_instance_state_cf(label, i, sd, a, b, pm, nl.value, C.byref(nl), _dp(ca),
+                                                           _dp(cb)))
+                            pgp = cg.create_group(part)
+                            pgp.create_dataset("a", ca)
+                            pgp.create_dataset("b", cb)
+    f.close()
+
+
+def read_instance_from_hdf5(filename: str, group: str, label: int = 0):
+    """qcm.read_instance_from_hdf5 (src_python/qcm_ED_wrap.hpp:371-376 -> ED::read_instance_hdf5,
+    src_ed/qcm_ED.cpp:392-403, model_instance::read_hdf5): replaces the states of
+    instance `label` by those of `group`, which then counts as solved (Green
+    function, its average and density from the file). As the reference does, a
+    parameter value in the file that differs from the instance's by more than
+    1e-4 only prints a warning."""
+    from . import hdf5
+    L = lib()
+    g = hdf5.File(filename, "r").root.group(group)
+    fmt = _GF_FORMATS.index(g.attrs["GF_format"])
+    mix = int(g.attrs["mixing"])
+    cap, npar = 4096, C.c_int()
+    names = C.create_string_buffer(1 << 16)
+    vals = np.zeros(cap)
+    _check(L.qed_instance_parameters(label, cap, C.byref(npar), names, 1 << 16, _dp(vals)))
+    current = dict(zip(names.value.decode().split("\n")[:npar.value], vals))
+    stored = g.group("params").attrs if "params" in g else {}
+    for k, v in current.items():
+        if k in stored and abs(float(stored[k]) - v) > 1e-4:
+            print(f"WARNING : The value of {k} from the HDF5 solution ({stored[k]}) differs from the expected "
+                  f"value ({v}).")
+    nsites = Green_function_dimension(label)
+    _check(L.qed_instance_load_begin(label, float(g.attrs["GS_energy"]), fmt, mix))
+    for i in range(int(g.attrs["nstates"])):
+        sg = g.group(f"state_{i}")
+        idx = C.c_int()
+        _check(L.qed_instance_load_state(label, sg.attrs["sec"].encode(), float(sg.attrs["energy"]),
+                                         float(sg.attrs["weight"]), C.byref(idx)))
+        for sd, gname in ((0, "gf"), (1, "gf_down")):
+            if gname not in sg:
+                continue
+            gg = sg.group(gname)
+            if fmt == 0:
+                if int(gg.attrs["nblocks"]) != 1:
+                    raise QEDError(QED_ERR_UNSUPPORTED, "Q-matrix sets of more than one block (point groups)")
+                bg = gg.group("block_0")
+                e = np.ascontiguousarray(bg.dataset("e"), dtype=np.float64)
+                v = np.ascontiguousarray(bg.group("v").dataset("data"), dtype=np.float64)
+                _check(L.qed_instance_load_qmatrix(label, idx.value, sd, int(bg.attrs["L"]), int(bg.attrs["M"]),
+                                                   _dp(e), _dp(v)))
+            else:
+                for a in range(nsites):
+                    for b in range(a + 1):
+                        cg = gg.group(f"r0_a{a}_b{b}")
+                        for part, pm in (("e", 1), ("h", -1)):
+                            ca = np.ascontiguousarray(cg.group(part).dataset("a"), dtype=np.float64)
+                            cb = np.ascontiguousarray(cg.group(part).dataset("b"), dtype=np.float64)
+                            _check(L.qed_instance_load_cf(label, idx.value, sd, a, b, pm, len(ca), _dp(ca), _dp(cb)))
+    _check(L.qed_instance_load_end(label))

@@ -985,6 +985,184 @@ int qed_cf_coefficients(int label, int spin_down, int o1, int o2, int pm, int *n
   });
 }
 
+// ---- instance checkpoints (model_instance::write_hdf5 / read_hdf5,
+// src_ed/model_instance.hpp:1339-1421; the file itself is written by the caller)
+
+int qed_instance_states(int label, int *n_states, double *gs_energy, char *gs_sectors, int len, int *gf_format,
+                        int *mixing) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    if (I->has_group()) fail(QED_ERR_UNSUPPORTED, "checkpoints of models with a point group are not supported");
+    I->green_solve(ws());  // write_hdf5 solves the Green function first
+    *n_states = (int)I->states.size();
+    *gs_energy = I->GS_energy;
+    const std::string g = I->gs_string();
+    if (gs_sectors && len > 0) {
+      std::strncpy(gs_sectors, g.c_str(), (size_t)len - 1);
+      gs_sectors[len - 1] = 0;
+    }
+    *gf_format = I->use_cf ? 1 : I->use_mcf ? 2 : 0;
+    *mixing = I->mix;
+  });
+}
+
+int qed_instance_parameters(int label, int cap, int *n, char *names, int names_size, double *values) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    *n = (int)I->value.size();
+    if (*n > cap) fail(QED_ERR_ARGUMENT, "qed_instance_parameters: capacity too small");
+    std::string all;
+    int k = 0;
+    for (auto &kv : I->value) {
+      all += kv.first + '\n';
+      values[k++] = kv.second;
+    }
+    if ((int)all.size() + 1 > names_size) fail(QED_ERR_ARGUMENT, "qed_instance_parameters: name buffer too small");
+    std::memcpy(names, all.c_str(), all.size() + 1);
+  });
+}
+
+int qed_instance_state(int label, int i, char *sector, int len, double *energy, double *weight) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    if (i < 0 || i >= (int)I->states.size()) fail(QED_ERR_ARGUMENT, "state index out of range");
+    const State &st = *I->states[i];
+    std::strncpy(sector, st.sec.name().c_str(), (size_t)len - 1);
+    sector[len - 1] = 0;
+    *energy = st.energy;
+    *weight = st.weight;
+  });
+}
+
+int qed_instance_state_qmatrix(int label, int i, int spin_down, int cap, int *L, int *M, double *e, double *v) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    if (i < 0 || i >= (int)I->states.size()) fail(QED_ERR_ARGUMENT, "state index out of range");
+    if (I->use_cf || I->use_mcf) fail(QED_ERR_ARGUMENT, "the instance's Green function is not a Q-matrix");
+    const QMat &q = I->states[i]->q[spin_down ? 1 : 0];
+    *L = q.L;
+    *M = q.M;
+    if (!e) return;  // sizes only
+    if (q.M > cap) fail(QED_ERR_ARGUMENT, "qed_instance_state_qmatrix: capacity too small");
+    std::copy(q.e.begin(), q.e.end(), e);
+    std::copy(q.V.begin(), q.V.end(), v);
+  });
+}
+
+int qed_instance_state_cf(int label, int i, int spin_down, int o1, int o2, int pm, int cap, int *n, double *a,
+                          double *b) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    if (i < 0 || i >= (int)I->states.size()) fail(QED_ERR_ARGUMENT, "state index out of range");
+    if (!I->use_cf) fail(QED_ERR_ARGUMENT, "not a continued-fraction instance");
+    const CFSet &cf = I->states[i]->cf[spin_down ? 1 : 0];
+    if (o1 < 0 || o2 < 0 || o2 > o1 || o1 >= cf.n) fail(QED_ERR_ARGUMENT, "bad orbital pair");
+    const size_t idx = (size_t)o1 * cf.n + o2;
+    const auto &A = pm > 0 ? cf.ea[idx] : cf.ha[idx];
+    const auto &B = pm > 0 ? cf.eb[idx] : cf.hb[idx];
+    *n = (int)A.size();
+    if (!a) return;
+    if ((int)A.size() > cap) fail(QED_ERR_ARGUMENT, "qed_instance_state_cf: capacity too small");
+    std::copy(A.begin(), A.end(), a);
+    for (size_t k = 0; k < A.size(); ++k) b[k] = k < B.size() ? B[k] : 0.0;
+  });
+}
+
+int qed_instance_load_begin(int label, double gs_energy, int gf_format, int mixing) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    if (I->has_group()) fail(QED_ERR_UNSUPPORTED, "checkpoints of models with a point group are not supported");
+    if (gf_format == 2) fail(QED_ERR_UNSUPPORTED, "matrix continued-fraction checkpoints are not supported");
+    if (gf_format != 0 && gf_format != 1) fail(QED_ERR_ARGUMENT, "unknown Green-function format");
+    I->states.clear();
+    I->use_cf = gf_format == 1;
+    I->use_mcf = false;
+    I->mix = mixing;
+    I->GS_energy = gs_energy;
+    I->gs_solved = false;
+    I->gf_solved = false;
+  });
+}
+
+int qed_instance_load_state(int label, const char *sector, double energy, double weight, int *index) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    auto st = std::make_shared<State>();
+    st->sec = Sector(sector);
+    st->energy = energy;
+    st->weight = weight;
+    const int n = I->model->n_sites;
+    for (auto &c : st->cf) {
+      c.n = n;
+      c.ea.assign((size_t)n * n, {});
+      c.eb.assign((size_t)n * n, {});
+      c.ha.assign((size_t)n * n, {});
+      c.hb.assign((size_t)n * n, {});
+    }
+    I->states.push_back(st);
+    *index = (int)I->states.size() - 1;
+  });
+}
+
+int qed_instance_load_qmatrix(int label, int i, int spin_down, int L, int M, const double *e, const double *v) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    if (i < 0 || i >= (int)I->states.size()) fail(QED_ERR_ARGUMENT, "state index out of range");
+    if (L != I->model->n_sites) fail(QED_ERR_ARGUMENT, "Q-matrix with " + std::to_string(L) + " rows for " +
+                                                          std::to_string(I->model->n_sites) + " cluster sites");
+    QMat &q = I->states[i]->q[spin_down ? 1 : 0];
+    q.L = L;
+    q.M = M;
+    q.e.assign(e, e + M);
+    q.V.assign(v, v + (size_t)L * M);
+  });
+}
+
+int qed_instance_load_cf(int label, int i, int spin_down, int o1, int o2, int pm, int n, const double *a,
+                         const double *b) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    if (i < 0 || i >= (int)I->states.size()) fail(QED_ERR_ARGUMENT, "state index out of range");
+    CFSet &cf = I->states[i]->cf[spin_down ? 1 : 0];
+    if (o1 < 0 || o2 < 0 || o2 > o1 || o1 >= cf.n) fail(QED_ERR_ARGUMENT, "bad orbital pair");
+    const size_t idx = (size_t)o1 * cf.n + o2;
+    (pm > 0 ? cf.ea : cf.ha)[idx].assign(a, a + n);
+    (pm > 0 ? cf.eb : cf.hb)[idx].assign(b, b + n);
+  });
+}
+
+int qed_instance_load_end(int label) {
+  return guarded([&] {
+    auto I = instance(label);
+    std::lock_guard<std::mutex> li(I->mtx);
+    if (I->states.empty()) fail(QED_ERR_ARGUMENT, "a checkpoint without states");
+    I->E0 = 0.0;
+    for (auto &st : I->states) {
+      I->E0 += st->weight * st->energy;
+      for (int sd = 0; sd < 2; ++sd) {
+        QMat &q = st->q[sd];
+        if (q.M > 0) {
+          q.de.upload(q.e, ws().stream);
+          q.dV.upload(q.V, ws().stream);
+        }
+      }
+    }
+    ws().sync();
+    I->is_correlated = true;
+    I->gs_solved = true;
+    I->finish_gf();  // gf_solved, Green_function_average, Green_function_density
+  });
+}
+
 int qed_ground_state_vector(int label, long *dim, double *psi) {
   return guarded([&] {
     auto I = instance(label);

@@ -56,6 +56,16 @@ struct Table {
     // 4900 states 83 / 57 ms; p = 10, 63504 states 107 / 68 ms; p = 12, 853776
     // states 588 / 432 ms; p = 4, 16 concurrent 853776-state instances, 32.8 / 32.7
     // solves/s. Smaller p and sectors were not measured.
+    // solver option: the 16-step chunks of the ground-state Lanczos of sectors of
+    // at least lanczos_graphs_min_dim states are captured once per solve into
+    // CUDA graphs (one per rotation of the three Krylov buffers) and replayed.
+    // Measured on a B200 (default bench batches): 256 points of the 2x2 + 8-bath
+    // model (853776 states) 43.3 solves/s with graphs, 40.6 without; 1024 random
+    // clusters (sectors up to 63504 states) 49-61 with graphs for every sector
+    // above the job table, 72 without: the three captures per solve cost more than
+    // the replays save on sectors of tens of thousands of states.
+    b["lanczos_graphs"] = true;
+    i["lanczos_graphs_min_dim"] = 131072;
     i["block_lanczos_min_dim"] = 1000;
     i["block_lanczos_min_p"] = 4;
     i["seed"] = 0;

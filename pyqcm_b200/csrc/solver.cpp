@@ -479,6 +479,44 @@ void lanczos_energy_batch(std::vector<LanczosBatchItem> &items, Workspace &ws) {
   }
 }
 
+// CUDA graphs of one launch sequence per key (here: the Krylov buffers' rotation
+// at the start of a chunk). run() captures the sequence on its first use for a
+// key (the captured launches are then replayed once, so the stream does the work
+// exactly once either way) and replays the instantiated graph afterwards;
+// captured_now tells the caller which happened. Graphs are released with the
+// object.
+struct ChunkGraphs {
+  cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+  bool captured_now = false;
+  ChunkGraphs() = default;
+  ChunkGraphs(const ChunkGraphs &) = delete;
+  ChunkGraphs &operator=(const ChunkGraphs &) = delete;
+  ~ChunkGraphs() {
+    for (auto &e : exec)
+      if (e) cudaGraphExecDestroy(e);
+  }
+  template <class F> void run(int key, cudaStream_t s, F &&record) {
+    captured_now = false;
+    if (!exec[key]) {
+      cudaGraph_t g = nullptr;
+      QED_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      try {
+        record();
+      } catch (...) {
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      QED_CUDA(cudaStreamEndCapture(s, &g));
+      const cudaError_t e = cudaGraphInstantiate(&exec[key], g, 0);
+      cudaGraphDestroy(g);
+      QED_CUDA(e);
+      captured_now = true;
+    }
+    QED_CUDA(cudaGraphLaunch(exec[key], s));
+  }
+};
+
 LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed) {
   if (H.D <= kLanczosCtaMaxDim) {
     LanczosResult res;
@@ -520,23 +558,48 @@ LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed) {
   double lambda0 = 0.0;
   RitzTracker tracker;
   size_t launched = 0;
+  // One Lanczos step on the current buffers, then the rotation
+  // v_{j-1} <- v_j <- v_{j+1}. Every scalar lives in device memory (ls), so a
+  // chunk of steps is the same launch sequence whatever the step index: after
+  // the first chunk, the full chunks are replayed from CUDA graphs, one per
+  // rotation of (pa, pb, pc) at the chunk's start (kChunk = 16 steps shift the
+  // rotation by one).
+  auto one_step = [&] {
+    sub.z[0] = pa;
+    int nb = launch_hv(H.op, pb, 1.0, pc, sub, 1, ws.red, s);
+    launch_finalize(ws.red.partials, nb, 1, ls.alpha_cur, s);      // alpha_j = <v_j, w>
+    nb = launch_axpy_dev(D, pc, pb, ls.alpha_cur, ws.red, s);      // w -= alpha_j v_j
+    launch_finalize(ws.red.partials, nb, 1, ls.b2_cur, s);          // |w|^2
+    launch_lanczos_advance(D, pc, ls, s);                           // v_{j+1} = w / beta_j
+    double *t = pa;
+    pa = pb;
+    pb = pc;
+    pc = t;
+  };
+  ChunkGraphs graphs;
+  const bool use_graphs = opt_bool("lanczos_graphs") && (long)D >= opt_int("lanczos_graphs_min_dim");
+  int rot = 0;  // rotations of (pa, pb, pc) since the start, mod 3
   // a first short chunk: tiny sectors stop after about D steps
   int chunk = (int)std::min<size_t>(std::max<size_t>(D, 2), 8);
   bool stop = false;
   while (!stop) {
     if (launched + chunk > cap) fail(QED_ERR_INTERNAL, "Lanczos history overflow");
-    for (int k = 0; k < chunk; ++k) {
-      sub.z[0] = pa;
-      int nb = launch_hv(H.op, pb, 1.0, pc, sub, 1, ws.red, s);
-      launch_finalize(ws.red.partials, nb, 1, ls.alpha_cur, s);      // alpha_j = <v_j, w>
-      nb = launch_axpy_dev(D, pc, pb, ls.alpha_cur, ws.red, s);      // w -= alpha_j v_j
-      launch_finalize(ws.red.partials, nb, 1, ls.b2_cur, s);          // |w|^2
-      launch_lanczos_advance(D, pc, ls, s);                           // v_{j+1} = w / beta_j
-      double *t = pa;  // v_{j-1} <- v_j <- v_{j+1}
-      pa = pb;
-      pb = pc;
-      pc = t;
+    if (use_graphs && chunk == kChunk && launched > 0) {
+      graphs.run(rot, s, [&] {
+        for (int k = 0; k < kChunk; ++k) one_step();
+      });
+      if (!graphs.captured_now) {  // replayed: advance the host's view of the rotation
+        for (int k = 0; k < kChunk; ++k) {
+          double *t = pa;
+          pa = pb;
+          pb = pc;
+          pc = t;
+        }
+      }
+    } else {
+      for (int k = 0; k < chunk; ++k) one_step();
     }
+    rot = (rot + chunk) % 3;
     QED_CUDA(cudaMemcpyAsync(ws.host, ls.alpha_hist + launched, chunk * sizeof(double),
                              cudaMemcpyDeviceToHost, s));
     QED_CUDA(cudaMemcpyAsync(ws.host + kChunk, ls.beta_hist + launched, chunk * sizeof(double),

@@ -218,6 +218,37 @@ def test_ground_state_staged_kernels(qed, oracle, fresh):
     assert s1 == s2
 
 
+def test_lanczos_graphs_replay_the_same_steps(qed, oracle, fresh):
+    """The ground-state Lanczos of a 924^2-state sector with its 16-step chunks
+    replayed from CUDA graphs gives the bits of the directly launched chunks and
+    the reference's energy; so does a 63504-state sector (chain of 10 sites) with
+    the graphs' size threshold lowered to include it."""
+    def solve(prob, graphs, min_dim=None):
+        suffix, label = fresh()
+        qed.set_global_parameter("lanczos_graphs", graphs)
+        if min_dim is not None:
+            qed.set_global_parameter("lanczos_graphs_min_dim", min_dim)
+        load_both(qed, oracle, prob, suffix, label, fmt="F")
+        try:
+            return qed.ground_state_solve(label), label
+        finally:
+            qed.set_global_parameter("lanczos_graphs", True)
+            qed.set_global_parameter("lanczos_graphs_min_dim", 131072)
+
+    prob = W.hubbard_cluster(6, 2, tp=0.3, U=6.0, mu=3.0)
+    prob.sectors = "R0:N12:S0"
+    (e1, s1), _ = solve(prob, False)
+    (e2, s2), label = solve(prob, True)
+    e_ref, s_ref = oracle.ground_state(label)
+    assert e1 == e2 and s1 == s2 == s_ref, (e1, e2)
+    assert abs(e2 - e_ref) <= 1e-10 * abs(e_ref)
+    chain = W.hubbard_cluster(10, 1, U=4.0, mu=2.0)
+    chain.sectors = "R0:N10:S0"
+    (c1, _), _ = solve(chain, False)
+    (c2, _), _ = solve(chain, True, min_dim=0)
+    assert c1 == c2, (c1, c2)
+
+
 def test_batched_solves_match_reference(qed, oracle, fresh):
     """Many random clusters (every sector listed, staggered field) solved concurrently."""
     probs = W.random_batch(12, seed=77, geoms=[(2, 2), (2, 3), (2, 4), (8, 1)])

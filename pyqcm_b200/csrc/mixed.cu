@@ -5,6 +5,7 @@
 #include <mutex>
 
 #include "kernels.cuh"
+#include "options.hpp"
 #include "qed_b200.h"
 
 namespace qed {
@@ -180,12 +181,59 @@ __global__ void k_mixed_diag(const uint64_t *__restrict__ states, uint64_t D, co
   }
 }
 
+// Where a row's off-diagonal entries come from. CsrRows: the stored matrix
+// (each lane takes every eighth stored entry). OtfRows: computed on the fly,
+// with no stored matrix (each lane takes every eighth one-body element and
+// evaluates it on the row's state exactly as k_mixed_rows does: Pauli test,
+// fermion sign, representative of the image, its basis index, phase and
+// orbit-length factor), for sectors whose matrix would not fit or when asked.
+struct CsrRows {
+  const uint64_t *row_ptr;
+  const uint32_t *col;
+  const double *val;
+  __device__ __forceinline__ double lane_sum(uint64_t J, int lane, const double *__restrict__ x) const {
+    double s = 0.0;
+    const uint64_t a = row_ptr[J], e = row_ptr[J + 1];
+    for (uint64_t k = a + lane; k < e; k += 8) s += val[k] * __ldg(x + col[k]);
+    return s;
+  }
+};
+
+struct OtfRows {
+  SymGroup G;
+  int irrep;
+  OffTerms t;
+  const uint64_t *states;
+  const uint8_t *len;
+  const int32_t *fmap;
+  uint32_t du;
+  __device__ __forceinline__ double lane_sum(uint64_t J, int lane, const double *__restrict__ x) const {
+    const int n = G.N;
+    const uint64_t b = states[J];
+    const double lj = (double)len[J];
+    double s = 0.0;
+    for (int e = lane; e < t.n; e += 8) {
+      const uint64_t mc = orb_mask(t.c[e], n), mr = orb_mask(t.r[e], n);
+      if (!(b & mc) || (b & mr)) continue;
+      const uint64_t lo = mc < mr ? mc : mr, hi = mc < mr ? mr : mc;
+      const int sign = (__popcll(b & (hi - (lo << 1))) & 1) ? -1 : 1;
+      const RepMap m = sym_representative(G, b - mc + mr, irrep);
+      if (m.length == 0) continue;
+      const uint64_t f = (uint64_t)colex_rank((uint32_t)m.rep) + (uint64_t)du * colex_rank((uint32_t)(m.rep >> 32));
+      const int32_t K = fmap[f];
+      if (K < 0) continue;
+      s += (m.phase ? -1.0 : 1.0) * t.v[e] * sign * sqrt(lj / (double)len[K]) * __ldg(x + K);
+    }
+    return s;
+  }
+};
+
 // y = H x: eight lanes per row stride over its entries, then a shuffle sum. A
 // warp takes four consecutive rows per pass; the loop bound is the warp's first
 // row, the same for all its lanes, so every shuffle sees the whole warp.
-__global__ void k_mixed_spmv(const uint64_t *__restrict__ row_ptr, const uint32_t *__restrict__ col,
-                             const double *__restrict__ val, const double *__restrict__ dg,
-                             const double *__restrict__ x, double *__restrict__ y, uint64_t D) {
+template <class Rows>
+__global__ void k_mixed_spmv(const Rows R, const double *__restrict__ dg, const double *__restrict__ x,
+                             double *__restrict__ y, uint64_t D) {
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t n_warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 7;
@@ -193,10 +241,7 @@ __global__ void k_mixed_spmv(const uint64_t *__restrict__ row_ptr, const uint32_
   for (uint64_t J0 = warp * 4; J0 < D; J0 += n_warps * 4) {
     const uint64_t J = J0 + group;
     double s = 0.0;
-    if (J < D) {
-      const uint64_t a = row_ptr[J], e = row_ptr[J + 1];
-      for (uint64_t k = a + lane; k < e; k += 8) s += val[k] * __ldg(x + col[k]);
-    }
+    if (J < D) s = R.lane_sum(J, lane, x);
     s += __shfl_xor_sync(0xffffffffu, s, 4);
     s += __shfl_xor_sync(0xffffffffu, s, 2);
     s += __shfl_xor_sync(0xffffffffu, s, 1);
@@ -207,10 +252,8 @@ __global__ void k_mixed_spmv(const uint64_t *__restrict__ row_ptr, const uint32_
 // One ground-state Lanczos step on the mixed basis: w = H v - beta v_prev with
 // the per-block partial sums of <v, w> at partials[block * ld] (the layout the
 // factorized path's reductions use), rows as in k_mixed_spmv.
-__global__ void __launch_bounds__(256) k_mixed_lanczos_w(const uint64_t *__restrict__ row_ptr,
-                                                         const uint32_t *__restrict__ col,
-                                                         const double *__restrict__ val,
-                                                         const double *__restrict__ dg,
+template <class Rows>
+__global__ void __launch_bounds__(256) k_mixed_lanczos_w(const Rows R, const double *__restrict__ dg,
                                                          const double *__restrict__ v,
                                                          const double *__restrict__ vprev,
                                                          const double *__restrict__ beta_dev,
@@ -225,10 +268,7 @@ __global__ void __launch_bounds__(256) k_mixed_lanczos_w(const uint64_t *__restr
   for (uint64_t J0 = warp * 4; J0 < D; J0 += n_warps * 4) {
     const uint64_t J = J0 + group;
     double s = 0.0;
-    if (J < D) {
-      const uint64_t a = row_ptr[J], e = row_ptr[J + 1];
-      for (uint64_t k = a + lane; k < e; k += 8) s += val[k] * __ldg(v + col[k]);
-    }
+    if (J < D) s = R.lane_sum(J, lane, v);
     s += __shfl_xor_sync(0xffffffffu, s, 4);
     s += __shfl_xor_sync(0xffffffffu, s, 2);
     s += __shfl_xor_sync(0xffffffffu, s, 1);
@@ -253,9 +293,8 @@ __global__ void __launch_bounds__(256) k_mixed_lanczos_w(const uint64_t *__restr
 // y = xs H x - sum_k c_k z_k with the reductions of the factorized column pass
 // (block partials at partials[block * Reducer::kMaxRed + i]); rows as in
 // k_mixed_spmv. *skip != 0: the whole call does nothing.
-__global__ void __launch_bounds__(256) k_mixed_full(const uint64_t *__restrict__ row_ptr,
-                                                    const uint32_t *__restrict__ col,
-                                                    const double *__restrict__ val, const double *__restrict__ dg,
+template <class Rows>
+__global__ void __launch_bounds__(256) k_mixed_full(const Rows R, const double *__restrict__ dg,
                                                     const double *__restrict__ x, double xs, double *y, uint64_t D,
                                                     SubList sub, int red_mask, double *partials, const int *skip) {
   if (skip && *skip) return;
@@ -267,10 +306,7 @@ __global__ void __launch_bounds__(256) k_mixed_full(const uint64_t *__restrict__
   for (uint64_t J0 = warp * 4; J0 < D; J0 += n_warps * 4) {
     const uint64_t J = J0 + group;
     double s = 0.0;
-    if (J < D) {
-      const uint64_t a = row_ptr[J], e = row_ptr[J + 1];
-      for (uint64_t k = a + lane; k < e; k += 8) s += val[k] * __ldg(x + col[k]);
-    }
+    if (J < D) s = R.lane_sum(J, lane, x);
     s += __shfl_xor_sync(0xffffffffu, s, 4);
     s += __shfl_xor_sync(0xffffffffu, s, 2);
     s += __shfl_xor_sync(0xffffffffu, s, 1);
@@ -454,12 +490,11 @@ MixedHamiltonian::MixedHamiltonian(const SymmetryGroup &G, const MixedTerms &t, 
     QED_CUDA(cudaStreamSynchronize(s));
     return;
   }
-  DevBuf<int> tr, tcol;
-  DevBuf<double> tv;
-  tr.upload(t.r, s);
-  tcol.upload(t.c, s);
-  tv.upload(t.v, s);
-  const OffTerms ot{(int)t.r.size(), tr.p, tcol.p, tv.p};
+  term_r.upload(t.r, s);
+  term_c.upload(t.c, s);
+  term_v.upload(t.v, s);
+  n_terms = (int)t.r.size();
+  const OffTerms ot{n_terms, term_r.p, term_c.p, term_v.p};
   DevBuf<uint32_t> cnt(D);
   k_mixed_rows<false><<<grid_for(D, 128), 128, 0, s>>>(G.tab, irrep, ot, states.p, len.p, D, fmap.p, (uint32_t)du,
                                                        cnt.p, nullptr, nullptr, nullptr);
@@ -471,13 +506,21 @@ MixedHamiltonian::MixedHamiltonian(const SymmetryGroup &G, const MixedTerms &t, 
   rp[0] = 0;
   for (size_t J = 0; J < D; ++J) rp[J + 1] = rp[J] + hc[J];
   nnz = rp[D];
-  row_ptr.upload(rp, s);
-  col.alloc(nnz);
-  val.alloc(nnz);
-  if (nnz)
-    k_mixed_rows<true><<<grid_for(D, 128), 128, 0, s>>>(G.tab, irrep, ot, states.p, len.p, D, fmap.p, (uint32_t)du,
-                                                        nullptr, row_ptr.p, col.p, val.p);
-  QED_LAUNCH();
+  // the stored matrix (12 bytes per entry + the row pointers) or, above the
+  // size budget or when asked, entries recomputed at every product; sectors
+  // that may be diagonalised in full keep the stored form
+  const double csr_bytes = 12.0 * (double)nnz + 8.0 * (double)(D + 1);
+  on_the_fly = (long)D >= opt_int("max_dim_full") &&
+               (opt_bool("mixed_on_the_fly") || csr_bytes > opt_double("mixed_csr_max_gb") * 1e9);
+  if (!on_the_fly) {
+    row_ptr.upload(rp, s);
+    col.alloc(nnz);
+    val.alloc(nnz);
+    if (nnz)
+      k_mixed_rows<true><<<grid_for(D, 128), 128, 0, s>>>(G.tab, irrep, ot, states.p, len.p, D, fmap.p,
+                                                          (uint32_t)du, nullptr, row_ptr.p, col.p, val.p);
+    QED_LAUNCH();
+  }
   DevBuf<uint64_t> dm;
   DevBuf<double> dv;
   dm.upload(t.dmask, s);
@@ -487,18 +530,32 @@ MixedHamiltonian::MixedHamiltonian(const SymmetryGroup &G, const MixedTerms &t, 
   QED_CUDA(cudaStreamSynchronize(s));
 }
 
+namespace {
+CsrRows csr_rows(const MixedHamiltonian &H) { return CsrRows{H.row_ptr.p, H.col.p, H.val.p}; }
+OtfRows otf_rows(const MixedHamiltonian &H) {
+  return OtfRows{H.group, H.irrep, OffTerms{H.n_terms, H.term_r.p, H.term_c.p, H.term_v.p}, H.states.p, H.len.p,
+                 H.fmap.p, H.du};
+}
+}  // namespace
+
 int MixedHamiltonian::lanczos_w(const double *v, const double *vprev, const double *beta_dev, double *w,
                                 double *partials, int ld, int max_blocks, cudaStream_t s) const {
   unsigned nb = grid_for(D * 8, 256);
   if (nb > (unsigned)max_blocks) nb = (unsigned)max_blocks;
-  k_mixed_lanczos_w<<<nb, 256, 0, s>>>(row_ptr.p, col.p, val.p, dg.p, v, vprev, beta_dev, w, D, partials, ld);
+  if (on_the_fly)
+    k_mixed_lanczos_w<<<nb, 256, 0, s>>>(otf_rows(*this), dg.p, v, vprev, beta_dev, w, D, partials, ld);
+  else
+    k_mixed_lanczos_w<<<nb, 256, 0, s>>>(csr_rows(*this), dg.p, v, vprev, beta_dev, w, D, partials, ld);
   QED_LAUNCH();
   return (int)nb;
 }
 
 void MixedHamiltonian::apply(const double *x, double *y, cudaStream_t s) const {
   if (!D) return;
-  k_mixed_spmv<<<grid_for(D * 8, 256), 256, 0, s>>>(row_ptr.p, col.p, val.p, dg.p, x, y, D);
+  if (on_the_fly)
+    k_mixed_spmv<<<grid_for(D * 8, 256), 256, 0, s>>>(otf_rows(*this), dg.p, x, y, D);
+  else
+    k_mixed_spmv<<<grid_for(D * 8, 256), 256, 0, s>>>(csr_rows(*this), dg.p, x, y, D);
   QED_LAUNCH();
 }
 
@@ -507,12 +564,16 @@ int MixedHamiltonian::apply_full(const double *x, double xs, double *y, const Su
   if (!D) return 0;
   unsigned nb = grid_for(D * 8, 256);
   if (red_mask && nb > (unsigned)r.max_blocks) nb = (unsigned)r.max_blocks;
-  k_mixed_full<<<nb, 256, 0, s>>>(row_ptr.p, col.p, val.p, dg.p, x, xs, y, D, sub, red_mask, r.partials, skip);
+  if (on_the_fly)
+    k_mixed_full<<<nb, 256, 0, s>>>(otf_rows(*this), dg.p, x, xs, y, D, sub, red_mask, r.partials, skip);
+  else
+    k_mixed_full<<<nb, 256, 0, s>>>(csr_rows(*this), dg.p, x, xs, y, D, sub, red_mask, r.partials, skip);
   QED_LAUNCH();
   return (int)nb;
 }
 
 std::vector<double> MixedHamiltonian::dense(cudaStream_t s) const {
+  if (on_the_fly) fail(QED_ERR_INTERNAL, "dense form of an on-the-fly mixed Hamiltonian");
   std::vector<uint64_t> rp(D + 1);
   std::vector<uint32_t> c(nnz);
   std::vector<double> v(nnz), d(D), out(D * D, 0.0);

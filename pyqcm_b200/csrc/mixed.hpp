@@ -18,7 +18,11 @@
 // src_ed/Operators/HS_interaction_operator.hpp:44-53) is its own vector.
 //
 // H x is then a CSR product: eight lanes per row, HBM-bound on the column and
-// value arrays (12 bytes per entry), x gathered through L2.
+// value arrays (12 bytes per entry), x gathered through L2. Sectors whose CSR
+// would exceed mixed_csr_max_gb (or every sector of at least max_dim_full
+// states, with mixed_on_the_fly) store no matrix: each product recomputes the
+// entries from the states, eight lanes per row over the one-body elements
+// (on_the_fly), with the same epilogues.
 #pragma once
 
 #include <cstdint>
@@ -58,6 +62,10 @@ struct MixedHamiltonian {
   DevBuf<uint32_t> col;
   DevBuf<double> val;
   DevBuf<double> dg;         // diagonal
+  bool on_the_fly = false;   // no stored matrix: entries recomputed by every product
+  int n_terms = 0;           // off-diagonal one-body elements (kept for the on-the-fly products)
+  DevBuf<int> term_r, term_c;
+  DevBuf<double> term_v;
 
   MixedHamiltonian(const SymmetryGroup &G, const MixedTerms &t, int irrep, int n_up, int n_dn, cudaStream_t s);
   // y = H x on device vectors of D doubles, on stream s

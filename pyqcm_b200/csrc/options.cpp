@@ -65,6 +65,11 @@ struct Table {
     // above the job table, 72 without: the three captures per solve cost more than
     // the replays save on sectors of tens of thousands of states.
     b["lanczos_graphs"] = true;
+    // solver options: the symmetry-adapted (mixed-basis) Hamiltonian of a sector
+    // is stored as CSR unless that takes more than mixed_csr_max_gb gigabytes;
+    // then (or always, with mixed_on_the_fly) every product recomputes its entries.
+    b["mixed_on_the_fly"] = false;
+    d["mixed_csr_max_gb"] = 32.0;
     i["lanczos_graphs_min_dim"] = 131072;
     i["block_lanczos_min_dim"] = 1000;
     i["block_lanczos_min_p"] = 4;

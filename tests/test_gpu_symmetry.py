@@ -41,6 +41,42 @@ def test_mixed_hamiltonian_matches_reference_csr(qed, oracle, fresh, case, secto
         del H, R
 
 
+@pytest.mark.parametrize("case,sectors", [
+    ("sq2x3_c2v", ["R0:N6:S0", "R3:N6:S0", "R1:N5:S1"]),
+    ("c2v_8b_record", ["R0:N12:S0", "R2:N11:S1"]),
+])
+def test_mixed_on_the_fly_products_match_the_stored_matrix(qed, oracle, fresh, case, sectors):
+    """With no stored matrix (mixed_on_the_fly: every product recomputes the
+    entries) H x and the sector's lowest level are those of the CSR form and of
+    the reference's CSR Hamiltonian."""
+    prob = c2v_problem(c2v_golden(), True) if case == "c2v_8b_record" else _sq2x3_c2v()
+    suffix, label = fresh()
+    name = "otf" + suffix
+    qed.load_problem(prob, label, model_name=name)
+    oracle.load_problem(prob, label, model_name=name, fmt="S")
+    for sec in sectors:
+        qed.set_global_parameter("mixed_on_the_fly", False)
+        Hc = qed.MixedHamiltonian(label, sec)
+        qed.set_global_parameter("mixed_on_the_fly", True)
+        try:
+            Ho = qed.MixedHamiltonian(label, sec)
+        finally:
+            qed.set_global_parameter("mixed_on_the_fly", False)
+        R = oracle.RefHamiltonian(label, sec, csr=True)
+        x = np.random.default_rng(8).standard_normal(Hc.dim)
+        yc, yo, yr = np.zeros(Hc.dim), np.zeros(Hc.dim), np.zeros(Hc.dim)
+        Hc.mult_add(x, yc)
+        Ho.mult_add(x, yo)
+        R.mult_add(x, yr)
+        scale = max(1.0, np.max(np.abs(yr)))
+        assert np.max(np.abs(yo - yc)) <= 1e-13 * scale and np.max(np.abs(yo - yr)) <= 1e-13 * scale, sec
+        if Hc.dim > 256:
+            ec, _ = Hc.ground_state_energy()
+            eo, _ = Ho.ground_state_energy()
+            assert abs(eo - ec) <= 1e-12 * abs(ec), (sec, eo, ec)
+        del Hc, Ho, R
+
+
 def test_mixed_basis_ground_state_matches_reference_record(qed, oracle, fresh):
     """Lanczos on the device in the symmetry-adapted basis of the reference's C2v
     record: the record's ground-state energy (6 digits) and the compiled

@@ -354,8 +354,10 @@ def run_ours(args, world, rank, local):
                      "unit_of_work": "one H.v (column pass k_hv_cols16w + row pass k_hv_rows16), 16 B per basis state"},
         "e2e": {"value": aggregate_value(alg, e2e_s * 1e3, world), "unit": UNIT, "h2d_bytes_per_step": 8 * D,
                 "d2h_bytes_per_step": 8 * D,
-                "path": "qed_hamiltonian_mult_add (y += H x) on pinned host buffers: x up and H x down in row "
-                        "blocks overlapped with the row pass, y += H x on host threads"},
+                "path": "qed_hamiltonian_mult_add (y += H x) on pinned host buffers: x up in row blocks "
+                        "overlapped with the row pass, the down-spin pass by row blocks with H x down overlapped "
+                        "with it, y += H x on host threads; bound by the two transfers (H x needs all of x), "
+                        "8 B per state each way"},
         "gpu_launches": 2 * args.steps,
         "hv_tuning": qed.hv_tuning_report(),
         "clocks": clk,

@@ -1239,11 +1239,16 @@ int qed_hamiltonian_mult_add(qed_hamiltonian *h, const double *x, double *y) {
       blk.dn.dim = r1 - r0;
       launch_hv_rows(blk, h->x.p + off[k], 1.0, h->z.p + off[k], none, w.stream);
     }
-    launch_hv_cols(op, h->x.p, 1.0, h->z.p, 0, w.red, w.stream);
+    // the down-spin pass needs all of x; it runs by row blocks so that each
+    // block's download (copy stream) overlaps the next blocks' work
     for (int k = 0; k < kMultAddChunks; ++k) {
       const size_t n = off[k + 1] - off[k];
-      if (n) QED_CUDA(cudaMemcpyAsync(h->hz + off[k], h->z.p + off[k], n * sizeof(double), cudaMemcpyDeviceToHost, w.stream));
-      QED_CUDA(cudaEventRecord(h->ev_out[k], w.stream));
+      if (n) launch_hv_cols_rows(op, h->x.p, 1.0, h->z.p, (uint32_t)(off[k] / du), (uint32_t)(off[k + 1] / du),
+                                 w.stream);
+      QED_CUDA(cudaEventRecord(h->ev_in[k], w.stream));
+      QED_CUDA(cudaStreamWaitEvent(h->copy, h->ev_in[k], 0));
+      if (n) QED_CUDA(cudaMemcpyAsync(h->hz + off[k], h->z.p + off[k], n * sizeof(double), cudaMemcpyDeviceToHost, h->copy));
+      QED_CUDA(cudaEventRecord(h->ev_out[k], h->copy));
     }
     int nt = (int)std::thread::hardware_concurrency();
     nt = std::max(1, std::min(nt, 16));
@@ -1263,6 +1268,7 @@ int qed_hamiltonian_mult_add(qed_hamiltonian *h, const double *x, double *y) {
     add(0);
     for (auto &th : pool) th.join();
     if (bad) fail(QED_ERR_CUDA, "qed_hamiltonian_mult_add: device work failed");
+    QED_CUDA(cudaStreamSynchronize(h->copy));
     w.sync();
   });
 }

@@ -428,31 +428,33 @@ template <class T> __device__ __forceinline__ T gather_ld(const T *p, bool l2onl
   return l2only ? __ldcg(p) : __ldg(p);
 }
 
+// Output rows [r0, r1) of the down-spin pass (every row: r0 = 0, r1 = dd); the
+// gathers read every row of x.
 template <int VEC, bool CG>
 __global__ void __launch_bounds__(kThreads) k_hv_cols2(HvOperator op, const double *__restrict__ x,
                                                         double xs, double *y, int red_mask,
-                                                        double *partials) {
+                                                        double *partials, uint32_t r0, uint32_t r1) {
   if (op.skip && *op.skip) return;
   __shared__ double cval[kColsR][kMaxHops];
   __shared__ uint32_t cidx[kColsR][kMaxHops];
   __shared__ int ccnt[kColsR];
-  const uint32_t du = op.up.dim, dd = op.dn.dim;
+  const uint32_t du = op.up.dim, dd = r1;
   const uint32_t W = VEC * blockDim.x;
-  const uint32_t nchunk = (du + W - 1) / W, nrg = (dd + kColsR - 1) / kColsR;
+  const uint32_t nchunk = (du + W - 1) / W, nrg = (r1 - r0 + kColsR - 1) / kColsR;
   const size_t nitems = (size_t)nchunk * nrg;
   double red[3] = {0.0, 0.0, 0.0};
   for (size_t t = blockIdx.x; t < nitems; t += gridDim.x) {
     const uint32_t chunk = (uint32_t)(t / nrg), rg = (uint32_t)(t % nrg);
     __syncthreads();  // the previous item is done with the staged entries
     if (threadIdx.x < kColsR) {
-      const uint32_t d = rg * kColsR + threadIdx.x;
+      const uint32_t d = r0 + rg * kColsR + threadIdx.x;
       ccnt[threadIdx.x] = d < dd ? (int)op.dn.cnt[d] : 0;
     }
     for (int j = threadIdx.x; j < kColsR * kMaxHops; j += blockDim.x) {
       const int rr = j / kMaxHops, k = j % kMaxHops;
-      const uint32_t d = rg * kColsR + rr;
+      const uint32_t d = r0 + rg * kColsR + rr;
       if (d < dd && k < (int)op.dn.cnt[d]) {
-        const uint32_t e = __ldg(op.dn.ell + (size_t)k * dd + d);
+        const uint32_t e = __ldg(op.dn.ell + (size_t)k * op.dn.dim + d);
         cval[rr][k] = op.dn.vals[e & 255u];
         cidx[rr][k] = e >> 8;
       }
@@ -461,7 +463,7 @@ __global__ void __launch_bounds__(kThreads) k_hv_cols2(HvOperator op, const doub
     const uint32_t u0 = chunk * W + VEC * threadIdx.x;
     if (u0 >= du) continue;
     for (int rr = 0; rr < kColsR; ++rr) {
-      const uint32_t d = rg * kColsR + rr;
+      const uint32_t d = r0 + rg * kColsR + rr;
       if (d >= dd) break;
       const int c = ccnt[rr];
       const size_t base = (size_t)d * du + u0;
@@ -1842,14 +1844,26 @@ int launch_hv_cols(const HvOperator &op, const double *x, double xs, double *y, 
   int grid = hv_cols_grid(op);
   if (red_mask && grid > r.max_blocks) grid = r.max_blocks;
   const bool cg = hv_variant() & 1;
+  const uint32_t dd = op.dn.dim;
   if (vec2 && cg)
-    k_hv_cols2<2, true><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
+    k_hv_cols2<2, true><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials, 0u, dd);
   else if (vec2)
-    k_hv_cols2<2, false><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
+    k_hv_cols2<2, false><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials, 0u, dd);
   else
-    k_hv_cols2<1, false><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials);
+    k_hv_cols2<1, false><<<grid, kThreads, 0, s>>>(op, x, xs, y, red_mask, r.partials, 0u, dd);
   QED_LAUNCH();
   return grid;
+}
+
+void launch_hv_cols_rows(const HvOperator &op, const double *x, double xs, double *y, uint32_t r0, uint32_t r1,
+                         cudaStream_t s) {
+  if (r1 <= r0) return;
+  const int grid = hv_cols_grid(op);
+  if (op.up.dim % 2 == 0)
+    k_hv_cols2<2, false><<<grid, kThreads, 0, s>>>(op, x, xs, y, 0, nullptr, r0, r1);
+  else
+    k_hv_cols2<1, false><<<grid, kThreads, 0, s>>>(op, x, xs, y, 0, nullptr, r0, r1);
+  QED_LAUNCH();
 }
 
 // ---- staged H.v launch shapes and their autotuner ----

@@ -179,6 +179,9 @@ void launch_hv_rows(const HvOperator &op, const double *x, double xs, double *y,
 //   red_mask bit0: sum x*y, bit1: sum y*y, bit2: sum x*x   (post-update y)
 int launch_hv_cols(const HvOperator &op, const double *x, double xs, double *y, int red_mask,
                     Reducer &r, cudaStream_t s);
+// y += xs * (down-spin hops) x for output rows [r0, r1) only (x: every row)
+void launch_hv_cols_rows(const HvOperator &op, const double *x, double xs, double *y, uint32_t r0, uint32_t r1,
+                         cudaStream_t s);
 
 // Whole H.v with the column pass's reductions: y = xs H x - sum_k sub.c[k]
 // sub.z[k], reductions of the final y as launch_hv_cols; returns the block count

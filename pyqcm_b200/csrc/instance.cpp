@@ -493,7 +493,7 @@ void Instance::solve_sector(const Sector &s, SectorSolve &out, Workspace &ws, De
       it.out = &out.lanczos;
       it.where = where(s);
       std::lock_guard<std::mutex> l(defer->m);
-      (H.D <= kLanczosCtaMaxDim ? defer->items : defer->large).push_back(it);
+      (H.D <= lanczos_job_max_dim() ? defer->items : defer->large).push_back(it);
       defer->ops.push_back(std::move(Hp));
     } else {
       out.lanczos = lanczos_energy(H, ws, (uint64_t)opt_int("seed"));

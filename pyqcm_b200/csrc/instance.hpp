@@ -74,7 +74,7 @@ struct SectorSolve {
 struct DeferredSectors {
   std::mutex m;
   std::vector<std::unique_ptr<SectorOp>> ops;
-  std::vector<LanczosBatchItem> items;  // at most kLanczosCtaMaxDim states: one batched pass
+  std::vector<LanczosBatchItem> items;  // at most lanczos_job_max_dim() states: one batched pass
   std::vector<LanczosBatchItem> large;  // the others: one task each
 };
 

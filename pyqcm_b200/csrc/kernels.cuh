@@ -111,10 +111,15 @@ int launch_axpy_dev(size_t D, double *y, const double *x, const double *a_dev, R
                     const int *skip = nullptr);
 // y *= 1 / sqrt(*b2_cur) (0 if that is 0); records alpha_j, beta_j and advances *j.
 void launch_lanczos_advance(size_t D, double *y, const LanczosScalars &ls, cudaStream_t s);
-constexpr size_t kLanczosCtaMaxDim = 8192;
+// Largest sector the one-CTA-per-sector job table takes (the option
+// lanczos_job_max_dim, at most kLanczosCtaMaxDimCap; larger sectors run the
+// whole-GPU kernels step by step). Read once per solve step: the eigenvalue and
+// the eigenvector pass of a state must see the same value.
+constexpr size_t kLanczosCtaMaxDimCap = 1u << 20;
+size_t lanczos_job_max_dim();
 
 // Ground-state Lanczos of many small sectors in one launch, one CTA of kLanczosJobThreads threads per
-// sector (dimension at most kLanczosCtaMaxDim): the ground-state Lanczos
+// sector (dimension at most lanczos_job_max_dim()): the ground-state Lanczos
 // chunks of a whole batch of sectors advance together. Buffer roles of a job:
 // v_{j-1} = v[rot], v_j = v[(rot + 1) % 3], scratch = v[(rot + 2) % 3]; they
 // rotate once per step. out receives alpha then beta of the launch's steps

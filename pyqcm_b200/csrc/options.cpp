@@ -65,6 +65,13 @@ struct Table {
     // above the job table, 72 without: the three captures per solve cost more than
     // the replays save on sectors of tens of thousands of states.
     b["lanczos_graphs"] = true;
+    // solver option: sectors of at most this many states run the ground-state
+    // Lanczos in the one-CTA-per-sector job table (see lanczos_energy_batch).
+    // Measured on a B200 (1024 random clusters, default bench batch): 73 solves/s
+    // at 8192 (sectors above it step by step on whole-GPU kernels, 16 host
+    // threads), 125-128 at 65536 (every sector of those clusters in the table;
+    // energies equal to 1e-15, G to 5e-12).
+    i["lanczos_job_max_dim"] = 65536;
     // solver options: the symmetry-adapted (mixed-basis) Hamiltonian of a sector
     // is stored as CSR unless that takes more than mixed_csr_max_gb gigabytes;
     // then (or always, with mixed_on_the_fly) every product recomputes its entries.

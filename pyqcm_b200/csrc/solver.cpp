@@ -301,7 +301,7 @@ namespace {
 // it from the per-sector start kernel of the batched eigenvalue pass, so that
 // the eigenvector pass replays the same v_0.
 void start_vector(size_t D, uint64_t seed, double *v, Workspace &ws) {
-  if (D <= kLanczosCtaMaxDim) {
+  if (D <= lanczos_job_max_dim()) {
     DevBuf<double> prev(D), bp(1);
     LanczosJob J;
     J.op.up.dim = (uint32_t)D;
@@ -358,6 +358,11 @@ ParallelFor &parallel_for_hook() {
 
 void set_parallel_for(ParallelFor f) { parallel_for_hook() = std::move(f); }
 
+size_t lanczos_job_max_dim() {
+  const long v = opt_int("lanczos_job_max_dim");
+  return (size_t)std::max<long>(0, std::min<long>(v, (long)kLanczosCtaMaxDimCap));
+}
+
 void lanczos_energy_batch(std::vector<LanczosBatchItem> &items, Workspace &ws) {
   PhaseScope ps(kPhGsLanczos);
   const int n = (int)items.size();
@@ -371,7 +376,7 @@ void lanczos_energy_batch(std::vector<LanczosBatchItem> &items, Workspace &ws) {
   std::vector<size_t> off(n);
   size_t tot = 0;
   for (int i = 0; i < n; ++i) {
-    if (items[i].H->D > kLanczosCtaMaxDim) fail(QED_ERR_INTERNAL, "lanczos_energy_batch: sector too large");
+    if (items[i].H->D > lanczos_job_max_dim()) fail(QED_ERR_INTERNAL, "lanczos_energy_batch: sector too large");
     off[i] = tot;
     tot += 3 * ((items[i].H->D + 3) / 4 * 4);
   }
@@ -518,7 +523,7 @@ struct ChunkGraphs {
 };
 
 LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed) {
-  if (H.D <= kLanczosCtaMaxDim) {
+  if (H.D <= lanczos_job_max_dim()) {
     LanczosResult res;
     std::vector<LanczosBatchItem> one(1);
     one[0].H = &H;

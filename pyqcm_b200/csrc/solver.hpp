@@ -86,7 +86,7 @@ struct LanczosResult {
   std::vector<double> alpha, beta;
 };
 LanczosResult lanczos_energy(const SectorOp &H, Workspace &ws, uint64_t seed);
-// The eigenvalue pass of many sectors of at most kLanczosCtaMaxDim states at
+// The eigenvalue pass of many sectors of at most lanczos_job_max_dim() states at
 // once: one CTA per sector, all sectors advancing by chunks in one launch, the
 // Ritz test of each applied on the host after every chunk. Results are those
 // of lanczos_energy, which runs a single small sector through the same path.

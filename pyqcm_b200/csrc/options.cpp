@@ -70,7 +70,8 @@ struct Table {
     // Measured on a B200 (1024 random clusters, default bench batch): 73 solves/s
     // at 8192 (sectors above it step by step on whole-GPU kernels, 16 host
     // threads), 125-128 at 65536 (every sector of those clusters in the table;
-    // energies equal to 1e-15, G to 5e-12).
+    // energies equal to 1e-15, G to 5e-12). 256 bath points (853776-state
+    // sectors): 44.7 solves/s at 65536, 24.8 at 2^20 (one CTA is too little there).
     i["lanczos_job_max_dim"] = 65536;
     // solver options: the symmetry-adapted (mixed-basis) Hamiltonian of a sector
     // is stored as CSR unless that takes more than mixed_csr_max_gb gigabytes;

@@ -55,7 +55,9 @@ struct Table {
     // on a B200 (Green function of one instance, band against block form): p = 8,
     // 4900 states 83 / 57 ms; p = 10, 63504 states 107 / 68 ms; p = 12, 853776
     // states 588 / 432 ms; p = 4, 16 concurrent 853776-state instances, 32.8 / 32.7
-    // solves/s. Smaller p and sectors were not measured.
+    // solves/s; 1024 random clusters (bench batch): 112 solves/s with the block form
+    // from 1000 states, 142 from 200 states (also 142 from 50 states and p = 2; G
+    // equal to 2e-13 between the three).
     // solver option: the 16-step chunks of the ground-state Lanczos of sectors of
     // at least lanczos_graphs_min_dim states are captured once per solve into
     // CUDA graphs (one per rotation of the three Krylov buffers) and replayed.
@@ -79,7 +81,7 @@ struct Table {
     b["mixed_on_the_fly"] = false;
     d["mixed_csr_max_gb"] = 32.0;
     i["lanczos_graphs_min_dim"] = 131072;
-    i["block_lanczos_min_dim"] = 1000;
+    i["block_lanczos_min_dim"] = 200;
     i["block_lanczos_min_p"] = 4;
     i["seed"] = 0;
     i["GF_lookup_depth"] = 64;

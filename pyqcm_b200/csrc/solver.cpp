@@ -406,8 +406,12 @@ void lanczos_energy_batch(std::vector<LanczosBatchItem> &items, Workspace &ws) {
   }
   djobs.upload(jobs.data(), n, s);
   launch_lanczos_start_jobs(djobs.p, n, s);
+  // largest sectors first: CTAs start in table order, so the longest jobs of a
+  // chunk do not wait behind the short ones (each job's arithmetic does not
+  // depend on its place in the table)
   std::vector<int> active(n);
   for (int i = 0; i < n; ++i) active[i] = i;
+  std::stable_sort(active.begin(), active.end(), [&](int a, int b) { return items[a].H->D > items[b].H->D; });
   std::vector<LanczosJob> batch;
   std::vector<double> hout;
   while (!active.empty()) {

@@ -15,7 +15,9 @@ then their Omega on the GPU grid).
 """
 from __future__ import annotations
 
+import os
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -57,7 +59,16 @@ class OmegaEvaluator:
         try:
             qed.ground_state_solve_batch(labels, threads=self.threads)
             qed.Green_function_solve_batch(labels, threads=self.threads)
-            out = np.array([I.Potthoff_functional(self.freqs, self.weights, self.nk) for I in insts])
+            # the (frequency, k) sums of the instances on host threads: each call
+            # holds only its own instance and its thread's stream, and the C calls
+            # release the interpreter lock
+            omega = lambda I: I.Potthoff_functional(self.freqs, self.weights, self.nk)
+            nt = min(len(insts), self.threads or min(16, os.cpu_count() or 1))
+            if nt > 1:
+                with ThreadPoolExecutor(max_workers=nt) as pool:
+                    out = np.array(list(pool.map(omega, insts)))
+            else:
+                out = np.array([omega(I) for I in insts])
         finally:
             for I in insts:
                 I.erase()

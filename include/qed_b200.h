@@ -55,6 +55,21 @@ int qed_last_error(char *buf, int len);
  * of every candidate (ms per H.v). Writes at most len - 1 bytes
  * and a terminating 0; returns the full length. */
 int qed_hv_tuning_report(char *buf, int len);
+/* No counterpart in the reference: diagnostics of the window H.v kernels of
+ * large sectors (host only, no device needed). qed_window_plan plans the windows
+ * of one spin (L sites, N particles, npairs directed hopping pairs pd[q] <- ps[q]
+ * of amplitude amp[q]) and, when they fit, applies the window form of that
+ * spin's hop operator to x (C(L, N) doubles in basis order) on the host into y;
+ * *nwindows = 0 when the pairs do not fit windows. qed_window_compile compiles
+ * the window kernels of a sector whose two spins have those pairs (N_up, N_dn
+ * particles) with NVRTC and writes its log (ptxas registers and spills) to buf;
+ * *ok = 1 on success. */
+int qed_window_plan(int L, int N, int npairs, const int *pd, const int *ps, const double *amp, const double *x,
+                    double *y, int *nwindows);
+int qed_window_compile(int L, int n_up, int n_dn, int npairs, const int *pd, const int *ps, char *buf, int len,
+                       int *ok);
+/* Number of H.v calls that ran the window kernels so far in this process. */
+int qed_window_launches(long long *n);
 
 /* Selects the CUDA device used by this process (default 0). */
 int qed_init(int device);

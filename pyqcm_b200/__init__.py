@@ -64,6 +64,9 @@ def lib():
     sig = {
         "qed_last_error": [C.c_char_p, C.c_int],
         "qed_hv_tuning_report": [C.c_char_p, C.c_int],
+        "qed_window_plan": [C.c_int, C.c_int, C.c_int, ip, ip, dp, dp, dp, ip],
+        "qed_window_compile": [C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, C.c_char_p, C.c_int, ip],
+        "qed_window_launches": [C.POINTER(C.c_longlong)],
         "qed_init": [C.c_int],
         "qed_set_global_int": [C.c_char_p, C.c_long],
         "qed_set_global_double": [C.c_char_p, C.c_double],
@@ -725,6 +728,39 @@ def hv_tuning_report():
     buf = C.create_string_buffer(n + 1)
     lib().qed_hv_tuning_report(buf, n + 1)
     return json.loads(buf.value.decode() or "[]")
+
+
+def window_plan(L: int, N: int, pd, ps, amp, x):
+    """The window form of one spin's hop operator applied on the host
+    (qed_window_plan): returns (number of windows, y); 0 windows and y = None when
+    the pairs pd[q] <- ps[q] do not fit windows of eight consecutive sites."""
+    pd = np.ascontiguousarray(pd, dtype=np.int32)
+    ps = np.ascontiguousarray(ps, dtype=np.int32)
+    amp = np.ascontiguousarray(amp, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros_like(x)
+    nw = C.c_int()
+    _check(lib().qed_window_plan(L, N, len(pd), _ip(pd), _ip(ps), _dp(amp), _dp(x), _dp(y), C.byref(nw)))
+    return nw.value, (y if nw.value else None)
+
+
+def window_compile(L: int, n_up: int, n_dn: int, pd, ps):
+    """Compiles the window H.v kernels for a sector whose spins hop on pairs
+    pd[q] <- ps[q] (NVRTC, no device needed); returns (ok, log with the ptxas
+    register and spill lines)."""
+    pd = np.ascontiguousarray(pd, dtype=np.int32)
+    ps = np.ascontiguousarray(ps, dtype=np.int32)
+    buf = C.create_string_buffer(1 << 16)
+    ok = C.c_int()
+    _check(lib().qed_window_compile(L, n_up, n_dn, len(pd), _ip(pd), _ip(ps), buf, len(buf), C.byref(ok)))
+    return bool(ok.value), buf.value.decode(errors="replace")
+
+
+def window_launches() -> int:
+    """H.v calls that ran the window kernels so far in this process."""
+    n = C.c_longlong()
+    _check(lib().qed_window_launches(C.byref(n)))
+    return n.value
 
 
 # ------------------------------------------------------------ instance checkpoints --

@@ -62,7 +62,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if verbose and out.strip():
             print(out)
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs])
+        _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs, "-ldl"])
     return LIB
 
 

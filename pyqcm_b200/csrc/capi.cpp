@@ -337,6 +337,55 @@ int qed_hv_tuning_report(char *buf, int len) {
   return (int)r.size();
 }
 
+namespace {
+std::vector<uint32_t> all_strings(int L, int N) {
+  if (L < 1 || L > 24 || N < 0 || N > L) fail(QED_ERR_ARGUMENT, "window diagnostics: L in [1, 24], N in [0, L]");
+  std::vector<uint32_t> b;
+  for (uint32_t s = 0; s < (1u << L); ++s)
+    if (__builtin_popcount(s) == N) b.push_back(s);
+  return b;
+}
+}  // namespace
+
+int qed_window_plan(int L, int N, int npairs, const int *pd, const int *ps, const double *amp, const double *x,
+                    double *y, int *nwindows) {
+  return guarded([&] {
+    if (npairs < 0 || !nwindows) fail(QED_ERR_ARGUMENT, "qed_window_plan: bad arguments");
+    const std::vector<uint32_t> bits = all_strings(L, N);
+    WindowPlan P;
+    *nwindows = 0;
+    if (!plan_windows(L, N, bits, std::vector<int>(pd, pd + npairs), std::vector<int>(ps, ps + npairs), P)) return;
+    *nwindows = (int)P.win.size();
+    window_apply_host(P, std::vector<double>(amp, amp + npairs), x, y);
+  });
+}
+
+int qed_window_compile(int L, int n_up, int n_dn, int npairs, const int *pd, const int *ps, char *buf, int len,
+                       int *ok) {
+  return guarded([&] {
+    if (npairs < 0 || !ok) fail(QED_ERR_ARGUMENT, "qed_window_compile: bad arguments");
+    const std::vector<int> vd(pd, pd + npairs), vs(ps, ps + npairs);
+    WindowPlan pu, pdn;
+    if (!plan_windows(L, n_up, all_strings(L, n_up), vd, vs, pu) ||
+        !plan_windows(L, n_dn, all_strings(L, n_dn), vd, vs, pdn))
+      fail(QED_ERR_UNSUPPORTED, "qed_window_compile: the pairs do not fit windows");
+    bool good = false;
+    const std::string log = window_compile_log(pu, pdn, &good);
+    *ok = good ? 1 : 0;
+    if (buf && len > 0) {
+      std::strncpy(buf, log.c_str(), (size_t)len - 1);
+      buf[len - 1] = 0;
+    }
+  });
+}
+
+int qed_window_launches(long long *n) {
+  return guarded([&] {
+    if (!n) fail(QED_ERR_ARGUMENT, "qed_window_launches: null pointer");
+    *n = window_launches();
+  });
+}
+
 int qed_init(int device) {
   return guarded([&] {
     if (g_device_fixed && device != g_device) fail(QED_ERR_ARGUMENT, "qed_init: device already selected");

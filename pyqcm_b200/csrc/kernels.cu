@@ -17,6 +17,7 @@
 
 #include "common.hpp"
 #include "kernels.cuh"
+#include "winhv.hpp"
 
 namespace qed {
 
@@ -1993,6 +1994,7 @@ int staged_shape(const HvOperator &op, const double *x, double *y, Reducer &r, s
 
 int launch_hv_impl(const HvOperator &op, const double *x, double xs, double *y, const SubList &sub, int red_mask,
                    Reducer &r, cudaStream_t s, bool may_tune) {
+  if (op.win && window_usable(op, x, y, sub)) return launch_hv_windows(op, x, xs, y, sub, red_mask, r, s);
   const size_t smr = staged_disabled() ? 0 : rows16_smem(op);
   const size_t smc = smr ? cols16_smem(op) : 0;
   bool staged = smr && smc && aligned16(x) && aligned16(y);
@@ -2034,7 +2036,7 @@ void launch_block_hv(const HvOperator &op, int p, const BlockIn &X, const BlockO
   if (p < 1 || p > 16) fail(QED_ERR_ARGUMENT, "block H.v: block size outside [1, 16]");
   const size_t D = (size_t)op.up.dim * op.dn.dim;
   if (!D) return;
-  bool staged = !staged_disabled() && rows16_smem(op) && cols16_smem(op);
+  bool staged = op.win || (!staged_disabled() && rows16_smem(op) && cols16_smem(op));
   for (int c = 0; c < p && staged; ++c) staged = aligned16(X.v[c]) && aligned16(Y.v[c]);
   if (staged) {  // large sectors: the staged single-vector kernels, one vector at a time
     SubList none;

@@ -50,6 +50,9 @@ struct HvOperator {
   InterSpin inter;
   int num_sms = 148;
   const int *skip = nullptr;  // if set and *skip != 0 (device), the H.v passes do nothing
+  // host-side binding of the window kernels (WinBinding, winhv.hpp), null when
+  // the sector does not use them; device code never reads it
+  const void *win = nullptr;
 };
 
 // List of (coefficient, vector) pairs subtracted in the row pass epilogue:

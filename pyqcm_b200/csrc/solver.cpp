@@ -120,6 +120,10 @@ void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
       pslot.push_back(slot);
     }
   if (vals.size() > 256) fail(QED_ERR_UNSUPPORTED, "more than 128 distinct hopping amplitudes per spin");
+  h.pd = pd;
+  h.ps = ps;
+  h.pv.resize(pd.size());
+  for (size_t q = 0; q < pd.size(); ++q) h.pv[q] = t[(size_t)pd[q] * L + ps[q]];
   int width = std::min<int>((int)pd.size(), N * (L - N));
   if (width > 255) fail(QED_ERR_UNSUPPORTED, "more than 255 hops per basis string");
   h.width = width;
@@ -265,7 +269,25 @@ SectorOp::SectorOp(const SpinData &t, const Sector &s, Workspace &ws, HalfCache 
   int dev = 0;
   QED_CUDA(cudaGetDevice(&dev));
   QED_CUDA(cudaDeviceGetAttribute(&op.num_sms, cudaDevAttrMultiProcessorCount, dev));
+  bind_windows();
   ws.sync();
+}
+
+void SectorOp::bind_windows() {
+  if (!opt_bool("hv_windows") || D < (size_t)opt_int("hv_windows_min_dim") || up->pd.empty() || dn->pd.empty())
+    return;
+  WindowPlan pu, pdn;
+  if (!plan_windows(up->L, up->N, up->hbits, up->pd, up->ps, pu) ||
+      !plan_windows(dn->L, dn->N, dn->hbits, dn->pd, dn->ps, pdn))
+    return;
+  std::string why;
+  auto mod = window_module(pu, pdn, &why);
+  if (!mod) return;  // the staged kernels take the sector
+  win = std::make_shared<WinBinding>();
+  win->mod = mod;
+  win->amp_up = up->pv;
+  win->amp_dn = dn->pv;
+  op.win = win.get();
 }
 
 KrylovOp::KrylovOp(const MixedHamiltonian &h) : D(h.D), mixed(&h) {}

@@ -15,6 +15,7 @@
 #include "common.hpp"
 #include "kernels.cuh"
 #include "model.hpp"
+#include "winhv.hpp"
 
 namespace qed {
 
@@ -50,6 +51,9 @@ struct HalfTables {
   DevBuf<uint16_t> pk[2];
   DevBuf<uint8_t> cntw;
   double mag[2] = {0.0, 0.0};
+  // the directed hopping pairs (destination r, source c) and their t[r][c]
+  std::vector<int> pd, ps;
+  std::vector<double> pv;
 };
 
 // Per-instance cache of the spin tables: a sector (N_up, N_dn) uses the up
@@ -65,6 +69,7 @@ struct SectorOp {
   int L = 0;
   std::shared_ptr<const HalfTables> up, dn;
   DevBuf<double> vinter;
+  std::shared_ptr<WinBinding> win;  // window H.v kernels of large sectors (winhv.hpp)
   HvOperator op;
   size_t D = 0;
   // Builds (or takes from `cache`) the tables for `sec` from the collected
@@ -72,6 +77,9 @@ struct SectorOp {
   SectorOp(const SpinData &terms, const Sector &sec, Workspace &ws, HalfCache *cache = nullptr);
   // y = H x (device vectors)
   void apply(const double *x, double *y, Workspace &ws) const;
+  // Plans the window kernels for this sector and binds them to op (large
+  // sectors whose hops fit windows; see hv_windows / hv_windows_min_dim).
+  void bind_windows();
 };
 
 // Ground state by Lanczos (LanczosEigenvalue + LanczosEigenvector,

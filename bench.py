@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: warm-up and timed H.v only (no e2e, clocks or CPU baseline)")
     ap.add_argument("--sector", default=None, help="sector of the 4x4 cluster to use (default R0:N16:S0)")
+    ap.add_argument("--hv-windows", action="store_true",
+                    help="with --profile: H.v through the window kernels (option hv_windows) instead of the "
+                         "staged ones")
     ap.add_argument("--workload", default="hv", choices=["hv", "batch", "baths", "vca", "cdmft"],
                     help="hv: H.v on the 4x4 cluster (default); batch: independent random clusters, "
                          "every sector, ground state + Green function; baths: 2x2 + 8-bath points; "
@@ -255,6 +258,10 @@ def run_ours(args, world, rank, local):
         prob.sectors = args.sector
     label = 7000 + rank
     qed.load_problem(prob, label, model_name="bench_sq4x4", fmt="F")
+    if args.hv_windows:
+        if not args.profile:
+            raise SystemExit("--hv-windows is a profiling switch: use it with --profile")
+        qed.set_global_parameter("hv_windows", True)
     H = qed.Hamiltonian(label, prob.sectors)
     D = H.dim
     g = torch.Generator(device=f"cuda:{local}").manual_seed(1234 + rank)
@@ -288,6 +295,7 @@ def run_ours(args, world, rank, local):
         if rank == 0:
             print(json.dumps({"profile": True, "dim": D, "ms_per_hv": ms,
                               "GBps_16D": 16.0 * D / (ms * 1e-3) / 1e9,
+                              "window_launches": qed.window_launches(),
                               "hv_tuning": qed.hv_tuning_report()}), flush=True)
         return
     # end to end through the C ABI with host buffers (y += H x, copies inside)

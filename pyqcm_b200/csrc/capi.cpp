@@ -18,14 +18,38 @@
 #include "symmetry.hpp"
 #include "mixed.hpp"
 #include "qed_b200.h"
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 #include "worker_pool.hpp"
 
 using namespace qed;
 
 // mult_add pipeline: x goes up in kMultAddChunks row blocks, each block's row
 // pass starting as soon as its copy lands; H x comes back in the same blocks and
-// the host adds each block into y while the next one is in flight.
-constexpr int kMultAddChunks = 8;
+// the host adds each block into y while the next one is in flight. Only the
+// last block's add runs after the transfers end, so blocks are small (41 MB of
+// H x each on the 4x4 sector).
+constexpr int kMultAddChunks = 32;
+
+// y[i] += s[i]. The sums are not read again soon, so where y is 16-byte aligned
+// they are written with non-temporal stores: no read-for-ownership of y's lines,
+// 24 instead of 32 bytes of host memory traffic per element. Same sums as the
+// scalar loop (plain IEEE additions).
+static void add_streaming(double *y, const double *s, size_t n) {
+  size_t i = 0;
+#if defined(__SSE2__)
+  for (; i < n && ((uintptr_t)(y + i) & 15u); ++i) y[i] += s[i];
+  for (; i + 4 <= n; i += 4) {
+    const __m128d a = _mm_add_pd(_mm_load_pd(y + i), _mm_loadu_pd(s + i));
+    const __m128d b = _mm_add_pd(_mm_load_pd(y + i + 2), _mm_loadu_pd(s + i + 2));
+    _mm_stream_pd(y + i, a);
+    _mm_stream_pd(y + i + 2, b);
+  }
+  _mm_sfence();
+#endif
+  for (; i < n; ++i) y[i] += s[i];
+}
 
 struct qed_mixed_hamiltonian {
   std::unique_ptr<MixedHamiltonian> H;
@@ -1309,7 +1333,7 @@ int qed_hamiltonian_mult_add(qed_hamiltonian *h, const double *x, double *y) {
           return;
         }
         const size_t n = off[k + 1] - off[k], a = off[k] + n * t / nt, b = off[k] + n * (t + 1) / nt;
-        for (size_t i = a; i < b; ++i) y[i] += h->hz[i];
+        add_streaming(y + a, h->hz + a, b - a);
       }
     };
     std::vector<std::thread> pool;

@@ -16,6 +16,7 @@
 #include <string>
 
 #include "common.hpp"
+#include "options.hpp"
 #include "kernels.cuh"
 #include "winhv.hpp"
 
@@ -1701,16 +1702,12 @@ constexpr size_t kRowSmemMax = 112 * 1024;
 constexpr size_t kRowSmem2Max = 220 * 1024;  // below the 227 KB per-CTA limit
 }
 
-// Launch variant of the H.v passes (bit 0: column-pass gathers cached in L2
-// only; bit 1: row pass with four gathers in flight). QED_HV_VARIANT overrides
-// the default 2 (on the 4x4 sector: 5.47 ms per H.v against 5.57 ms for 0).
-int hv_variant() {
-  static const int v = [] {
-    const char *e = getenv("QED_HV_VARIANT");
-    return e ? atoi(e) : 2;
-  }();
-  return v;
-}
+// Launch variant of the H.v passes of sectors without the staged kernels (the
+// solver option hv_variant; bit 0: column-pass gathers cached in L2 only; bit 1:
+// row pass with four gathers in flight; bit 2: staged kernels off). Default 2
+// (on the 4x4 sector with the staged kernels off: 5.47 ms per H.v against 5.57 ms
+// for 0). The staged kernels pick their launch shape by timing (below).
+int hv_variant() { return (int)opt_int("hv_variant"); }
 
 namespace {
 

@@ -81,6 +81,10 @@ struct Table {
     b["mixed_on_the_fly"] = false;
     d["mixed_csr_max_gb"] = 32.0;
     i["lanczos_graphs_min_dim"] = 131072;
+    // solver option: launch variant of the H.v kernels of sectors without the
+    // staged kernels (bits: 1 L2-only column gathers, 2 row pass with four
+    // gathers in flight, 4 staged kernels off); see hv_variant (kernels.cu).
+    i["hv_variant"] = 2;
     // solver options: with hv_windows, sectors of at least hv_windows_min_dim
     // states whose hops fit windows of eight consecutive sites run their H.v
     // through the window kernels (winhv.hpp), compiled at run time for the

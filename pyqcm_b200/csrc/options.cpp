@@ -85,6 +85,9 @@ struct Table {
     // staged kernels (bits: 1 L2-only column gathers, 2 row pass with four
     // gathers in flight, 4 staged kernels off); see hv_variant (kernels.cu).
     i["hv_variant"] = 2;
+    // solver option: spin tables of at most this many strings are built on the
+    // host (the same tables as the device build, uploaded at once).
+    i["host_table_max_dim"] = 4096;
     // solver options: with hv_windows, sectors of at least hv_windows_min_dim
     // states whose hops fit windows of eight consecutive sites run their H.v
     // through the window kernels (winhv.hpp), compiled at run time for the

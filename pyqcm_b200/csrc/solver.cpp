@@ -86,6 +86,96 @@ constexpr double kSmall = 1.0e-12;  // SMALL_VALUE (src_util/vector_num.hpp:23)
 // staged-row H.v kernels read (smaller sectors never take those kernels).
 constexpr uint64_t kPackMinDim = 512;
 
+// Host build of a small spin table: the same strings (increasing), ELL entries
+// (in the order of k_build_hops, which applies c+_r c_c when bit c is set and
+// bit r empty with the parity of the set bits strictly between r and c), bank
+// ordering / packing and diagonal (in the summation order of k_diag_half) as the
+// device path.
+void build_half_host(HalfTables &h, int L, int N, const std::vector<double> &tdiag,
+                     const std::vector<double> &vsame, const std::vector<int> &pd, const std::vector<int> &ps,
+                     const std::vector<int> &pslot, const std::vector<double> &vals, int width, Workspace &ws,
+                     bool bank_order) {
+  const uint32_t dim = h.dim;
+  std::vector<uint32_t> hb;
+  hb.reserve(dim);
+  uint64_t sv = N >= 64 ? ~0ull : (1ull << N) - 1ull;
+  while (true) {  // N-subsets of L bits in increasing order (Gosper's successor)
+    hb.push_back((uint32_t)sv);
+    if (hb.size() == dim) break;
+    const uint64_t c = sv & (~sv + 1ull), r = sv + c;
+    sv = (((r ^ sv) >> 2) / c) | r;
+  }
+  std::vector<uint32_t> he((size_t)width * dim, 0u);
+  std::vector<uint8_t> hc(dim, 0);
+  std::vector<double> hd(dim);
+  for (uint32_t i = 0; i < dim; ++i) {
+    const uint32_t b = hb[i];
+    int k = 0;
+    for (size_t q = 0; q < pd.size(); ++q) {
+      const int r = pd[q], c = ps[q];
+      if (!((b >> c) & 1u) || ((b >> r) & 1u)) continue;
+      const uint32_t nb = b ^ (1u << c) ^ (1u << r);
+      const int lo = std::min(r, c), hi = std::max(r, c);
+      const uint32_t between = (uint32_t)(((1ull << hi) - 1ull) & ~((2ull << lo) - 1ull));
+      const int sgn = __builtin_popcount(nb & between) & 1;
+      const uint32_t J = (uint32_t)(std::lower_bound(hb.begin(), hb.end(), nb) - hb.begin());
+      if (k < width) he[(size_t)k * dim + i] = (J << 8) | (uint32_t)(pslot[q] + sgn);
+      ++k;
+    }
+    hc[i] = (uint8_t)std::min(k, width);
+    double sd = 0.0;
+    for (int r = 0; r < L; ++r)
+      if ((b >> r) & 1u) {
+        sd += tdiag[r];
+        for (int c = r; c < L; ++c)
+          if ((b >> c) & 1u) sd += vsame[(size_t)r * L + c];
+      }
+    hd[i] = sd;
+  }
+  // the bank-ordered copy: packed for the staged kernels, and the ELL itself for the up spin
+  std::vector<double> fvals(vals);
+  int fwidth = width;
+  PackedHops ph;
+  bool packed = false;
+  const bool want_pack = dim >= kPackMinDim && dim + 8 <= (1u << 14);
+  if (width > 0 && (bank_order || want_pack) && dim >= 64 && vals.size() < 256) {
+    std::vector<uint32_t> eo(he);
+    std::vector<uint8_t> co(hc);
+    const int zero_slot = (int)vals.size();
+    int w2 = width;
+    std::vector<double> vz(vals);
+    vz.push_back(0.0);
+    if (order_for_banks(eo, co, dim, w2, zero_slot)) {
+      packed = want_pack && pack_hops16(eo, co, dim, vz, zero_slot, ph);
+      if (bank_order) {
+        fvals = vz;
+        fwidth = w2;
+        he.swap(eo);
+        hc.swap(co);
+      }
+    }
+  }
+  h.width = fwidth;
+  h.nvals = (int)fvals.size();
+  h.bits.upload(hb, ws.stream);
+  h.cnt.upload(hc, ws.stream);
+  h.vals.alloc(std::max<size_t>(fvals.size(), 1));
+  if (!fvals.empty()) h.vals.upload(fvals, ws.stream);
+  if (fwidth > 0) h.ell.upload(he, ws.stream);
+  h.diag.upload(hd, ws.stream);
+  if (packed) {
+    for (int c = 0; c < 2; ++c) {
+      if (ph.pk[c].empty()) ph.pk[c].assign(4, 0);  // a valid pointer for an empty class
+      h.pk[c].upload(ph.pk[c], ws.stream);
+    }
+    h.cntw.upload(ph.cnt, ws.stream);
+    h.mag[0] = ph.mag[0];
+    h.mag[1] = ph.mag[1];
+  }
+  h.hbits = std::move(hb);
+  ws.sync();
+}
+
 void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
                 const std::vector<double> &vsame, Workspace &ws, bool bank_order) {
   h.L = L;
@@ -94,8 +184,6 @@ void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
   if (dim >= (1ull << 24)) fail(QED_ERR_UNSUPPORTED, "half basis dimension above 2^24");
   h.dim = (uint32_t)dim;
   if (!dim) return;
-  h.bits.alloc(dim);
-  launch_unrank(L, N, h.dim, h.bits.p, ws.stream);
   // directed hop pairs (dst r, src c) with value slots; value table dedupes |t|
   std::vector<int> pd, ps, pslot;
   std::vector<double> vals;
@@ -126,6 +214,17 @@ void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
   for (size_t q = 0; q < pd.size(); ++q) h.pv[q] = t[(size_t)pd[q] * L + ps[q]];
   int width = std::min<int>((int)pd.size(), N * (L - N));
   if (width > 255) fail(QED_ERR_UNSUPPORTED, "more than 255 hops per basis string");
+  std::vector<double> tdiag(L);
+  for (int r = 0; r < L; ++r) tdiag[r] = t[(size_t)r * L + r];
+  // Spin tables of at most host_table_max_dim strings are built on the host and
+  // uploaded once (one stream synchronisation instead of five, no kernel
+  // launches): a batch of small clusters builds tens of thousands of them.
+  if ((long)dim <= opt_int("host_table_max_dim")) {
+    build_half_host(h, L, N, tdiag, vsame, pd, ps, pslot, vals, width, ws, bank_order);
+    return;
+  }
+  h.bits.alloc(dim);
+  launch_unrank(L, N, h.dim, h.bits.p, ws.stream);
   h.width = width;
   h.nvals = (int)vals.size();
   h.cnt.alloc(dim);
@@ -178,8 +277,6 @@ void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
   } else {
     QED_CUDA(cudaMemsetAsync(h.cnt.p, 0, dim, ws.stream));
   }
-  std::vector<double> tdiag(L);
-  for (int r = 0; r < L; ++r) tdiag[r] = t[(size_t)r * L + r];
   DevBuf<double> dt(L), dv(vsame.size());
   dt.upload(tdiag, ws.stream);
   dv.upload(vsame, ws.stream);

@@ -1707,7 +1707,16 @@ constexpr size_t kRowSmem2Max = 220 * 1024;  // below the 227 KB per-CTA limit
 // row pass with four gathers in flight; bit 2: staged kernels off). Default 2
 // (on the 4x4 sector with the staged kernels off: 5.47 ms per H.v against 5.57 ms
 // for 0). The staged kernels pick their launch shape by timing (below).
-int hv_variant() { return (int)opt_int("hv_variant"); }
+int hv_variant() {
+  thread_local unsigned long long gen = ~0ull;  // read once per thread and option change
+  thread_local int v = 2;
+  const unsigned long long g = options_generation();
+  if (g != gen) {
+    v = (int)opt_int("hv_variant");
+    gen = g;
+  }
+  return v;
+}
 
 namespace {
 

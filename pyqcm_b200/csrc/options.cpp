@@ -1,6 +1,7 @@
 // Global options (see options.hpp). Defaults follow src_util/global_parameter.cpp:10-92.
 #include "options.hpp"
 
+#include <atomic>
 #include <map>
 #include <mutex>
 
@@ -125,6 +126,8 @@ Table &T() {
   return t;
 }
 
+std::atomic<unsigned long long> g_generation{0};
+
 template <class M> typename M::mapped_type get(M &m, const std::string &name) {
   auto it = m.find(name);
   if (it == m.end()) fail(QED_ERR_ARGUMENT, "global parameter " + name + " does not exist.");
@@ -143,9 +146,27 @@ long opt_int(const std::string &n) { std::lock_guard<std::mutex> l(T().m); retur
 double opt_double(const std::string &n) { std::lock_guard<std::mutex> l(T().m); return get(T().d, n); }
 char opt_char(const std::string &n) { std::lock_guard<std::mutex> l(T().m); return get(T().c, n); }
 
-void set_opt_bool(const std::string &n, bool v) { std::lock_guard<std::mutex> l(T().m); put(T().b, n, v); }
-void set_opt_int(const std::string &n, long v) { std::lock_guard<std::mutex> l(T().m); put(T().i, n, v); }
-void set_opt_double(const std::string &n, double v) { std::lock_guard<std::mutex> l(T().m); put(T().d, n, v); }
-void set_opt_char(const std::string &n, char v) { std::lock_guard<std::mutex> l(T().m); put(T().c, n, v); }
+void set_opt_bool(const std::string &n, bool v) {
+  std::lock_guard<std::mutex> l(T().m);
+  put(T().b, n, v);
+  ++g_generation;
+}
+void set_opt_int(const std::string &n, long v) {
+  std::lock_guard<std::mutex> l(T().m);
+  put(T().i, n, v);
+  ++g_generation;
+}
+void set_opt_double(const std::string &n, double v) {
+  std::lock_guard<std::mutex> l(T().m);
+  put(T().d, n, v);
+  ++g_generation;
+}
+void set_opt_char(const std::string &n, char v) {
+  std::lock_guard<std::mutex> l(T().m);
+  put(T().c, n, v);
+  ++g_generation;
+}
+
+unsigned long long options_generation() { return g_generation.load(std::memory_order_acquire); }
 
 }  // namespace qed

@@ -18,4 +18,8 @@ void set_opt_int(const std::string &name, long v);
 void set_opt_double(const std::string &name, double v);
 void set_opt_char(const std::string &name, char v);
 
+// Incremented by every set_opt_*: a value read in a hot path can be cached per
+// thread and read again only when this changes.
+unsigned long long options_generation();
+
 }  // namespace qed

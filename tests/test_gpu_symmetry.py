@@ -146,9 +146,19 @@ def test_record_green_function_in_the_symmetry_adapted_basis(qed, oracle, fresh)
     ground state and sector against the record (6 digits) and the compiled
     reference's own solve of the same model (1e-10); G(z) in the site basis,
     built from the per-irrep band-Lanczos Q-matrices, against the reference's
-    (1e-8) and, projected on each irrep's symmetric orbital, against the record's
+    (5e-8) and, projected on each irrep's symmetric orbital, against the record's
     14-digit poles (1e-7, the oracle's own pin); the averages of every operator
-    against the reference's (1e-9)."""
+    against the reference's (1e-9).
+
+    Why 5e-8 against the compiled reference. The reference does not reproduce
+    this model's G more closely than about 1e-8 from one solve to the next. Its
+    CSR Hamiltonian adds the operator terms in the order of a map keyed by the
+    operators' heap addresses (src_ed/Hamiltonian/Hamiltonian_CSR.hpp:137-141).
+    So the summation order of its sector matrix changes with the heap layout, and
+    round-off then moves where its band Lanczos stops. Measured on a B200 over
+    seven solves of this model, the same for this solver to the bit, this
+    solver's G differed from the reference's by 1.2e-9 to 1.35e-8. The record's
+    poles stay the fixed pin."""
     from tests.helpers import C2V_Z, c2v_irrep_gf, project_irreps
     gold = c2v_golden()
     prob = c2v_problem(gold, True)
@@ -159,10 +169,10 @@ def test_record_green_function_in_the_symmetry_adapted_basis(qed, oracle, fresh)
     assert abs(e - e_ref) <= 1e-10 * abs(e_ref), (e, e_ref)
     G = qed.Green_function(C2V_Z, label=label)
     G_ref = oracle.green_function(label, C2V_Z)
-    assert np.max(np.abs(G - G_ref)) < 1e-8
+    assert np.max(np.abs(G - G_ref)) < 5e-8
     assert np.max(np.abs(project_irreps(G) - c2v_irrep_gf(gold, C2V_Z))) < 1e-7
     z = W.matsubara(64)
-    assert np.max(np.abs(qed.Green_function(z, label=label) - oracle.green_function(label, z))) < 1e-8
+    assert np.max(np.abs(qed.Green_function(z, label=label) - oracle.green_function(label, z))) < 5e-8
     ave = {n: (a, v) for n, a, v in qed.cluster_averages(label)}
     for n, a, v in oracle.cluster_averages(label):
         assert abs(ave[n][0] - a) < 1e-9 * max(1.0, abs(a)), (n, ave[n], a)

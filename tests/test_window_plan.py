@@ -54,7 +54,11 @@ def direct_hops(L, N, pd, ps, amp, x):
 
 
 @pytest.mark.parametrize("nx,ny,N,diag,nwin", [(4, 4, 5, True, 3), (4, 3, 6, True, 2), (2, 4, 3, True, 1),
-                                               (6, 2, 5, False, 3), (5, 2, 5, False, 2), (3, 3, 4, True, 2)])
+                                               (6, 2, 5, False, 3), (5, 2, 5, False, 2), (3, 3, 4, True, 2),
+                                               # edge cases: one window narrower than 8 sites, empty
+                                               # and full fillings, one particle, one hole
+                                               (2, 2, 2, True, 1), (2, 2, 0, True, 1), (2, 2, 4, True, 1),
+                                               (4, 4, 1, True, 3), (4, 4, 15, True, 3)])
 def test_window_form_equals_direct_hops(qed, nx, ny, N, diag, nwin):
     L = nx * ny
     pd, ps = lattice_pairs(nx, ny, diag)

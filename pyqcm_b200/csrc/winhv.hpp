@@ -19,6 +19,12 @@
 // constant bank): one shared-memory load per state and window instead of one
 // per hop. The code depends on the lattice (pairs, L, N) and is compiled at run
 // time with NVRTC for sm_100a, once per structure and process.
+//
+// Opt-in (option hv_windows, off by default). On a B200 these kernels are
+// slower than the staged ones: 10.9 ms against 4.6 ms per H.v on the 4x4 sector.
+// Holding a group in registers takes up to 255 registers per thread, so only
+// eight warps fit on an SM, and the kernels are latency-bound. The down-spin
+// pass also copies and stores its columns 8 bytes at a time.
 #pragma once
 #include <cuda_runtime.h>
 

@@ -70,6 +70,17 @@ int qed_window_compile(int L, int n_up, int n_dn, int npairs, const int *pd, con
                        int *ok);
 /* Number of H.v calls that ran the window kernels so far in this process. */
 int qed_window_launches(long long *n);
+/* No counterpart in the reference: one spin's tables as this solver builds them
+ * (host computation, no device needed), for checks of the hop rule of
+ * HS_half_operator (src_ed/Operators/HS_half_operator.hpp:17-45). t and vsame:
+ * L x L row-major one-body matrix and same-spin density-density terms. Writes
+ * dim = C(L, N) strings (increasing), cnt and diag, *width entries per string
+ * of the ELL table into ell (entry k of string i at ell[k * dim + i] = rank << 8
+ * | value slot; at most ell_capacity entries) and *nvals value slots into vals
+ * (at most 258). bank_order != 0 returns the bank-ordered table. */
+int qed_spin_table_host(int L, int N, const double *t, const double *vsame, int bank_order, unsigned *bits,
+                        unsigned char *cnt, double *diag, unsigned *ell, long ell_capacity, int *width,
+                        double *vals, int *nvals);
 
 /* Selects the CUDA device used by this process (default 0). */
 int qed_init(int device);

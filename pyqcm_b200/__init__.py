@@ -67,6 +67,8 @@ def lib():
         "qed_window_plan": [C.c_int, C.c_int, C.c_int, ip, ip, dp, dp, dp, ip],
         "qed_window_compile": [C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, C.c_char_p, C.c_int, ip],
         "qed_window_launches": [C.POINTER(C.c_longlong)],
+        "qed_spin_table_host": [C.c_int, C.c_int, dp, dp, C.c_int, up, C.POINTER(C.c_ubyte), dp, up, C.c_long,
+                                ip, dp, ip],
         "qed_init": [C.c_int],
         "qed_set_global_int": [C.c_char_p, C.c_long],
         "qed_set_global_double": [C.c_char_p, C.c_double],
@@ -754,6 +756,30 @@ def window_compile(L: int, n_up: int, n_dn: int, pd, ps):
     ok = C.c_int()
     _check(lib().qed_window_compile(L, n_up, n_dn, len(pd), _ip(pd), _ip(ps), buf, len(buf), C.byref(ok)))
     return bool(ok.value), buf.value.decode(errors="replace")
+
+
+def spin_table_host(L: int, N: int, t, vsame, bank_order: bool = False) -> dict:
+    """One spin's tables as the solver builds them (qed_spin_table_host, host
+    only): strings, hop counts, diagonal, ELL entries (rank << 8 | value slot,
+    shape (width, dim)) and the value slots."""
+    from math import comb
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    vsame = np.ascontiguousarray(vsame, dtype=np.float64)
+    dim = comb(L, N)
+    bits = np.zeros(dim, np.uint32)
+    cnt = np.zeros(dim, np.uint8)
+    diag = np.zeros(dim)
+    cap = 256 * dim
+    ell = np.zeros(cap, np.uint32)
+    vals = np.zeros(258)
+    w = C.c_int()
+    nv = C.c_int()
+    _check(lib().qed_spin_table_host(L, N, _dp(t), _dp(vsame), int(bank_order),
+                                     bits.ctypes.data_as(C.POINTER(C.c_uint)), cnt.ctypes.data_as(C.POINTER(C.c_ubyte)),
+                                     _dp(diag), ell.ctypes.data_as(C.POINTER(C.c_uint)), cap, C.byref(w),
+                                     _dp(vals), C.byref(nv)))
+    return {"bits": bits, "cnt": cnt, "diag": diag, "ell": ell[:w.value * dim].reshape(w.value, dim),
+            "vals": vals[:nv.value], "width": w.value}
 
 
 def window_launches() -> int:

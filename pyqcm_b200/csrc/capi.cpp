@@ -410,6 +410,33 @@ int qed_window_launches(long long *n) {
   });
 }
 
+int qed_spin_table_host(int L, int N, const double *t, const double *vsame, int bank_order, unsigned *bits,
+                        unsigned char *cnt, double *diag, unsigned *ell, long ell_capacity, int *width,
+                        double *vals, int *nvals) {
+  return guarded([&] {
+    if (L < 1 || L > 24 || N < 0 || N > L || !t || !vsame || !width || !nvals)
+      fail(QED_ERR_ARGUMENT, "qed_spin_table_host: L in [1, 24], N in [0, L], non-null t, vsame, width, nvals");
+    const std::vector<double> tv(t, t + (size_t)L * L), vs(vsame, vsame + (size_t)L * L);
+    std::vector<int> pd, ps, pslot;
+    std::vector<double> vl;
+    hop_pairs(L, tv, pd, ps, pslot, vl);
+    if (vl.size() > 256) fail(QED_ERR_UNSUPPORTED, "more than 128 distinct hopping amplitudes per spin");
+    const int w = std::min<int>((int)pd.size(), N * (L - N));
+    std::vector<double> tdiag(L);
+    for (int r = 0; r < L; ++r) tdiag[r] = tv[(size_t)r * L + r];
+    const uint32_t dim = (uint32_t)binom(L, N);
+    const HostHalf T = host_half_tables(L, N, dim, tdiag, vs, pd, ps, pslot, vl, w, bank_order != 0);
+    if ((long)T.ell.size() > ell_capacity) fail(QED_ERR_ARGUMENT, "qed_spin_table_host: ell_capacity too small");
+    std::copy(T.bits.begin(), T.bits.end(), bits);
+    std::copy(T.cnt.begin(), T.cnt.end(), cnt);
+    std::copy(T.diag.begin(), T.diag.end(), diag);
+    std::copy(T.ell.begin(), T.ell.end(), ell);
+    std::copy(T.vals.begin(), T.vals.end(), vals);
+    *width = T.width;
+    *nvals = (int)T.vals.size();
+  });
+}
+
 int qed_init(int device) {
   return guarded([&] {
     if (g_device_fixed && device != g_device) fail(QED_ERR_ARGUMENT, "qed_init: device already selected");

@@ -91,15 +91,16 @@ constexpr uint64_t kPackMinDim = 512;
 // bit r empty with the parity of the set bits strictly between r and c), bank
 // ordering / packing and diagonal (in the summation order of k_diag_half) as the
 // device path.
-void build_half_host(HalfTables &h, int L, int N, const std::vector<double> &tdiag,
-                     const std::vector<double> &vsame, const std::vector<int> &pd, const std::vector<int> &ps,
-                     const std::vector<int> &pslot, const std::vector<double> &vals, int width, Workspace &ws,
-                     bool bank_order) {
-  const uint32_t dim = h.dim;
-  std::vector<uint32_t> hb;
+}  // namespace
+
+HostHalf host_half_tables(int L, int N, uint32_t dim, const std::vector<double> &tdiag,
+                          const std::vector<double> &vsame, const std::vector<int> &pd, const std::vector<int> &ps,
+                          const std::vector<int> &pslot, const std::vector<double> &vals, int width, bool bank_order) {
+  HostHalf T;
+  std::vector<uint32_t> &hb = T.bits;
   hb.reserve(dim);
   uint64_t sv = N >= 64 ? ~0ull : (1ull << N) - 1ull;
-  while (true) {  // N-subsets of L bits in increasing order (Gosper's successor)
+  while (dim) {  // N-subsets of L bits in increasing order (Gosper's successor)
     hb.push_back((uint32_t)sv);
     if (hb.size() == dim) break;
     const uint64_t c = sv & (~sv + 1ull), r = sv + c;
@@ -107,7 +108,8 @@ void build_half_host(HalfTables &h, int L, int N, const std::vector<double> &tdi
   }
   std::vector<uint32_t> he((size_t)width * dim, 0u);
   std::vector<uint8_t> hc(dim, 0);
-  std::vector<double> hd(dim);
+  std::vector<double> &hd = T.diag;
+  hd.assign(dim, 0.0);
   for (uint32_t i = 0; i < dim; ++i) {
     const uint32_t b = hb[i];
     int k = 0;
@@ -133,10 +135,8 @@ void build_half_host(HalfTables &h, int L, int N, const std::vector<double> &tdi
     hd[i] = sd;
   }
   // the bank-ordered copy: packed for the staged kernels, and the ELL itself for the up spin
-  std::vector<double> fvals(vals);
-  int fwidth = width;
-  PackedHops ph;
-  bool packed = false;
+  T.vals = vals;
+  T.width = width;
   const bool want_pack = dim >= kPackMinDim && dim + 8 <= (1u << 14);
   if (width > 0 && (bank_order || want_pack) && dim >= 64 && vals.size() < 256) {
     std::vector<uint32_t> eo(he);
@@ -146,47 +146,26 @@ void build_half_host(HalfTables &h, int L, int N, const std::vector<double> &tdi
     std::vector<double> vz(vals);
     vz.push_back(0.0);
     if (order_for_banks(eo, co, dim, w2, zero_slot)) {
-      packed = want_pack && pack_hops16(eo, co, dim, vz, zero_slot, ph);
+      T.packed = want_pack && pack_hops16(eo, co, dim, vz, zero_slot, T.ph);
       if (bank_order) {
-        fvals = vz;
-        fwidth = w2;
+        T.vals = vz;
+        T.width = w2;
         he.swap(eo);
         hc.swap(co);
       }
     }
   }
-  h.width = fwidth;
-  h.nvals = (int)fvals.size();
-  h.bits.upload(hb, ws.stream);
-  h.cnt.upload(hc, ws.stream);
-  h.vals.alloc(std::max<size_t>(fvals.size(), 1));
-  if (!fvals.empty()) h.vals.upload(fvals, ws.stream);
-  if (fwidth > 0) h.ell.upload(he, ws.stream);
-  h.diag.upload(hd, ws.stream);
-  if (packed) {
-    for (int c = 0; c < 2; ++c) {
-      if (ph.pk[c].empty()) ph.pk[c].assign(4, 0);  // a valid pointer for an empty class
-      h.pk[c].upload(ph.pk[c], ws.stream);
-    }
-    h.cntw.upload(ph.cnt, ws.stream);
-    h.mag[0] = ph.mag[0];
-    h.mag[1] = ph.mag[1];
-  }
-  h.hbits = std::move(hb);
-  ws.sync();
+  T.ell = std::move(he);
+  T.cnt = std::move(hc);
+  return T;
 }
 
-void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
-                const std::vector<double> &vsame, Workspace &ws, bool bank_order) {
-  h.L = L;
-  h.N = N;
-  uint64_t dim = (N < 0 || N > L) ? 0 : binom(L, N);
-  if (dim >= (1ull << 24)) fail(QED_ERR_UNSUPPORTED, "half basis dimension above 2^24");
-  h.dim = (uint32_t)dim;
-  if (!dim) return;
-  // directed hop pairs (dst r, src c) with value slots; value table dedupes |t|
-  std::vector<int> pd, ps, pslot;
-  std::vector<double> vals;
+void hop_pairs(int L, const std::vector<double> &t, std::vector<int> &pd, std::vector<int> &ps,
+               std::vector<int> &pslot, std::vector<double> &vals) {
+  pd.clear();
+  ps.clear();
+  pslot.clear();
+  vals.clear();
   std::map<double, int> slot_of;
   for (int r = 0; r < L; ++r)
     for (int c = 0; c < L; ++c) {
@@ -207,6 +186,49 @@ void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
       ps.push_back(c);
       pslot.push_back(slot);
     }
+}
+
+namespace {
+
+// Host build of a small spin table (host_half_tables), uploaded at once.
+void build_half_host(HalfTables &h, int L, int N, const std::vector<double> &tdiag,
+                     const std::vector<double> &vsame, const std::vector<int> &pd, const std::vector<int> &ps,
+                     const std::vector<int> &pslot, const std::vector<double> &vals, int width, Workspace &ws,
+                     bool bank_order) {
+  HostHalf T = host_half_tables(L, N, h.dim, tdiag, vsame, pd, ps, pslot, vals, width, bank_order);
+  h.width = T.width;
+  h.nvals = (int)T.vals.size();
+  h.bits.upload(T.bits, ws.stream);
+  h.cnt.upload(T.cnt, ws.stream);
+  h.vals.alloc(std::max<size_t>(T.vals.size(), 1));
+  if (!T.vals.empty()) h.vals.upload(T.vals, ws.stream);
+  if (T.width > 0) h.ell.upload(T.ell, ws.stream);
+  h.diag.upload(T.diag, ws.stream);
+  if (T.packed) {
+    for (int c = 0; c < 2; ++c) {
+      if (T.ph.pk[c].empty()) T.ph.pk[c].assign(4, 0);  // a valid pointer for an empty class
+      h.pk[c].upload(T.ph.pk[c], ws.stream);
+    }
+    h.cntw.upload(T.ph.cnt, ws.stream);
+    h.mag[0] = T.ph.mag[0];
+    h.mag[1] = T.ph.mag[1];
+  }
+  h.hbits = std::move(T.bits);
+  ws.sync();
+}
+
+void build_half(HalfTables &h, int L, int N, const std::vector<double> &t,
+                const std::vector<double> &vsame, Workspace &ws, bool bank_order) {
+  h.L = L;
+  h.N = N;
+  uint64_t dim = (N < 0 || N > L) ? 0 : binom(L, N);
+  if (dim >= (1ull << 24)) fail(QED_ERR_UNSUPPORTED, "half basis dimension above 2^24");
+  h.dim = (uint32_t)dim;
+  if (!dim) return;
+  // directed hop pairs (dst r, src c) with value slots; value table dedupes |t|
+  std::vector<int> pd, ps, pslot;
+  std::vector<double> vals;
+  hop_pairs(L, t, pd, ps, pslot, vals);
   if (vals.size() > 256) fail(QED_ERR_UNSUPPORTED, "more than 128 distinct hopping amplitudes per spin");
   h.pd = pd;
   h.ps = ps;

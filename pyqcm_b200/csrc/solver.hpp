@@ -14,6 +14,7 @@
 
 #include "common.hpp"
 #include "kernels.cuh"
+#include "bank_order.hpp"
 #include "model.hpp"
 #include "winhv.hpp"
 
@@ -55,6 +56,29 @@ struct HalfTables {
   std::vector<int> pd, ps;
   std::vector<double> pv;
 };
+
+// The directed hopping pairs of one spin (destination r, source c, scanned row by
+// row, skipping the diagonal and |t| below SMALL_VALUE) with their value slots:
+// vals holds each distinct amplitude v at an even slot and -v after it.
+void hop_pairs(int L, const std::vector<double> &t, std::vector<int> &pd, std::vector<int> &ps,
+               std::vector<int> &pslot, std::vector<double> &vals);
+
+// One spin's tables computed on the host: the N-of-L strings in increasing order,
+// the ELL hops (entry k of string i at ell[k * dim + i] = rank << 8 | value slot,
+// cnt[i] entries, the sign in the slot's parity), the one-body + same-spin
+// interaction diagonal, and the bank-ordered (for bank_order, the ELL itself)
+// and packed copies (bank_order.hpp). The device build gives the same tables.
+struct HostHalf {
+  std::vector<uint32_t> bits, ell;
+  std::vector<uint8_t> cnt;
+  std::vector<double> vals, diag;
+  int width = 0;
+  PackedHops ph;
+  bool packed = false;
+};
+HostHalf host_half_tables(int L, int N, uint32_t dim, const std::vector<double> &tdiag,
+                          const std::vector<double> &vsame, const std::vector<int> &pd, const std::vector<int> &ps,
+                          const std::vector<int> &pslot, const std::vector<double> &vals, int width, bool bank_order);
 
 // Per-instance cache of the spin tables: a sector (N_up, N_dn) uses the up
 // table of N_up and the down table of N_dn, so the sectors of one instance

@@ -400,7 +400,13 @@ void SectorOp::bind_windows() {
       !plan_windows(dn->L, dn->N, dn->hbits, dn->pd, dn->ps, pdn))
     return;
   std::string why;
-  auto mod = window_module(pu, pdn, &why);
+  std::shared_ptr<const WinModule> mod;
+  try {
+    mod = window_module(pu, pdn, &why);
+  } catch (const Error &) {
+    (void)cudaGetLastError();  // clear the failed call's error for the next launch check
+    mod = nullptr;             // the module did not load: the staged kernels take the sector
+  }
   if (!mod) return;  // the staged kernels take the sector
   win = std::make_shared<WinBinding>();
   win->mod = mod;
